@@ -1,0 +1,320 @@
+"""Benchmark: grad+HVP evaluations per second of the matrix-free brickwall objective.
+
+Workload (default): L=16 qubits, periodic brickwall of depth 9 (Haar gates,
+seed 10) against a matrix-free depth-5 brickwall target (seed 11); one step is
+one f + projected gradient + projected Hessian-vector product evaluation summed
+over all 65,536 basis columns (random tangent direction, seed 12).  Inputs are
+seeded synthetic data; the working set is many GB, far larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision c128|c64] [--L 16 --depth 9 --tdepth 5]
+
+One JSON line on rank 0.  `value` is device-timed throughput with the inputs
+resident in HBM (CUDA events on the library stream); `e2e` is the same metric
+through the C ABI with host buffers (gates in, gradient and HVP out).  With
+N > 1 (torchrun) every rank evaluates its own replica (no collective on the
+data path); throughput is the sum over ranks divided by the slowest rank's time.
+`--impl reference` times the reference's C implementation (oracle/_ref) on the
+host cores on a bounded column sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns)"
+
+
+def haar(rng):
+    z = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) / np.sqrt(2)
+    q, r = np.linalg.qr(z)
+    d = np.diagonal(r)
+    return q * (d / np.abs(d))
+
+
+def perms_for(L, nlayers):
+    even, odd = np.arange(L), np.roll(np.arange(L), -1)
+    return np.stack([even if l % 2 == 0 else odd for l in range(nlayers)]).astype(np.int32)
+
+
+def antisymm(r):
+    w = np.zeros((4, 4), np.complex128)
+    for a in range(4):
+        w[a, a] = 1j * r[5 * a]
+        for c in range(a + 1, 4):
+            p, q = r[4 * a + c], r[4 * c + a]
+            w[a, c] = 0.5 * (p - q) + 0.5j * (p + q)
+            w[c, a] = -np.conj(w[a, c])
+    return w
+
+
+def workload(L, depth, tdepth, seed=10, tseed=11, dseed=12):
+    rng = np.random.default_rng(seed)
+    vlist = np.stack([haar(rng) for _ in range(depth)])
+    trng = np.random.default_rng(tseed)
+    tvlist = np.stack([haar(trng) for _ in range(tdepth)])
+    r = np.random.default_rng(dseed).standard_normal((depth, 16))
+    vdirs = np.stack([vlist[k] @ antisymm(r[k]) for k in range(depth)])
+    return vlist, perms_for(L, depth), tvlist, perms_for(L, tdepth), vdirs
+
+
+def flops_per_eval(L, G, Gt):
+    """Algorithmic flops of one evaluation as the reference executes it:
+    N^2 (32 G_t + 292 G - 124) (N = 2^L basis columns of 2^L amplitudes)."""
+    N = 1 << L
+    return float(N) * N * (32 * Gt + 292 * G - 124)
+
+
+def reverse_bytes_per_eval(L, G, itemsize):
+    """Algorithmic HBM bytes of the reverse (gradient/HVP) passes of one evaluation:
+    per column 6G - 5 statevector passes (reads of phi, dphi, psi_k, dpsi_k and writes of
+    phi', dphi'; the first gate has no dphi, the last no psi / outputs)."""
+    N = 1 << L
+    return float(6 * G - 5) * N * N * itemsize
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in self.rows:
+            for k, nm in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------- CPU baseline
+
+def _ref_columns_worker(args):
+    L, depth, tdepth, b0, b1 = args
+    from oracle.oracle import Reference
+    vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
+    t0 = time.perf_counter()
+    Reference().brickwall_hvp_columns(vlist, vdirs, perms, L, tvlist, tperms, b0, b1)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(L, depth, tdepth, seconds=15.0, cores=None):
+    """Reference C implementation (oracle/_ref, per-column grad+HVP function of the
+    column loop) on a bounded contiguous column sample, one process per core (spawn)."""
+    import multiprocessing as mp
+    from oracle.oracle import Reference
+    if not Reference.available():
+        return None
+    cores = cores or os.cpu_count() or 1
+    N = 1 << L
+    # calibrate: time one column on this process
+    vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
+    t0 = time.perf_counter()
+    Reference().brickwall_hvp_columns(vlist, vdirs, perms, L, tvlist, tperms, 0, 1)
+    per_col = max(time.perf_counter() - t0, 1e-6)
+    cols_per_core = max(1, min(N // cores, int(seconds / per_col)))
+    jobs = [(L, depth, tdepth, k * cols_per_core, (k + 1) * cols_per_core) for k in range(cores)]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(cores) as pool:
+        pool.map(_ref_columns_worker, jobs)
+    wall = time.perf_counter() - t0
+    cols = cols_per_core * cores
+    return {"value": (cols / N) / wall, "unit": "evals/s", "cores": cores, "kind": "reference",
+            "sample": f"{cols} of {N} basis columns ({cols_per_core} per core) through the reference's "
+                      f"quantum_circuit_gates_hessian_vector_product with its brickwall target, "
+                      f"{wall:.1f} s wall; evals/s = sampled fraction / wall time"}
+
+
+# ----------------------------------------------------------------------------- main
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="c128", choices=["c128", "c64"])
+    ap.add_argument("--L", type=int, default=16)
+    ap.add_argument("--depth", type=int, default=9)
+    ap.add_argument("--tdepth", type=int, default=5)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    a = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    L, depth, tdepth = a.L, a.depth, a.tdepth
+    G, Gt = depth * (L // 2), tdepth * (L // 2)
+    config = {"workload": f"brickwall L={L} depth={depth} vs matrix-free brickwall target depth={tdepth}, "
+                          f"grad+HVP over all {1 << L} basis columns",
+              "L": L, "depth": depth, "target_depth": tdepth, "columns": 1 << L,
+              "l2": "working set of many GB, larger than L2 (no flush needed)",
+              "parallelism": f"replicas x{world}"}
+
+    if a.impl == "reference":
+        if rank != 0:
+            return
+        steps = []
+        base = None
+        for k in range(a.warmup + a.steps):
+            base = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds / 3)
+            if base is None:
+                print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref not present"}))
+                return
+            if k >= a.warmup:
+                steps.append(base["value"])
+        v = float(np.median(steps))
+        base["value"] = v
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": v, "unit": "evals/s", "n_gpus": a.gpus,
+                          "steps": a.steps, "warmup": a.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+                          "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
+                          "config": config, "cpu_baseline": base,
+                          "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    else:
+        torch.cuda.set_device(0)
+
+    from rqcopt_hpc_b200 import gpu
+    lib = gpu.lib()
+    prec = gpu.PRECISION_C128 if a.precision == "c128" else gpu.PRECISION_C64
+    gpu.set_precision(prec)
+    vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
+    target = gpu.Target(brickwall=(tvlist, tperms))
+
+    def step():
+        return gpu.brickwall_unitary_target_projected_hessian_vector_product(target, vlist, vdirs, perms, L)
+
+    for _ in range(a.warmup):
+        step()
+    stream = torch.cuda.ExternalStream(lib.rqcopt_gpu_stream())
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    # device-timed region (value) with per-kernel event timing and clock sampling
+    gpu.enable_kernel_timing(True)
+    gpu.reset_launch_count()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            res = step()
+        ev1.record(stream)
+        barrier()
+    launches = gpu.launch_count()
+    dev_ms = ev0.elapsed_time(ev1)
+    rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
+    fwd_ms, fwd_n = gpu.kernel_time(gpu.KC_FORWARD)
+    app_ms, app_n = gpu.kernel_time(gpu.KC_APPLY)
+    gpu.enable_kernel_timing(False)
+
+    # end-to-end through the C ABI with host buffers
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        step()
+    barrier()
+    e2e_ms = (time.perf_counter() - t0) * 1e3
+
+    t = torch.tensor([dev_ms, e2e_ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    dev_ms, e2e_ms = float(t[0]), float(t[1])
+
+    if rank == 0:
+        itemsize = 16 if prec == gpu.PRECISION_C128 else 8
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except (OSError, ValueError):
+            pass
+        hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        rbytes = reverse_bytes_per_eval(L, G, itemsize) * a.steps
+        achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
+        value = world * a.steps / (dev_ms * 1e-3)
+        flops = flops_per_eval(L, G, Gt)
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128 (f64)" if itemsize == 16 else "c64 (f32, f64 sums)",
+            "data": "synthetic (seeded Haar gates)", "config": config,
+            "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "evals/s",
+                    "h2d_bytes_per_step": int(vlist.nbytes + vdirs.nbytes + tvlist.nbytes + perms.nbytes + tperms.nbytes),
+                    "d2h_bytes_per_step": int(16 + 2 * 16 * depth * 8)},
+            "roofline": {"kernel": "k_reverse (gradient/HVP pass of one gate over a column chunk)", "bound": "hbm",
+                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                         "frac": achieved / hbm_peak if achieved else None,
+                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650",
+                         "traffic": None, "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)},
+            "kernel_share": {"reverse_ms": rev_ms, "forward_ms": fwd_ms, "apply_ms": app_ms, "device_ms": dev_ms},
+            "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
+            "clocks": clk.summary(), "gpu_launches": int(launches),
+        }
+        if not a.no_cpu_baseline and world == 1:
+            line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)
+        print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

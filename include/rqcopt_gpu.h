@@ -1,0 +1,337 @@
+/*
+ * rqcopt_gpu.h -- C ABI of the B200 library librqcopt_gpu.so.
+ *
+ * The first part declares, with identical names, argument types and meaning,
+ * the functions of cmendl/rqcopt_hpc on the matrix-free circuit-optimisation
+ * path, so that C host code written against the reference headers links
+ * against this library unchanged.  Every declaration names the reference
+ * declaration it replaces (path:line within the reference project).  The
+ * second part declares additions that have no counterpart in the reference.
+ *
+ * Conventions (as in the reference, COMPLEX_CIRCUIT build):
+ *   - `numeric` is double complex; a statevector holds 2^nqubits amplitudes,
+ *     qubit 0 is the most significant bit of the amplitude index;
+ *   - `struct mat4x4` is a row-major 4x4 gate whose row/column index is
+ *     2*b_i + b_j for the bits of its wires (i, j);
+ *   - every call is synchronous: when it returns, all GPU work it issued has
+ *     finished and its outputs are visible to the host;
+ *   - statevector data pointers may be host memory (pageable or pinned),
+ *     CUDA managed memory (what allocate_statevector returns) or device
+ *     memory of the current device; host buffers are staged through HBM;
+ *   - int-returning functions return 0 on success and a negative code on
+ *     failure: -1 allocation, -2 target-callback failure, -3/-4 internal pass
+ *     failure, -5 CUDA error, -6 invalid argument (the last two are additions);
+ *   - void functions that receive invalid arguments print a message to stderr,
+ *     leave their outputs untouched and record the error, readable through
+ *     rqcopt_gpu_last_error().
+ */
+#pragma once
+
+#ifdef __cplusplus
+#include <complex>
+typedef std::complex<double> numeric;
+extern "C" {
+#else
+#include <complex.h>
+#include <stdbool.h>
+typedef double complex numeric;
+#endif
+
+#include <stddef.h>
+
+/* src/config.h:62 */
+typedef long int intqs;
+
+/* src/matrix.h:10-13 */
+struct mat4x4
+{
+	numeric data[16];
+};
+
+/* src/statevector.h:11-15 */
+struct statevector
+{
+	numeric* data;
+	int nqubits;
+};
+
+/* src/quantum_circuit.h:16-21 */
+struct quantum_circuit_cache
+{
+	struct statevector* psi_list;
+	int nqubits;
+	int ngates;
+};
+
+/* src/target.h:7 */
+typedef int (*linear_func)(const struct statevector* psi, void* fdata, struct statevector* psi_out);
+
+/* ------------------------------------------------------------------ statevector.h */
+
+/* src/statevector.h:18 -- returns CUDA managed memory (host- and device-accessible) */
+int allocate_statevector(int nqubits, struct statevector* psi);
+/* src/statevector.h:20 */
+void free_statevector(struct statevector* psi);
+/* src/statevector.h:32 */
+void add_statevectors(const struct statevector* psi1, const struct statevector* psi2, struct statevector* psi_sum);
+
+/* ------------------------------------------------------------------ gate.h */
+
+/* src/gate.h:7 */
+void apply_gate(const struct mat4x4* gate, const int i, const int j,
+	const struct statevector* psi, struct statevector* psi_out);
+/* src/gate.h:9-10 */
+void apply_gate_backward(const struct mat4x4* gate, const int i, const int j, const struct statevector* psi,
+	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4* dgate);
+
+/* ------------------------------------------------------------------ quantum_circuit.h */
+
+/* src/quantum_circuit.h:7-8 */
+int apply_quantum_circuit(const struct mat4x4 gates[], const int ngates, const int wires[],
+	const struct statevector* psi, struct statevector* psi_out);
+/* src/quantum_circuit.h:23 -- cache states are CUDA managed memory */
+int allocate_quantum_circuit_cache(const int nqubits, const int ngates, struct quantum_circuit_cache* cache);
+/* src/quantum_circuit.h:25 */
+void free_quantum_circuit_cache(struct quantum_circuit_cache* cache);
+/* src/quantum_circuit.h:27-28 */
+int quantum_circuit_forward(const struct mat4x4 gates[], const int ngates, const int wires[],
+	const struct statevector* psi, struct quantum_circuit_cache* cache, struct statevector* psi_out);
+/* src/quantum_circuit.h:30-31 */
+int quantum_circuit_backward(const struct mat4x4 gates[], const int ngates, const int wires[], const struct quantum_circuit_cache* cache,
+	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4 dgates[]);
+/* src/quantum_circuit.h:34-36 */
+int quantum_circuit_gates_hessian_vector_product(const struct mat4x4 gates[], const struct mat4x4 gatedirs[], const int ngates, const int wires[],
+	const struct statevector* psi, const struct statevector* phi,
+	struct statevector* psi_out, struct mat4x4 dgates[], struct mat4x4 hess_gatedirs[]);
+
+/* ------------------------------------------------------------------ brickwall_circuit.h */
+
+/* src/brickwall_circuit.h:8-9 */
+int apply_brickwall_unitary(const struct mat4x4 vlist[], const int nlayers, const int* perms[],
+	const struct statevector* psi, struct statevector* psi_out);
+/* src/brickwall_circuit.h:11-12 */
+int brickwall_unitary_forward(const struct mat4x4 vlist[], int nlayers, const int* perms[],
+	const struct statevector* psi, struct quantum_circuit_cache* cache, struct statevector* psi_out);
+/* src/brickwall_circuit.h:14-15 */
+int brickwall_unitary_backward(const struct mat4x4 vlist[], int nlayers, const int* perms[], const struct quantum_circuit_cache* cache,
+	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4 dvlist[]);
+
+/* ------------------------------------------------------------------ target.h */
+
+/* src/target.h:10-12 */
+int circuit_unitary_target(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
+	numeric* fval);
+/* src/target.h:20-22 */
+int circuit_unitary_target_and_gradient(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
+	numeric* fval, struct mat4x4 dgates[]);
+/* src/target.h:24-26 */
+int circuit_unitary_target_and_projected_gradient(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
+	numeric* fval, double* grad_vec);
+/* src/target.h:29-31 */
+int circuit_unitary_target_hessian_vector_product(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const struct mat4x4 gatedirs[], const int ngates, const int wires[], const int nqubits,
+	numeric* fval, struct mat4x4 dgates[], struct mat4x4 hess_gatedirs[]);
+/* src/target.h:33-35 */
+int circuit_unitary_target_projected_hessian_vector_product(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const struct mat4x4 gatedirs[], const int ngates, const int wires[], const int nqubits,
+	numeric* fval, double* grad_vec, double* hvp_vec);
+/* src/target.h:42-44 */
+int brickwall_unitary_target(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval);
+/* src/target.h:52-54 */
+int brickwall_unitary_target_and_gradient(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval, struct mat4x4 dvlist[]);
+/* src/target.h:56-58 */
+int brickwall_unitary_target_and_projected_gradient(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval, double* grad_vec);
+/* src/target.h:61-63 */
+int brickwall_unitary_target_hessian_vector_product(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const struct mat4x4 vdirs[], const int nlayers, const int* perms[], const int nqubits,
+	numeric* fval, struct mat4x4 dvlist[], struct mat4x4 hess_vdirs[]);
+/* src/target.h:65-67 */
+int brickwall_unitary_target_projected_hessian_vector_product(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const struct mat4x4 vdirs[], const int nlayers, const int* perms[], const int nqubits,
+	numeric* fval, double* grad_vec, double* hvp_vec);
+
+/* ------------------------------------------------------------------ trust_region.h */
+
+/* src/trust_region.h:10-16 */
+struct truncated_cg_params
+{
+	int maxiter;
+	double abstol;
+	double reltol;
+};
+
+/* src/trust_region.h:23-28 */
+static inline void set_truncated_cg_default_params(int n, struct truncated_cg_params* params)
+{
+	params->maxiter = 2 * n;
+	params->abstol  = 1e-8;
+	params->reltol  = 1e-6;
+}
+
+/* src/trust_region.h:34 */
+typedef void (*hessian_vector_product_func)(const double* x, void* fdata, double* vec, double* hvp);
+/* src/trust_region.h:39 */
+typedef double (*target_func)(const double* x, void* fdata);
+/* src/trust_region.h:41 */
+typedef double (*target_gradient_func)(const double* x, void* fdata, double* grad);
+/* src/trust_region.h:45 */
+typedef void (*retract_func)(const double* x, const double* eta, void* rdata, double* xs);
+
+/* src/trust_region.h:52-61 */
+struct rtr_params
+{
+	struct truncated_cg_params tcg_params;
+	double rho_trust;
+	double radius_init;
+	double maxradius;
+	target_func g_func;
+	void*       g_data;
+	double*     g_iter;
+};
+
+/* src/trust_region.h:68-77 */
+static inline void set_rtr_default_params(int n, struct rtr_params* params)
+{
+	set_truncated_cg_default_params(n, &params->tcg_params);
+	params->rho_trust   = 0.125;
+	params->radius_init = 0.01;
+	params->maxradius   = 0.1;
+	params->g_func      = NULL;
+	params->g_data      = NULL;
+	params->g_iter      = NULL;
+}
+
+/* src/trust_region.h:36 */
+bool truncated_cg_hvp(const double* x, const double* grad, const hessian_vector_product_func f_hvp, void* fdata,
+	const int n, const double radius, const struct truncated_cg_params* params, double* z);
+/* src/trust_region.h:83-85 */
+void riemannian_trust_region_optimize_hvp(const target_func f, const target_gradient_func f_deriv,
+	const hessian_vector_product_func f_hvp, void* fdata, retract_func retract, void* rdata,
+	const int n, const double* x_init, const int m, const struct rtr_params* params, const int niter,
+	double* f_iter, double* x_final);
+
+/* ------------------------------------------------------------------ brickwall_opt.h, circuit_opt.h */
+
+/* src/brickwall_opt.h:8-10 */
+void optimize_brickwall_circuit_hvp(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist_start[], const int nlayers, const int nqubits, const int* perms[],
+	struct rtr_params* params, const int niter, double* f_iter, struct mat4x4 vlist_opt[]);
+/* src/circuit_opt.h:8 */
+void optimize_quantum_circuit(linear_func ufunc, void* udata, const struct mat4x4 gates_start[], const int ngates,
+	const int nqubits, const int wires[], struct rtr_params* params, const int niter, double* f_iter,
+	struct mat4x4 gates_opt[]);
+
+/* ------------------------------------------------------------------ matrix.h */
+
+/* src/matrix.h:42-46 (COMPLEX_CIRCUIT) */
+static const int num_tangent_params = 16;
+
+void zero_matrix(struct mat4x4* a);                                          /* src/matrix.h:16 */
+void identity_matrix(struct mat4x4* a);                                      /* src/matrix.h:18 */
+void scale_matrix(struct mat4x4* a, const double x);                         /* src/matrix.h:21 */
+void conjugate_matrix(struct mat4x4* a);                                     /* src/matrix.h:24 */
+void add_matrix(struct mat4x4* a, const struct mat4x4* b);                   /* src/matrix.h:27 */
+void sub_matrix(struct mat4x4* a, const struct mat4x4* b);                   /* src/matrix.h:28 */
+void add_matrices(const struct mat4x4* a, const struct mat4x4* b, struct mat4x4* c);  /* src/matrix.h:30 */
+void sub_matrices(const struct mat4x4* a, const struct mat4x4* b, struct mat4x4* c);  /* src/matrix.h:31 */
+void transpose(const struct mat4x4* a, struct mat4x4* at);                   /* src/matrix.h:34 */
+void adjoint(const struct mat4x4* a, struct mat4x4* ah);                     /* src/matrix.h:35 */
+void symm(const struct mat4x4* w, struct mat4x4* z);                         /* src/matrix.h:38 */
+void antisymm(const struct mat4x4* w, struct mat4x4* z);                     /* src/matrix.h:39 */
+void real_to_antisymm(const double* r, struct mat4x4* w);                    /* src/matrix.h:48 */
+void antisymm_to_real(const struct mat4x4* w, double* r);                    /* src/matrix.h:49 */
+void real_to_tangent(const double* r, const struct mat4x4* v, struct mat4x4* z);       /* src/matrix.h:51 */
+void tangent_to_real(const struct mat4x4* v, const struct mat4x4* z, double* r);       /* src/matrix.h:52 */
+void project_tangent(const struct mat4x4* u, const struct mat4x4* z, struct mat4x4* p); /* src/matrix.h:55 */
+void multiply_matrices(const struct mat4x4* a, const struct mat4x4* b, struct mat4x4* c); /* src/matrix.h:58 */
+void symmetric_triple_matrix_product(const struct mat4x4* a, const struct mat4x4* b,
+	const struct mat4x4* c, struct mat4x4* ret);                                 /* src/matrix.h:61 */
+int inverse_matrix(const struct mat4x4* a, struct mat4x4* ainv);            /* src/matrix.h:64 */
+void polar_factor(const struct mat4x4* a, struct mat4x4* u);                 /* src/matrix.h:67 */
+void retract(const struct mat4x4* u, const double* eta, struct mat4x4* v);   /* src/matrix.h:70 */
+
+/* ------------------------------------------------------------------ util.h */
+
+double uniform_distance_real(long n, const double* x, const double* y);     /* src/util.h:19 */
+double uniform_distance(long n, const numeric* x, const numeric* y);        /* src/util.h:21 */
+double relative_distance(long n, const numeric* x, const numeric* y, double eps);  /* src/util.h:23 */
+
+/* ==================================================================================
+ * Additions (no counterpart in the reference)
+ * ================================================================================== */
+
+/*
+ * Device-native targets.  These are ordinary `linear_func`s (applying a
+ * brickwall or a general circuit to one column through the GPU), and the
+ * target functions and optimisers recognise them by address: given one of
+ * them as `ufunc`, the basis-column sums evaluate the target on the GPU next
+ * to the circuit, without one host callback per column.
+ */
+struct rqcopt_brickwall_target
+{
+	const struct mat4x4* vlist;  /* nlayers gates, one per layer */
+	int nlayers;
+	const int* const* perms;     /* nlayers permutations of [0, nqubits) */
+};
+int rqcopt_brickwall_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out);
+
+struct rqcopt_circuit_target
+{
+	const struct mat4x4* gates;
+	int ngates;
+	const int* wires;            /* 2 * ngates wire indices */
+};
+int rqcopt_circuit_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out);
+
+/* precision of the basis-column passes */
+enum rqcopt_precision
+{
+	RQCOPT_PRECISION_C128  = 0,  /* complex128 end to end (the drop-in default) */
+	RQCOPT_PRECISION_MIXED = 1,  /* complex64 passes, FP64 sums; optimisers switch to
+	                                complex128 once the gradient norm falls below the
+	                                refinement threshold */
+	RQCOPT_PRECISION_C64   = 2   /* complex64 passes, FP64 sums, no refinement */
+};
+int rqcopt_gpu_set_precision(int precision);
+int rqcopt_gpu_get_precision(void);
+/* gradient-norm threshold for the switch from complex64 to complex128 (default 1e-5) */
+void rqcopt_gpu_set_refine_threshold(double gnorm);
+
+/* upper bound on the device memory (bytes) the evaluation engine may use for
+ * column chunks and caches; 0 selects 75 % of the free memory at first use */
+void rqcopt_gpu_set_workspace_limit(size_t bytes);
+/* number of basis columns per chunk; 0 selects it from the workspace limit */
+void rqcopt_gpu_set_column_chunk(long columns);
+
+/* last error recorded by a void function (0 if none); reading clears it */
+int rqcopt_gpu_last_error(void);
+
+/* number of kernels this library launched since the counter was last reset */
+unsigned long long rqcopt_gpu_launch_count(void);
+void rqcopt_gpu_reset_launch_count(void);
+
+/*
+ * Per-kernel timing with CUDA events recorded on the launching stream.  While
+ * enabled, each launch of a kernel class is bracketed by events; the totals
+ * are read with rqcopt_gpu_kernel_time (milliseconds summed over launches and
+ * number of launches).  Kernel classes: 0 gate apply, 1 forward tangent pass,
+ * 2 reverse (gradient/HVP) pass, 3 fused multi-gate apply.
+ */
+void rqcopt_gpu_enable_kernel_timing(int enable);
+int  rqcopt_gpu_kernel_time(int kernel_class, double* total_ms, long* launches);
+
+/* the CUDA stream (cudaStream_t) all library work is issued on */
+void* rqcopt_gpu_stream(void);
+
+#ifdef __cplusplus
+}
+#endif

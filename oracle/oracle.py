@@ -1,0 +1,380 @@
+"""ctypes wrappers of the CPU checkers.  TEST INFRASTRUCTURE ONLY.
+
+``Oracle`` wraps ``_build/librqc_oracle.so`` (the plain-C restatement in
+rqc_oracle.c) and ``Reference`` wraps ``_ref/librqcopt_ref.so`` (the reference
+sources compiled by the Makefile in this folder).  Only the tests, the smoke
+check and the CPU-baseline leg of the benchmark use them, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "_build", "librqc_oracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "librqcopt_ref.so")
+
+VP, I, D, L_ = C.c_void_p, C.c_int, C.c_double, C.c_long
+
+
+class SV(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("nqubits", C.c_int)]
+
+
+class TcgParams(C.Structure):
+    _fields_ = [("maxiter", C.c_int), ("abstol", C.c_double), ("reltol", C.c_double)]
+
+
+class RtrParams(C.Structure):
+    _fields_ = [("tcg", TcgParams), ("rho_trust", C.c_double), ("radius_init", C.c_double), ("maxradius", C.c_double)]
+
+
+class BrickwallUdata(C.Structure):
+    _fields_ = [("vlist", C.c_void_p), ("nlayers", C.c_int), ("perms", C.c_void_p)]
+
+
+HVP_FUNC = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
+LINEAR_FUNC = C.CFUNCTYPE(C.c_int, C.POINTER(SV), C.c_void_p, C.POINTER(SV))
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def _i(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _nq(psi):
+    return int(psi.shape[0]).bit_length() - 1
+
+
+def ensure_built():
+    """Build the oracle (and, when the reference sources are present, the reference)."""
+    if not os.path.exists(ORACLE_LIB) or not os.path.exists(REF_LIB):
+        subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
+
+
+def default_rtr(n):
+    return RtrParams(TcgParams(2 * n, 1e-8, 1e-6), 0.125, 0.01, 0.1)
+
+
+class _Target:
+    """Target for the oracle: 'fixture' (the reference tests' sparse map), a brickwall
+    (vlist, perms) applied matrix-free, or a dense matrix."""
+
+    def __init__(self, lib, kind, data=None):
+        self.keep = []
+        if kind == "fixture":
+            self.ufunc = C.cast(lib.orc_fixture_ufunc, VP)
+            self.udata = None
+        elif kind == "brickwall":
+            vlist, perms = _c(data[0]), _i(data[1])
+            self.ud = BrickwallUdata(vlist.ctypes.data, vlist.shape[0], perms.ctypes.data)
+            self.keep += [vlist, perms]
+            self.ufunc = C.cast(lib.orc_brickwall_ufunc, VP)
+            self.udata = C.cast(C.pointer(self.ud), VP)
+        elif kind == "dense":
+            u = _c(data)
+            self.keep.append(u)
+            self.ufunc = C.cast(lib.orc_dense_ufunc, VP)
+            self.udata = _p(u)
+        else:
+            raise ValueError(kind)
+
+
+class Oracle:
+    def __init__(self):
+        ensure_built()
+        self.lib = C.CDLL(ORACLE_LIB)
+
+    def target(self, kind, data=None):
+        return _Target(self.lib, kind, data)
+
+    # gates and circuits
+    def apply_gate(self, V, i, j, psi):
+        psi, V = _c(psi), _c(V)
+        out = np.empty_like(psi)
+        L = _nq(psi)
+        self.lib.orc_apply_gate(_p(V), i, j, C.byref(SV(psi.ctypes.data, L)), C.byref(SV(out.ctypes.data, L)))
+        return out
+
+    def apply_gate_backward(self, V, i, j, psi, dpsi_out):
+        psi, dpsi_out, V = _c(psi), _c(dpsi_out), _c(V)
+        L = _nq(psi)
+        dpsi = np.empty_like(psi)
+        dV = np.empty((4, 4), np.complex128)
+        self.lib.orc_apply_gate_backward(_p(V), i, j, C.byref(SV(psi.ctypes.data, L)),
+                                         C.byref(SV(dpsi_out.ctypes.data, L)), C.byref(SV(dpsi.ctypes.data, L)), _p(dV))
+        return dpsi, dV
+
+    def apply_quantum_circuit(self, gates, wires, psi):
+        gates, wires, psi = _c(gates), _i(wires), _c(psi)
+        L = _nq(psi)
+        out = np.empty_like(psi)
+        self.lib.orc_apply_circuit(_p(gates), gates.shape[0], _p(wires), C.byref(SV(psi.ctypes.data, L)),
+                                   C.byref(SV(out.ctypes.data, L)))
+        return out
+
+    def _cache(self, L, n):
+        states = [np.zeros(1 << L, np.complex128) for _ in range(n)]
+        arr = (SV * n)(*[SV(s.ctypes.data, L) for s in states])
+        return arr, states
+
+    def quantum_circuit_forward(self, gates, wires, psi):
+        gates, wires, psi = _c(gates), _i(wires), _c(psi)
+        L = _nq(psi)
+        arr, states = self._cache(L, gates.shape[0])
+        out = np.empty_like(psi)
+        self.lib.orc_circuit_forward(_p(gates), gates.shape[0], _p(wires), C.byref(SV(psi.ctypes.data, L)), arr,
+                                     C.byref(SV(out.ctypes.data, L)))
+        return out, states
+
+    def quantum_circuit_backward(self, gates, wires, states, dpsi_out):
+        gates, wires, dpsi_out = _c(gates), _i(wires), _c(dpsi_out)
+        L = _nq(dpsi_out)
+        arr = (SV * len(states))(*[SV(s.ctypes.data, L) for s in states])
+        dpsi = np.empty_like(dpsi_out)
+        dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+        self.lib.orc_circuit_backward(_p(gates), gates.shape[0], _p(wires), arr, C.byref(SV(dpsi_out.ctypes.data, L)),
+                                      C.byref(SV(dpsi.ctypes.data, L)), _p(dg))
+        return dpsi, dg
+
+    def quantum_circuit_gates_hessian_vector_product(self, gates, dirs, wires, psi, phi):
+        gates, dirs, wires, psi, phi = _c(gates), _c(dirs), _i(wires), _c(psi), _c(phi)
+        L = _nq(psi)
+        out = np.empty_like(psi)
+        dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+        hg = np.empty_like(dg)
+        self.lib.orc_circuit_gates_hvp(_p(gates), _p(dirs), gates.shape[0], _p(wires), C.byref(SV(psi.ctypes.data, L)),
+                                       C.byref(SV(phi.ctypes.data, L)), C.byref(SV(out.ctypes.data, L)), _p(dg), _p(hg))
+        return out, dg, hg
+
+    def apply_brickwall_unitary(self, vlist, perms, psi):
+        vlist, perms, psi = _c(vlist), _i(perms), _c(psi)
+        L = _nq(psi)
+        out = np.empty_like(psi)
+        self.lib.orc_apply_brickwall(_p(vlist), vlist.shape[0], _p(perms), C.byref(SV(psi.ctypes.data, L)),
+                                     C.byref(SV(out.ctypes.data, L)))
+        return out
+
+    # targets
+    def circuit_unitary_target(self, tgt, gates, wires, L, b0=0, b1=None):
+        gates, wires = _c(gates), _i(wires)
+        f = np.zeros(1, np.complex128)
+        self.lib.orc_circuit_target(tgt.ufunc, tgt.udata, _p(gates), gates.shape[0], _p(wires), L, L_(b0),
+                                    L_(b1 if b1 is not None else 1 << L), _p(f))
+        return f[0]
+
+    def circuit_unitary_target_and_gradient(self, tgt, gates, wires, L):
+        gates, wires = _c(gates), _i(wires)
+        f = np.zeros(1, np.complex128)
+        dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+        self.lib.orc_circuit_target_and_gradient(tgt.ufunc, tgt.udata, _p(gates), gates.shape[0], _p(wires), L,
+                                                 L_(0), L_(1 << L), _p(f), _p(dg))
+        return f[0], dg
+
+    def circuit_unitary_target_hessian_vector_product(self, tgt, gates, dirs, wires, L):
+        gates, dirs, wires = _c(gates), _c(dirs), _i(wires)
+        f = np.zeros(1, np.complex128)
+        dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+        hg = np.empty_like(dg)
+        self.lib.orc_circuit_target_hvp(tgt.ufunc, tgt.udata, _p(gates), _p(dirs), gates.shape[0], _p(wires), L, L_(0),
+                                        L_(1 << L), _p(f), _p(dg), _p(hg))
+        return f[0], dg, hg
+
+    def circuit_unitary_target_and_projected_gradient(self, tgt, gates, wires, L):
+        gates, wires = _c(gates), _i(wires)
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * gates.shape[0])
+        self.lib.orc_circuit_target_projected_gradient(tgt.ufunc, tgt.udata, _p(gates), gates.shape[0], _p(wires), L,
+                                                       _p(f), _p(g))
+        return f[0], g
+
+    def circuit_unitary_target_projected_hessian_vector_product(self, tgt, gates, dirs, wires, L):
+        gates, dirs, wires = _c(gates), _c(dirs), _i(wires)
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * gates.shape[0])
+        h = np.empty_like(g)
+        self.lib.orc_circuit_target_projected_hvp(tgt.ufunc, tgt.udata, _p(gates), _p(dirs), gates.shape[0], _p(wires),
+                                                  L, _p(f), _p(g), _p(h))
+        return f[0], g, h
+
+    def brickwall_unitary_target(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1, np.complex128)
+        self.lib.orc_brickwall_target(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L, _p(perms), _p(f))
+        return f[0]
+
+    def brickwall_unitary_target_and_gradient(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1, np.complex128)
+        dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+        self.lib.orc_brickwall_target_and_gradient(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L, _p(perms),
+                                                   _p(f), _p(dv))
+        return f[0], dv
+
+    def brickwall_unitary_target_and_projected_gradient(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * vlist.shape[0])
+        self.lib.orc_brickwall_target_projected_gradient(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L,
+                                                         _p(perms), _p(f), _p(g))
+        return f[0], g
+
+    def brickwall_unitary_target_hessian_vector_product(self, tgt, vlist, vdirs, perms, L, b0=0, b1=None):
+        vlist, vdirs, perms = _c(vlist), _c(vdirs), _i(perms)
+        f = np.zeros(1, np.complex128)
+        dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+        hv = np.empty_like(dv)
+        self.lib.orc_brickwall_target_hvp(tgt.ufunc, tgt.udata, _p(vlist), _p(vdirs), vlist.shape[0], _p(perms), L,
+                                          L_(b0), L_(b1 if b1 is not None else 1 << L), _p(f), _p(dv), _p(hv))
+        return f[0], dv, hv
+
+    def brickwall_unitary_target_projected_hessian_vector_product(self, tgt, vlist, vdirs, perms, L):
+        vlist, vdirs, perms = _c(vlist), _c(vdirs), _i(perms)
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * vlist.shape[0])
+        h = np.empty_like(g)
+        self.lib.orc_brickwall_target_projected_hvp(tgt.ufunc, tgt.udata, _p(vlist), _p(vdirs), vlist.shape[0],
+                                                    _p(perms), L, _p(f), _p(g), _p(h))
+        return f[0], g, h
+
+    # matrix algebra
+    def real_to_tangent(self, r, v):
+        r, v = np.ascontiguousarray(r, np.float64), _c(v)
+        z = np.empty((4, 4), np.complex128)
+        self.lib.orc_real_to_tangent(_p(r), _p(v), _p(z))
+        return z
+
+    def tangent_to_real(self, v, z):
+        v, z = _c(v), _c(z)
+        r = np.empty(16)
+        self.lib.orc_tangent_to_real(_p(v), _p(z), _p(r))
+        return r
+
+    def project_tangent(self, u, z):
+        u, z = _c(u), _c(z)
+        p = np.empty((4, 4), np.complex128)
+        self.lib.orc_project_tangent(_p(u), _p(z), _p(p))
+        return p
+
+    def polar_factor(self, a):
+        a = _c(a)
+        u = np.empty((4, 4), np.complex128)
+        self.lib.orc_polar_factor(_p(a), _p(u))
+        return u
+
+    def multiply(self, a, b):
+        a, b = _c(a), _c(b)
+        c = np.empty((4, 4), np.complex128)
+        self.lib.orc_multiply(_p(a), _p(b), _p(c))
+        return c
+
+    def retract(self, u, eta):
+        u, eta = _c(u), np.ascontiguousarray(eta, np.float64)
+        v = np.empty((4, 4), np.complex128)
+        self.lib.orc_retract(_p(u), _p(eta), _p(v))
+        return v
+
+    # trust region
+    def truncated_cg_hvp(self, grad, hvp_fn, radius):
+        grad = np.ascontiguousarray(grad, np.float64)
+        n = grad.shape[0]
+
+        def cb(x, fd, vec, hvp):
+            np.ctypeslib.as_array(hvp, shape=(n,))[:] = hvp_fn(np.ctypeslib.as_array(vec, shape=(n,)).copy())
+
+        f = HVP_FUNC(cb)
+        z = np.empty(n)
+        params = TcgParams(2 * n, 1e-8, 1e-6)
+        self.lib.orc_truncated_cg_hvp.restype = C.c_bool
+        b = self.lib.orc_truncated_cg_hvp(None, _p(grad), C.cast(f, VP), None, n, D(radius), C.byref(params), _p(z))
+        return z, bool(b)
+
+    def optimize_brickwall_circuit_hvp(self, tgt, vstart, perms, L, niter):
+        vstart, perms = _c(vstart), _i(perms)
+        nl = vstart.shape[0]
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        acc = np.zeros(niter, np.int32)
+        bnd = np.zeros(niter, np.int32)
+        params = default_rtr(16 * nl)
+        self.lib.orc_optimize_brickwall_hvp(tgt.ufunc, tgt.udata, _p(vstart), nl, L, _p(perms), C.byref(params), niter,
+                                            _p(f_iter), _p(vopt), _p(acc), _p(bnd))
+        return f_iter, vopt, acc, bnd
+
+    def optimize_quantum_circuit(self, tgt, gstart, wires, L, niter):
+        gstart, wires = _c(gstart), _i(wires)
+        ng = gstart.shape[0]
+        f_iter = np.empty(niter + 1)
+        gopt = np.empty_like(gstart)
+        acc = np.zeros(niter, np.int32)
+        bnd = np.zeros(niter, np.int32)
+        params = default_rtr(16 * ng)
+        self.lib.orc_optimize_circuit_hvp(tgt.ufunc, tgt.udata, _p(gstart), ng, L, _p(wires), C.byref(params), niter,
+                                          _p(f_iter), _p(gopt), _p(acc), _p(bnd))
+        return f_iter, gopt, acc, bnd
+
+
+class Reference:
+    """The reference's own C sources compiled in _ref/ (built only where the sources exist)."""
+
+    def __init__(self):
+        if not os.path.exists(REF_LIB):
+            raise FileNotFoundError(REF_LIB)
+        self.lib = C.CDLL(REF_LIB)
+
+    @staticmethod
+    def available():
+        return os.path.exists(REF_LIB)
+
+    def brickwall_hvp_columns(self, vlist, vdirs, perms, L, tvlist, tperms, b0, b1):
+        vlist, vdirs, perms, tvlist, tperms = _c(vlist), _c(vdirs), _i(perms), _c(tvlist), _i(tperms)
+        G = vlist.shape[0] * (L // 2)
+        f = np.zeros(2)
+        dg = np.empty((G, 4, 4), np.complex128)
+        hg = np.empty_like(dg)
+        ret = self.lib.refdrv_brickwall_hvp_columns(_p(vlist), _p(vdirs), vlist.shape[0], _p(perms), L, _p(tvlist),
+                                                    tvlist.shape[0], _p(tperms), L_(b0), L_(b1), _p(f), _p(dg), _p(hg))
+        assert ret == 0
+        return f[0] + 1j * f[1], dg, hg
+
+    def brickwall_projected_hvp(self, vlist, vdirs, perms, L, tvlist, tperms):
+        vlist, vdirs, perms, tvlist, tperms = _c(vlist), _c(vdirs), _i(perms), _c(tvlist), _i(tperms)
+        f = np.zeros(2)
+        g = np.empty(16 * vlist.shape[0])
+        h = np.empty_like(g)
+        ret = self.lib.refdrv_brickwall_projected_hvp(_p(vlist), _p(vdirs), vlist.shape[0], _p(perms), L, _p(tvlist),
+                                                      tvlist.shape[0], _p(tperms), _p(f), _p(g), _p(h))
+        assert ret == 0
+        return f[0] + 1j * f[1], g, h
+
+    def optimize_brickwall(self, vstart, perms, L, tvlist, tperms, niter):
+        vstart, perms, tvlist, tperms = _c(vstart), _i(perms), _c(tvlist), _i(tperms)
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        self.lib.refdrv_optimize_brickwall(_p(vstart), vstart.shape[0], L, _p(perms), _p(tvlist), tvlist.shape[0],
+                                           _p(tperms), niter, _p(f_iter), _p(vopt))
+        return f_iter, vopt
+
+    def truncated_cg_hvp(self, grad, hvp_fn, radius):
+        grad = np.ascontiguousarray(grad, np.float64)
+        n = grad.shape[0]
+
+        def cb(x, fd, vec, hvp):
+            np.ctypeslib.as_array(hvp, shape=(n,))[:] = hvp_fn(np.ctypeslib.as_array(vec, shape=(n,)).copy())
+
+        f = HVP_FUNC(cb)
+        z = np.empty(n)
+        params = TcgParams(2 * n, 1e-8, 1e-6)
+        self.lib.truncated_cg_hvp.restype = C.c_bool
+        b = self.lib.truncated_cg_hvp(None, _p(grad), C.cast(f, VP), None, n, D(radius), C.byref(params), _p(z))
+        return z, bool(b)

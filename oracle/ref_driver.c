@@ -1,0 +1,140 @@
+/*
+ * Small driver compiled together with the unmodified reference sources into
+ * oracle/_ref/librqcopt_ref.so.  It calls only the reference's own public
+ * functions; it adds a matrix-free brickwall target as a `linear_func`, the
+ * synthetic target map of the reference tests, and a column-range form of the
+ * grad+HVP column loop (the loop body of src/target.c:335-369) so that a
+ * bounded sample of a large evaluation can be timed.
+ *
+ * TEST / BASELINE INFRASTRUCTURE ONLY.
+ */
+#include <stdlib.h>
+#include <string.h>
+#include "config.h"
+#include "matrix.h"
+#include "statevector.h"
+#include "gate.h"
+#include "quantum_circuit.h"
+#include "brickwall_circuit.h"
+#include "target.h"
+#include "trust_region.h"
+#include "brickwall_opt.h"
+#include "circuit_opt.h"
+
+struct refdrv_brickwall
+{
+	const struct mat4x4* vlist;
+	int nlayers;
+	const int** perms;
+};
+
+/* matrix-free brickwall target: psi_out = W psi via the reference's apply_brickwall_unitary */
+int refdrv_brickwall_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out)
+{
+	const struct refdrv_brickwall* t = udata;
+	return apply_brickwall_unitary(t->vlist, t->nlayers, t->perms, psi, psi_out);
+}
+
+/* synthetic sparse target of the reference tests (test/test_target.c:16-34) */
+int refdrv_fixture_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out)
+{
+	(void)udata;
+	const intqs n = (intqs)1 << psi->nqubits;
+	for (intqs i = 0; i < n; i++)
+		psi_out->data[i] = (-1.1 + 0.8*I) * psi->data[((i + 3) * 113) % n]
+		                 + ( 0.4 - 0.7*I) * psi->data[((i + 9) * 173) % n]
+		                 + ( 0.5 + 0.1*I) * psi->data[i]
+		                 + (-0.3 + 0.2*I) * psi->data[((i + 4) * 199) % n];
+	return 0;
+}
+
+static const int** perm_ptrs(const int* flat, int nlayers, int L)
+{
+	const int** p = malloc(nlayers * sizeof(int*));
+	for (int l = 0; l < nlayers; l++) p[l] = flat + (size_t)l * L;
+	return p;
+}
+
+/*
+ * Grad+HVP basis-column sum restricted to columns [b0, b1) for a brickwall
+ * circuit against a brickwall target, through the reference's per-column
+ * function quantum_circuit_gates_hessian_vector_product.  Outputs are the
+ * per-gate sums (not yet folded per layer), ngates = nlayers * L / 2.
+ */
+int refdrv_brickwall_hvp_columns(const struct mat4x4* vlist, const struct mat4x4* vdirs, int nlayers,
+                                 const int* perms_flat, int L,
+                                 const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                                 long b0, long b1, double* fval, struct mat4x4* dgates, struct mat4x4* hess)
+{
+	const int per = L / 2, G = nlayers * per;
+	struct mat4x4* gates = malloc(G * sizeof(struct mat4x4));
+	struct mat4x4* dirs = malloc(G * sizeof(struct mat4x4));
+	struct mat4x4* dg = malloc(G * sizeof(struct mat4x4));
+	struct mat4x4* hg = malloc(G * sizeof(struct mat4x4));
+	int* wires = malloc(2 * G * sizeof(int));
+	for (int l = 0; l < nlayers; l++)
+		for (int p = 0; p < per; p++) {
+			gates[l*per + p] = vlist[l];
+			dirs[l*per + p] = vdirs[l];
+			wires[2*(l*per + p)] = perms_flat[l*L + 2*p];
+			wires[2*(l*per + p) + 1] = perms_flat[l*L + 2*p + 1];
+		}
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+
+	struct statevector psi, upsi, cpsi;
+	allocate_statevector(L, &psi);
+	allocate_statevector(L, &upsi);
+	allocate_statevector(L, &cpsi);
+	memset(dgates, 0, G * sizeof(struct mat4x4));
+	memset(hess, 0, G * sizeof(struct mat4x4));
+	numeric f = 0;
+	const intqs n = (intqs)1 << L;
+	int ret = 0;
+	for (long b = b0; b < b1; b++) {
+		memset(psi.data, 0, n * sizeof(numeric));
+		psi.data[b] = 1;
+		refdrv_brickwall_ufunc(&psi, &target, &upsi);
+		for (intqs a = 0; a < n; a++) upsi.data[a] = -conj(upsi.data[a]);
+		if (quantum_circuit_gates_hessian_vector_product(gates, dirs, G, wires, &psi, &upsi, &cpsi, dg, hg) < 0) { ret = -3; break; }
+		for (intqs a = 0; a < n; a++) f += upsi.data[a] * cpsi.data[a];
+		for (int k = 0; k < G; k++) { add_matrix(&dgates[k], &dg[k]); add_matrix(&hess[k], &hg[k]); }
+	}
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free_statevector(&psi); free_statevector(&upsi); free_statevector(&cpsi);
+	free(tp); free(gates); free(dirs); free(dg); free(hg); free(wires);
+	return ret;
+}
+
+/* one f + projected gradient + projected HVP evaluation with a brickwall target */
+int refdrv_brickwall_projected_hvp(const struct mat4x4* vlist, const struct mat4x4* vdirs, int nlayers,
+                                   const int* perms_flat, int L,
+                                   const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                                   double* fval, double* grad_vec, double* hvp_vec)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	numeric f;
+	int ret = brickwall_unitary_target_projected_hessian_vector_product(refdrv_brickwall_ufunc, &target, vlist, vdirs,
+		nlayers, p, L, &f, grad_vec, hvp_vec);
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free(p); free(tp);
+	return ret;
+}
+
+/* the north-star driver with a brickwall target and default RTR parameters */
+void refdrv_optimize_brickwall(const struct mat4x4* vstart, int nlayers, int L, const int* perms_flat,
+                               const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                               int niter, double* f_iter, struct mat4x4* vopt)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	struct rtr_params params;
+	set_rtr_default_params(nlayers * num_tangent_params, &params);
+	optimize_brickwall_circuit_hvp(refdrv_brickwall_ufunc, &target, vstart, nlayers, L, p, &params, niter, f_iter, vopt);
+	free(p); free(tp);
+}

@@ -1,0 +1,856 @@
+/*
+ * CPU oracle: plain-C restatement of the rqcopt_hpc hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY -- the checker for the GPU library, loaded by the
+ * tests, the smoke check and the CPU-baseline leg of the benchmark.  It is
+ * never linked into or called by the product library.
+ *
+ * Each function cites the reference file:line whose algorithm it restates
+ * (paths relative to the cmendl/rqcopt_hpc project root).  The arithmetic is
+ * the reference's: double complex, sequential basis-column sums.
+ */
+#include "rqc_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ utilities */
+
+static orc_cplx* sv_alloc(int L)
+{
+	return (orc_cplx*)calloc((size_t)1 << L, sizeof(orc_cplx));
+}
+
+/* index of amplitude group member (bi, bj) for the rest index r; qubit q is bit L-1-q */
+static inline long group_base(long r, int pa, int pb)
+{
+	/* insert zero bits at positions pa < pb */
+	r = ((r >> pa) << (pa + 1)) | (r & ((1L << pa) - 1));
+	r = ((r >> pb) << (pb + 1)) | (r & ((1L << pb) - 1));
+	return r;
+}
+
+static inline void group_indices(long r, int L, int i, int j, long idx[4])
+{
+	const int pi = L - 1 - i, pj = L - 1 - j;
+	const long base = group_base(r, pi < pj ? pi : pj, pi < pj ? pj : pi);
+	const long si = 1L << pi, sj = 1L << pj;
+	idx[0] = base;
+	idx[1] = base + sj;
+	idx[2] = base + si;
+	idx[3] = base + si + sj;
+}
+
+/* ---------------------------------------------------------------- 4x4 algebra */
+
+/* src/matrix.c:354-370 */
+void orc_multiply(const orc_mat4* a, const orc_mat4* b, orc_mat4* c)
+{
+	orc_mat4 t;
+	for (int r = 0; r < 4; r++)
+		for (int k = 0; k < 4; k++) {
+			orc_cplx s = 0;
+			for (int m = 0; m < 4; m++) s += a->data[4*r + m] * b->data[4*m + k];
+			t.data[4*r + k] = s;
+		}
+	*c = t;
+}
+
+/* src/matrix.c:135-144 */
+void orc_adjoint(const orc_mat4* a, orc_mat4* ah)
+{
+	orc_mat4 t;
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) t.data[4*r + c] = conj(a->data[4*c + r]);
+	*ah = t;
+}
+
+/* src/matrix.c:119-128 */
+void orc_transpose(const orc_mat4* a, orc_mat4* at)
+{
+	orc_mat4 t;
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) t.data[4*r + c] = a->data[4*c + r];
+	*at = t;
+}
+
+/* src/matrix.c:151-174 (Hermitian part) */
+void orc_symm(const orc_mat4* w, orc_mat4* z)
+{
+	orc_mat4 t;
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) {
+			if (r == c) t.data[5*r] = creal(w->data[5*r]);
+			else if (r < c) t.data[4*r + c] = 0.5 * (w->data[4*r + c] + conj(w->data[4*c + r]));
+		}
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < r; c++) t.data[4*r + c] = conj(t.data[4*c + r]);
+	*z = t;
+}
+
+/* src/matrix.c:181-211 (anti-Hermitian part) */
+void orc_antisymm(const orc_mat4* w, orc_mat4* z)
+{
+	orc_mat4 t;
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) {
+			if (r == c) t.data[5*r] = I * cimag(w->data[5*r]);
+			else if (r < c) t.data[4*r + c] = 0.5 * (w->data[4*r + c] - conj(w->data[4*c + r]));
+		}
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < r; c++) t.data[4*r + c] = -conj(t.data[4*c + r]);
+	*z = t;
+}
+
+/* src/matrix.c:218-243: 16 reals -> anti-Hermitian matrix */
+void orc_real_to_antisymm(const double* x, orc_mat4* w)
+{
+	for (int r = 0; r < 4; r++) {
+		w->data[5*r] = I * x[5*r];
+		for (int c = r + 1; c < 4; c++) {
+			const double p = x[4*r + c], q = x[4*c + r];
+			w->data[4*r + c] = 0.5 * (p - q) + 0.5 * I * (p + q);
+			w->data[4*c + r] = -conj(w->data[4*r + c]);
+		}
+	}
+}
+
+/* src/matrix.c:279-286 */
+void orc_antisymm_to_real(const orc_mat4* w, double* x)
+{
+	for (int k = 0; k < 16; k++) x[k] = creal(w->data[k]) + cimag(w->data[k]);
+}
+
+/* src/matrix.c:309-314 */
+void orc_real_to_tangent(const double* x, const orc_mat4* v, orc_mat4* z)
+{
+	orc_mat4 a;
+	orc_real_to_antisymm(x, &a);
+	orc_multiply(v, &a, z);
+}
+
+/* src/matrix.c:322-329 */
+void orc_tangent_to_real(const orc_mat4* v, const orc_mat4* z, double* x)
+{
+	orc_mat4 vh, t, a;
+	orc_adjoint(v, &vh);
+	orc_multiply(&vh, z, &t);
+	orc_antisymm(&t, &a);
+	orc_antisymm_to_real(&a, x);
+}
+
+/* src/matrix.c:336-347 */
+void orc_project_tangent(const orc_mat4* u, const orc_mat4* z, orc_mat4* p)
+{
+	orc_mat4 uh, w, s;
+	orc_adjoint(u, &uh);
+	orc_multiply(&uh, z, &w);
+	orc_symm(&w, &s);
+	orc_multiply(u, &s, &w);
+	for (int k = 0; k < 16; k++) p->data[k] = z->data[k] - w.data[k];
+}
+
+/* src/matrix.c:376-389: (a b c + c b a) / 2 */
+void orc_symmetric_triple_product(const orc_mat4* a, const orc_mat4* b, const orc_mat4* c, orc_mat4* ret)
+{
+	orc_mat4 ab, abc, cb, cba;
+	orc_multiply(a, b, &ab);
+	orc_multiply(&ab, c, &abc);
+	orc_multiply(c, b, &cb);
+	orc_multiply(&cb, a, &cba);
+	for (int k = 0; k < 16; k++) ret->data[k] = 0.5 * (abc.data[k] + cba.data[k]);
+}
+
+/* src/matrix.c:410-475: Gauss-Jordan with partial pivoting */
+int orc_inverse(const orc_mat4* a, orc_mat4* ainv)
+{
+	orc_cplx m[4][4], v[4][4];
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) { m[r][c] = a->data[4*r + c]; v[r][c] = (r == c); }
+	for (int k = 0; k < 4; k++) {
+		int piv = k;
+		double best = cabs(m[k][k]);
+		for (int r = k + 1; r < 4; r++)
+			if (cabs(m[r][k]) > best) { best = cabs(m[r][k]); piv = r; }
+		if (best == 0) return -1;
+		if (piv != k)
+			for (int c = 0; c < 4; c++) {
+				orc_cplx t = m[k][c]; m[k][c] = m[piv][c]; m[piv][c] = t;
+				t = v[k][c]; v[k][c] = v[piv][c]; v[piv][c] = t;
+			}
+		for (int r = 0; r < 4; r++) {
+			if (r == k) continue;
+			const orc_cplx s = m[r][k] / m[k][k];
+			for (int c = k + 1; c < 4; c++) m[r][c] -= s * m[k][c];
+			m[r][k] = 0;
+			for (int c = 0; c < 4; c++) v[r][c] -= s * v[k][c];
+		}
+		for (int c = k + 1; c < 4; c++) m[k][c] /= m[k][k];
+		for (int c = 0; c < 4; c++) v[k][c] /= m[k][k];
+		m[k][k] = 1;
+	}
+	for (int r = 0; r < 4; r++)
+		for (int c = 0; c < 4; c++) ainv->data[4*r + c] = v[r][c];
+	return 0;
+}
+
+/* src/matrix.c:488-510: Newton iteration u <- (u + u^{-H}) / 2, early stop after k >= 4 */
+void orc_polar_factor(const orc_mat4* a, orc_mat4* u)
+{
+	orc_mat4 x = *a;
+	for (int k = 0; k < 14; k++) {
+		orc_mat4 xi, w;
+		orc_inverse(&x, &xi);
+		orc_adjoint(&xi, &w);
+		double d = 0;
+		for (int e = 0; e < 16; e++) {
+			x.data[e] = 0.5 * (x.data[e] + w.data[e]);
+			const double de = cabs(x.data[e] - w.data[e]);   /* src/util.c:24-33 */
+			d = fmax(d, de);
+		}
+		if (k >= 4 && d < 1e-14) break;
+	}
+	*u = x;
+}
+
+/* src/matrix.c:517-531 */
+void orc_retract(const orc_mat4* u, const double* eta, orc_mat4* v)
+{
+	orc_mat4 z, w;
+	orc_real_to_antisymm(eta, &z);
+	for (int r = 0; r < 4; r++) z.data[5*r] += 1;
+	orc_multiply(u, &z, &w);
+	orc_polar_factor(&w, v);
+}
+
+/* ------------------------------------------------------------------- gates */
+
+/* src/gate.c:10-76: psi_out = (gate on wires i, j) psi; row index of the gate is 2*b_i + b_j */
+void orc_apply_gate(const orc_mat4* g, int i, int j, const orc_sv* psi, orc_sv* out)
+{
+	const int L = psi->nqubits;
+	const long ngroups = 1L << (L - 2);
+	for (long r = 0; r < ngroups; r++) {
+		long idx[4];
+		group_indices(r, L, i, j, idx);
+		orc_cplx x[4];
+		for (int c = 0; c < 4; c++) x[c] = psi->data[idx[c]];
+		for (int k = 0; k < 4; k++) {
+			orc_cplx s = 0;
+			for (int c = 0; c < 4; c++) s += g->data[4*k + c] * x[c];
+			out->data[idx[k]] = s;
+		}
+	}
+}
+
+/* src/gate.c:83-188: dpsi = gate^T dpsi_out; dgate = sum dpsi_out (x) psi (no conjugation) */
+void orc_apply_gate_backward(const orc_mat4* g, int i, int j, const orc_sv* psi,
+                             const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dg)
+{
+	const int L = psi->nqubits;
+	const long ngroups = 1L << (L - 2);
+	orc_mat4 acc;
+	memset(&acc, 0, sizeof(acc));
+	for (long r = 0; r < ngroups; r++) {
+		long idx[4];
+		group_indices(r, L, i, j, idx);
+		orc_cplx x[4], d[4];
+		for (int c = 0; c < 4; c++) { x[c] = psi->data[idx[c]]; d[c] = dpsi_out->data[idx[c]]; }
+		for (int a = 0; a < 4; a++)
+			for (int c = 0; c < 4; c++) acc.data[4*a + c] += d[a] * x[c];
+		for (int c = 0; c < 4; c++) {
+			orc_cplx s = 0;
+			for (int a = 0; a < 4; a++) s += g->data[4*a + c] * d[a];
+			dpsi->data[idx[c]] = s;
+		}
+	}
+	*dg = acc;
+}
+
+/* ---------------------------------------------------------------- circuits */
+
+/* src/quantum_circuit.c:13-35 */
+int orc_apply_circuit(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* psi, orc_sv* out)
+{
+	const int L = psi->nqubits;
+	const size_t bytes = ((size_t)1 << L) * sizeof(orc_cplx);
+	orc_sv a = { sv_alloc(L), L }, b = { sv_alloc(L), L };
+	if (!a.data || !b.data) { free(a.data); free(b.data); return -1; }
+	memcpy(a.data, psi->data, bytes);
+	for (int k = 0; k < ngates; k++) {
+		orc_apply_gate(&gates[k], wires[2*k], wires[2*k + 1], &a, &b);
+		orc_cplx* t = a.data; a.data = b.data; b.data = t;
+	}
+	memcpy(out->data, a.data, bytes);
+	free(a.data); free(b.data);
+	return 0;
+}
+
+/* src/quantum_circuit.c:90-108: cache[k] = state entering gate k */
+int orc_circuit_forward(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* psi,
+                        orc_sv* cache, orc_sv* out)
+{
+	const size_t bytes = ((size_t)1 << psi->nqubits) * sizeof(orc_cplx);
+	memcpy(cache[0].data, psi->data, bytes);
+	for (int k = 0; k < ngates; k++)
+		orc_apply_gate(&gates[k], wires[2*k], wires[2*k + 1], &cache[k], k + 1 < ngates ? &cache[k + 1] : out);
+	return 0;
+}
+
+/* src/quantum_circuit.c:115-140 */
+int orc_circuit_backward(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* cache,
+                         const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dgates)
+{
+	const int L = dpsi->nqubits;
+	const size_t bytes = ((size_t)1 << L) * sizeof(orc_cplx);
+	orc_sv cur = { sv_alloc(L), L }, nxt = { sv_alloc(L), L };
+	if (!cur.data || !nxt.data) { free(cur.data); free(nxt.data); return -1; }
+	memcpy(cur.data, dpsi_out->data, bytes);
+	for (int k = ngates - 1; k >= 0; k--) {
+		orc_apply_gate_backward(&gates[k], wires[2*k], wires[2*k + 1], &cache[k], &cur, &nxt, &dgates[k]);
+		orc_cplx* t = cur.data; cur.data = nxt.data; nxt.data = t;
+	}
+	memcpy(dpsi->data, cur.data, bytes);
+	free(cur.data); free(nxt.data);
+	return 0;
+}
+
+/* src/quantum_circuit.c:147-236: forward with cache, reverse pass from phi with cache,
+ * then the ascending sweep (tangent of the forward states) and the descending sweep
+ * (tangent of the reverse states). */
+int orc_circuit_gates_hvp(const orc_mat4* gates, const orc_mat4* gatedirs, int ngates, const int* wires,
+                          const orc_sv* psi, const orc_sv* phi, orc_sv* psi_out,
+                          orc_mat4* dgates, orc_mat4* hess)
+{
+	const int L = psi->nqubits;
+	const size_t bytes = ((size_t)1 << L) * sizeof(orc_cplx);
+	orc_sv* fwd = (orc_sv*)calloc(ngates, sizeof(orc_sv));
+	orc_sv* rev = (orc_sv*)calloc(ngates, sizeof(orc_sv));
+	orc_sv t1 = { sv_alloc(L), L }, t2 = { sv_alloc(L), L }, d = { sv_alloc(L), L }, sink = { sv_alloc(L), L };
+	int fail = !fwd || !rev || !t1.data || !t2.data || !d.data || !sink.data;
+	for (int k = 0; k < ngates && !fail; k++) {
+		fwd[k].nqubits = rev[k].nqubits = L;
+		fwd[k].data = sv_alloc(L);
+		rev[k].data = sv_alloc(L);
+		fail = !fwd[k].data || !rev[k].data;
+	}
+	if (!fail) {
+		orc_circuit_forward(gates, ngates, wires, psi, fwd, psi_out);
+		/* reverse states: rev[k] = adjoint vector at the output of gate k */
+		memcpy(rev[ngates - 1].data, phi->data, bytes);
+		for (int k = ngates - 1; k >= 0; k--)
+			orc_apply_gate_backward(&gates[k], wires[2*k], wires[2*k + 1], &fwd[k], &rev[k],
+			                        k > 0 ? &rev[k - 1] : &sink, &dgates[k]);
+		/* ascending sweep: d = tangent of the state entering gate k */
+		memset(&hess[0], 0, sizeof(orc_mat4));
+		orc_apply_gate(&gatedirs[0], wires[0], wires[1], &fwd[0], &d);
+		for (int k = 1; k < ngates; k++) {
+			orc_mat4 gt, dg;
+			orc_transpose(&gates[k], &gt);
+			orc_apply_gate_backward(&gt, wires[2*k], wires[2*k + 1], &rev[k], &d, &t1, &dg);
+			orc_transpose(&dg, &hess[k]);
+			orc_apply_gate(&gatedirs[k], wires[2*k], wires[2*k + 1], &fwd[k], &t2);
+			for (long a = 0; a < (1L << L); a++) d.data[a] = t1.data[a] + t2.data[a];
+		}
+		/* descending sweep: d = tangent of the adjoint vector at the output of gate k */
+		{
+			orc_mat4 zt;
+			orc_transpose(&gatedirs[ngates - 1], &zt);
+			orc_apply_gate(&zt, wires[2*ngates - 2], wires[2*ngates - 1], &rev[ngates - 1], &d);
+		}
+		for (int k = ngates - 2; k >= 0; k--) {
+			orc_mat4 dg, zt;
+			orc_apply_gate_backward(&gates[k], wires[2*k], wires[2*k + 1], &fwd[k], &d, &t1, &dg);
+			for (int e = 0; e < 16; e++) hess[k].data[e] += dg.data[e];
+			orc_transpose(&gatedirs[k], &zt);
+			orc_apply_gate(&zt, wires[2*k], wires[2*k + 1], &rev[k], &t2);
+			for (long a = 0; a < (1L << L); a++) d.data[a] = t1.data[a] + t2.data[a];
+		}
+	}
+	for (int k = 0; k < ngates && fwd && rev; k++) { free(fwd[k].data); free(rev[k].data); }
+	free(fwd); free(rev); free(t1.data); free(t2.data); free(d.data); free(sink.data);
+	return fail ? -1 : 0;
+}
+
+/* brickwall -> sequential gate list (src/target.c:443-458); perms is [nlayers][L] */
+static void brickwall_expand(int L, int nlayers, const orc_mat4* vlist, const int* perms,
+                             orc_mat4* gates, int* wires)
+{
+	const int per = L / 2;
+	for (int l = 0; l < nlayers; l++)
+		for (int p = 0; p < per; p++) {
+			if (gates) gates[l*per + p] = vlist[l];
+			wires[2*(l*per + p)]     = perms[l*L + 2*p];
+			wires[2*(l*per + p) + 1] = perms[l*L + 2*p + 1];
+		}
+}
+
+/* src/brickwall_circuit.c:14-43 */
+int orc_apply_brickwall(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* psi, orc_sv* out)
+{
+	const int L = psi->nqubits, G = nlayers * (L / 2);
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_apply_circuit(gates, G, wires, psi, out);
+	free(gates); free(wires);
+	return ret;
+}
+
+/* src/brickwall_circuit.c:51-77 */
+int orc_brickwall_forward(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* psi,
+                          orc_sv* cache, orc_sv* out)
+{
+	const int L = psi->nqubits, G = nlayers * (L / 2);
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_circuit_forward(gates, G, wires, psi, cache, out);
+	free(gates); free(wires);
+	return ret;
+}
+
+/* src/brickwall_circuit.c:85-124: per-layer gradient = sum over the layer's gate copies */
+int orc_brickwall_backward(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* cache,
+                           const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dvlist)
+{
+	const int L = dpsi->nqubits, per = L / 2, G = nlayers * per;
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	orc_mat4* dg = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_circuit_backward(gates, G, wires, cache, dpsi_out, dpsi, dg);
+	for (int l = 0; l < nlayers; l++) {
+		memset(&dvlist[l], 0, sizeof(orc_mat4));
+		for (int p = per - 1; p >= 0; p--)
+			for (int e = 0; e < 16; e++) dvlist[l].data[e] += dg[l*per + p].data[e];
+	}
+	free(gates); free(dg); free(wires);
+	return ret;
+}
+
+/* ------------------------------------------------------------------ targets */
+
+/* one basis column of -conj(U): src/target.c:41-53 */
+static int target_column(orc_linear_func uf, void* ud, long b, orc_sv* e, orc_sv* u)
+{
+	const long n = 1L << e->nqubits;
+	memset(e->data, 0, n * sizeof(orc_cplx));
+	e->data[b] = 1;
+	int ret = uf(e, ud, u);
+	if (ret < 0) return -2;
+	for (long a = 0; a < n; a++) u->data[a] = -conj(u->data[a]);
+	return 0;
+}
+
+/* src/target.c:15-75 */
+int orc_circuit_target(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates, const int* wires,
+                       int L, long b_begin, long b_end, orc_cplx* fval)
+{
+	const long n = 1L << L;
+	orc_sv e = { sv_alloc(L), L }, u = { sv_alloc(L), L }, c = { sv_alloc(L), L };
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = b_begin; b < b_end && ret == 0; b++) {
+		ret = target_column(uf, ud, b, &e, &u);
+		if (ret) break;
+		e.data[b] = 1;
+		orc_apply_circuit(gates, ngates, wires, &e, &c);
+		for (long a = 0; a < n; a++) f += u.data[a] * c.data[a];
+	}
+	free(e.data); free(u.data); free(c.data);
+	*fval = f;
+	return ret;
+}
+
+/* src/target.c:158-247 */
+int orc_circuit_target_and_gradient(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates,
+                                    const int* wires, int L, long b_begin, long b_end,
+                                    orc_cplx* fval, orc_mat4* dgates)
+{
+	const long n = 1L << L;
+	orc_sv e = { sv_alloc(L), L }, u = { sv_alloc(L), L }, c = { sv_alloc(L), L };
+	orc_sv* cache = (orc_sv*)calloc(ngates, sizeof(orc_sv));
+	orc_mat4* dg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	for (int k = 0; k < ngates; k++) { cache[k].nqubits = L; cache[k].data = sv_alloc(L); }
+	memset(dgates, 0, ngates * sizeof(orc_mat4));
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = b_begin; b < b_end; b++) {
+		ret = target_column(uf, ud, b, &e, &u);
+		if (ret) break;
+		e.data[b] = 1;
+		orc_circuit_forward(gates, ngates, wires, &e, cache, &c);
+		for (long a = 0; a < n; a++) f += u.data[a] * c.data[a];
+		orc_circuit_backward(gates, ngates, wires, cache, &u, &e, dg);
+		for (int k = 0; k < ngates; k++)
+			for (int x = 0; x < 16; x++) dgates[k].data[x] += dg[k].data[x];
+	}
+	for (int k = 0; k < ngates; k++) free(cache[k].data);
+	free(cache); free(dg); free(e.data); free(u.data); free(c.data);
+	*fval = f;
+	return ret;
+}
+
+/* src/target.c:289-380 */
+int orc_circuit_target_hvp(orc_linear_func uf, void* ud, const orc_mat4* gates, const orc_mat4* gatedirs,
+                           int ngates, const int* wires, int L, long b_begin, long b_end,
+                           orc_cplx* fval, orc_mat4* dgates, orc_mat4* hess)
+{
+	const long n = 1L << L;
+	orc_sv e = { sv_alloc(L), L }, u = { sv_alloc(L), L }, c = { sv_alloc(L), L };
+	orc_mat4* dg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	orc_mat4* hg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	memset(dgates, 0, ngates * sizeof(orc_mat4));
+	memset(hess, 0, ngates * sizeof(orc_mat4));
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = b_begin; b < b_end; b++) {
+		ret = target_column(uf, ud, b, &e, &u);
+		if (ret) break;
+		e.data[b] = 1;
+		if (orc_circuit_gates_hvp(gates, gatedirs, ngates, wires, &e, &u, &c, dg, hg) < 0) { ret = -3; break; }
+		for (long a = 0; a < n; a++) f += u.data[a] * c.data[a];
+		for (int k = 0; k < ngates; k++)
+			for (int x = 0; x < 16; x++) { dgates[k].data[x] += dg[k].data[x]; hess[k].data[x] += hg[k].data[x]; }
+	}
+	free(dg); free(hg); free(e.data); free(u.data); free(c.data);
+	*fval = f;
+	return ret;
+}
+
+/* src/target.c:256-280 */
+int orc_circuit_target_projected_gradient(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates,
+                                          const int* wires, int L, orc_cplx* fval, double* grad_vec)
+{
+	orc_mat4* dg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	int ret = orc_circuit_target_and_gradient(uf, ud, gates, ngates, wires, L, 0, 1L << L, fval, dg);
+	for (int k = 0; k < ngates && ret == 0; k++) {
+		for (int x = 0; x < 16; x++) dg[k].data[x] = conj(dg[k].data[x]);
+		orc_tangent_to_real(&gates[k], &dg[k], &grad_vec[16*k]);
+	}
+	free(dg);
+	return ret;
+}
+
+/* projection of gradient and HVP for one gate: src/target.c:410-430 */
+static void project_grad_hvp(const orc_mat4* g, const orc_mat4* z, orc_mat4* dg, orc_mat4* hg,
+                             double* grad_vec, double* hvp_vec)
+{
+	for (int x = 0; x < 16; x++) { dg->data[x] = conj(dg->data[x]); hg->data[x] = conj(hg->data[x]); }
+	orc_tangent_to_real(g, dg, grad_vec);
+	orc_mat4 gradh, pd;
+	orc_adjoint(dg, &gradh);
+	orc_symmetric_triple_product(z, &gradh, g, &pd);
+	for (int x = 0; x < 16; x++) hg->data[x] -= pd.data[x];
+	orc_tangent_to_real(g, hg, hvp_vec);
+}
+
+/* src/target.c:389-436 */
+int orc_circuit_target_projected_hvp(orc_linear_func uf, void* ud, const orc_mat4* gates, const orc_mat4* gatedirs,
+                                     int ngates, const int* wires, int L,
+                                     orc_cplx* fval, double* grad_vec, double* hvp_vec)
+{
+	orc_mat4* dg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	orc_mat4* hg = (orc_mat4*)malloc(ngates * sizeof(orc_mat4));
+	int ret = orc_circuit_target_hvp(uf, ud, gates, gatedirs, ngates, wires, L, 0, 1L << L, fval, dg, hg);
+	for (int k = 0; k < ngates && ret == 0; k++)
+		project_grad_hvp(&gates[k], &gatedirs[k], &dg[k], &hg[k], &grad_vec[16*k], &hvp_vec[16*k]);
+	free(dg); free(hg);
+	return ret < 0 ? -2 : 0;
+}
+
+/* src/target.c:467-481 */
+int orc_brickwall_target(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int L,
+                         const int* perms, orc_cplx* fval)
+{
+	const int G = nlayers * (L / 2);
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_circuit_target(uf, ud, gates, G, wires, L, 0, 1L << L, fval);
+	free(gates); free(wires);
+	return ret;
+}
+
+/* src/target.c:514-542 */
+int orc_brickwall_target_and_gradient(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                      int L, const int* perms, orc_cplx* fval, orc_mat4* dvlist)
+{
+	const int per = L / 2, G = nlayers * per;
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	orc_mat4* dg = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_circuit_target_and_gradient(uf, ud, gates, G, wires, L, 0, 1L << L, fval, dg);
+	for (int l = 0; l < nlayers; l++) {
+		memset(&dvlist[l], 0, sizeof(orc_mat4));
+		for (int p = 0; p < per; p++)
+			for (int x = 0; x < 16; x++) dvlist[l].data[x] += dg[l*per + p].data[x];
+	}
+	free(gates); free(dg); free(wires);
+	return ret;
+}
+
+/* src/target.c:551-575 */
+int orc_brickwall_target_projected_gradient(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                            int L, const int* perms, orc_cplx* fval, double* grad_vec)
+{
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	int ret = orc_brickwall_target_and_gradient(uf, ud, vlist, nlayers, L, perms, fval, dv);
+	for (int l = 0; l < nlayers && ret == 0; l++) {
+		for (int x = 0; x < 16; x++) dv[l].data[x] = conj(dv[l].data[x]);
+		orc_tangent_to_real(&vlist[l], &dv[l], &grad_vec[16*l]);
+	}
+	free(dv);
+	return ret;
+}
+
+/* src/target.c:584-622 */
+int orc_brickwall_target_hvp(orc_linear_func uf, void* ud, const orc_mat4* vlist, const orc_mat4* vdirs,
+                             int nlayers, const int* perms, int L, long b_begin, long b_end,
+                             orc_cplx* fval, orc_mat4* dvlist, orc_mat4* hess_vdirs)
+{
+	const int per = L / 2, G = nlayers * per;
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	orc_mat4* dirs = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	orc_mat4* dg = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	orc_mat4* hg = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	brickwall_expand(L, nlayers, vdirs, perms, dirs, wires);
+	int ret = orc_circuit_target_hvp(uf, ud, gates, dirs, G, wires, L, b_begin, b_end, fval, dg, hg);
+	for (int l = 0; l < nlayers; l++) {
+		memset(&dvlist[l], 0, sizeof(orc_mat4));
+		memset(&hess_vdirs[l], 0, sizeof(orc_mat4));
+		for (int p = 0; p < per; p++)
+			for (int x = 0; x < 16; x++) {
+				dvlist[l].data[x] += dg[l*per + p].data[x];
+				hess_vdirs[l].data[x] += hg[l*per + p].data[x];
+			}
+	}
+	free(gates); free(dirs); free(dg); free(hg); free(wires);
+	return ret;
+}
+
+/* src/target.c:631-678 */
+int orc_brickwall_target_projected_hvp(orc_linear_func uf, void* ud, const orc_mat4* vlist, const orc_mat4* vdirs,
+                                       int nlayers, const int* perms, int L,
+                                       orc_cplx* fval, double* grad_vec, double* hvp_vec)
+{
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_mat4* hv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	int ret = orc_brickwall_target_hvp(uf, ud, vlist, vdirs, nlayers, perms, L, 0, 1L << L, fval, dv, hv);
+	for (int l = 0; l < nlayers && ret == 0; l++)
+		project_grad_hvp(&vlist[l], &vdirs[l], &dv[l], &hv[l], &grad_vec[16*l], &hvp_vec[16*l]);
+	free(dv); free(hv);
+	return ret < 0 ? -2 : 0;
+}
+
+/* ------------------------------------------------------------- trust region */
+
+static double dot(int n, const double* a, const double* b)
+{
+	double s = 0;
+	for (int k = 0; k < n; k++) s += a[k] * b[k];
+	return s;
+}
+
+/* src/trust_region.c:14-40: roots of x^2 + 2 p x + q */
+static void quadratic_roots(double p, double q, double x[2])
+{
+	if (p == 0) { const double a = sqrt(-q); x[0] = -a; x[1] = a; return; }
+	const double a = -(p + copysign(1.0, p) * sqrt(p * p - q));
+	const double b = q / a;
+	if (a <= b) { x[0] = a; x[1] = b; } else { x[0] = b; x[1] = a; }
+}
+
+/* src/trust_region.c:49-65: positive t with ||b + t d|| = radius */
+static double to_boundary(const double* b, const double* d, int n, double radius)
+{
+	const double dsq = dot(n, d, d);
+	if (dsq == 0) return 0;
+	const double p = dot(n, b, d) / dsq;
+	const double q = (dot(n, b, b) - radius * radius) / dsq;
+	double t[2];
+	quadratic_roots(p, q, t);
+	return t[1];
+}
+
+/* src/trust_region.c:159-217 (Steihaug-Toint truncated CG) */
+bool orc_truncated_cg_hvp(const double* x, const double* grad, orc_hvp_func f_hvp, void* fdata, int n,
+                          double radius, const orc_tcg_params* params, double* z)
+{
+	double* r = (double*)malloc(n * sizeof(double));
+	double* d = (double*)malloc(n * sizeof(double));
+	double* hd = (double*)malloc(n * sizeof(double));
+	memcpy(r, grad, n * sizeof(double));
+	double rsq = dot(n, r, r);
+	const double stoptol = fmax(params->abstol, params->reltol * sqrt(rsq));
+	memset(z, 0, n * sizeof(double));
+	for (int k = 0; k < n; k++) d[k] = -r[k];
+	bool boundary = false;
+	for (int it = 0; it < params->maxiter; it++) {
+		f_hvp(x, fdata, d, hd);
+		const double dhd = dot(n, d, hd);
+		const double t = to_boundary(z, d, n, radius);
+		const double alpha = rsq / dhd;
+		if (dhd <= 0 || alpha > t) {
+			for (int k = 0; k < n; k++) z[k] += t * d[k];
+			boundary = true;
+			break;
+		}
+		for (int k = 0; k < n; k++) r[k] += alpha * hd[k];
+		for (int k = 0; k < n; k++) z[k] += alpha * d[k];
+		const double rsq_next = dot(n, r, r);
+		if (sqrt(rsq_next) <= stoptol) break;
+		const double beta = rsq_next / rsq;
+		for (int k = 0; k < n; k++) d[k] = beta * d[k] - r[k];
+		rsq = rsq_next;
+	}
+	free(r); free(d); free(hd);
+	return boundary;
+}
+
+/* src/trust_region.c:306-368 (Riemannian trust region, Absil et al. Algorithm 10) */
+void orc_rtr_optimize_hvp(orc_target_func f, orc_target_grad_func f_deriv, orc_hvp_func f_hvp, void* fdata,
+                          orc_retract_func retract, void* rdata, int n, const double* x_init, int m,
+                          const orc_rtr_params* params, int niter, double* f_iter, double* x_final,
+                          int* accepted, int* on_boundary)
+{
+	double* x = (double*)malloc(m * sizeof(double));
+	double* xn = (double*)malloc(m * sizeof(double));
+	double* grad = (double*)malloc(n * sizeof(double));
+	double* eta = (double*)malloc(n * sizeof(double));
+	double* heta = (double*)malloc(n * sizeof(double));
+	memcpy(x, x_init, m * sizeof(double));
+	double radius = params->radius_init;
+	for (int k = 0; k < niter; k++) {
+		const double fx = f_deriv(x, fdata, grad);
+		const bool bnd = orc_truncated_cg_hvp(x, grad, f_hvp, fdata, n, radius, &params->tcg, eta);
+		retract(x, eta, rdata, xn);
+		f_iter[k] = fx;
+		f_hvp(x, fdata, eta, heta);
+		const double rho = (f(xn, fdata) - fx) / (dot(n, grad, eta) + 0.5 * dot(n, eta, heta));
+		if (rho < 0.25) radius *= 0.25;
+		else if (rho > 0.75 && bnd) radius = fmin(2 * radius, params->maxradius);
+		const int acc = rho > params->rho_trust;
+		if (acc) { double* t = x; x = xn; xn = t; }
+		if (accepted) accepted[k] = acc;
+		if (on_boundary) on_boundary[k] = bnd;
+	}
+	memcpy(x_final, x, m * sizeof(double));
+	f_iter[niter] = f(x_final, fdata);
+	free(x); free(xn); free(grad); free(eta); free(heta);
+}
+
+/* ---------------------------------------------------------- optimiser glue */
+
+typedef struct {
+	orc_linear_func uf; void* ud; const int* perms_or_wires; int ngates_or_layers; int L; int brickwall;
+} glue;
+
+/* src/brickwall_opt.c:22-33, src/circuit_opt.c:22-33 */
+static double glue_f(const double* x, void* fd)
+{
+	const glue* g = (const glue*)fd;
+	orc_cplx f;
+	int ret = g->brickwall
+		? orc_brickwall_target(g->uf, g->ud, (const orc_mat4*)x, g->ngates_or_layers, g->L, g->perms_or_wires, &f)
+		: orc_circuit_target(g->uf, g->ud, (const orc_mat4*)x, g->ngates_or_layers, g->perms_or_wires, g->L, 0, 1L << g->L, &f);
+	return ret < 0 ? -1 : creal(f);
+}
+
+/* src/brickwall_opt.c:40-51, src/circuit_opt.c:40-51 */
+static double glue_fd(const double* x, void* fd, double* grad)
+{
+	const glue* g = (const glue*)fd;
+	orc_cplx f;
+	int ret = g->brickwall
+		? orc_brickwall_target_projected_gradient(g->uf, g->ud, (const orc_mat4*)x, g->ngates_or_layers, g->L, g->perms_or_wires, &f, grad)
+		: orc_circuit_target_projected_gradient(g->uf, g->ud, (const orc_mat4*)x, g->ngates_or_layers, g->perms_or_wires, g->L, &f, grad);
+	return ret < 0 ? -1 : creal(f);
+}
+
+/* src/brickwall_opt.c:58-78, src/circuit_opt.c:58-78 */
+static void glue_hvp(const double* x, void* fd, double* vec, double* hvp)
+{
+	const glue* g = (const glue*)fd;
+	const int k = g->ngates_or_layers;
+	const orc_mat4* v = (const orc_mat4*)x;
+	orc_mat4* dirs = (orc_mat4*)malloc(k * sizeof(orc_mat4));
+	double* gv = (double*)malloc(16 * k * sizeof(double));
+	for (int i = 0; i < k; i++) orc_real_to_tangent(&vec[16*i], &v[i], &dirs[i]);
+	orc_cplx f;
+	if (g->brickwall)
+		orc_brickwall_target_projected_hvp(g->uf, g->ud, v, dirs, k, g->perms_or_wires, g->L, &f, gv, hvp);
+	else
+		orc_circuit_target_projected_hvp(g->uf, g->ud, v, dirs, k, g->perms_or_wires, g->L, &f, gv, hvp);
+	free(dirs); free(gv);
+}
+
+/* src/brickwall_opt.c:107-119 */
+static void glue_retract(const double* x, const double* eta, void* rdata, double* xs)
+{
+	const int k = *(const int*)rdata;
+	for (int i = 0; i < k; i++) orc_retract(&((const orc_mat4*)x)[i], &eta[16*i], &((orc_mat4*)xs)[i]);
+}
+
+/* src/brickwall_opt.c:127-149 */
+void orc_optimize_brickwall_hvp(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int L,
+                                const int* perms, const orc_rtr_params* params, int niter,
+                                double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary)
+{
+	glue g = { uf, ud, perms, nlayers, L, 1 };
+	int k = nlayers;
+	orc_rtr_optimize_hvp(glue_f, glue_fd, glue_hvp, &g, glue_retract, &k, 16 * nlayers,
+	                     (const double*)vstart, 32 * nlayers, params, niter, f_iter, (double*)vopt,
+	                     accepted, on_boundary);
+}
+
+/* src/circuit_opt.c:104-124 */
+void orc_optimize_circuit_hvp(orc_linear_func uf, void* ud, const orc_mat4* gstart, int ngates, int L,
+                              const int* wires, const orc_rtr_params* params, int niter,
+                              double* f_iter, orc_mat4* gopt, int* accepted, int* on_boundary)
+{
+	glue g = { uf, ud, wires, ngates, L, 0 };
+	int k = ngates;
+	orc_rtr_optimize_hvp(glue_f, glue_fd, glue_hvp, &g, glue_retract, &k, 16 * ngates,
+	                     (const double*)gstart, 32 * ngates, params, niter, f_iter, (double*)gopt,
+	                     accepted, on_boundary);
+}
+
+/* ------------------------------------------------------------ target maps */
+
+int orc_brickwall_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out)
+{
+	const orc_brickwall_udata* t = (const orc_brickwall_udata*)udata;
+	return orc_apply_brickwall(t->vlist, t->nlayers, t->perms, psi, psi_out);
+}
+
+/* test/test_target.c:16-34 */
+int orc_fixture_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out)
+{
+	(void)udata;
+	const long n = 1L << psi->nqubits;
+	for (long i = 0; i < n; i++)
+		psi_out->data[i] = (-1.1 + 0.8*I) * psi->data[((i + 3) * 113) % n]
+		                 + ( 0.4 - 0.7*I) * psi->data[((i + 9) * 173) % n]
+		                 + ( 0.5 + 0.1*I) * psi->data[i]
+		                 + (-0.3 + 0.2*I) * psi->data[((i + 4) * 199) % n];
+	return 0;
+}
+
+int orc_dense_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out)
+{
+	const orc_cplx* u = (const orc_cplx*)udata;
+	const long n = 1L << psi->nqubits;
+	for (long r = 0; r < n; r++) {
+		orc_cplx s = 0;
+		for (long c = 0; c < n; c++) s += u[r*n + c] * psi->data[c];
+		psi_out->data[r] = s;
+	}
+	return 0;
+}

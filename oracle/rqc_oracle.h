@@ -1,0 +1,120 @@
+/*
+ * CPU oracle for the rqcopt_hpc matrix-free circuit-optimisation path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * algorithm (cmendl/rqcopt_hpc, src/*.c) used as the checker for the GPU
+ * library.  Only the tests, the smoke check and the CPU-baseline leg of the
+ * benchmark load it; the product library never links or calls it.
+ *
+ * Every function states the reference file:line it restates.  Types are
+ * layout-identical to the reference's `struct mat4x4` / `struct statevector`
+ * (src/matrix.h:10-13, src/statevector.h:11-15): 16 row-major double-complex
+ * gate entries, and a 2^nqubits double-complex amplitude vector with qubit 0
+ * the most significant index bit.
+ */
+#pragma once
+
+#include <complex.h>
+#include <stdbool.h>
+
+typedef double complex orc_cplx;
+
+typedef struct { orc_cplx data[16]; } orc_mat4;
+
+typedef struct { orc_cplx* data; int nqubits; } orc_sv;
+
+/* same calling convention as the reference's `linear_func` (src/target.h:7) */
+typedef int (*orc_linear_func)(const orc_sv* psi, void* udata, orc_sv* psi_out);
+
+typedef void (*orc_hvp_func)(const double* x, void* fdata, double* vec, double* hvp);
+typedef double (*orc_target_func)(const double* x, void* fdata);
+typedef double (*orc_target_grad_func)(const double* x, void* fdata, double* grad);
+typedef void (*orc_retract_func)(const double* x, const double* eta, void* rdata, double* xs);
+
+typedef struct { int maxiter; double abstol; double reltol; } orc_tcg_params;
+typedef struct { orc_tcg_params tcg; double rho_trust, radius_init, maxradius; } orc_rtr_params;
+
+/* ---- 4x4 algebra (src/matrix.c) ---- */
+void orc_multiply(const orc_mat4* a, const orc_mat4* b, orc_mat4* c);
+void orc_adjoint(const orc_mat4* a, orc_mat4* ah);
+void orc_transpose(const orc_mat4* a, orc_mat4* at);
+void orc_symm(const orc_mat4* w, orc_mat4* z);
+void orc_antisymm(const orc_mat4* w, orc_mat4* z);
+void orc_real_to_antisymm(const double* r, orc_mat4* w);
+void orc_antisymm_to_real(const orc_mat4* w, double* r);
+void orc_real_to_tangent(const double* r, const orc_mat4* v, orc_mat4* z);
+void orc_tangent_to_real(const orc_mat4* v, const orc_mat4* z, double* r);
+void orc_project_tangent(const orc_mat4* u, const orc_mat4* z, orc_mat4* p);
+void orc_symmetric_triple_product(const orc_mat4* a, const orc_mat4* b, const orc_mat4* c, orc_mat4* ret);
+int  orc_inverse(const orc_mat4* a, orc_mat4* ainv);
+void orc_polar_factor(const orc_mat4* a, orc_mat4* u);
+void orc_retract(const orc_mat4* u, const double* eta, orc_mat4* v);
+
+/* ---- gates and circuits (src/gate.c, src/quantum_circuit.c, src/brickwall_circuit.c) ---- */
+void orc_apply_gate(const orc_mat4* g, int i, int j, const orc_sv* psi, orc_sv* out);
+void orc_apply_gate_backward(const orc_mat4* g, int i, int j, const orc_sv* psi,
+                             const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dg);
+int  orc_apply_circuit(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* psi, orc_sv* out);
+int  orc_circuit_forward(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* psi,
+                         orc_sv* cache /* ngates states */, orc_sv* out);
+int  orc_circuit_backward(const orc_mat4* gates, int ngates, const int* wires, const orc_sv* cache,
+                          const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dgates);
+int  orc_circuit_gates_hvp(const orc_mat4* gates, const orc_mat4* gatedirs, int ngates, const int* wires,
+                           const orc_sv* psi, const orc_sv* phi, orc_sv* psi_out,
+                           orc_mat4* dgates, orc_mat4* hess_gatedirs);
+int  orc_apply_brickwall(const orc_mat4* vlist, int nlayers, const int* perms /* [nlayers][L] */,
+                         const orc_sv* psi, orc_sv* out);
+int  orc_brickwall_forward(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* psi,
+                           orc_sv* cache, orc_sv* out);
+int  orc_brickwall_backward(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* cache,
+                            const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dvlist);
+
+/* ---- targets (src/target.c); column range [b_begin, b_end) of the basis-column sum ---- */
+int orc_circuit_target(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates, const int* wires,
+                       int nqubits, long b_begin, long b_end, orc_cplx* fval);
+int orc_circuit_target_and_gradient(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates,
+                                    const int* wires, int nqubits, long b_begin, long b_end,
+                                    orc_cplx* fval, orc_mat4* dgates);
+int orc_circuit_target_hvp(orc_linear_func uf, void* ud, const orc_mat4* gates, const orc_mat4* gatedirs,
+                           int ngates, const int* wires, int nqubits, long b_begin, long b_end,
+                           orc_cplx* fval, orc_mat4* dgates, orc_mat4* hess);
+int orc_circuit_target_projected_gradient(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates,
+                                          const int* wires, int nqubits, orc_cplx* fval, double* grad_vec);
+int orc_circuit_target_projected_hvp(orc_linear_func uf, void* ud, const orc_mat4* gates, const orc_mat4* gatedirs,
+                                     int ngates, const int* wires, int nqubits,
+                                     orc_cplx* fval, double* grad_vec, double* hvp_vec);
+int orc_brickwall_target(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int nqubits,
+                         const int* perms, orc_cplx* fval);
+int orc_brickwall_target_and_gradient(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                      int nqubits, const int* perms, orc_cplx* fval, orc_mat4* dvlist);
+int orc_brickwall_target_projected_gradient(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                            int nqubits, const int* perms, orc_cplx* fval, double* grad_vec);
+int orc_brickwall_target_hvp(orc_linear_func uf, void* ud, const orc_mat4* vlist, const orc_mat4* vdirs,
+                             int nlayers, const int* perms, int nqubits, long b_begin, long b_end,
+                             orc_cplx* fval, orc_mat4* dvlist, orc_mat4* hess_vdirs);
+int orc_brickwall_target_projected_hvp(orc_linear_func uf, void* ud, const orc_mat4* vlist, const orc_mat4* vdirs,
+                                       int nlayers, const int* perms, int nqubits,
+                                       orc_cplx* fval, double* grad_vec, double* hvp_vec);
+
+/* ---- trust region (src/trust_region.c) ---- */
+bool orc_truncated_cg_hvp(const double* x, const double* grad, orc_hvp_func f_hvp, void* fdata, int n,
+                          double radius, const orc_tcg_params* params, double* z);
+void orc_rtr_optimize_hvp(orc_target_func f, orc_target_grad_func f_deriv, orc_hvp_func f_hvp, void* fdata,
+                          orc_retract_func retract, void* rdata, int n, const double* x_init, int m,
+                          const orc_rtr_params* params, int niter, double* f_iter, double* x_final,
+                          int* accepted /* niter entries or NULL */, int* on_boundary /* niter or NULL */);
+void orc_optimize_brickwall_hvp(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int nqubits,
+                                const int* perms, const orc_rtr_params* params, int niter,
+                                double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary);
+void orc_optimize_circuit_hvp(orc_linear_func uf, void* ud, const orc_mat4* gstart, int ngates, int nqubits,
+                              const int* wires, const orc_rtr_params* params, int niter,
+                              double* f_iter, orc_mat4* gopt, int* accepted, int* on_boundary);
+
+/* ---- targets used by tests and benchmarks ---- */
+/* matrix-free brickwall target U: udata points to orc_brickwall_udata */
+typedef struct { const orc_mat4* vlist; int nlayers; const int* perms; } orc_brickwall_udata;
+int orc_brickwall_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out);
+/* the synthetic four-term sparse map of the reference tests (test/test_target.c:16-34) */
+int orc_fixture_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out);
+/* dense row-major N x N target: udata points to the matrix */
+int orc_dense_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out);

@@ -1,0 +1,81 @@
+// Exported configuration and instrumentation entry points (additions; no
+// counterpart in the reference).
+#include "rqc_runtime.h"
+#include "rqcopt_gpu.h"
+
+using namespace rqc;
+
+namespace rqc { int take_last_error(); }
+
+extern "C" {
+
+int rqcopt_gpu_set_precision(int precision)
+{
+	if (precision < RQCOPT_PRECISION_C128 || precision > RQCOPT_PRECISION_C64) return E_ARG;
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	rt->precision = precision;
+	return 0;
+}
+
+int rqcopt_gpu_get_precision(void)
+{
+	Runtime* rt = runtime();
+	return rt ? rt->precision : E_CUDA;
+}
+
+void rqcopt_gpu_set_refine_threshold(double gnorm)
+{
+	if (Runtime* rt = runtime()) rt->refine_threshold = gnorm;
+}
+
+void rqcopt_gpu_set_workspace_limit(size_t bytes)
+{
+	if (Runtime* rt = runtime()) rt->workspace_limit = bytes;
+}
+
+void rqcopt_gpu_set_column_chunk(long columns)
+{
+	if (Runtime* rt = runtime()) rt->column_chunk = columns > 0 ? columns : 0;
+}
+
+int rqcopt_gpu_last_error(void) { return take_last_error(); }
+
+unsigned long long rqcopt_gpu_launch_count(void)
+{
+	Runtime* rt = runtime();
+	return rt ? rt->launches : 0;
+}
+
+void rqcopt_gpu_reset_launch_count(void)
+{
+	if (Runtime* rt = runtime()) rt->launches = 0;
+}
+
+void rqcopt_gpu_enable_kernel_timing(int enable)
+{
+	Runtime* rt = runtime();
+	if (!rt) return;
+	sync(*rt);
+	rt->timing = enable != 0;
+	for (int k = 0; k < KC_COUNT; k++) { rt->time_ms[k] = 0; rt->time_count[k] = 0; }
+}
+
+int rqcopt_gpu_kernel_time(int kernel_class, double* total_ms, long* launches)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	if (kernel_class < 0 || kernel_class >= KC_COUNT) return E_ARG;
+	int ret = sync(*rt);
+	*total_ms = rt->time_ms[kernel_class];
+	*launches = rt->time_count[kernel_class];
+	return ret;
+}
+
+void* rqcopt_gpu_stream(void)
+{
+	Runtime* rt = runtime();
+	return rt ? (void*)rt->stream : nullptr;
+}
+
+}  // extern "C"

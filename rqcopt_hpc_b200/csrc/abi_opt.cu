@@ -1,0 +1,469 @@
+// Truncated CG, Riemannian trust region and the circuit optimisers
+// (src/trust_region.c:14-65, 159-217, 306-368; src/brickwall_opt.c:22-149;
+// src/circuit_opt.c:22-124).
+//
+// The vector algebra and every scalar decision of tCG and of the ratio test run
+// in FP64 on the device, in single-thread kernels whose dot products and axpys
+// use explicitly rounded multiplies and adds in index order (no fused
+// multiply-add), the arithmetic of a sequential BLAS level-1 loop.  The host
+// only reads the resulting status flags to decide whether to launch the next
+// Hessian-vector product.  In the optimisers every evaluation (f, gradient,
+// HVP), the tangent conversion and the polar retraction run on the device as
+// well; the gates cross to the host only as kernel arguments of the passes.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+#include <vector>
+
+#include "engine.h"
+#include "manifold.cuh"
+#include "rqc_runtime.h"
+#include "rqcopt_gpu.h"
+#include "target_problem.h"
+
+using namespace rqc;
+
+namespace {
+
+enum TcgStatus { TCG_CONTINUE = 0, TCG_BOUNDARY = 1, TCG_CONVERGED = 2 };
+
+struct TcgState
+{
+	double rsq, stoptol, radius;
+	int status;
+};
+
+struct RtrState
+{
+	double radius, rho, fx, fnext, maxradius, rho_trust;
+	int accept;
+};
+
+__device__ double dot_seq(int n, const double* a, const double* b)
+{
+	double s = 0;
+	for (int k = 0; k < n; k++) s = __dadd_rn(s, __dmul_rn(a[k], b[k]));
+	return s;
+}
+
+// t > 0 with ||z + t d|| = radius (src/trust_region.c:14-65)
+__device__ double to_boundary(int n, const double* z, const double* d, double radius)
+{
+	const double dsq = dot_seq(n, d, d);
+	if (dsq == 0) return 0;
+	const double p = __ddiv_rn(dot_seq(n, z, d), dsq);
+	const double q = __ddiv_rn(__dsub_rn(dot_seq(n, z, z), __dmul_rn(radius, radius)), dsq);
+	if (p == 0) return sqrt(-q);
+	const double a = -__dadd_rn(p, copysign(1.0, p) * sqrt(__dsub_rn(__dmul_rn(p, p), q)));
+	const double b = __ddiv_rn(q, a);
+	return a <= b ? b : a;
+}
+
+// r = grad, rsq, stop tolerance, z = 0, d = -r (src/trust_region.c:161-175)
+__global__ void k_tcg_init(int n, const double* grad, double* r, double* d, double* z, TcgState* st, double radius,
+                           double abstol, double reltol)
+{
+	if (threadIdx.x | blockIdx.x) return;
+	for (int k = 0; k < n; k++) { r[k] = grad[k]; z[k] = 0; d[k] = -grad[k]; }
+	st->rsq = dot_seq(n, r, r);
+	st->stoptol = fmax(abstol, reltol * sqrt(st->rsq));
+	st->radius = radius;
+	st->status = TCG_CONTINUE;
+}
+
+// One tCG step after Hd = H d (src/trust_region.c:181-209)
+__global__ void k_tcg_step(int n, double* d, const double* hd, double* z, double* r, TcgState* st)
+{
+	if (threadIdx.x | blockIdx.x) return;
+	const double dhd = dot_seq(n, d, hd);
+	const double t = to_boundary(n, z, d, st->radius);
+	const double alpha = __ddiv_rn(st->rsq, dhd);
+	if (dhd <= 0 || alpha > t) {
+		for (int k = 0; k < n; k++) z[k] = __dadd_rn(z[k], __dmul_rn(t, d[k]));
+		st->status = TCG_BOUNDARY;
+		return;
+	}
+	for (int k = 0; k < n; k++) r[k] = __dadd_rn(r[k], __dmul_rn(alpha, hd[k]));
+	for (int k = 0; k < n; k++) z[k] = __dadd_rn(z[k], __dmul_rn(alpha, d[k]));
+	const double rsq_next = dot_seq(n, r, r);
+	if (sqrt(rsq_next) <= st->stoptol) {
+		st->status = TCG_CONVERGED;
+		return;
+	}
+	const double beta = __ddiv_rn(rsq_next, st->rsq);
+	for (int k = 0; k < n; k++) d[k] = __dadd_rn(__dmul_rn(beta, d[k]), -r[k]);
+	st->rsq = rsq_next;
+	st->status = TCG_CONTINUE;
+}
+
+// Ratio test and radius update (src/trust_region.c:336-352); fx / fnext read from
+// the given device doubles unless null.
+__global__ void k_rtr_rho(int n, const double* grad, const double* eta, const double* heta, const double* fx_dev,
+                          const double* fnext_dev, RtrState* st, int on_boundary)
+{
+	if (threadIdx.x | blockIdx.x) return;
+	if (fx_dev) st->fx = *fx_dev;
+	if (fnext_dev) st->fnext = *fnext_dev;
+	const double den = __dadd_rn(dot_seq(n, grad, eta), __dmul_rn(0.5, dot_seq(n, eta, heta)));
+	const double rho = __ddiv_rn(__dsub_rn(st->fnext, st->fx), den);
+	if (rho < 0.25) st->radius = __dmul_rn(st->radius, 0.25);
+	else if (rho > 0.75 && on_boundary) st->radius = fmin(2 * st->radius, st->maxradius);
+	st->rho = rho;
+	st->accept = rho > st->rho_trust;
+}
+
+// Z_u = V_u A(vec_u) for every unit (src/matrix.c:309-314)
+__global__ void k_real_to_tangent(int nunits, const double* vec, const double2* x, double2* dirs)
+{
+	const int u = blockIdx.x * blockDim.x + threadIdx.x;
+	if (u >= nunits) return;
+	M4 v, z;
+	for (int e = 0; e < 16; e++) v.a[e] = x[16 * u + e];
+	m4_real_to_tangent(vec + 16 * u, v, z);
+	for (int e = 0; e < 16; e++) dirs[16 * u + e] = z.a[e];
+}
+
+// polar retraction of every unit (src/matrix.c:517-531)
+__global__ void k_retract(int nunits, const double2* x, const double* eta, double2* xs)
+{
+	const int u = blockIdx.x * blockDim.x + threadIdx.x;
+	if (u >= nunits) return;
+	M4 v, w;
+	for (int e = 0; e < 16; e++) v.a[e] = x[16 * u + e];
+	m4_retract(v, eta + 16 * u, w);
+	for (int e = 0; e < 16; e++) xs[16 * u + e] = w.a[e];
+}
+
+int launched(Runtime& rt)
+{
+	rt.launches++;
+	return RQC_CUDA(cudaGetLastError());
+}
+
+template <typename S>
+int read_state(Runtime& rt, const S* d, S* h)
+{
+	int ret = RQC_CUDA(cudaMemcpyAsync(h, d, sizeof(S), cudaMemcpyDeviceToHost, rt.stream));
+	return ret ? ret : sync(rt);
+}
+
+// ----------------------------------------------------------------------------- generic API
+
+struct DevVecs
+{
+	double *r, *d, *hd, *z, *grad, *eta, *heta;
+	TcgState* tcg;
+	RtrState* rtr;
+};
+
+int alloc_vecs(Runtime& rt, int n, DevVecs& v, Buffer& buf)
+{
+	const size_t bytes = 7 * (size_t)n * sizeof(double) + 256 + sizeof(TcgState) + sizeof(RtrState);
+	int ret = ensure_device(buf, bytes);
+	if (ret) return ret;
+	double* p = reinterpret_cast<double*>(buf.ptr);
+	v.r = p; v.d = p + n; v.hd = p + 2 * n; v.z = p + 3 * n; v.grad = p + 4 * n; v.eta = p + 5 * n; v.heta = p + 6 * n;
+	char* s = reinterpret_cast<char*>(p + 7 * n);
+	s = reinterpret_cast<char*>(((uintptr_t)s + 127) & ~(uintptr_t)127);
+	v.tcg = reinterpret_cast<TcgState*>(s);
+	v.rtr = reinterpret_cast<RtrState*>(s + 128);
+	return OK;
+}
+
+// tCG with a host callback; grad already in v.grad; solution in v.z; returns <0 on error
+int tcg_host_callback(Runtime& rt, const double* x, hessian_vector_product_func f_hvp, void* fdata, int n, double radius,
+                      const struct truncated_cg_params* params, DevVecs& v, std::vector<double>& hbuf, bool* on_boundary)
+{
+	k_tcg_init<<<1, 1, 0, rt.stream>>>(n, v.grad, v.r, v.d, v.z, v.tcg, radius, params->abstol, params->reltol);
+	int ret = launched(rt);
+	*on_boundary = false;
+	hbuf.resize(2 * (size_t)n);
+	for (int it = 0; it < params->maxiter && !ret; it++) {
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(hbuf.data(), v.d, n * sizeof(double), cudaMemcpyDeviceToHost, rt.stream)))) break;
+		if ((ret = sync(rt))) break;
+		f_hvp(x, fdata, hbuf.data(), hbuf.data() + n);
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.hd, hbuf.data() + n, n * sizeof(double), cudaMemcpyHostToDevice, rt.stream)))) break;
+		k_tcg_step<<<1, 1, 0, rt.stream>>>(n, v.d, v.hd, v.z, v.r, v.tcg);
+		if ((ret = launched(rt))) break;
+		TcgState st;
+		if ((ret = read_state(rt, v.tcg, &st))) break;
+		if (st.status == TCG_BOUNDARY) { *on_boundary = true; break; }
+		if (st.status == TCG_CONVERGED) break;
+	}
+	return ret;
+}
+
+}  // namespace
+
+extern "C" bool truncated_cg_hvp(const double* x, const double* grad, const hessian_vector_product_func f_hvp, void* fdata,
+                                 const int n, const double radius, const struct truncated_cg_params* params, double* z)
+{
+	Runtime* rt = runtime();
+	if (!rt || n < 1) {
+		set_last_error(rt ? E_ARG : E_CUDA);
+		return false;
+	}
+	DevVecs v;
+	int ret = alloc_vecs(*rt, n, v, rt->opt);
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(v.grad, grad, n * sizeof(double), cudaMemcpyHostToDevice, rt->stream));
+	std::vector<double> hbuf;
+	bool boundary = false;
+	if (!ret) ret = tcg_host_callback(*rt, x, f_hvp, fdata, n, radius, params, v, hbuf, &boundary);
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(z, v.z, n * sizeof(double), cudaMemcpyDeviceToHost, rt->stream));
+	if (!ret) ret = sync(*rt);
+	if (ret) set_last_error(ret);
+	return boundary;
+}
+
+extern "C" void riemannian_trust_region_optimize_hvp(const target_func f, const target_gradient_func f_deriv,
+                                                     const hessian_vector_product_func f_hvp, void* fdata,
+                                                     retract_func retract_fn, void* rdata, const int n,
+                                                     const double* x_init, const int m, const struct rtr_params* params,
+                                                     const int niter, double* f_iter, double* x_final)
+{
+	Runtime* rt = runtime();
+	if (!rt || n < 1 || m < 1 || !(params->rho_trust >= 0 && params->rho_trust < 0.25)) {
+		fail_arg("riemannian_trust_region_optimize_hvp", "invalid arguments");
+		return;
+	}
+	DevVecs v;
+	int ret = alloc_vecs(*rt, n, v, rt->opt);
+	std::vector<double> x(x_init, x_init + m), xn(m), hgrad(n), heta(n), hheta(n), hbuf;
+	RtrState rs = {};
+	rs.radius = params->radius_init;
+	rs.maxradius = params->maxradius;
+	rs.rho_trust = params->rho_trust;
+	if (params->g_func) params->g_iter[0] = params->g_func(x.data(), params->g_data);
+	for (int k = 0; k < niter && !ret; k++) {
+		const double fx = f_deriv(x.data(), fdata, hgrad.data());
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.grad, hgrad.data(), n * sizeof(double), cudaMemcpyHostToDevice, rt->stream)))) break;
+		bool boundary = false;
+		if ((ret = tcg_host_callback(*rt, x.data(), f_hvp, fdata, n, rs.radius, &params->tcg_params, v, hbuf, &boundary))) break;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(heta.data(), v.z, n * sizeof(double), cudaMemcpyDeviceToHost, rt->stream)))) break;
+		if ((ret = sync(*rt))) break;
+		retract_fn(x.data(), heta.data(), rdata, xn.data());
+		f_iter[k] = fx;
+		f_hvp(x.data(), fdata, heta.data(), hheta.data());
+		rs.fx = fx;
+		rs.fnext = f(xn.data(), fdata);
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.heta, hheta.data(), n * sizeof(double), cudaMemcpyHostToDevice, rt->stream)))) break;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.rtr, &rs, sizeof(rs), cudaMemcpyHostToDevice, rt->stream)))) break;
+		k_rtr_rho<<<1, 1, 0, rt->stream>>>(n, v.grad, v.z, v.heta, nullptr, nullptr, v.rtr, boundary ? 1 : 0);
+		if ((ret = launched(*rt))) break;
+		if ((ret = read_state(*rt, v.rtr, &rs))) break;
+		if (rs.accept) x.swap(xn);
+		if (params->g_func) params->g_iter[k + 1] = params->g_func(x.data(), params->g_data);
+	}
+	if (ret) {
+		set_last_error(ret);
+		return;
+	}
+	memcpy(x_final, x.data(), m * sizeof(double));
+	f_iter[niter] = f(x_final, fdata);
+}
+
+// ----------------------------------------------------------------------------- device-resident optimiser
+
+namespace rqc {
+
+// Optimisation of a brickwall or general circuit with all vectors on the device.
+struct DeviceOptimizer
+{
+	Runtime& rt;
+	Problem& pb;
+	const TargetHolder& th;
+	int n;
+	DevVecs v;
+	double2 *x, *xn, *dirs, *res, *ug;
+	double* scratch;   // projected-gradient output of HVP evaluations
+	std::vector<double2> hx;
+	int hvp_prec;
+	long evals_hvp = 0, evals_grad = 0, evals_f = 0;
+
+	DeviceOptimizer(Runtime& r, Problem& p, const TargetHolder& t) : rt(r), pb(p), th(t), n(16 * p.nunits) {}
+
+	int init(const double2* x0)
+	{
+		const size_t nu = pb.nunits;
+		const size_t nres = result_count(pb.G);
+		const size_t bytes = 7 * (size_t)n * sizeof(double) + 512 + (4 * 16 * nu + nres) * sizeof(double2) + (n + 8) * sizeof(double);
+		int ret = ensure_device(rt.opt, bytes);
+		if (ret) return ret;
+		if ((ret = alloc_vecs(rt, n, v, rt.opt))) return ret;
+		char* base = reinterpret_cast<char*>(rt.opt.ptr) + 7 * (size_t)n * sizeof(double) + 512;
+		x = reinterpret_cast<double2*>(base);
+		xn = x + 16 * nu;
+		dirs = xn + 16 * nu;
+		ug = dirs + 16 * nu;
+		res = ug + 16 * nu;
+		scratch = reinterpret_cast<double*>(res + nres);
+		hx.assign(x0, x0 + 16 * nu);
+		return RQC_CUDA(cudaMemcpyAsync(x, x0, 16 * nu * sizeof(double2), cudaMemcpyHostToDevice, rt.stream));
+	}
+
+	// gates of the device array `src` become the kernel arguments of the next passes
+	int load_gates(const double2* src)
+	{
+		int ret = RQC_CUDA(cudaMemcpyAsync(hx.data(), src, hx.size() * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream));
+		if (!ret) ret = sync(rt);
+		if (!ret) pb.set_gates_from_units(hx.data());
+		if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(ug, src, hx.size() * sizeof(double2), cudaMemcpyDeviceToDevice, rt.stream));
+		return ret;
+	}
+
+	CircuitSpec spec(bool with_dirs) const
+	{
+		CircuitSpec cs;
+		cs.L = pb.L;
+		cs.ngates = pb.G;
+		cs.gates = pb.gates.data();
+		cs.dirs = with_dirs ? pb.dirs.data() : nullptr;
+		cs.wires = pb.wires.data();
+		return cs;
+	}
+
+	// f at the loaded gates -> res[0]
+	int eval_f(int prec)
+	{
+		evals_f++;
+		return evaluate(rt, spec(false), th.spec, EVAL_F, prec, res);
+	}
+
+	// f and projected gradient at the loaded gates -> res[0], v.grad
+	int eval_grad(int prec)
+	{
+		evals_grad++;
+		int ret = evaluate(rt, spec(false), th.spec, EVAL_GRAD, prec, res);
+		if (!ret) ret = post_launch(rt, res, pb, ug, nullptr, 0, nullptr, nullptr, v.grad, nullptr);
+		return ret;
+	}
+
+	// projected HVP at the loaded gates in direction vec (device, 16 per unit) -> out
+	int eval_hvp(const double* vec, double* out, int prec)
+	{
+		evals_hvp++;
+		const int threads = 64, blocks = (pb.nunits + threads - 1) / threads;
+		k_real_to_tangent<<<blocks, threads, 0, rt.stream>>>(pb.nunits, vec, ug, dirs);
+		int ret = launched(rt);
+		std::vector<double2> hd(16 * (size_t)pb.nunits);
+		if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(hd.data(), dirs, hd.size() * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream));
+		if (!ret) ret = sync(rt);
+		if (ret) return ret;
+		pb.set_dirs_from_units(hd.data());
+		if ((ret = evaluate(rt, spec(true), th.spec, EVAL_HVP, prec, res))) return ret;
+		return post_launch(rt, res, pb, ug, dirs, 1, nullptr, nullptr, scratch, out);
+	}
+
+	int run(const struct rtr_params* params, int niter, double* f_iter, double2* x_final, int precision)
+	{
+		RtrState rs = {};
+		rs.radius = params->radius_init;
+		rs.maxradius = params->maxradius;
+		rs.rho_trust = params->rho_trust;
+		int ret = RQC_CUDA(cudaMemcpyAsync(v.rtr, &rs, sizeof(rs), cudaMemcpyHostToDevice, rt.stream));
+		// precision policy: f and gradient (the ratio test) in complex128 unless plain
+		// complex64 was asked for; HVPs in complex64 until the gradient norm falls
+		// below the refinement threshold (mixed mode)
+		const int fprec = precision == PREC_C64 ? PREC_C64 : PREC_C128;
+		hvp_prec = precision == PREC_C128 ? PREC_C128 : PREC_C64;
+		double* fx_slot = scratch + n;
+		const int threads = 64, blocks = (pb.nunits + threads - 1) / threads;
+		for (int k = 0; k < niter && !ret; k++) {
+			// f and gradient at x (src/trust_region.c:328)
+			if ((ret = load_gates(x))) break;
+			if ((ret = eval_grad(fprec))) break;
+			if ((ret = RQC_CUDA(cudaMemcpyAsync(fx_slot, res, sizeof(double), cudaMemcpyDeviceToDevice, rt.stream)))) break;
+			if ((ret = RQC_CUDA(cudaMemcpyAsync(&rs, v.rtr, sizeof(rs), cudaMemcpyDeviceToHost, rt.stream)))) break;
+			if ((ret = sync(rt))) break;
+			// tCG (src/trust_region.c:159-217)
+			k_tcg_init<<<1, 1, 0, rt.stream>>>(n, v.grad, v.r, v.d, v.z, v.tcg, rs.radius, params->tcg_params.abstol,
+			                                   params->tcg_params.reltol);
+			if ((ret = launched(rt))) break;
+			TcgState st;
+			if ((ret = read_state(rt, v.tcg, &st))) break;
+			if (precision == PREC_MIXED && hvp_prec != PREC_C128 && sqrt(st.rsq) < rt.refine_threshold) hvp_prec = PREC_C128;
+			bool boundary = false;
+			for (int it = 0; it < params->tcg_params.maxiter; it++) {
+				if ((ret = eval_hvp(v.d, v.hd, hvp_prec))) break;
+				k_tcg_step<<<1, 1, 0, rt.stream>>>(n, v.d, v.hd, v.z, v.r, v.tcg);
+				if ((ret = launched(rt))) break;
+				if ((ret = read_state(rt, v.tcg, &st))) break;
+				if (st.status == TCG_BOUNDARY) { boundary = true; break; }
+				if (st.status == TCG_CONVERGED) break;
+			}
+			if (ret) break;
+			// candidate point, model decrease and ratio test (src/trust_region.c:330-352)
+			k_retract<<<blocks, threads, 0, rt.stream>>>(pb.nunits, x, v.z, xn);
+			if ((ret = launched(rt))) break;
+			if ((ret = eval_hvp(v.z, v.heta, hvp_prec))) break;
+			if ((ret = load_gates(xn))) break;
+			if ((ret = eval_f(fprec))) break;
+			k_rtr_rho<<<1, 1, 0, rt.stream>>>(n, v.grad, v.z, v.heta, fx_slot, reinterpret_cast<const double*>(res), v.rtr,
+			                                   boundary ? 1 : 0);
+			if ((ret = launched(rt))) break;
+			if ((ret = read_state(rt, v.rtr, &rs))) break;
+			f_iter[k] = rs.fx;
+			if (rs.accept) std::swap(x, xn);
+		}
+		if (ret) return ret;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(x_final, x, hx.size() * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
+		if ((ret = load_gates(x))) return ret;
+		if ((ret = eval_f(fprec))) return ret;
+		double2 ff;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(&ff, res, sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
+		if ((ret = sync(rt))) return ret;
+		f_iter[niter] = ff.x;
+		return OK;
+	}
+};
+
+}  // namespace rqc
+
+namespace {
+
+void run_optimizer(const char* fn, Problem& pb, linear_func ufunc, void* udata, struct rtr_params* params, int niter,
+                   double* f_iter, const struct mat4x4* start, struct mat4x4* out)
+{
+	TargetHolder th;
+	if (!th.set(ufunc, udata, pb.L)) {
+		fail_arg(fn, "invalid target");
+		return;
+	}
+	Runtime* rt = runtime();
+	if (!rt) { set_last_error(E_CUDA); return; }
+	// the drivers disable the per-iteration callback (src/brickwall_opt.c:141-143)
+	params->g_func = NULL;
+	params->g_data = NULL;
+	params->g_iter = NULL;
+	DeviceOptimizer opt(*rt, pb, th);
+	int ret = opt.init(reinterpret_cast<const double2*>(start));
+	if (!ret) ret = opt.run(params, niter, f_iter, reinterpret_cast<double2*>(out), rt->precision);
+	if (ret) set_last_error(ret);
+}
+
+}  // namespace
+
+extern "C" void optimize_brickwall_circuit_hvp(linear_func ufunc, void* udata, const struct mat4x4 vlist_start[],
+                                               const int nlayers, const int nqubits, const int* perms[],
+                                               struct rtr_params* params, const int niter, double* f_iter,
+                                               struct mat4x4 vlist_opt[])
+{
+	Problem pb;
+	if (!pb.set_brickwall(nqubits, nlayers, vlist_start, nullptr, perms)) {
+		fail_arg("optimize_brickwall_circuit_hvp", "invalid arguments");
+		return;
+	}
+	run_optimizer("optimize_brickwall_circuit_hvp", pb, ufunc, udata, params, niter, f_iter, vlist_start, vlist_opt);
+}
+
+extern "C" void optimize_quantum_circuit(linear_func ufunc, void* udata, const struct mat4x4 gates_start[],
+                                         const int ngates, const int nqubits, const int wires[], struct rtr_params* params,
+                                         const int niter, double* f_iter, struct mat4x4 gates_opt[])
+{
+	Problem pb;
+	if (!pb.set_circuit(nqubits, ngates, gates_start, nullptr, wires)) {
+		fail_arg("optimize_quantum_circuit", "invalid arguments");
+		return;
+	}
+	run_optimizer("optimize_quantum_circuit", pb, ufunc, udata, params, niter, f_iter, gates_start, gates_opt);
+}

@@ -1,0 +1,92 @@
+// Per-device runtime state of the library: the stream every call issues its
+// work on, device workspaces that grow on demand and are reused across calls,
+// staging of host buffers, error reporting, launch counting and per-kernel
+// event timing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+#include <vector>
+
+namespace rqc {
+
+enum ErrorCode { OK = 0, E_ALLOC = -1, E_UFUNC = -2, E_PASS = -3, E_PASS2 = -4, E_CUDA = -5, E_ARG = -6 };
+
+enum KernelClass { KC_APPLY = 0, KC_FORWARD = 1, KC_REVERSE = 2, KC_FUSED = 3, KC_COUNT = 4 };
+
+struct Buffer
+{
+	void* ptr = nullptr;
+	size_t bytes = 0;
+};
+
+struct Runtime
+{
+	int device = -1;
+	int num_sms = 0;
+	cudaStream_t stream = nullptr;
+
+	// device buffers, grown on demand
+	Buffer work;          // evaluation-engine column chunks and caches
+	Buffer partials;      // per-block partial sums
+	Buffer small;         // inputs of the exported calls (gates, directions)
+	Buffer result;        // reduction results of the engine and single-gate passes
+	Buffer opt;           // optimiser vectors
+	Buffer stage[4];      // staging of host statevectors
+	Buffer hpin;          // pinned host scratch
+
+	// configuration
+	int precision = 0;
+	double refine_threshold = 1e-5;
+	size_t workspace_limit = 0;
+	long column_chunk = 0;
+
+	// instrumentation
+	unsigned long long launches = 0;
+	bool timing = false;
+	double time_ms[KC_COUNT] = {0, 0, 0, 0};
+	long time_count[KC_COUNT] = {0, 0, 0, 0};
+	std::vector<cudaEvent_t> event_pool;
+	struct Pending { cudaEvent_t a, b; int cls; };
+	std::vector<Pending> pending;
+};
+
+// runtime of the current device; initialises it on first use (nullptr if no usable GPU)
+Runtime* runtime();
+
+// report a CUDA error (prints to stderr); returns E_CUDA if e != cudaSuccess
+int cuda_check(cudaError_t e, const char* what, const char* file, int line);
+#define RQC_CUDA(call) ::rqc::cuda_check((call), #call, __FILE__, __LINE__)
+
+// record an error of a void entry point (readable through rqcopt_gpu_last_error)
+void set_last_error(int code);
+void fail_arg(const char* fn, const char* msg);
+
+// ensure a buffer holds at least `bytes` (device or pinned host); returns 0 or E_ALLOC
+int ensure_device(Buffer& b, size_t bytes);
+int ensure_host_pinned(Buffer& b, size_t bytes);
+
+// true if the pointer is device-accessible memory of this context (device or managed)
+bool is_device_pointer(const void* p);
+
+// A statevector-sized span on the device: either the caller's pointer (device or
+// managed memory) or a staging buffer filled from / written back to host memory.
+struct DeviceSpan
+{
+	void* dev = nullptr;
+	void* host = nullptr;   // non-null if staged
+	size_t bytes = 0;
+};
+int span_in(Runtime& rt, const void* p, size_t bytes, int slot, DeviceSpan& s);
+int span_out(Runtime& rt, void* p, size_t bytes, int slot, DeviceSpan& s);
+int span_finish(Runtime& rt, DeviceSpan& s);   // copy back if staged (async on rt.stream)
+
+// synchronise the stream and fold pending kernel timings; returns 0 or E_CUDA
+int sync(Runtime& rt);
+
+// kernel launch bookkeeping
+void launch_begin(Runtime& rt, int cls, cudaEvent_t* ev_start);
+void launch_end(Runtime& rt, int cls, cudaEvent_t ev_start);
+
+}  // namespace rqc

@@ -1,0 +1,515 @@
+"""Python host mirror of the rqcopt_hpc interface, calling librqcopt_gpu.so through its C ABI.
+
+Function names, argument meaning and error behaviour follow the reference's C
+functions (src/gate.h, src/quantum_circuit.h, src/brickwall_circuit.h,
+src/target.h, src/trust_region.h, src/brickwall_opt.h, src/circuit_opt.h):
+statevectors and gates are numpy complex128 arrays, perms an (nlayers, L)
+integer array, and integer error codes are raised as ``RqcError``.  Arrays
+passed in live in host memory, so every call exercises the staging path of the
+C ABI; torch CUDA tensors may be passed where a statevector is expected to
+keep data on the device.
+
+Loading fails loudly (``OSError``) when the compiled library is missing: there
+is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .abi import (HVP_FUNC, LINEAR_FUNC, RETRACT_FUNC, TARGET_FUNC, TARGET_GRAD_FUNC, BrickwallTarget,
+                  CircuitTarget, QuantumCircuitCache, RTRParams, Statevector, TruncatedCGParams, cplx,
+                  default_rtr_params, default_tcg_params, ints, perm_pointers, ptr, wrap_ufunc)
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librqcopt_gpu.so")
+
+_lib = None
+
+VP = C.c_void_p
+I = C.c_int
+D = C.c_double
+PSV = C.POINTER(Statevector)
+PD = C.POINTER(C.c_double)
+
+
+class RqcError(RuntimeError):
+    def __init__(self, fn, code):
+        super().__init__(f"{fn} failed with code {code}")
+        self.code = code
+
+
+_SIGS = {
+    "allocate_statevector": (I, [I, PSV]),
+    "free_statevector": (None, [PSV]),
+    "add_statevectors": (None, [PSV, PSV, PSV]),
+    "apply_gate": (None, [VP, I, I, PSV, PSV]),
+    "apply_gate_backward": (None, [VP, I, I, PSV, PSV, PSV, VP]),
+    "apply_quantum_circuit": (I, [VP, I, VP, PSV, PSV]),
+    "allocate_quantum_circuit_cache": (I, [I, I, C.POINTER(QuantumCircuitCache)]),
+    "free_quantum_circuit_cache": (None, [C.POINTER(QuantumCircuitCache)]),
+    "quantum_circuit_forward": (I, [VP, I, VP, PSV, C.POINTER(QuantumCircuitCache), PSV]),
+    "quantum_circuit_backward": (I, [VP, I, VP, C.POINTER(QuantumCircuitCache), PSV, PSV, VP]),
+    "quantum_circuit_gates_hessian_vector_product": (I, [VP, VP, I, VP, PSV, PSV, PSV, VP, VP]),
+    "apply_brickwall_unitary": (I, [VP, I, VP, PSV, PSV]),
+    "brickwall_unitary_forward": (I, [VP, I, VP, PSV, C.POINTER(QuantumCircuitCache), PSV]),
+    "brickwall_unitary_backward": (I, [VP, I, VP, C.POINTER(QuantumCircuitCache), PSV, PSV, VP]),
+    "circuit_unitary_target": (I, [VP, VP, VP, I, VP, I, VP]),
+    "circuit_unitary_target_and_gradient": (I, [VP, VP, VP, I, VP, I, VP, VP]),
+    "circuit_unitary_target_and_projected_gradient": (I, [VP, VP, VP, I, VP, I, VP, VP]),
+    "circuit_unitary_target_hessian_vector_product": (I, [VP, VP, VP, VP, I, VP, I, VP, VP, VP]),
+    "circuit_unitary_target_projected_hessian_vector_product": (I, [VP, VP, VP, VP, I, VP, I, VP, VP, VP]),
+    "brickwall_unitary_target": (I, [VP, VP, VP, I, I, VP, VP]),
+    "brickwall_unitary_target_and_gradient": (I, [VP, VP, VP, I, I, VP, VP, VP]),
+    "brickwall_unitary_target_and_projected_gradient": (I, [VP, VP, VP, I, I, VP, VP, VP]),
+    "brickwall_unitary_target_hessian_vector_product": (I, [VP, VP, VP, VP, I, VP, I, VP, VP, VP]),
+    "brickwall_unitary_target_projected_hessian_vector_product": (I, [VP, VP, VP, VP, I, VP, I, VP, VP, VP]),
+    "truncated_cg_hvp": (C.c_bool, [VP, VP, VP, VP, I, D, C.POINTER(TruncatedCGParams), VP]),
+    "riemannian_trust_region_optimize_hvp": (None, [VP, VP, VP, VP, VP, VP, I, VP, I, C.POINTER(RTRParams), I, VP, VP]),
+    "optimize_brickwall_circuit_hvp": (None, [VP, VP, VP, I, I, VP, C.POINTER(RTRParams), I, VP, VP]),
+    "optimize_quantum_circuit": (None, [VP, VP, VP, I, I, VP, C.POINTER(RTRParams), I, VP, VP]),
+    "real_to_tangent": (None, [VP, VP, VP]),
+    "tangent_to_real": (None, [VP, VP, VP]),
+    "project_tangent": (None, [VP, VP, VP]),
+    "polar_factor": (None, [VP, VP]),
+    "retract": (None, [VP, VP, VP]),
+    "multiply_matrices": (None, [VP, VP, VP]),
+    "inverse_matrix": (I, [VP, VP]),
+    "symmetric_triple_matrix_product": (None, [VP, VP, VP, VP]),
+    "rqcopt_brickwall_ufunc": (I, [PSV, VP, PSV]),
+    "rqcopt_circuit_ufunc": (I, [PSV, VP, PSV]),
+    "rqcopt_gpu_set_precision": (I, [I]),
+    "rqcopt_gpu_get_precision": (I, []),
+    "rqcopt_gpu_set_refine_threshold": (None, [D]),
+    "rqcopt_gpu_set_workspace_limit": (None, [C.c_size_t]),
+    "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
+    "rqcopt_gpu_last_error": (I, []),
+    "rqcopt_gpu_launch_count": (C.c_ulonglong, []),
+    "rqcopt_gpu_reset_launch_count": (None, []),
+    "rqcopt_gpu_enable_kernel_timing": (None, [I]),
+    "rqcopt_gpu_kernel_time": (I, [I, PD, C.POINTER(C.c_long)]),
+    "rqcopt_gpu_stream": (VP, []),
+}
+
+PRECISION_C128, PRECISION_MIXED, PRECISION_C64 = 0, 1, 2
+KC_APPLY, KC_FORWARD, KC_REVERSE, KC_FUSED = 0, 1, 2, 3
+
+
+def lib():
+    """The loaded C library (raises OSError if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} not found: build it with `python -m rqcopt_hpc_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(fn, ret):
+    if ret != 0:
+        raise RqcError(fn, ret)
+
+
+def _check_void(fn):
+    err = lib().rqcopt_gpu_last_error()
+    if err != 0:
+        raise RqcError(fn, err)
+
+
+def _sv(a, L):
+    """Statevector over a numpy complex128 array or a CUDA tensor (device pointer)."""
+    if hasattr(a, "data_ptr"):
+        return Statevector(a.data_ptr(), L)
+    return Statevector(a.ctypes.data, L)
+
+
+def _nq(psi):
+    n = psi.shape[0] if hasattr(psi, "shape") else len(psi)
+    L = int(n).bit_length() - 1
+    assert 1 << L == n, "statevector length must be a power of two"
+    return L
+
+
+# ------------------------------------------------------------------------ gates and circuits
+
+def apply_gate(V, i, j, psi):
+    psi = cplx(psi)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    V = cplx(V)
+    lib().apply_gate(ptr(V), i, j, C.byref(_sv(psi, L)), C.byref(_sv(out, L)))
+    _check_void("apply_gate")
+    return out
+
+
+def apply_gate_backward(V, i, j, psi, dpsi_out):
+    psi, dpsi_out, V = cplx(psi), cplx(dpsi_out), cplx(V)
+    L = _nq(psi)
+    dpsi = np.empty_like(psi)
+    dV = np.empty((4, 4), np.complex128)
+    lib().apply_gate_backward(ptr(V), i, j, C.byref(_sv(psi, L)), C.byref(_sv(dpsi_out, L)), C.byref(_sv(dpsi, L)), ptr(dV))
+    _check_void("apply_gate_backward")
+    return dpsi, dV
+
+
+def apply_quantum_circuit(gates, wires, psi):
+    gates, wires, psi = cplx(gates), ints(wires), cplx(psi)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    _check("apply_quantum_circuit", lib().apply_quantum_circuit(ptr(gates), gates.shape[0], ptr(wires),
+                                                               C.byref(_sv(psi, L)), C.byref(_sv(out, L))))
+    return out
+
+
+class Cache:
+    """quantum_circuit_cache allocated through the library (managed memory states)."""
+
+    def __init__(self, nqubits, ngates):
+        self.c = QuantumCircuitCache()
+        _check("allocate_quantum_circuit_cache", lib().allocate_quantum_circuit_cache(nqubits, ngates, C.byref(self.c)))
+
+    def state(self, k):
+        s = self.c.psi_list[k]
+        n = 1 << s.nqubits
+        return np.ctypeslib.as_array(C.cast(s.data, C.POINTER(C.c_double)), shape=(2 * n,)).view(np.complex128).copy()
+
+    def __del__(self):
+        if _lib is not None and self.c.psi_list:
+            _lib.free_quantum_circuit_cache(C.byref(self.c))
+
+
+def quantum_circuit_forward(gates, wires, psi, cache=None):
+    gates, wires, psi = cplx(gates), ints(wires), cplx(psi)
+    L = _nq(psi)
+    cache = cache or Cache(L, gates.shape[0])
+    out = np.empty_like(psi)
+    _check("quantum_circuit_forward", lib().quantum_circuit_forward(ptr(gates), gates.shape[0], ptr(wires),
+                                                                   C.byref(_sv(psi, L)), C.byref(cache.c),
+                                                                   C.byref(_sv(out, L))))
+    return out, cache
+
+
+def quantum_circuit_backward(gates, wires, cache, dpsi_out):
+    gates, wires, dpsi_out = cplx(gates), ints(wires), cplx(dpsi_out)
+    L = _nq(dpsi_out)
+    dpsi = np.empty_like(dpsi_out)
+    dgates = np.empty((gates.shape[0], 4, 4), np.complex128)
+    _check("quantum_circuit_backward", lib().quantum_circuit_backward(ptr(gates), gates.shape[0], ptr(wires),
+                                                                     C.byref(cache.c), C.byref(_sv(dpsi_out, L)),
+                                                                     C.byref(_sv(dpsi, L)), ptr(dgates)))
+    return dpsi, dgates
+
+
+def quantum_circuit_gates_hessian_vector_product(gates, gatedirs, wires, psi, phi):
+    gates, gatedirs, wires, psi, phi = cplx(gates), cplx(gatedirs), ints(wires), cplx(psi), cplx(phi)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+    hg = np.empty_like(dg)
+    _check("quantum_circuit_gates_hessian_vector_product",
+           lib().quantum_circuit_gates_hessian_vector_product(ptr(gates), ptr(gatedirs), gates.shape[0], ptr(wires),
+                                                              C.byref(_sv(psi, L)), C.byref(_sv(phi, L)),
+                                                              C.byref(_sv(out, L)), ptr(dg), ptr(hg)))
+    return out, dg, hg
+
+
+def apply_brickwall_unitary(vlist, perms, psi):
+    vlist, psi = cplx(vlist), cplx(psi)
+    L = _nq(psi)
+    pp, keep = perm_pointers(perms)
+    out = np.empty_like(psi)
+    _check("apply_brickwall_unitary", lib().apply_brickwall_unitary(ptr(vlist), vlist.shape[0], C.cast(pp, VP),
+                                                                   C.byref(_sv(psi, L)), C.byref(_sv(out, L))))
+    return out
+
+
+def brickwall_unitary_forward(vlist, perms, psi):
+    vlist, psi = cplx(vlist), cplx(psi)
+    L = _nq(psi)
+    pp, keep = perm_pointers(perms)
+    cache = Cache(L, vlist.shape[0] * (L // 2))
+    out = np.empty_like(psi)
+    _check("brickwall_unitary_forward", lib().brickwall_unitary_forward(ptr(vlist), vlist.shape[0], C.cast(pp, VP),
+                                                                       C.byref(_sv(psi, L)), C.byref(cache.c),
+                                                                       C.byref(_sv(out, L))))
+    return out, cache
+
+
+def brickwall_unitary_backward(vlist, perms, cache, dpsi_out):
+    vlist, dpsi_out = cplx(vlist), cplx(dpsi_out)
+    L = _nq(dpsi_out)
+    pp, keep = perm_pointers(perms)
+    dpsi = np.empty_like(dpsi_out)
+    dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+    _check("brickwall_unitary_backward", lib().brickwall_unitary_backward(ptr(vlist), vlist.shape[0], C.cast(pp, VP),
+                                                                         C.byref(cache.c), C.byref(_sv(dpsi_out, L)),
+                                                                         C.byref(_sv(dpsi, L)), ptr(dv)))
+    return dpsi, dv
+
+
+# ------------------------------------------------------------------------ targets
+
+class Target:
+    """A target U for the basis-column sums: a Python callable (host callback, one
+    call per column), or a device-native brickwall / circuit target."""
+
+    def __init__(self, fn=None, brickwall=None, circuit=None):
+        self._keep = []
+        if fn is not None:
+            self.cb = wrap_ufunc(fn)
+            self.ufunc = C.cast(self.cb, VP)
+            self.udata = None
+        elif brickwall is not None:
+            vlist, perms = brickwall
+            vlist = cplx(vlist)
+            pp, pk = perm_pointers(perms)
+            self.desc = BrickwallTarget(vlist.ctypes.data, vlist.shape[0], pp)
+            self._keep += [vlist, pp, pk]
+            self.ufunc = C.cast(lib().rqcopt_brickwall_ufunc, VP)
+            self.udata = C.cast(C.pointer(self.desc), VP)
+        elif circuit is not None:
+            gates, wires = cplx(circuit[0]), ints(circuit[1])
+            self.desc = CircuitTarget(gates.ctypes.data, gates.shape[0], C.cast(wires.ctypes.data, C.POINTER(C.c_int)))
+            self._keep += [gates, wires]
+            self.ufunc = C.cast(lib().rqcopt_circuit_ufunc, VP)
+            self.udata = C.cast(C.pointer(self.desc), VP)
+        else:
+            raise ValueError("target needs fn, brickwall or circuit")
+
+
+def circuit_unitary_target(target, gates, wires, nqubits):
+    gates, wires = cplx(gates), ints(wires)
+    f = np.zeros(1, np.complex128)
+    _check("circuit_unitary_target", lib().circuit_unitary_target(target.ufunc, target.udata, ptr(gates), gates.shape[0],
+                                                                 ptr(wires), nqubits, ptr(f)))
+    return f[0]
+
+
+def circuit_unitary_target_and_gradient(target, gates, wires, nqubits):
+    gates, wires = cplx(gates), ints(wires)
+    f = np.zeros(1, np.complex128)
+    dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+    _check("circuit_unitary_target_and_gradient",
+           lib().circuit_unitary_target_and_gradient(target.ufunc, target.udata, ptr(gates), gates.shape[0], ptr(wires),
+                                                     nqubits, ptr(f), ptr(dg)))
+    return f[0], dg
+
+
+def circuit_unitary_target_and_projected_gradient(target, gates, wires, nqubits):
+    gates, wires = cplx(gates), ints(wires)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * gates.shape[0])
+    _check("circuit_unitary_target_and_projected_gradient",
+           lib().circuit_unitary_target_and_projected_gradient(target.ufunc, target.udata, ptr(gates), gates.shape[0],
+                                                               ptr(wires), nqubits, ptr(f), ptr(g)))
+    return f[0], g
+
+
+def circuit_unitary_target_hessian_vector_product(target, gates, gatedirs, wires, nqubits):
+    gates, gatedirs, wires = cplx(gates), cplx(gatedirs), ints(wires)
+    f = np.zeros(1, np.complex128)
+    dg = np.empty((gates.shape[0], 4, 4), np.complex128)
+    hg = np.empty_like(dg)
+    _check("circuit_unitary_target_hessian_vector_product",
+           lib().circuit_unitary_target_hessian_vector_product(target.ufunc, target.udata, ptr(gates), ptr(gatedirs),
+                                                               gates.shape[0], ptr(wires), nqubits, ptr(f), ptr(dg),
+                                                               ptr(hg)))
+    return f[0], dg, hg
+
+
+def circuit_unitary_target_projected_hessian_vector_product(target, gates, gatedirs, wires, nqubits):
+    gates, gatedirs, wires = cplx(gates), cplx(gatedirs), ints(wires)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * gates.shape[0])
+    h = np.empty_like(g)
+    _check("circuit_unitary_target_projected_hessian_vector_product",
+           lib().circuit_unitary_target_projected_hessian_vector_product(target.ufunc, target.udata, ptr(gates),
+                                                                         ptr(gatedirs), gates.shape[0], ptr(wires),
+                                                                         nqubits, ptr(f), ptr(g), ptr(h)))
+    return f[0], g, h
+
+
+def brickwall_unitary_target(target, vlist, perms, nqubits):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    _check("brickwall_unitary_target", lib().brickwall_unitary_target(target.ufunc, target.udata, ptr(vlist),
+                                                                     vlist.shape[0], nqubits, C.cast(pp, VP), ptr(f)))
+    return f[0]
+
+
+def brickwall_unitary_target_and_gradient(target, vlist, perms, nqubits):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+    _check("brickwall_unitary_target_and_gradient",
+           lib().brickwall_unitary_target_and_gradient(target.ufunc, target.udata, ptr(vlist), vlist.shape[0], nqubits,
+                                                       C.cast(pp, VP), ptr(f), ptr(dv)))
+    return f[0], dv
+
+
+def brickwall_unitary_target_and_projected_gradient(target, vlist, perms, nqubits):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * vlist.shape[0])
+    _check("brickwall_unitary_target_and_projected_gradient",
+           lib().brickwall_unitary_target_and_projected_gradient(target.ufunc, target.udata, ptr(vlist), vlist.shape[0],
+                                                                 nqubits, C.cast(pp, VP), ptr(f), ptr(g)))
+    return f[0], g
+
+
+def brickwall_unitary_target_hessian_vector_product(target, vlist, vdirs, perms, nqubits):
+    vlist, vdirs = cplx(vlist), cplx(vdirs)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+    hv = np.empty_like(dv)
+    _check("brickwall_unitary_target_hessian_vector_product",
+           lib().brickwall_unitary_target_hessian_vector_product(target.ufunc, target.udata, ptr(vlist), ptr(vdirs),
+                                                                 vlist.shape[0], C.cast(pp, VP), nqubits, ptr(f), ptr(dv),
+                                                                 ptr(hv)))
+    return f[0], dv, hv
+
+
+def brickwall_unitary_target_projected_hessian_vector_product(target, vlist, vdirs, perms, nqubits):
+    vlist, vdirs = cplx(vlist), cplx(vdirs)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * vlist.shape[0])
+    h = np.empty_like(g)
+    _check("brickwall_unitary_target_projected_hessian_vector_product",
+           lib().brickwall_unitary_target_projected_hessian_vector_product(target.ufunc, target.udata, ptr(vlist),
+                                                                           ptr(vdirs), vlist.shape[0], C.cast(pp, VP),
+                                                                           nqubits, ptr(f), ptr(g), ptr(h)))
+    return f[0], g, h
+
+
+# ------------------------------------------------------------------------ trust region and optimisers
+
+def truncated_cg_hvp(grad, hvp_fn, radius, params=None, x=None):
+    """Steihaug tCG with a Python Hessian-vector product `hvp_fn(vec) -> H vec`."""
+    grad = np.ascontiguousarray(grad, dtype=np.float64)
+    n = grad.shape[0]
+    params = params or default_tcg_params(n)
+
+    def cb(xp, fdata, vec, hvp):
+        v = np.ctypeslib.as_array(vec, shape=(n,))
+        h = np.ctypeslib.as_array(hvp, shape=(n,))
+        h[:] = hvp_fn(v.copy())
+
+    f_hvp = HVP_FUNC(cb)
+    z = np.empty(n)
+    xv = ptr(np.ascontiguousarray(x, dtype=np.float64)) if x is not None else None
+    b = lib().truncated_cg_hvp(xv, ptr(grad), C.cast(f_hvp, VP), None, n, radius, C.byref(params), ptr(z))
+    _check_void("truncated_cg_hvp")
+    return z, bool(b)
+
+
+def optimize_brickwall_circuit_hvp(target, vlist_start, perms, nqubits, niter, params=None):
+    vlist_start = cplx(vlist_start)
+    nl = vlist_start.shape[0]
+    pp, keep = perm_pointers(perms)
+    params = params or default_rtr_params(16 * nl)
+    f_iter = np.empty(niter + 1)
+    vopt = np.empty_like(vlist_start)
+    lib().optimize_brickwall_circuit_hvp(target.ufunc, target.udata, ptr(vlist_start), nl, nqubits, C.cast(pp, VP),
+                                         C.byref(params), niter, ptr(f_iter), ptr(vopt))
+    _check_void("optimize_brickwall_circuit_hvp")
+    return f_iter, vopt
+
+
+def optimize_quantum_circuit(target, gates_start, wires, nqubits, niter, params=None):
+    gates_start, wires = cplx(gates_start), ints(wires)
+    ng = gates_start.shape[0]
+    params = params or default_rtr_params(16 * ng)
+    f_iter = np.empty(niter + 1)
+    gopt = np.empty_like(gates_start)
+    lib().optimize_quantum_circuit(target.ufunc, target.udata, ptr(gates_start), ng, nqubits, ptr(wires),
+                                   C.byref(params), niter, ptr(f_iter), ptr(gopt))
+    _check_void("optimize_quantum_circuit")
+    return f_iter, gopt
+
+
+# ------------------------------------------------------------------------ matrix helpers
+
+def real_to_tangent(r, v):
+    r, v = np.ascontiguousarray(r, dtype=np.float64), cplx(v)
+    z = np.empty((4, 4), np.complex128)
+    lib().real_to_tangent(ptr(r), ptr(v), ptr(z))
+    return z
+
+
+def tangent_to_real(v, z):
+    v, z = cplx(v), cplx(z)
+    r = np.empty(16)
+    lib().tangent_to_real(ptr(v), ptr(z), ptr(r))
+    return r
+
+
+def project_tangent(u, z):
+    u, z = cplx(u), cplx(z)
+    p = np.empty((4, 4), np.complex128)
+    lib().project_tangent(ptr(u), ptr(z), ptr(p))
+    return p
+
+
+def polar_factor(a):
+    a = cplx(a)
+    u = np.empty((4, 4), np.complex128)
+    lib().polar_factor(ptr(a), ptr(u))
+    return u
+
+
+def multiply_matrices(a, b):
+    a, b = cplx(a), cplx(b)
+    c = np.empty((4, 4), np.complex128)
+    lib().multiply_matrices(ptr(a), ptr(b), ptr(c))
+    return c
+
+
+def inverse_matrix(a):
+    a = cplx(a)
+    ai = np.empty((4, 4), np.complex128)
+    ret = lib().inverse_matrix(ptr(a), ptr(ai))
+    return ret, ai
+
+
+# ------------------------------------------------------------------------ configuration
+
+def set_precision(mode: int):
+    _check("rqcopt_gpu_set_precision", lib().rqcopt_gpu_set_precision(mode))
+
+
+def set_column_chunk(cols: int):
+    lib().rqcopt_gpu_set_column_chunk(cols)
+
+
+def set_workspace_limit(nbytes: int):
+    lib().rqcopt_gpu_set_workspace_limit(nbytes)
+
+
+def launch_count() -> int:
+    return int(lib().rqcopt_gpu_launch_count())
+
+
+def reset_launch_count():
+    lib().rqcopt_gpu_reset_launch_count()
+
+
+def enable_kernel_timing(on: bool):
+    lib().rqcopt_gpu_enable_kernel_timing(1 if on else 0)
+
+
+def kernel_time(kernel_class: int):
+    ms = C.c_double()
+    n = C.c_long()
+    _check("rqcopt_gpu_kernel_time", lib().rqcopt_gpu_kernel_time(kernel_class, C.byref(ms), C.byref(n)))
+    return ms.value, n.value

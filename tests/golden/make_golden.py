@@ -1,0 +1,43 @@
+"""Convert the reference's HDF5 golden vectors for the hot path into .npz fixtures.
+
+Run in a checkout that has the reference project next to it:
+
+    python tests/golden/make_golden.py /root/reference/test/data
+
+Each ``test_<name>_cplx.hdf5`` (complex-circuit fixtures of the reference's
+``test/data`` directory, generated there by ``test/test_*.py``) becomes
+``tests/golden/<name>.npz`` with the same dataset names and the interleaved
+(real, imag) layout unchanged.  The reader is ``hdf5_lite`` in this folder.
+"""
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import hdf5_lite  # noqa: E402
+
+FIXTURES = [
+    "apply_gate", "apply_gate_backward", "apply_quantum_circuit", "quantum_circuit_backward",
+    "quantum_circuit_gates_hessian_vector_product", "apply_brickwall_unitary", "brickwall_unitary_backward",
+    "circuit_unitary_target", "circuit_unitary_target_and_gradient",
+    "circuit_unitary_target_hessian_vector_product", "circuit_unitary_target_projected_hessian_vector_product",
+    "brickwall_unitary_target", "brickwall_unitary_target_and_gradient",
+    "brickwall_unitary_target_and_projected_gradient", "brickwall_unitary_target_hessian_vector_product",
+    "brickwall_unitary_target_projected_hessian_vector_product",
+    "real_to_tangent", "project_tangent", "polar_factor", "multiply",
+]
+
+
+def main(data_dir):
+    out_dir = os.path.dirname(os.path.abspath(__file__))
+    for name in FIXTURES:
+        arrays = hdf5_lite.read_all(os.path.join(data_dir, f"test_{name}_cplx.hdf5"))
+        np.savez(os.path.join(out_dir, f"{name}.npz"), **arrays)
+    arrays = hdf5_lite.read_all(os.path.join(data_dir, "test_truncated_cg.hdf5"))
+    np.savez(os.path.join(out_dir, "truncated_cg.npz"), **arrays)
+    print(f"wrote {len(FIXTURES) + 1} fixtures to {out_dir}")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/test/data")

@@ -1,0 +1,80 @@
+"""The C ABI: the library loads without a GPU, exports every function that
+include/rqcopt_gpu.h declares, and the header compiles as C and C++.  Where the
+reference sources are present, each reference declaration the header restates
+is compared with it token by token (ignoring `restrict` and whitespace)."""
+import os
+import re
+import subprocess
+import ctypes
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "rqcopt_gpu.h")
+LIB = os.path.join(ROOT, "rqcopt_hpc_b200", "librqcopt_gpu.so")
+REF_SRC = "/root/reference/src"
+
+
+def _declared_functions(text):
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    text = re.sub(r"static inline[^{]*\{.*?\n\}", "", text, flags=re.S)
+    names = set()
+    for m in re.finditer(r"^[A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\(", text, flags=re.M):
+        name = m.group(1)
+        if name not in ("if", "for", "while", "return", "sizeof") and not m.group(0).lstrip().startswith("typedef"):
+            names.add(name)
+    return names
+
+
+def test_library_exports_every_declared_function():
+    assert os.path.exists(LIB), "build the library first (python -m rqcopt_hpc_b200.build)"
+    lib = ctypes.CDLL(LIB)
+    names = _declared_functions(open(HEADER).read())
+    assert len(names) > 60
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+@pytest.mark.parametrize("lang", ["c", "c++"])
+def test_header_compiles(tmp_path, lang):
+    src = tmp_path / ("t.c" if lang == "c" else "t.cpp")
+    src.write_text('#include "rqcopt_gpu.h"\nint main(void) { struct rtr_params p; set_rtr_default_params(16, &p); return p.tcg_params.maxiter == 32 ? 0 : 1; }\n')
+    cc = "gcc" if lang == "c" else "g++"
+    subprocess.run([cc, "-fsyntax-only", "-Wall", "-I" + os.path.dirname(HEADER), str(src)], check=True)
+
+
+def _ref_prototypes():
+    protos = {}
+    for fn in os.listdir(REF_SRC):
+        if fn.endswith(".h"):
+            text = open(os.path.join(REF_SRC, fn)).read()
+            text = re.sub(r"//.*", "", text)
+            for m in re.finditer(r"^([A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\))\s*;", text, flags=re.M):
+                if not m.group(1).startswith("typedef"):
+                    protos[m.group(2)] = m.group(1)
+    return protos
+
+
+def _norm(p):
+    p = p.replace("restrict", " ")
+    p = re.sub(r"\bconst\s+hessian_vector_product_func", "hessian_vector_product_func", p)
+    p = re.sub(r"\bconst\s+(target_func|target_gradient_func)", r"\1", p)
+    p = re.sub(r"\s+", " ", p).strip()
+    p = re.sub(r"\s*([\(\)\*,\[\]])\s*", r"\1", p)
+    return p
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")
+def test_signatures_match_reference():
+    ref = _ref_prototypes()
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    ours = {}
+    for m in re.finditer(r"^([A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\))\s*;", text, flags=re.M):
+        if not m.group(1).startswith("typedef"):
+            ours[m.group(2)] = m.group(1)
+    checked = 0
+    for name, proto in ours.items():
+        if name in ref:
+            assert _norm(proto) == _norm(ref[name]), (name, proto, ref[name])
+            checked += 1
+    assert checked >= 50

@@ -1,0 +1,128 @@
+"""GPU library against the CPU oracle on the seeded brickwall workloads, through
+the C ABI.  Bar: 1e-12 relative (infinity norm relative to the oracle's infinity
+norm) in f, gradient and HVP for the complex128 path; 1e-5 for complex64
+passes.  Also checks the host-callback target path, general circuits,
+column chunking and the forward/adjoint round trip at a larger size."""
+import numpy as np
+import pytest
+
+from helpers import (brickwall_instance, crandn, haar_unitary, periodic_perms, random_tangent_dirs,
+                     real_to_antisymm, rel_err)
+
+pytestmark = pytest.mark.gpu
+
+
+def _dirs(vlist, seed):
+    r = random_tangent_dirs(vlist, seed)
+    return np.stack([vlist[k] @ real_to_antisymm(r[k]) for k in range(vlist.shape[0])])
+
+
+@pytest.fixture(autouse=True)
+def _defaults(gpu):
+    gpu.set_precision(gpu.PRECISION_C128)
+    gpu.set_column_chunk(0)
+    yield
+    gpu.set_precision(gpu.PRECISION_C128)
+    gpu.set_column_chunk(0)
+
+
+@pytest.mark.parametrize("L,depth,tdepth", [(4, 3, 3), (6, 5, 3), (8, 5, 3), (10, 7, 3)])
+def test_brickwall_projected_hvp_matches_oracle(gpu, oracle, L, depth, tdepth):
+    vlist, perms, tvlist, tperms = brickwall_instance(L, depth, 100 + L, tdepth, 200 + L)
+    vdirs = _dirs(vlist, 300 + L)
+    f, g, h = gpu.brickwall_unitary_target_projected_hessian_vector_product(
+        gpu.Target(brickwall=(tvlist, tperms)), vlist, vdirs, perms, L)
+    fo, go, ho = oracle.brickwall_unitary_target_projected_hessian_vector_product(
+        oracle.target("brickwall", (tvlist, tperms)), vlist, vdirs, perms, L)
+    assert abs(f - fo) <= 1e-12 * abs(fo)
+    assert rel_err(g, go) <= 1e-12
+    assert rel_err(h, ho) <= 1e-12
+
+
+def test_chunked_columns_match_single_chunk(gpu):
+    L = 8
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 5, 7, 3, 8)
+    vdirs = _dirs(vlist, 9)
+    t = gpu.Target(brickwall=(tvlist, tperms))
+    ref = gpu.brickwall_unitary_target_projected_hessian_vector_product(t, vlist, vdirs, perms, L)
+    for chunk in (1, 3, 64, 100):
+        gpu.set_column_chunk(chunk)
+        got = gpu.brickwall_unitary_target_projected_hessian_vector_product(t, vlist, vdirs, perms, L)
+        assert abs(got[0] - ref[0]) <= 1e-12 * abs(ref[0])
+        assert rel_err(got[1], ref[1]) <= 1e-12 and rel_err(got[2], ref[2]) <= 1e-12
+
+
+def test_host_callback_target_matches_device_target(gpu):
+    L = 6
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 3, 11, 3, 12)
+    vdirs = _dirs(vlist, 13)
+    dev = gpu.brickwall_unitary_target_projected_hessian_vector_product(
+        gpu.Target(brickwall=(tvlist, tperms)), vlist, vdirs, perms, L)
+    host = gpu.brickwall_unitary_target_projected_hessian_vector_product(
+        gpu.Target(fn=lambda x: gpu.apply_brickwall_unitary(tvlist, tperms, x)), vlist, vdirs, perms, L)
+    for a, b in zip(dev, host):
+        assert rel_err(a, b) <= 1e-12
+
+
+def test_general_circuit_hvp_matches_oracle(gpu, oracle):
+    L, G = 7, 9
+    rng = np.random.default_rng(21)
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    dirs = 0.5 * crandn((G, 4, 4), rng)
+    u = crandn((1 << L, 1 << L), rng)
+    fg = gpu.circuit_unitary_target_hessian_vector_product(gpu.Target(fn=lambda x: u @ x), gates, dirs, wires, L)
+    fo = oracle.circuit_unitary_target_hessian_vector_product(oracle.target("dense", u), gates, dirs, wires, L)
+    assert abs(fg[0] - fo[0]) <= 1e-12 * abs(fo[0])
+    assert rel_err(fg[1], fo[1]) <= 1e-12
+    assert rel_err(fg[2], fo[2]) <= 1e-12
+
+
+def test_circuit_target_descriptor(gpu, oracle):
+    L = 6
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 3, 31, 3, 32)
+    per = L // 2
+    tgates = np.repeat(tvlist, per, axis=0)
+    twires = np.concatenate([tperms[l].reshape(per, 2) for l in range(3)]).astype(np.int32)
+    a = gpu.brickwall_unitary_target(gpu.Target(circuit=(tgates, twires)), vlist, perms, L)
+    b = oracle.brickwall_unitary_target(oracle.target("brickwall", (tvlist, tperms)), vlist, perms, L)
+    assert abs(a - b) <= 1e-12 * abs(b)
+
+
+def test_complex64_passes_within_single_precision(gpu, oracle):
+    L = 8
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 5, 0, 3, 1)
+    vdirs = _dirs(vlist, 2)
+    gpu.set_precision(gpu.PRECISION_C64)
+    f, g, h = gpu.brickwall_unitary_target_projected_hessian_vector_product(
+        gpu.Target(brickwall=(tvlist, tperms)), vlist, vdirs, perms, L)
+    fo, go, ho = oracle.brickwall_unitary_target_projected_hessian_vector_product(
+        oracle.target("brickwall", (tvlist, tperms)), vlist, vdirs, perms, L)
+    assert abs(f - fo) <= 1e-5 * abs(fo)
+    assert rel_err(g, go) <= 1e-5
+    assert rel_err(h, ho) <= 1e-5
+
+
+def test_trust_region_retraces_oracle(gpu, oracle):
+    L = 8
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 5, 0, 3, 1)
+    f_g, v_g = gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L, 10)
+    f_o, v_o, acc, bnd = oracle.optimize_brickwall_circuit_hvp(oracle.target("brickwall", (tvlist, tperms)),
+                                                                vlist, perms, L, 10)
+    assert rel_err(f_g, f_o) <= 1e-12
+    assert rel_err(v_g, v_o) <= 1e-10
+
+
+def test_forward_adjoint_round_trip(gpu):
+    """Forward through 64 random Haar gates on random distinct pairs, then the adjoint
+    gates in reverse order, recovers the input state (L = 20, complex128)."""
+    L, G = 20, 64
+    rng = np.random.default_rng(20)
+    psi = crandn(1 << L, rng)
+    psi /= np.linalg.norm(psi)
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    out = gpu.apply_quantum_circuit(gates, wires, psi)
+    back = gpu.apply_quantum_circuit(np.conj(np.transpose(gates[::-1], (0, 2, 1))), wires[::-1], out)
+    assert np.max(np.abs(back - psi)) <= 1e-12
+    assert abs(np.linalg.norm(out) - 1) <= 1e-12
