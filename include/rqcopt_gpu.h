@@ -332,6 +332,34 @@ int  rqcopt_gpu_kernel_time(int kernel_class, double* total_ms, long* launches);
 /* the CUDA stream (cudaStream_t) all library work is issued on */
 void* rqcopt_gpu_stream(void);
 
+/*
+ * Allocation-free gate backward pass.  No counterpart in the reference; it
+ * computes what apply_gate_backward (src/gate.h:9-10) computes, without any
+ * device allocation, for callers that cannot call cudaMalloc at that point (a
+ * process whose device memory belongs to its own pool, a latency-critical
+ * thread that must not take the device-wide synchronisation an allocation or
+ * free can imply, a host callback running inside other GPU work).
+ *
+ * Its only scratch (per-tile partial sums of dgate) is a static device array
+ * of 2 MiB + 256 B that every GPU loading the library keeps until exit.
+ *   - psi, dpsi_out and dpsi must hold device or managed memory (host buffers
+ *     would need staging, i.e. allocation); dgate may be host or device memory;
+ *   - at most RQCOPT_NOALLOC_MAX_QUBITS qubits; larger states are rejected
+ *     with -6 and a message on stderr;
+ *   - work is issued on `stream` (a cudaStream_t, NULL for the legacy default
+ *     stream) and the call returns after the stream has finished it;
+ *   - the first call on a device resolves the scratch address there
+ *     (cudaGetSymbolAddress), so make that first call before any stream
+ *     capture;
+ *   - all calls share the scratch: calls whose GPU work overlaps (other
+ *     streams, other host threads) race on it.
+ * Returns 0, -5 (CUDA error) or -6 (invalid argument).
+ */
+#define RQCOPT_NOALLOC_MAX_QUBITS 25
+int rqcopt_apply_gate_backward_noalloc(const struct mat4x4* gate, const int i, const int j,
+	const struct statevector* psi, const struct statevector* dpsi_out, struct statevector* dpsi,
+	struct mat4x4* dgate, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
