@@ -76,12 +76,13 @@ def flops_per_eval(L, G, Gt):
     return float(N) * N * (32 * Gt + 292 * G - 124)
 
 
-def reverse_bytes_per_eval(L, G, itemsize):
-    """Algorithmic HBM bytes of the reverse (gradient/HVP) passes of one evaluation:
-    per column 6G - 5 statevector passes (reads of phi, dphi, psi_k, dpsi_k and writes of
-    phi', dphi'; the first gate has no dphi, the last no psi / outputs)."""
+def reverse_bytes_per_eval(L, P, itemsize):
+    """Algorithmic HBM bytes of the reverse (gradient/HVP) passes of one evaluation with P
+    passes (one per gate, or one per group of fused gates): per column 6P - 5 statevector
+    passes (reads of phi, dphi, psi, dpsi and writes of phi', dphi' per pass; the pass at the
+    circuit output has no dphi to read, the pass at its input no psi / outputs)."""
     N = 1 << L
-    return float(6 * G - 5) * N * N * itemsize
+    return float(6 * P - 5) * N * N * itemsize
 
 
 # ----------------------------------------------------------------------------- clocks
@@ -186,6 +187,7 @@ def main():
     ap.add_argument("--depth", type=int, default=9)
     ap.add_argument("--tdepth", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--gates-per-pass", type=int, default=4, help="gates fused per HBM round trip (1-4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     a = ap.parse_args()
 
@@ -233,6 +235,8 @@ def main():
     lib = gpu.lib()
     prec = gpu.PRECISION_C128 if a.precision == "c128" else gpu.PRECISION_C64
     gpu.set_precision(prec)
+    gpu.set_gates_per_pass(a.gates_per_pass)
+    config["gates_per_pass"] = a.gates_per_pass
     vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
     target = gpu.Target(brickwall=(tvlist, tperms))
 
@@ -265,6 +269,7 @@ def main():
     rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
     fwd_ms, fwd_n = gpu.kernel_time(gpu.KC_FORWARD)
     app_ms, app_n = gpu.kernel_time(gpu.KC_APPLY)
+    fus_ms, fus_n = gpu.kernel_time(gpu.KC_FUSED)
     gpu.enable_kernel_timing(False)
 
     # end-to-end through the C ABI with host buffers
@@ -288,7 +293,8 @@ def main():
         except (OSError, ValueError):
             pass
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
-        rbytes = reverse_bytes_per_eval(L, G, itemsize) * a.steps
+        npass = G if a.gates_per_pass == 1 else -(-G // a.gates_per_pass)
+        rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
         achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
         value = world * a.steps / (dev_ms * 1e-3)
         flops = flops_per_eval(L, G, Gt)
@@ -300,12 +306,15 @@ def main():
             "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "evals/s",
                     "h2d_bytes_per_step": int(vlist.nbytes + vdirs.nbytes + tvlist.nbytes + perms.nbytes + tperms.nbytes),
                     "d2h_bytes_per_step": int(16 + 2 * 16 * depth * 8)},
-            "roofline": {"kernel": "k_reverse (gradient/HVP pass of one gate over a column chunk)", "bound": "hbm",
+            "roofline": {"kernel": ("k_reverse (gradient/HVP pass of one gate over a column chunk)" if a.gates_per_pass == 1
+                                    else f"k2_rev (gradient/HVP pass of {a.gates_per_pass} fused gates over a column chunk)"),
+                         "bound": "hbm",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak if achieved else None,
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650",
                          "traffic": None, "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)},
-            "kernel_share": {"reverse_ms": rev_ms, "forward_ms": fwd_ms, "apply_ms": app_ms, "device_ms": dev_ms},
+            "kernel_share": {"reverse_ms": rev_ms, "forward_ms": fwd_ms, "apply_ms": app_ms,
+                             "fused_forward_ms": fus_ms, "device_ms": dev_ms},
             "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
             "clocks": clk.summary(), "gpu_launches": int(launches),
         }

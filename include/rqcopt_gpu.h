@@ -312,6 +312,11 @@ void rqcopt_gpu_set_workspace_limit(size_t bytes);
 /* number of basis columns per chunk; 0 selects it from the workspace limit */
 void rqcopt_gpu_set_column_chunk(long columns);
 
+/* gates fused per HBM round trip in the basis-column passes: 1 runs one kernel
+ * per gate, 2..4 (default 4) group consecutive gates into passes over
+ * eight-qubit tiles of column-interleaved chunks */
+int rqcopt_gpu_set_gates_per_pass(int gates);
+
 /* last error recorded by a void function (0 if none); reading clears it */
 int rqcopt_gpu_last_error(void);
 

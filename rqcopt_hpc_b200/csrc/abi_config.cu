@@ -39,6 +39,15 @@ void rqcopt_gpu_set_column_chunk(long columns)
 	if (Runtime* rt = runtime()) rt->column_chunk = columns > 0 ? columns : 0;
 }
 
+int rqcopt_gpu_set_gates_per_pass(int gates)
+{
+	if (gates < 1 || gates > 4) return E_ARG;
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	rt->gates_per_pass = gates;
+	return 0;
+}
+
 int rqcopt_gpu_last_error(void) { return take_last_error(); }
 
 unsigned long long rqcopt_gpu_launch_count(void)

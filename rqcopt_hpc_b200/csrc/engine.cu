@@ -20,6 +20,7 @@
 // (complex64 passes accumulate FP32 products in short runs that are added into
 // FP64), then per block, then over blocks with compensated summation.
 #include "engine.h"
+#include "engine_fused.h"
 
 #include <stdio.h>
 #include <string.h>
@@ -595,6 +596,7 @@ int evaluate(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, i
 	}
 	int ret;
 	if ((ret = RQC_CUDA(cudaMemsetAsync(d_out, 0, result_count(c.ngates) * sizeof(double2), rt.stream)))) return ret;
+	if (rt.gates_per_pass > 1 && c.L >= 4) return evaluate_fused(rt, c, t, mode, precision, rt.gates_per_pass, d_out);
 	if (precision == PREC_C128) return evaluate_t<double>(rt, c, t, mode, d_out);
 	return evaluate_t<float>(rt, c, t, mode, d_out);
 }

@@ -1,0 +1,1262 @@
+// Fused basis-column evaluation engine: the gates of a circuit are grouped into
+// passes of up to four consecutive gates acting on at most eight qubits (for
+// the periodic brickwall a pass is one half of a layer), and each pass is one
+// HBM round trip over a column chunk.
+//
+// Layout: a chunk of C basis columns is stored column-interleaved, [2^L][C]
+// (amplitude row a, column j at a*C + j), so that a tile over ANY eight qubits
+// -- 256 rows -- reads and writes contiguous runs of CW columns (CW*sizeof =
+// 64 B) per row, whatever the qubits' positions.
+//
+// Per pass (gates g_0..g_{K-1} of the pass, directions z_k):
+//   forward  : psi, dpsi (pass input) -> pass output, in shared memory,
+//              dpsi <- g dpsi + z psi, psi <- g psi for each gate;
+//              only the pass-boundary states are stored (checkpoints);
+//   reverse  : from the checkpoint (psi, dpsi at the pass input) the K-1
+//              intermediate states are recomputed in shared memory, then for
+//              k = K-1..0, with phi, dphi the adjoint at the output of gate k:
+//                dG_k += phi (x) psi_k,   HZ_k += phi (x) dpsi_k + dphi (x) psi_k,
+//                dphi <- g_k^T dphi + z_k^T phi,  phi <- g_k^T phi;
+//              only phi, dphi at the pass input are stored.
+// Inside a gate step four threads share an amplitude group (4 amplitudes);
+// thread q owns gate row q of the outer products and output component q, so
+// each thread keeps 8 complex accumulators per gate of the pass in registers.
+//
+// These are the same per-column recurrences as the per-gate engine (the
+// scheme of src/quantum_circuit.c:147-236), evaluated in a different order of
+// memory traffic; results agree to rounding.
+#include <stdio.h>
+#include <string.h>
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "engine.h"
+#include "engine_fused.h"
+#include "rqc_common.cuh"
+#include "rqcopt_gpu.h"
+
+namespace rqc {
+
+namespace {
+
+constexpr int TPB2 = 256;
+constexpr int MAXK = 4;
+constexpr int MAXNB = 8;
+constexpr int NPART2 = 64;
+constexpr int EPT = (1 << MAXNB) * 4 / TPB2;   // complex128 tile elements per thread (4 columns per row)
+
+template <typename T> struct ColsPer;
+template <> struct ColsPer<double> { static constexpr int v = 4; };   // 4 x 16 B = 64 B runs
+template <> struct ColsPer<float>  { static constexpr int v = 8; };   // 8 x 8 B  = 64 B runs
+
+// Geometry of one pass over one chunk (kernel argument).
+struct PassGeom
+{
+	int K;                 // gates in the pass
+	int NB;                // tile bits (rows per tile = 2^NB)
+	int L;
+	int tbit[MAXNB];       // state row bit of tile bit b
+	int gi[MAXK], gj[MAXK];// tile-local bits of wire i / wire j of each gate
+	int64_t C;             // allocated columns of the chunk (row pitch)
+	int64_t ncg;           // column groups of CW columns covering the valid columns
+	int64_t ntiles;        // row tiles (2^(L-NB)) x column groups
+	int64_t b0;            // basis index of the chunk's first column
+	uint32_t rest_mask;    // state row bits that are not tile bits
+};
+
+template <typename T> struct PassGates { Gate4<T> g[MAXK]; Gate4<T> z[MAXK]; };
+
+// deposit the bits of v into the positions set in mask (ascending)
+__device__ __forceinline__ int64_t deposit(int64_t v, uint32_t mask)
+{
+	int64_t r = 0;
+	for (int b = 0; mask; b++) {
+		const uint32_t low = mask & (0u - mask);
+		if ((v >> b) & 1) r |= (int64_t)low;
+		mask &= mask - 1;
+	}
+	return r;
+}
+
+template <typename T>
+__device__ __forceinline__ void gates_to_smem(const PassGates<T>& pg, int K, bool tan, cplx<T>* sg)
+{
+	for (int e = threadIdx.x; e < 32 * MAXK; e += blockDim.x) {
+		const int k = e / 32, w = e % 32;
+		if (k >= K) continue;
+		sg[e] = w < 16 ? pg.g[k].m[w] : (tan ? pg.z[k].m[w - 16] : czero<cplx<T>>());
+	}
+}
+
+__device__ __forceinline__ void row_offsets(const PassGeom& pg, int* rowoff)
+{
+	const int R = 1 << pg.NB;
+	for (int r = threadIdx.x; r < R; r += blockDim.x) {
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		rowoff[r] = o;
+	}
+}
+
+// rows of the 4 group members for gate bits (bi, bj) and group base b6
+__device__ __forceinline__ void group_rows(int b6, int bi, int bj, int rows[4])
+{
+	const int lo = bi < bj ? bi : bj, hi = bi < bj ? bj : bi;
+	int r = b6;
+	r = ((r >> lo) << (lo + 1)) | (r & ((1 << lo) - 1));
+	r = ((r >> hi) << (hi + 1)) | (r & ((1 << hi) - 1));
+	rows[0] = r;
+	rows[1] = r | (1 << bj);
+	rows[2] = r | (1 << bi);
+	rows[3] = r | (1 << bi) | (1 << bj);
+}
+
+template <typename T>
+__device__ __forceinline__ cplx<T> sel4(const cplx<T> v[4], int q)
+{
+	return q == 0 ? v[0] : q == 1 ? v[1] : q == 2 ? v[2] : v[3];
+}
+
+__device__ __forceinline__ int sel4_int(const int v[4], int q)
+{
+	return q == 0 ? v[0] : q == 1 ? v[1] : q == 2 ? v[2] : v[3];
+}
+
+// ------------------------------------------------------------------------------ forward kernel
+
+// One pass forward over tiles.  IN: 0 read psi/dpsi, 1 basis columns (dpsi = 0).
+// OUT: 0 store psi/dpsi, 1 store -conj(psi) (no tangent), 2 f += <phi, psi> (no store).
+template <typename T, bool TAN, int IN, int OUT>
+__global__ void __launch_bounds__(TPB2) k2_fwd(const cplx<T>* __restrict__ psi, const cplx<T>* __restrict__ dpsi,
+                                               cplx<T>* __restrict__ psi_o, cplx<T>* __restrict__ dpsi_o,
+                                               const cplx<T>* __restrict__ phi, PassGeom pg, PassGates<T> gates,
+                                               double2* __restrict__ fpart)
+{
+	using V = cplx<T>;
+	constexpr int CW = ColsPer<T>::v;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, A = R * CW;
+	V* sg = reinterpret_cast<V*>(smem_raw);                       // 32 * MAXK gate entries
+	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);          // R
+	V* S = reinterpret_cast<V*>(rowoff + (1 << MAXNB));            // psi tile [R][CW]
+	V* dS = S + A;                                                 // dpsi tile
+	gates_to_smem<T>(gates, pg.K, TAN, sg);
+	row_offsets(pg, rowoff);
+	const int64_t rtiles = (int64_t)1 << (pg.L - pg.NB);
+	double fx = 0, fy = 0;
+	__syncthreads();
+
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		(void)rtiles;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cg * CW;
+		// load
+		for (int e = threadIdx.x; e < A; e += blockDim.x) {
+			const int r = e / CW, cc = e - r * CW;
+			const int64_t row = rowbase + rowoff[r];
+			const int64_t col = colbase + cc;
+			if (IN == 0) {
+				const int64_t a = row * pg.C + col;
+				S[e] = psi[a];
+				if (TAN) dS[e] = dpsi[a];
+			} else {
+				S[e] = mk<T>(row == pg.b0 + col ? T(1) : T(0), T(0));
+				if (TAN) dS[e] = czero<V>();
+			}
+		}
+		__syncthreads();
+		// gate steps
+		for (int k = 0; k < pg.K; k++) {
+			const V* gk = sg + 32 * k;
+			const int bi = pg.gi[k], bj = pg.gj[k];
+			for (int base = 0; base < A; base += blockDim.x) {
+				const int task = base + threadIdx.x;
+				const bool active = task < A;
+				const int g = task >> 2, q = task & 3;
+				const int cc = g % CW, b6 = g / CW;
+				int rows[4];
+				group_rows(b6, bi, bj, rows);
+				V x[4], dx[4], y = czero<V>(), dy = czero<V>();
+				if (active) {
+#pragma unroll
+					for (int m = 0; m < 4; m++) {
+						x[m] = S[rows[m] * CW + cc];
+						if (TAN) dx[m] = dS[rows[m] * CW + cc];
+					}
+#pragma unroll
+					for (int m = 0; m < 4; m++) {
+						y = cfma(gk[4 * q + m], x[m], y);
+						if (TAN) {
+							dy = cfma(gk[4 * q + m], dx[m], dy);
+							dy = cfma(gk[16 + 4 * q + m], x[m], dy);
+						}
+					}
+				}
+				__syncwarp();
+				if (active) {
+					const int r = sel4_int(rows, q);
+					S[r * CW + cc] = y;
+					if (TAN) dS[r * CW + cc] = dy;
+				}
+			}
+			__syncthreads();
+		}
+		// store / reduce
+		for (int e = threadIdx.x; e < A; e += blockDim.x) {
+			const int r = e / CW, cc = e - r * CW;
+			const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+			if (OUT == 2) {
+				const V p = phi[a];
+				const V s = S[e];
+				fx += (double)p.x * s.x - (double)p.y * s.y;
+				fy += (double)p.x * s.y + (double)p.y * s.x;
+			} else if (OUT == 1) {
+				psi_o[a] = cneg_conj(S[e]);
+			} else {
+				psi_o[a] = S[e];
+				if (TAN) dpsi_o[a] = dS[e];
+			}
+		}
+		__syncthreads();
+	}
+	if (OUT == 2) {
+		__shared__ double red[2][TPB2 / 32];
+		fx = warp_sum(fx);
+		fy = warp_sum(fy);
+		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+		if (lane == 0) { red[0][warp] = fx; red[1][warp] = fy; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double sx = 0, sy = 0;
+			for (int w = 0; w < TPB2 / 32; w++) { sx += red[0][w]; sy += red[1][w]; }
+			fpart[blockIdx.x].x += sx;
+			fpart[blockIdx.x].y += sy;
+		}
+	}
+}
+
+// ------------------------------------------------------------------------------ reverse kernel
+
+// One pass in reverse over tiles.  FIRST: the pass ends the circuit (dphi = 0).
+// LAST: the pass starts the circuit (psi is the basis column, dpsi = 0, no outputs).
+// part: per-gate partial sums of the pass, gate k at part + k * nblk * 64, block b at + b * 64.
+template <typename T, bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(TPB2, 1) k2_rev(const cplx<T>* __restrict__ psi, const cplx<T>* __restrict__ dpsi,
+                                                  const cplx<T>* __restrict__ phi, const cplx<T>* __restrict__ dphi,
+                                                  cplx<T>* __restrict__ phi_o, cplx<T>* __restrict__ dphi_o,
+                                                  PassGeom pg, PassGates<T> gates, double* __restrict__ part, int nblk)
+{
+	using V = cplx<T>;
+	constexpr int CW = ColsPer<T>::v;
+	constexpr bool FLUSH = sizeof(T) == 4;
+	constexpr int RUN = 4;
+	constexpr int NV = TAN ? 16 : 8;   // accumulator reals per gate: row q of dG (and of HZ)
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
+	V* sg = reinterpret_cast<V*>(smem_raw);
+	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);
+	V* tiles = reinterpret_cast<V*>(rowoff + (1 << MAXNB));
+	V* Psi = tiles;                               // K tiles: state entering gate k
+	V* dPsi = TAN ? tiles + K * A : nullptr;      // K tiles
+	V* Phi = tiles + (TAN ? 2 * K : K) * A;       // adjoint
+	V* dPhi = TAN ? Phi + A : nullptr;
+	gates_to_smem<T>(gates, K, TAN, sg);
+	row_offsets(pg, rowoff);
+	const int q = threadIdx.x & 3;
+
+	T acc[MAXK][NV];
+	double accd[MAXK][FLUSH ? NV : 1];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++)
+#pragma unroll
+		for (int v = 0; v < NV; v++) {
+			acc[k][v] = 0;
+			if (FLUSH) accd[k][v] = 0;
+		}
+	int run = 0;
+	__syncthreads();
+
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cg * CW;
+		for (int e = threadIdx.x; e < A; e += blockDim.x) {
+			const int r = e / CW, cc = e - r * CW;
+			const int64_t row = rowbase + rowoff[r], col = colbase + cc;
+			const int64_t a = row * pg.C + col;
+			if (LAST) {
+				Psi[e] = mk<T>(row == pg.b0 + col ? T(1) : T(0), T(0));
+				if (TAN) dPsi[e] = czero<V>();
+			} else {
+				Psi[e] = psi[a];
+				if (TAN) dPsi[e] = dpsi[a];
+			}
+			Phi[e] = phi[a];
+			if (TAN) dPhi[e] = FIRST ? czero<V>() : dphi[a];
+		}
+		__syncthreads();
+		// recompute the states entering gates 1..K-1
+#pragma unroll
+		for (int k = 0; k < MAXK - 1; k++) {
+			if (k + 1 >= K) break;
+			const V* gk = sg + 32 * k;
+			const V* src = Psi + k * A;
+			V* dst = Psi + (k + 1) * A;
+			const V* dsrc = TAN ? dPsi + k * A : nullptr;
+			V* ddst = TAN ? dPsi + (k + 1) * A : nullptr;
+			for (int base = 0; base < A; base += blockDim.x) {
+				const int task = base + threadIdx.x;
+				if (task >= A) break;
+				const int g = task >> 2;
+				const int cc = g % CW, b6 = g / CW;
+				int rows[4];
+				group_rows(b6, pg.gi[k], pg.gj[k], rows);
+				V y = czero<V>(), dy = czero<V>();
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					const V x = src[rows[m] * CW + cc];
+					y = cfma(gk[4 * q + m], x, y);
+					if (TAN) {
+						dy = cfma(gk[16 + 4 * q + m], x, dy);
+						dy = cfma(gk[4 * q + m], dsrc[rows[m] * CW + cc], dy);
+					}
+				}
+				const int r = sel4_int(rows, q);
+				dst[r * CW + cc] = y;
+				if (TAN) ddst[r * CW + cc] = dy;
+			}
+			__syncthreads();
+		}
+		// reverse through the pass
+#pragma unroll
+		for (int k = MAXK - 1; k >= 0; k--) {
+			if (k >= K) continue;
+			const V* gk = sg + 32 * k;
+			const V* X = Psi + k * A;
+			const V* dX = TAN ? dPsi + k * A : nullptr;
+			const bool first_gate = FIRST && k == K - 1;   // adjoint tangent still zero
+			const bool last_gate = LAST && k == 0;         // entering state is the basis column, dpsi = 0
+			for (int base = 0; base < A; base += blockDim.x) {
+				const int task = base + threadIdx.x;
+				const bool active = task < A;
+				const int g = task >> 2;
+				const int cc = g % CW, b6 = g / CW;
+				int rows[4];
+				group_rows(b6, pg.gi[k], pg.gj[k], rows);
+				V p[4], dp[4], x[4], dx[4];
+				V np = czero<V>(), ndp = czero<V>();
+				if (active) {
+#pragma unroll
+					for (int m = 0; m < 4; m++) {
+						const int a = rows[m] * CW + cc;
+						p[m] = Phi[a];
+						x[m] = X[a];
+						if (TAN) {
+							dp[m] = dPhi[a];
+							dx[m] = dX[a];
+						}
+					}
+					const V pq = sel4<T>(p, q);
+					const V dpq = TAN ? sel4<T>(dp, q) : czero<V>();
+#pragma unroll
+					for (int c = 0; c < 4; c++) {
+						acc[k][2 * c]     = fma(pq.x, x[c].x, fma(-pq.y, x[c].y, acc[k][2 * c]));
+						acc[k][2 * c + 1] = fma(pq.x, x[c].y, fma(pq.y, x[c].x, acc[k][2 * c + 1]));
+						if (TAN) {
+							T hx = acc[k][8 + 2 * c], hy = acc[k][8 + 2 * c + 1];
+							if (!last_gate) {
+								hx = fma(pq.x, dx[c].x, fma(-pq.y, dx[c].y, hx));
+								hy = fma(pq.x, dx[c].y, fma(pq.y, dx[c].x, hy));
+							}
+							if (!first_gate) {
+								hx = fma(dpq.x, x[c].x, fma(-dpq.y, x[c].y, hx));
+								hy = fma(dpq.x, x[c].y, fma(dpq.y, x[c].x, hy));
+							}
+							acc[k][8 + 2 * c] = hx;
+							acc[k][8 + 2 * c + 1] = hy;
+						}
+					}
+					if (!(LAST && k == 0)) {
+#pragma unroll
+						for (int r = 0; r < 4; r++) {
+							np = cfma(gk[4 * r + q], p[r], np);
+							if (TAN) {
+								ndp = cfma(gk[16 + 4 * r + q], p[r], ndp);
+								if (!first_gate) ndp = cfma(gk[4 * r + q], dp[r], ndp);
+							}
+						}
+					}
+				}
+				__syncwarp();
+				if (active && !(LAST && k == 0)) {
+					const int r = sel4_int(rows, q);
+					Phi[r * CW + cc] = np;
+					if (TAN) dPhi[r * CW + cc] = ndp;
+				}
+			}
+			if (FLUSH && ++run == RUN) {
+				run = 0;
+#pragma unroll
+				for (int kk = 0; kk < MAXK; kk++)
+#pragma unroll
+					for (int v = 0; v < NV; v++) { accd[kk][v] += acc[kk][v]; acc[kk][v] = 0; }
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+			for (int e = threadIdx.x; e < A; e += blockDim.x) {
+				const int r = e / CW, cc = e - r * CW;
+				const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+				phi_o[a] = Phi[e];
+				if (TAN) dphi_o[a] = dPhi[e];
+			}
+		}
+		__syncthreads();
+	}
+
+	// reduce: lanes with equal q (xor 16, 8, 4), then over warps
+	double* red = reinterpret_cast<double*>(tiles);   // [warps][4][MAXK * NV]
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int k = 0; k < MAXK; k++)
+#pragma unroll
+		for (int v = 0; v < NV; v++) {
+			double x = FLUSH ? accd[k][v] + (double)acc[k][v] : (double)acc[k][v];
+			x += __shfl_xor_sync(0xffffffffu, x, 16);
+			x += __shfl_xor_sync(0xffffffffu, x, 8);
+			x += __shfl_xor_sync(0xffffffffu, x, 4);
+			if (lane < 4) red[(warp * 4 + lane) * (MAXK * NV) + k * NV + v] = x;
+		}
+	__syncthreads();
+	const int nwarps = blockDim.x >> 5;
+	for (int idx = threadIdx.x; idx < 4 * K * NV; idx += blockDim.x) {
+		const int qq = idx / (K * NV), rem = idx % (K * NV), k = rem / NV, v = rem % NV;
+		double s = 0;
+		for (int w = 0; w < nwarps; w++) s += red[(w * 4 + qq) * (MAXK * NV) + k * NV + v];
+		// v < 8: dG row qq (complex c = v/2); v >= 8: HZ row qq
+		const int dst = v < 8 ? 8 * qq + v : 32 + 8 * qq + (v - 8);
+		part[(size_t)k * nblk * NPART2 + (size_t)blockIdx.x * NPART2 + dst] += s;
+	}
+}
+
+// ------------------------------------------------------------------------------ complex128 kernels on the FP64 MMA
+
+// Every per-group step is a small product over real 8x8 embeddings of the 4x4
+// complex gates, issued as FP64 MMAs (mma.sync m8n8k4):
+//   outputs      out = in * M,  M the embedding of G (out[c] = sum_r in[r] G[r][c]) or of G^T,
+//                with in/out 8 groups x 8 components (re/im of 4 amplitudes, interleaved);
+//   outer sums   C += P^T X with P, X 4 groups x 8 components, C the raw 8x8 sum whose 2x2
+//                blocks hold re/im products (folded into complex dG, HZ by the reduction).
+// Shared-memory tiles store row r at physical row (r & ~1) | parity(r): the rows of an
+// amplitude group differ in one bit, so the 64-bit operand loads of a half warp hit both
+// halves of the bank window and are free of bank conflicts for any gate wires.
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
+{
+	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+	             : "+d"(d0), "+d"(d1)
+	             : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ int prow(int r) { return (r & ~1) | (__popc(r) & 1); }
+
+// element [rowk][coln] of the real embedding of m (or of m^T) for row-vector products
+__device__ __forceinline__ double embed(const double2* m, int rowk, int coln, bool tr)
+{
+	const int r = rowk >> 1, a = rowk & 1, c = coln >> 1, b = coln & 1;
+	const double2 v = tr ? m[4 * c + r] : m[4 * r + c];
+	return a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
+}
+
+constexpr int NTF = 256;   // threads of the complex128 forward kernel
+constexpr int NTR = 512;   // threads of the complex128 reverse kernel
+constexpr int NPART3 = 128;   // raw 8x8 sums per gate and block: dG then HZ
+
+__device__ __forceinline__ int insert2(int v, int lo, int hi)
+{
+	v = ((v >> lo) << (lo + 1)) | (v & ((1 << lo) - 1));
+	return ((v >> hi) << (hi + 1)) | (v & ((1 << hi) - 1));
+}
+
+// row bits of group member `amp` (row index 2*b_i + b_j) for wire bits (bi, bj)
+__device__ __forceinline__ int mbits(int amp, int bi, int bj) { return ((amp >> 1) << bi) | ((amp & 1) << bj); }
+
+// complex index of (row, column) in a swizzled tile of 4 columns
+__device__ __forceinline__ int sidx(int row, int cc) { return prow(row) * 4 + cc; }
+
+// Per-lane addressing of one gate step: member bits of the operands this lane loads.
+struct StepLane
+{
+	int lo, hi;
+	int m_outer, m_k0, m_k1, m_st;   // member bits: outer-product operand, output k-steps 0/1, store
+	int part_outer, part_out;
+	__device__ __forceinline__ StepLane(int bi, int bj, int lane)
+	{
+		lo = bi < bj ? bi : bj;
+		hi = bi < bj ? bj : bi;
+		m_outer = mbits(lane >> 3, bi, bj);
+		m_k0 = mbits((lane & 3) >> 1, bi, bj);
+		m_k1 = mbits(2 + ((lane & 3) >> 1), bi, bj);
+		m_st = mbits(lane & 3, bi, bj);
+		part_outer = (lane >> 2) & 1;
+		part_out = lane & 1;
+	}
+};
+
+// B fragments (k-steps 0, 1) of the embedding of gate matrix m (16 complex in smem)
+__device__ __forceinline__ void bfrag(const double2* m, bool tr, int lane, double b[2])
+{
+	b[0] = embed(m, lane & 3, lane >> 2, tr);
+	b[1] = embed(m, 4 + (lane & 3), lane >> 2, tr);
+}
+
+// out (8 groups of unit u) = in * B (+ in2 * B2 + in_extra * B), stored at the group members
+template <bool TAN>
+__device__ __forceinline__ void apply_unit(const double* in, const double* din, double2* out, double2* dout, int u,
+                                          const StepLane& sl, const double bg[2], const double bz[2], bool dzero,
+                                          int lane, bool inplace)
+{
+	const int bsel = insert2(2 * u + (lane >> 4), sl.lo, sl.hi);
+	const int cc = (lane >> 2) & 3;
+	const int j0 = sidx(bsel | sl.m_k0, cc) * 2 + sl.part_out;
+	const int j1 = sidx(bsel | sl.m_k1, cc) * 2 + sl.part_out;
+	const double a0 = in[j0], a1 = in[j1];
+	double y0 = 0, y1 = 0, z0 = 0, z1 = 0;
+	dmma(y0, y1, a0, bg[0]);
+	if (TAN) dmma(z0, z1, a0, bz[0]);
+	dmma(y0, y1, a1, bg[1]);
+	if (TAN) {
+		dmma(z0, z1, a1, bz[1]);
+		if (!dzero) {
+			dmma(z0, z1, din[j0], bg[0]);
+			dmma(z0, z1, din[j1], bg[1]);
+		}
+	}
+	if (inplace) __syncwarp();
+	const int st = sidx(bsel | sl.m_st, cc);
+	out[st] = make_double2(y0, y1);
+	if (TAN) dout[st] = make_double2(z0, z1);
+}
+
+// Forward pass (complex128).  Same contract as k2_fwd.
+template <bool TAN, int IN, int OUT>
+__global__ void __launch_bounds__(NTF) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+                                              double2* __restrict__ psi_o, double2* __restrict__ dpsi_o,
+                                              const double2* __restrict__ phi, PassGeom pg, PassGates<double> gates,
+                                              double2* __restrict__ fpart)
+{
+	constexpr int CW = 4;
+	constexpr int EPTF = (1 << MAXNB) * CW / NTF;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
+	double2* sg = reinterpret_cast<double2*>(smem_raw);
+	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);
+	double2* S = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));
+	double2* dS = S + A;
+	gates_to_smem<double>(gates, K, TAN, sg);
+	row_offsets(pg, rowoff);
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	double fx = 0, fy = 0;
+	const int units = R / 8;
+	double2 ra[EPTF], rb[EPTF];
+	auto fetch = [&](int64_t tile) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW;
+#pragma unroll
+		for (int i = 0; i < EPTF; i++) {
+			const int e = threadIdx.x + i * NTF;
+			if (e >= A || IN != 0 || tile >= pg.ntiles) continue;
+			const int64_t a = (rowbase + rowoff[e >> 2]) * pg.C + colbase + (e & 3);
+			ra[i] = psi[a];
+			if (TAN) rb[i] = dpsi[a];
+		}
+	};
+	fetch(blockIdx.x);
+
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cg * CW;
+#pragma unroll
+		for (int i = 0; i < EPTF; i++) {
+			const int e = threadIdx.x + i * NTF;
+			if (e >= A) continue;
+			const int r = e >> 2, cc = e & 3;
+			const int pe = sidx(r, cc);
+			if (IN == 0) {
+				S[pe] = ra[i];
+				if (TAN) dS[pe] = rb[i];
+			} else {
+				const int64_t row = rowbase + rowoff[r], col = colbase + cc;
+				S[pe] = make_double2(row == pg.b0 + col ? 1.0 : 0.0, 0.0);
+				if (TAN) dS[pe] = make_double2(0, 0);
+			}
+		}
+		__syncthreads();
+		fetch(tile + gridDim.x);
+#pragma unroll
+		for (int k = 0; k < MAXK; k++) {
+			if (k >= K) break;
+			const StepLane sl(pg.gi[k], pg.gj[k], lane);
+			double bg[2], bz[2] = {0, 0};
+			bfrag(sg + 32 * k, true, lane, bg);
+			if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
+			const bool dzero = IN == 1 && k == 0;
+			for (int u = warp; u < units; u += nwarps)
+				apply_unit<TAN>(reinterpret_cast<const double*>(S), reinterpret_cast<const double*>(dS), S, dS, u, sl, bg,
+				                bz, dzero, lane, true);
+			__syncthreads();
+		}
+		for (int i = 0; i < EPTF; i++) {
+			const int e = threadIdx.x + i * NTF;
+			if (e >= A) continue;
+			const int r = e >> 2, cc = e & 3;
+			const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+			const int pe = sidx(r, cc);
+			if (OUT == 2) {
+				const double2 p = phi[a], v = S[pe];
+				fx += p.x * v.x - p.y * v.y;
+				fy += p.x * v.y + p.y * v.x;
+			} else if (OUT == 1) {
+				psi_o[a] = cneg_conj(S[pe]);
+			} else {
+				psi_o[a] = S[pe];
+				if (TAN) dpsi_o[a] = dS[pe];
+			}
+		}
+		__syncthreads();
+	}
+	if (OUT == 2) {
+		__shared__ double red[2][NTF / 32];
+		fx = warp_sum(fx);
+		fy = warp_sum(fy);
+		if (lane == 0) { red[0][warp] = fx; red[1][warp] = fy; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double sx = 0, sy = 0;
+			for (int w = 0; w < nwarps; w++) { sx += red[0][w]; sy += red[1][w]; }
+			fpart[blockIdx.x].x += sx;
+			fpart[blockIdx.x].y += sy;
+		}
+	}
+}
+
+// Reverse pass (complex128).  Same contract as k2_rev; partials are raw 8x8 sums
+// (part + k * nblk * 128 + blockIdx.x * 128: [0, 64) dG, [64, 128) HZ, index m*8 + n).
+template <bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NTR, 1) k3_rev(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+                                                 const double2* __restrict__ phi, const double2* __restrict__ dphi,
+                                                 double2* __restrict__ phi_o, double2* __restrict__ dphi_o,
+                                                 PassGeom pg, PassGates<double> gates, double* __restrict__ part, int nblk)
+{
+	constexpr int CW = 4;
+	constexpr int EPTR = (1 << MAXNB) * CW / NTR;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
+	double2* sg = reinterpret_cast<double2*>(smem_raw);
+	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);
+	double2* tiles = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));
+	double2* Psi = tiles;
+	double2* dPsi = TAN ? tiles + K * A : nullptr;
+	double2* Phi = tiles + (TAN ? 2 * K : K) * A;
+	double2* dPhi = TAN ? Phi + A : nullptr;
+	gates_to_smem<double>(gates, K, TAN, sg);
+	row_offsets(pg, rowoff);
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	double cg0[MAXK], cg1[MAXK], ch0[MAXK], ch1[MAXK];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) { cg0[k] = cg1[k] = ch0[k] = ch1[k] = 0; }
+	const int units = R / 8;
+	double2 ra[EPTR], rb[EPTR], rc[EPTR], rd[EPTR];
+	auto fetch = [&](int64_t tile) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW;
+#pragma unroll
+		for (int i = 0; i < EPTR; i++) {
+			const int e = threadIdx.x + i * NTR;
+			if (e >= A || tile >= pg.ntiles) continue;
+			const int64_t a = (rowbase + rowoff[e >> 2]) * pg.C + colbase + (e & 3);
+			if (!LAST) {
+				ra[i] = psi[a];
+				if (TAN) rb[i] = dpsi[a];
+			}
+			rc[i] = phi[a];
+			if (TAN && !FIRST) rd[i] = dphi[a];
+		}
+	};
+	fetch(blockIdx.x);
+
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cgp * CW;
+#pragma unroll
+		for (int i = 0; i < EPTR; i++) {
+			const int e = threadIdx.x + i * NTR;
+			if (e >= A) continue;
+			const int r = e >> 2, cc = e & 3;
+			const int pe = sidx(r, cc);
+			if (LAST) {
+				const int64_t row = rowbase + rowoff[r], col = colbase + cc;
+				Psi[pe] = make_double2(row == pg.b0 + col ? 1.0 : 0.0, 0.0);
+				if (TAN) dPsi[pe] = make_double2(0, 0);
+			} else {
+				Psi[pe] = ra[i];
+				if (TAN) dPsi[pe] = rb[i];
+			}
+			Phi[pe] = rc[i];
+			if (TAN) dPhi[pe] = FIRST ? make_double2(0, 0) : rd[i];
+		}
+		__syncthreads();
+		fetch(tile + gridDim.x);
+		// recompute the states entering gates 1..K-1
+#pragma unroll
+		for (int k = 0; k < MAXK - 1; k++) {
+			if (k + 1 >= K) break;
+			const StepLane sl(pg.gi[k], pg.gj[k], lane);
+			double bg[2], bz[2] = {0, 0};
+			bfrag(sg + 32 * k, true, lane, bg);
+			if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
+			const bool dzero = LAST && k == 0;
+			for (int u = warp; u < units; u += nwarps)
+				apply_unit<TAN>(reinterpret_cast<const double*>(Psi + k * A),
+				                TAN ? reinterpret_cast<const double*>(dPsi + k * A) : nullptr, Psi + (k + 1) * A,
+				                TAN ? dPsi + (k + 1) * A : nullptr, u, sl, bg, bz, dzero, lane, false);
+			__syncthreads();
+		}
+		// reverse through the pass
+		const double* P = reinterpret_cast<const double*>(Phi);
+		const double* dP = TAN ? reinterpret_cast<const double*>(dPhi) : nullptr;
+#pragma unroll
+		for (int k = MAXK - 1; k >= 0; k--) {
+			if (k >= K) continue;
+			const StepLane sl(pg.gi[k], pg.gj[k], lane);
+			double bg[2], bz[2] = {0, 0};
+			bfrag(sg + 32 * k, false, lane, bg);
+			if (TAN) bfrag(sg + 32 * k + 16, false, lane, bz);
+			const bool first_gate = FIRST && k == K - 1;
+			const bool last_gate = LAST && k == 0;
+			const double* X = reinterpret_cast<const double*>(Psi + k * A);
+			const double* dX = TAN ? reinterpret_cast<const double*>(dPsi + k * A) : nullptr;
+			for (int u = warp; u < units; u += nwarps) {
+				const int base0 = insert2(2 * u, sl.lo, sl.hi), base1 = insert2(2 * u + 1, sl.lo, sl.hi);
+				// outer products over the two sets of four groups
+				const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+				const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+				const double p0 = P[i0], x0 = X[i0], p1 = P[i1], x1 = X[i1];
+				dmma(cg0[k], cg1[k], p0, x0);
+				if (TAN && !last_gate) dmma(ch0[k], ch1[k], p0, dX[i0]);
+				dmma(cg0[k], cg1[k], p1, x1);
+				if (TAN && !last_gate) dmma(ch0[k], ch1[k], p1, dX[i1]);
+				if (TAN && !first_gate) {
+					dmma(ch0[k], ch1[k], dP[i0], x0);
+					dmma(ch0[k], ch1[k], dP[i1], x1);
+				}
+				if (last_gate) continue;
+				// adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place)
+				apply_unit<TAN>(P, dP, Phi, dPhi, u, sl, bg, bz, first_gate, lane, true);
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+			for (int i = 0; i < EPTR; i++) {
+				const int e = threadIdx.x + i * NTR;
+				if (e >= A) continue;
+				const int r = e >> 2, cc = e & 3;
+				const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+				const int pe = sidx(r, cc);
+				phi_o[a] = Phi[pe];
+				if (TAN) dphi_o[a] = dPhi[pe];
+			}
+		}
+		__syncthreads();
+	}
+
+	// sum the warps' raw 8x8 accumulators; lane l holds entries 2l, 2l+1
+	double* red = reinterpret_cast<double*>(tiles);   // [warps][MAXK][128]
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) {
+		if (k >= K) break;
+		double* w = red + ((size_t)warp * MAXK + k) * NPART3;
+		w[2 * lane] = cg0[k];
+		w[2 * lane + 1] = cg1[k];
+		w[64 + 2 * lane] = TAN ? ch0[k] : 0.0;
+		w[64 + 2 * lane + 1] = TAN ? ch1[k] : 0.0;
+	}
+	__syncthreads();
+	for (int idx = threadIdx.x; idx < K * NPART3; idx += blockDim.x) {
+		const int k = idx / NPART3, v = idx % NPART3;
+		double s = 0;
+		for (int w = 0; w < nwarps; w++) s += red[((size_t)w * MAXK + k) * NPART3 + v];
+		part[(size_t)k * nblk * NPART3 + (size_t)blockIdx.x * NPART3 + v] += s;
+	}
+}
+
+// Sum raw 8x8 partials over blocks (compensated) and fold them into complex dG, HZ:
+// X[r][c] = (R[2r][2c] - R[2r+1][2c+1]) + i (R[2r][2c+1] + R[2r+1][2c]).
+__global__ void k3_reduce(const double* __restrict__ part, int nslots, int nblk, const double2* __restrict__ fpart,
+                          int nblk_f, int with_hvp, double2* __restrict__ out)
+{
+	__shared__ double raw[NPART3];
+	const int s = blockIdx.x, t = threadIdx.x;
+	if (s < nslots) {
+		if (t < NPART3) {
+			double sum = 0, comp = 0;
+			for (int b = 0; b < nblk; b++) {
+				const double y = part[((size_t)s * nblk + b) * NPART3 + t] - comp;
+				const double u = sum + y;
+				comp = (u - sum) - y;
+				sum = u;
+			}
+			raw[t] = sum;
+		}
+		__syncthreads();
+		if (t < 32) {
+			const int which = t >> 4, e = t & 15, r = e >> 2, c = e & 3;
+			if (which == 1 && !with_hvp) return;
+			const double* R = raw + 64 * which;
+			const double re = R[(2 * r) * 8 + 2 * c] - R[(2 * r + 1) * 8 + 2 * c + 1];
+			const double im = R[(2 * r) * 8 + 2 * c + 1] + R[(2 * r + 1) * 8 + 2 * c];
+			out[1 + 16 * (size_t)(which ? nslots + s : s) + e] = make_double2(re, im);
+		}
+	} else if (t < 2) {
+		double sum = 0, comp = 0;
+		for (int b = 0; b < nblk_f; b++) {
+			const double y = (t == 0 ? fpart[b].x : fpart[b].y) - comp;
+			const double u = sum + y;
+			comp = (u - sum) - y;
+			sum = u;
+		}
+		reinterpret_cast<double*>(out)[t] = sum;
+	}
+}
+
+// -conj of host columns [Cc][N] (complex128) into the interleaved chunk [N][C]
+template <typename T>
+__global__ void k2_target_from_host(const double2* __restrict__ in, cplx<T>* __restrict__ out, int64_t N, int64_t Cc,
+                                    int64_t C)
+{
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N * C; i += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t row = i / C, col = i - row * C;
+		if (col < Cc) {
+			const double2 v = in[col * N + row];
+			out[i] = mk<T>((T)(-v.x), (T)v.y);
+		} else {
+			out[i] = czero<cplx<T>>();
+		}
+	}
+}
+
+// f and per-gate sums over blocks; same record layout as the per-gate engine
+__global__ void k2_reduce(const double* __restrict__ part, int nslots, int nblk, const double2* __restrict__ fpart,
+                          int nblk_f, int with_hvp, double2* __restrict__ out)
+{
+	double* o = reinterpret_cast<double*>(out);
+	const int s = blockIdx.x, t = threadIdx.x;
+	if (s < nslots) {
+		if (t >= NPART2 || (!with_hvp && t >= 32)) return;
+		double sum = 0, comp = 0;
+		for (int b = 0; b < nblk; b++) {
+			const double y = part[((size_t)s * nblk + b) * NPART2 + t] - comp;
+			const double u = sum + y;
+			comp = (u - sum) - y;
+			sum = u;
+		}
+		if (t < 32) o[2 * (1 + 16 * (size_t)s) + t] = sum;
+		else o[2 * (1 + 16 * (size_t)nslots + 16 * (size_t)s) + (t - 32)] = sum;
+	} else if (t < 2) {
+		double sum = 0, comp = 0;
+		for (int b = 0; b < nblk_f; b++) {
+			const double y = (t == 0 ? fpart[b].x : fpart[b].y) - comp;
+			const double u = sum + y;
+			comp = (u - sum) - y;
+			sum = u;
+		}
+		o[t] = sum;
+	}
+}
+
+// ------------------------------------------------------------------------------ scheduling
+
+struct Pass
+{
+	int first, K;
+	PassGeom geom;   // chunk fields filled per launch
+};
+
+// Group consecutive gates into passes of up to MAXK gates; tile bits = the union of
+// their wires (state bits), padded with the lowest other bits to min(8, L).
+std::vector<Pass> schedule(int L, int G, const int* wires, int maxk)
+{
+	std::vector<Pass> out;
+	const int NB = std::min(MAXNB, L);
+	for (int i = 0; i < G;) {
+		const int K = std::min(maxk, G - i);
+		uint32_t bits = 0;
+		for (int k = 0; k < K; k++) {
+			bits |= 1u << (L - 1 - wires[2 * (i + k)]);
+			bits |= 1u << (L - 1 - wires[2 * (i + k) + 1]);
+		}
+		for (int b = 0; __builtin_popcount(bits) < NB && b < L; b++) bits |= 1u << b;
+		Pass p;
+		memset(&p.geom, 0, sizeof(p.geom));
+		p.first = i;
+		p.K = K;
+		p.geom.K = K;
+		p.geom.NB = NB;
+		p.geom.L = L;
+		int local[32];
+		int n = 0;
+		for (int b = 0; b < L; b++)
+			if ((bits >> b) & 1) { local[b] = n; p.geom.tbit[n++] = b; }
+		for (int k = 0; k < K; k++) {
+			p.geom.gi[k] = local[L - 1 - wires[2 * (i + k)]];
+			p.geom.gj[k] = local[L - 1 - wires[2 * (i + k) + 1]];
+		}
+		const uint32_t all = L >= 32 ? 0xffffffffu : ((1u << L) - 1);
+		p.geom.rest_mask = all & ~bits;
+		out.push_back(p);
+		i += K;
+	}
+	return out;
+}
+
+template <typename T>
+PassGates<T> pass_gates(const Pass& p, const double2* gates, const double2* dirs)
+{
+	PassGates<T> pg;
+	memset(&pg, 0, sizeof(pg));
+	for (int k = 0; k < p.K; k++)
+		for (int e = 0; e < 16; e++) {
+			const double2 g = gates[16 * (p.first + k) + e];
+			pg.g[k].m[e] = mk<T>((T)g.x, (T)g.y);
+			if (dirs) {
+				const double2 z = dirs[16 * (p.first + k) + e];
+				pg.z[k].m[e] = mk<T>((T)z.x, (T)z.y);
+			}
+		}
+	return pg;
+}
+
+template <typename T>
+size_t fwd_smem(int NB)
+{
+	return 32 * MAXK * sizeof(cplx<T>) + (1 << MAXNB) * sizeof(int) + 2 * ((size_t)1 << NB) * ColsPer<T>::v * sizeof(cplx<T>);
+}
+
+template <typename T>
+size_t rev_smem(int NB, int K, bool tan)
+{
+	const size_t A = ((size_t)1 << NB) * ColsPer<T>::v;
+	const size_t tiles = (tan ? 2 * K + 2 : K + 1) * A * sizeof(cplx<T>);
+	const size_t red = std::is_same<T, double>::value ? (size_t)(NTR / 32) * MAXK * NPART3 * sizeof(double)
+	                                                  : (TPB2 / 32) * 4 * MAXK * (tan ? 16 : 8) * sizeof(double);
+	return 32 * MAXK * sizeof(cplx<T>) + (1 << MAXNB) * sizeof(int) + std::max(tiles, red);
+}
+
+template <typename KernelT>
+int prepare(KernelT kernel, size_t smem, int* per_sm, int threads = TPB2)
+{
+	if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+		cudaGetLastError();
+		fprintf(stderr, "rqcopt_gpu: cannot reserve %zu bytes of shared memory\n", smem);
+		return E_CUDA;
+	}
+	int n = 0;
+	if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, threads, smem) != cudaSuccess || n < 1) {
+		cudaGetLastError();
+		n = 1;
+	}
+	*per_sm = n;
+	return OK;
+}
+
+#define RQC_LAUNCH2(RT, CLS, KERNEL, GRID, SMEM, ...)                             \
+	do {                                                                           \
+		cudaEvent_t ev__;                                                          \
+		launch_begin((RT), (CLS), &ev__);                                          \
+		KERNEL<<<(GRID), TPB2, (SMEM), (RT).stream>>>(__VA_ARGS__);                \
+		launch_end((RT), (CLS), ev__);                                             \
+		if (int e__ = RQC_CUDA(cudaGetLastError())) return e__;                    \
+	} while (0)
+
+#define RQC_LAUNCH3(RT, CLS, KERNEL, GRID, NT, SMEM, ...)                         \
+	do {                                                                           \
+		cudaEvent_t ev__;                                                          \
+		launch_begin((RT), (CLS), &ev__);                                          \
+		KERNEL<<<(GRID), (NT), (SMEM), (RT).stream>>>(__VA_ARGS__);                \
+		launch_end((RT), (CLS), ev__);                                             \
+		if (int e__ = RQC_CUDA(cudaGetLastError())) return e__;                    \
+	} while (0)
+
+template <typename T, bool TAN, int IN, int OUT>
+int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* psi_o, cplx<T>* dpsi_o, const cplx<T>* phi,
+               const PassGeom& pg, const PassGates<T>& gates, double2* fpart, int fgrid)
+{
+	const size_t smem = fwd_smem<T>(pg.NB);
+	static int per_sm = 0;
+	if constexpr (std::is_same<T, double>::value) {
+		if (!per_sm) {
+			int ret = prepare(k3_fwd<TAN, IN, OUT>, fwd_smem<T>(MAXNB), &per_sm, NTF);
+			if (ret) return ret;
+		}
+		const int grid = OUT == 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
+		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
+	} else {
+		if (!per_sm) {
+			int ret = prepare(k2_fwd<T, TAN, IN, OUT>, fwd_smem<T>(MAXNB), &per_sm);
+			if (ret) return ret;
+		}
+		const int grid = OUT == 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
+		RQC_LAUNCH2(rt, KC_FUSED, (k2_fwd<T, TAN, IN, OUT>), grid, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
+	}
+	return OK;
+}
+
+template <typename T, bool TAN, bool FIRST, bool LAST>
+int launch_rev(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<T>* phi, const cplx<T>* dphi,
+               cplx<T>* phi_o, cplx<T>* dphi_o, const PassGeom& pg, const PassGates<T>& gates, double* part, int nblk)
+{
+	const size_t smem = rev_smem<T>(pg.NB, pg.K, TAN);
+	static bool ready = false;
+	if constexpr (std::is_same<T, double>::value) {
+		if (!ready) {
+			int per_sm;
+			int ret = prepare(k3_rev<TAN, FIRST, LAST>, rev_smem<T>(MAXNB, MAXK, TAN), &per_sm, NTR);
+			if (ret) return ret;
+			ready = true;
+		}
+		RQC_LAUNCH3(rt, KC_REVERSE, (k3_rev<TAN, FIRST, LAST>), nblk, NTR, smem, psi, dpsi, phi, dphi, phi_o, dphi_o, pg,
+		            gates, part, nblk);
+	} else {
+		if (!ready) {
+			int per_sm;
+			int ret = prepare(k2_rev<T, TAN, FIRST, LAST>, rev_smem<T>(MAXNB, MAXK, TAN), &per_sm);
+			if (ret) return ret;
+			ready = true;
+		}
+		RQC_LAUNCH2(rt, KC_REVERSE, (k2_rev<T, TAN, FIRST, LAST>), nblk, smem, psi, dpsi, phi, dphi, phi_o, dphi_o, pg,
+		            gates, part, nblk);
+	}
+	return OK;
+}
+
+template <typename T, bool TAN>
+int launch_rev_any(Runtime& rt, bool first, bool last, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<T>* phi,
+                   const cplx<T>* dphi, cplx<T>* phi_o, cplx<T>* dphi_o, const PassGeom& pg, const PassGates<T>& gates,
+                   double* part, int nblk)
+{
+	if (first && last) return launch_rev<T, TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
+	if (first) return launch_rev<T, TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
+	if (last) return launch_rev<T, TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
+	return launch_rev<T, TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
+}
+
+// grid of the partial-sum kernels: one resident wave of the reverse kernel
+template <typename T>
+int rev_grid(Runtime& rt, bool tan)
+{
+	int per_sm = 1;
+	const size_t smem = rev_smem<T>(MAXNB, MAXK, tan);
+	int ret;
+	if constexpr (std::is_same<T, double>::value)
+		ret = tan ? prepare(k3_rev<true, false, false>, smem, &per_sm, NTR)
+		          : prepare(k3_rev<false, false, false>, smem, &per_sm, NTR);
+	else
+		ret = tan ? prepare(k2_rev<T, true, false, false>, smem, &per_sm)
+		          : prepare(k2_rev<T, false, false, false>, smem, &per_sm);
+	if (ret) per_sm = 1;
+	return rt.num_sms * per_sm;
+}
+
+size_t workspace_limit2(Runtime& rt)
+{
+	if (rt.workspace_limit) return rt.workspace_limit;
+	size_t free_b = 0, total_b = 0;
+	if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+		cudaGetLastError();
+		return (size_t)1 << 30;
+	}
+	return (size_t)((free_b + rt.work.bytes) * 0.75);
+}
+
+template <typename T>
+int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int maxk, double2* d_out)
+{
+	using V = cplx<T>;
+	constexpr int CW = ColsPer<T>::v;
+	const int L = c.L, G = c.ngates;
+	const int64_t N = (int64_t)1 << L;
+	const bool tan = mode == EVAL_HVP;
+	const bool host_target = t.ufunc != nullptr;
+	std::vector<Pass> passes = schedule(L, G, c.wires, maxk);
+	std::vector<Pass> tpasses = host_target ? std::vector<Pass>() : schedule(L, t.ngates, t.wires, maxk);
+	const int P = (int)passes.size(), Pt = (int)tpasses.size();
+	std::vector<PassGates<T>> pgates(P), tgates(Pt);
+	for (int p = 0; p < P; p++) pgates[p] = pass_gates<T>(passes[p], c.gates, tan ? c.dirs : nullptr);
+	for (int p = 0; p < Pt; p++) tgates[p] = pass_gates<T>(tpasses[p], t.gates, nullptr);
+
+	// states per column: PHI, P0, P1 (+ D0, D1) and the pass checkpoints
+	const int64_t nstates = mode == EVAL_F ? 3 : (mode == EVAL_GRAD ? 3 + (P - 1) : 5 + 2 * (int64_t)(P - 1));
+	const size_t col_bytes = (size_t)nstates * N * sizeof(V);
+	const int64_t C_mem = (int64_t)(workspace_limit2(rt) / col_bytes);
+	int64_t C = C_mem;
+	if (rt.column_chunk > 0) C = std::min<int64_t>(C, ((rt.column_chunk + CW - 1) / CW) * CW);
+	if (host_target) C = std::min<int64_t>(C, std::max<int64_t>(CW, ((int64_t)256 << 20) / (N * 16)));
+	C = std::min<int64_t>(C, ((N + CW - 1) / CW) * CW);
+	C = (C / CW) * CW;
+	if (C < CW || C > C_mem) {
+		fprintf(stderr, "rqcopt_gpu: %d columns need %zu bytes of workspace, more than the limit\n", CW, CW * col_bytes);
+		return E_ALLOC;
+	}
+	int ret = ensure_device(rt.work, (size_t)nstates * C * N * sizeof(V));
+	if (ret) return ret;
+	V* PHI = reinterpret_cast<V*>(rt.work.ptr);
+	V* Pb[2] = { PHI + C * N, PHI + 2 * C * N };
+	V* Db[2] = { tan ? PHI + 3 * C * N : nullptr, tan ? PHI + 4 * C * N : nullptr };
+	V* ck = PHI + (tan ? 5 : 3) * C * N;                             // psi at the input of pass p = 1..P-1
+	V* dck = tan ? ck + (int64_t)(P - 1) * C * N : nullptr;          // dpsi at the input of pass p
+	auto ck_at = [&](int p) { return ck + (int64_t)(p - 1) * C * N; };
+	auto dck_at = [&](int p) { return dck + (int64_t)(p - 1) * C * N; };
+
+	const int nblk = rev_grid<T>(rt, tan);
+	const int nps = std::is_same<T, double>::value ? NPART3 : NPART2;   // partial doubles per gate and block
+	const size_t part_doubles = (size_t)G * nblk * nps + 2 * (size_t)nblk;
+	if ((ret = ensure_device(rt.partials, part_doubles * sizeof(double)))) return ret;
+	double* part = reinterpret_cast<double*>(rt.partials.ptr);
+	double2* fpart = reinterpret_cast<double2*>(part + (size_t)G * nblk * nps);
+	if ((ret = RQC_CUDA(cudaMemsetAsync(part, 0, part_doubles * sizeof(double), rt.stream)))) return ret;
+
+	double2* hcols = nullptr;
+	double2* hbasis = nullptr;
+	double2* dstage = nullptr;
+	if (host_target) {
+		if ((ret = ensure_host_pinned(rt.hpin, (size_t)(C + 1) * N * sizeof(double2)))) return ret;
+		hcols = reinterpret_cast<double2*>(rt.hpin.ptr);
+		hbasis = hcols + C * N;
+		if ((ret = ensure_device(rt.stage[2], (size_t)C * N * sizeof(double2)))) return ret;
+		dstage = reinterpret_cast<double2*>(rt.stage[2].ptr);
+	}
+
+	for (int64_t b0 = 0; b0 < N; b0 += C) {
+		const int64_t Cc = std::min(C, N - b0);
+		const int64_t ncg = (Cc + CW - 1) / CW;
+		auto geom = [&](const Pass& p) {
+			PassGeom g = p.geom;
+			g.C = C;
+			g.ncg = ncg;
+			g.ntiles = ((int64_t)1 << (L - g.NB)) * ncg;
+			g.b0 = b0;
+			return g;
+		};
+
+		// target columns phi = -conj(U e_b)
+		if (host_target) {
+			const linear_func uf = reinterpret_cast<linear_func>(t.ufunc);
+			for (int64_t j = 0; j < Cc; j++) {
+				memset(hbasis, 0, N * sizeof(double2));
+				hbasis[b0 + j].x = 1;
+				statevector e = { reinterpret_cast<numeric*>(hbasis), L };
+				statevector u = { reinterpret_cast<numeric*>(hcols + j * N), L };
+				const int r = uf(&e, t.udata, &u);
+				if (r < 0) {
+					fprintf(stderr, "rqcopt_gpu: call of 'ufunc' failed, return value: %i\n", r);
+					return E_UFUNC;
+				}
+			}
+			if ((ret = RQC_CUDA(cudaMemcpyAsync(dstage, hcols, Cc * N * sizeof(double2), cudaMemcpyHostToDevice, rt.stream))))
+				return ret;
+			k2_target_from_host<T><<<rt.num_sms * 8, 256, 0, rt.stream>>>(dstage, PHI, N, Cc, C);
+			rt.launches++;
+			if ((ret = RQC_CUDA(cudaGetLastError()))) return ret;
+			if ((ret = RQC_CUDA(cudaStreamSynchronize(rt.stream)))) return ret;
+		} else {
+			for (int p = 0; p < Pt; p++) {
+				const PassGeom g = geom(tpasses[p]);
+				const bool first = p == 0, last = p == Pt - 1;
+				const V* in = first ? nullptr : Pb[(p - 1) & 1];
+				V* out = last ? PHI : Pb[p & 1];
+				if (first && last) ret = launch_fwd<T, false, 1, 1>(rt, in, nullptr, out, nullptr, nullptr, g, tgates[p], nullptr, 0);
+				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, nullptr, g, tgates[p], nullptr, 0);
+				else if (last) ret = launch_fwd<T, false, 0, 1>(rt, in, nullptr, out, nullptr, nullptr, g, tgates[p], nullptr, 0);
+				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, nullptr, g, tgates[p], nullptr, 0);
+				if (ret) return ret;
+			}
+		}
+
+		// forward passes
+		for (int p = 0; p < P; p++) {
+			const PassGeom g = geom(passes[p]);
+			const bool first = p == 0, last = p == P - 1;
+			if (mode == EVAL_F) {
+				const V* in = first ? nullptr : Pb[(p - 1) & 1];
+				V* out = last ? nullptr : Pb[p & 1];
+				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+			} else if (!tan) {
+				const V* in = first ? nullptr : ck_at(p);
+				V* out = last ? nullptr : ck_at(p + 1);
+				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+			} else {
+				const V* in = first ? nullptr : ck_at(p);
+				const V* din = first ? nullptr : dck_at(p);
+				V* out = last ? nullptr : ck_at(p + 1);
+				V* dout = last ? nullptr : dck_at(p + 1);
+				if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
+				else if (first) ret = launch_fwd<T, true, 1, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
+				else if (last) ret = launch_fwd<T, true, 0, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
+				else ret = launch_fwd<T, true, 0, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
+			}
+			if (ret) return ret;
+		}
+		if (mode == EVAL_F) continue;
+
+		// reverse passes
+		for (int p = P - 1; p >= 0; p--) {
+			const PassGeom g = geom(passes[p]);
+			const bool first = p == P - 1, last = p == 0;
+			const int cur = (P - 1 - p) & 1, nxt = cur ^ 1;
+			const V* ph = first ? PHI : Pb[cur];
+			const V* dph = (first || !tan) ? nullptr : Db[cur];
+			double* pp = part + (size_t)passes[p].first * nblk * nps;
+			if (tan)
+				ret = launch_rev_any<T, true>(rt, first, last, last ? nullptr : ck_at(p), last ? nullptr : dck_at(p), ph, dph,
+				                              last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pp, nblk);
+			else
+				ret = launch_rev_any<T, false>(rt, first, last, last ? nullptr : ck_at(p), nullptr, ph, nullptr,
+				                               last ? nullptr : Pb[nxt], nullptr, g, pgates[p], pp, nblk);
+			if (ret) return ret;
+		}
+	}
+
+	if (std::is_same<T, double>::value)
+		k3_reduce<<<G + 1, NPART3, 0, rt.stream>>>(part, G, nblk, fpart, nblk, tan ? 1 : 0, d_out);
+	else
+		k2_reduce<<<G + 1, 64, 0, rt.stream>>>(part, G, nblk, fpart, nblk, tan ? 1 : 0, d_out);
+	rt.launches++;
+	return RQC_CUDA(cudaGetLastError());
+}
+
+}  // namespace
+
+int evaluate_fused(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, int maxk, double2* d_out)
+{
+	maxk = std::max(1, std::min(MAXK, maxk));
+	int ret;
+	if ((ret = RQC_CUDA(cudaMemsetAsync(d_out, 0, result_count(c.ngates) * sizeof(double2), rt.stream)))) return ret;
+	if (mode != EVAL_GRAD && mode != EVAL_HVP) mode = EVAL_F;
+	if (precision == PREC_C128) return evaluate_fused_t<double>(rt, c, t, mode, maxk, d_out);
+	return evaluate_fused_t<float>(rt, c, t, mode, maxk, d_out);
+}
+
+}  // namespace rqc

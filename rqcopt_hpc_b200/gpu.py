@@ -85,6 +85,7 @@ _SIGS = {
     "rqcopt_gpu_set_workspace_limit": (None, [C.c_size_t]),
     "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
     "rqcopt_gpu_last_error": (I, []),
+    "rqcopt_gpu_set_gates_per_pass": (I, [I]),
     "rqcopt_gpu_launch_count": (C.c_ulonglong, []),
     "rqcopt_gpu_reset_launch_count": (None, []),
     "rqcopt_gpu_enable_kernel_timing": (None, [I]),
@@ -486,6 +487,10 @@ def inverse_matrix(a):
 
 def set_precision(mode: int):
     _check("rqcopt_gpu_set_precision", lib().rqcopt_gpu_set_precision(mode))
+
+
+def set_gates_per_pass(k: int):
+    _check("rqcopt_gpu_set_gates_per_pass", lib().rqcopt_gpu_set_gates_per_pass(k))
 
 
 def set_column_chunk(cols: int):

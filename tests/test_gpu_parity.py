@@ -126,3 +126,48 @@ def test_forward_adjoint_round_trip(gpu):
     back = gpu.apply_quantum_circuit(np.conj(np.transpose(gates[::-1], (0, 2, 1))), wires[::-1], out)
     assert np.max(np.abs(back - psi)) <= 1e-12
     assert abs(np.linalg.norm(out) - 1) <= 1e-12
+
+
+@pytest.mark.parametrize("L,depth", [(4, 3), (6, 5), (9, 4), (12, 5)])
+@pytest.mark.parametrize("per_pass", [2, 3, 4])
+def test_fused_passes_match_per_gate_engine(gpu, L, depth, per_pass):
+    """Fused passes of 2-4 gates against one kernel per gate: f, gradient and HVP
+    to 1e-12 for brickwalls of even and odd size (odd L: general circuit)."""
+    rng = np.random.default_rng(1000 + L)
+    if L % 2 == 0:
+        vlist, perms, tvlist, tperms = brickwall_instance(L, depth, 40 + L, 3, 50 + L)
+        vdirs = _dirs(vlist, 60 + L)
+        t = gpu.Target(brickwall=(tvlist, tperms))
+        run = lambda: gpu.brickwall_unitary_target_projected_hessian_vector_product(t, vlist, vdirs, perms, L)
+    else:
+        G = 3 * depth
+        gates = np.stack([haar_unitary(rng) for _ in range(G)])
+        wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+        dirs = 0.3 * crandn((G, 4, 4), rng)
+        tg = np.stack([haar_unitary(rng) for _ in range(6)])
+        tw = np.array([rng.choice(L, 2, replace=False) for _ in range(6)], np.int32)
+        t = gpu.Target(circuit=(tg, tw))
+        run = lambda: gpu.circuit_unitary_target_hessian_vector_product(t, gates, dirs, wires, L)
+    gpu.set_gates_per_pass(1)
+    ref = run()
+    gpu.set_gates_per_pass(per_pass)
+    got = run()
+    gpu.set_gates_per_pass(4)
+    for a, b in zip(got, ref):
+        assert rel_err(a, b) <= 1e-12
+
+
+@pytest.mark.parametrize("mode", ["f", "grad"])
+def test_fused_f_and_gradient_modes(gpu, oracle, mode):
+    L = 8
+    vlist, perms, tvlist, tperms = brickwall_instance(L, 5, 70, 3, 71)
+    t = gpu.Target(brickwall=(tvlist, tperms))
+    to = oracle.target("brickwall", (tvlist, tperms))
+    if mode == "f":
+        a, b = gpu.brickwall_unitary_target(t, vlist, perms, L), oracle.brickwall_unitary_target(to, vlist, perms, L)
+        assert abs(a - b) <= 1e-12 * abs(b)
+    else:
+        fa, ga = gpu.brickwall_unitary_target_and_gradient(t, vlist, perms, L)
+        fb, gb = oracle.brickwall_unitary_target_and_gradient(to, vlist, perms, L)
+        assert abs(fa - fb) <= 1e-12 * abs(fb)
+        assert rel_err(ga, gb) <= 1e-12
