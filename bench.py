@@ -174,6 +174,55 @@ def cpu_baseline(L, depth, tdepth, seconds=15.0, cores=None):
                       f"{wall:.1f} s wall; evals/s = sampled fraction / wall time"}
 
 
+# ----------------------------------------------------------------------------- gate throughput
+
+def gate_throughput(gpu, torch, L=28, G=256, seed=20):
+    """Forward through G Haar gates on uniformly random distinct qubit pairs, then the
+    adjoint gates in reverse order, on one L-qubit complex128 state resident in HBM,
+    with 1 and with 4 gates per HBM round trip; DRAM GB/s counts one read and one write
+    of the state per round trip."""
+    rng = np.random.default_rng(seed)
+    gates = np.stack([haar(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    adj = np.ascontiguousarray(np.conj(np.transpose(gates[::-1], (0, 2, 1))))
+    wires_rev = np.ascontiguousarray(wires[::-1])
+    gen = torch.Generator(device="cuda").manual_seed(seed)
+    psi = torch.randn(1 << L, dtype=torch.complex128, device="cuda", generator=gen)
+    psi /= torch.linalg.vector_norm(psi)
+    out, back = torch.empty_like(psi), torch.empty_like(psi)
+    lib = gpu.lib()
+    from rqcopt_hpc_b200.abi import Statevector
+    import ctypes
+    sv = lambda t: ctypes.byref(Statevector(t.data_ptr(), L))
+    stream = torch.cuda.ExternalStream(lib.rqcopt_gpu_stream())
+    state_bytes = (1 << L) * 16
+    res = {"workload": f"one L={L} complex128 state ({state_bytes / 2**30:.0f} GiB), {G} Haar gates on random "
+                       f"distinct pairs, forward then adjoint backward"}
+    for gpp in (1, 4):
+        gpu.set_gates_per_pass(gpp)
+        lib.apply_quantum_circuit(gates.ctypes.data, G, wires.ctypes.data, sv(psi), sv(out))   # warm-up
+        torch.cuda.synchronize()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record(stream)
+        lib.apply_quantum_circuit(gates.ctypes.data, G, wires.ctypes.data, sv(psi), sv(out))
+        e[1].record(stream)
+        lib.apply_quantum_circuit(adj.ctypes.data, G, wires_rev.ctypes.data, sv(out), sv(back))
+        e[2].record(stream)
+        torch.cuda.synchronize()
+        t_f, t_b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+        trips = G if gpp == 1 else -(-G // gpp)
+        err = float(torch.max(torch.abs(back - psi)))
+        res[f"gates_per_round_trip_{gpp}"] = {
+            "forward_ms": t_f, "backward_ms": t_b, "round_trips": trips,
+            "dram_gbs": 2 * trips * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
+            "gate_equivalent_gbs": 2 * G * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
+            "recovery_max_abs_err": err}
+    gpu.set_gates_per_pass(4)
+    del psi, out, back
+    torch.cuda.empty_cache()
+    return res
+
+
 # ----------------------------------------------------------------------------- main
 
 def main():
@@ -189,6 +238,7 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--gates-per-pass", type=int, default=4, help="gates fused per HBM round trip (1-4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-gate-throughput", action="store_true")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -318,6 +368,8 @@ def main():
             "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
             "clocks": clk.summary(), "gpu_launches": int(launches),
         }
+        if not a.no_gate_throughput:
+            line["gate_throughput"] = gate_throughput(gpu, torch)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)
         print(json.dumps(line))

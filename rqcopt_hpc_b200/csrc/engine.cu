@@ -613,6 +613,8 @@ int gate_apply_device(Runtime& rt, int L, const double2* gate, int i, int j, con
 int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const double2* d_in,
                          double2* d_out, long ncols)
 {
+	if (ncols == 1 && rt.gates_per_pass > 1 && L >= 10)
+		return apply_circuit_fused_device(rt, L, ngates, gates, wires, d_in, d_out, rt.gates_per_pass);
 	// ping-pong between d_out and one scratch buffer so that the last gate writes d_out
 	const size_t bytes = (size_t)ncols * ((size_t)1 << L) * sizeof(double2);
 	int ret;

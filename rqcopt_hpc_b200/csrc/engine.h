@@ -44,6 +44,11 @@ int evaluate(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, i
 int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
                          const double2* d_in, double2* d_out, long ncols);
 
+// Same for one statevector with up to maxk consecutive gates per HBM round trip
+// (shared-memory tiles over the gates' qubits plus the lowest amplitude bits).
+int apply_circuit_fused_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
+                               const double2* d_in, double2* d_out, int maxk);
+
 // Single-gate kernels on device statevectors (ncols states one after another).
 int gate_apply_device(Runtime& rt, int L, const double2* gate, int i, int j,
                       const double2* d_in, double2* d_out, long ncols);

@@ -171,3 +171,21 @@ def test_fused_f_and_gradient_modes(gpu, oracle, mode):
         fb, gb = oracle.brickwall_unitary_target_and_gradient(to, vlist, perms, L)
         assert abs(fa - fb) <= 1e-12 * abs(fb)
         assert rel_err(ga, gb) <= 1e-12
+
+
+@pytest.mark.parametrize("per_pass", [1, 2, 4])
+def test_single_state_fused_passes(gpu, oracle, per_pass):
+    """apply_quantum_circuit on one L=14 state with 1-4 gates per round trip (random
+    pairs, adjacent and wrapped, either order) against the oracle to 1e-12."""
+    L, G = 14, 23
+    rng = np.random.default_rng(77)
+    psi = crandn(1 << L, rng)
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    wires[0] = (L - 1, L - 2)
+    wires[1] = (0, L - 1)
+    gpu.set_gates_per_pass(per_pass)
+    out = gpu.apply_quantum_circuit(gates, wires, psi)
+    gpu.set_gates_per_pass(4)
+    ref = oracle.apply_quantum_circuit(gates, wires, psi)
+    assert rel_err(out, ref) <= 1e-12
