@@ -836,6 +836,579 @@ __global__ void k3_reduce(const double* __restrict__ part, int nslots, int nblk,
 	}
 }
 
+// ------------------------------------------------------------------------------ complex64 kernels on TF32 MMAs
+
+// complex64 passes on the tensor cores: every product of the passes is a
+// mma.sync m16n8k8 with TF32 inputs, split three ways (a = big + small, both
+// TF32; a*b = big*big + big*small + small*big), which keeps FP32 accuracy.
+//   outputs       (16 groups x 8 components) * (8 x 8 embedding of G, G^T, Z or Z^T);
+//   outer sums    [P; dP]^T (16 components x 8 groups) * X (8 groups x 8 components)
+//                 plus [0; P]^T * dX into the same accumulator: rows 0-7 give dG,
+//                 rows 8-15 give HZ (raw real 8x8 blocks).
+// Tiles hold 256 rows x 8 complex64 columns (64-byte runs), rows swizzled as in the
+// complex128 kernels.  The FP32 MMA accumulators are added every few tiles into FP64
+// per-lane sums in global scratch (resident in L2) and reduced in FP64.
+
+constexpr int NT4 = 512;
+constexpr int CW4 = 8;
+constexpr int NRAW4 = 128;      // raw partial sums per gate and block: lane*4 + v
+constexpr int FLUSH4 = 4;       // tiles between FP32 -> FP64 flushes
+
+// x = big + small: big is x rounded to the 10 explicit mantissa bits of TF32
+// (round half away from zero on the bit pattern), small = x - big exactly; the
+// tensor core reads small truncated, an error below 2^-22 |x|.
+__device__ __forceinline__ void tf32_split(float x, uint32_t& big, uint32_t& small)
+{
+	big = (__float_as_uint(x) + 0x1000u) & 0xffffe000u;
+	small = __float_as_uint(x - __uint_as_float(big));
+}
+
+__device__ __forceinline__ void split4(const float a[4], uint32_t ab[4], uint32_t as[4])
+{
+#pragma unroll
+	for (int i = 0; i < 4; i++) tf32_split(a[i], ab[i], as[i]);
+}
+
+__device__ __forceinline__ void mma_tf32(float c[4], const uint32_t a[4], const uint32_t b[2])
+{
+	asm("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+	             : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+	             : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// c += a * b with 3xTF32 on split operands (a = ab + as, b = bb + bs)
+__device__ __forceinline__ void mma3(float c[4], const uint32_t ab[4], const uint32_t as[4], const uint32_t bb[2],
+                                     const uint32_t bs[2])
+{
+	mma_tf32(c, as, bb);
+	mma_tf32(c, ab, bs);
+	mma_tf32(c, ab, bb);
+}
+
+// B fragment (rows t, t+4; column g) of the embedding of the complex 4x4 matrix m (float2 smem)
+__device__ __forceinline__ void bfrag4(const float2* m, bool tr, int lane, uint32_t bb[2], uint32_t bs[2])
+{
+	const int t = lane & 3, g = lane >> 2;
+#pragma unroll
+	for (int h = 0; h < 2; h++) {
+		const int rowk = t + 4 * h, coln = g;
+		const int r = rowk >> 1, a = rowk & 1, c = coln >> 1, b = coln & 1;
+		const float2 v = tr ? m[4 * c + r] : m[4 * r + c];
+		const float x = a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
+		tf32_split(x, bb[h], bs[h]);
+	}
+}
+
+// Float index of (row, column cc, part) in a swizzled complex64 tile of 8 columns is
+// 16 prow(row) + 2 cc + part.  prow(r) = r ^ (parity of r >> 1), so for disjoint bit
+// sets 16 prow(x | y) = roff(x) ^ roff(y): every operand address of a gate step is the
+// unit's base offset XOR a per-lane offset fixed for the gate.
+__device__ __forceinline__ int roff(int x) { return (x ^ (__popc(x >> 1) & 1)) << 4; }
+
+struct Lane4
+{
+	int lo, hi;
+	int E0;              // offset of the unit's second set of groups (b6 odd)
+	int LA, LB, LS, LO;  // lane offsets: output operand k-steps 0 / 1, output store, outer-product operand
+	__device__ __forceinline__ Lane4(int bi, int bj, int lane)
+	{
+		const int g = lane >> 2, t = lane & 3;
+		lo = bi < bj ? bi : bj;
+		hi = bi < bj ? bj : bi;
+		E0 = roff(insert2(1, lo, hi));
+		LA = roff(mbits(t >> 1, bi, bj)) | (2 * g + (t & 1));
+		LB = roff(mbits(2 + (t >> 1), bi, bj)) | (2 * g + (t & 1));
+		LS = roff(mbits(t, bi, bj)) | (2 * g);
+		LO = roff(mbits(g >> 1, bi, bj)) | (2 * t + (g & 1));
+	}
+	// base offset of unit u (groups b6 = 2u, 2u + 1): roff(insert2(2u)), whose parity is popc(u)
+	__device__ __forceinline__ int unit_base(int u) const
+	{
+		const int b = insert2(2 * u, lo, hi);
+		return (b ^ ((__popc(u) ^ b) & 1)) << 4;
+	}
+};
+
+// out = in * Bg (dout = din * Bg + in * Bz) for the 16 groups of the unit at base offset B0
+// (b6 = 2u, 2u+1; cc = 0..7)
+template <bool TAN>
+__device__ __forceinline__ void apply_unit4(const float* in, const float* din, float* out, float* dout, int B0,
+                                           const Lane4& ln, const uint32_t gb[2], const uint32_t gs[2],
+                                           const uint32_t zb[2], const uint32_t zs[2], bool dzero, bool inplace)
+{
+	const int B1 = B0 ^ ln.E0;
+	const int i0 = B0 ^ ln.LA, i1 = B1 ^ ln.LA, i2 = B0 ^ ln.LB, i3 = B1 ^ ln.LB;
+	const float a[4] = { in[i0], in[i1], in[i2], in[i3] };
+	uint32_t ab[4], as[4];
+	split4(a, ab, as);
+	float y[4] = {0, 0, 0, 0}, z[4] = {0, 0, 0, 0};
+	mma3(y, ab, as, gb, gs);
+	if (TAN) {
+		mma3(z, ab, as, zb, zs);
+		if (!dzero) {
+			const float da[4] = { din[i0], din[i1], din[i2], din[i3] };
+			split4(da, ab, as);
+			mma3(z, ab, as, gb, gs);
+		}
+	}
+	if (inplace) __syncwarp();
+	const int s0 = B0 ^ ln.LS, s1 = B1 ^ ln.LS;
+	*reinterpret_cast<float2*>(out + s0) = make_float2(y[0], y[1]);
+	*reinterpret_cast<float2*>(out + s1) = make_float2(y[2], y[3]);
+	if (TAN) {
+		*reinterpret_cast<float2*>(dout + s0) = make_float2(z[0], z[1]);
+		*reinterpret_cast<float2*>(dout + s1) = make_float2(z[2], z[3]);
+	}
+}
+
+// apply_unit4 with the lane offsets passed explicitly (kept in registers by the caller)
+template <bool TAN>
+__device__ __forceinline__ void apply_unit4o(const float* in, const float* din, float* out, float* dout, int B0, int E0,
+                                            int LA, int LB, int LS, const uint32_t gb[2], const uint32_t gs[2],
+                                            const uint32_t zb[2], const uint32_t zs[2], bool dzero, bool inplace)
+{
+	const int B1 = B0 ^ E0;
+	const int i0 = B0 ^ LA, i1 = B1 ^ LA, i2 = B0 ^ LB, i3 = B1 ^ LB;
+	const float a[4] = { in[i0], in[i1], in[i2], in[i3] };
+	uint32_t ab[4], as[4];
+	split4(a, ab, as);
+	float y[4] = {0, 0, 0, 0}, z[4] = {0, 0, 0, 0};
+	mma3(y, ab, as, gb, gs);
+	if (TAN) {
+		mma3(z, ab, as, zb, zs);
+		if (!dzero) {
+			const float da[4] = { din[i0], din[i1], din[i2], din[i3] };
+			split4(da, ab, as);
+			mma3(z, ab, as, gb, gs);
+		}
+	}
+	if (inplace) __syncwarp();
+	const int s0 = B0 ^ LS, s1 = B1 ^ LS;
+	*reinterpret_cast<float2*>(out + s0) = make_float2(y[0], y[1]);
+	*reinterpret_cast<float2*>(out + s1) = make_float2(y[2], y[3]);
+	if (TAN) {
+		*reinterpret_cast<float2*>(dout + s0) = make_float2(z[0], z[1]);
+		*reinterpret_cast<float2*>(dout + s1) = make_float2(z[2], z[3]);
+	}
+}
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+constexpr int NT4F = 256;   // threads of the complex64 forward kernel (two blocks per SM)
+constexpr int NT4R = 256;   // threads of the complex64 reverse kernel
+constexpr int UPW4 = (1 << MAXNB) / 8 / (NT4R / 32); // units per warp and gate step (full tiles)
+static_assert(NT4F == NT4R, "the unit tables assume equal block sizes");
+
+constexpr int AMAX4 = (1 << MAXNB) * CW4;   // tile stride (complex64 elements) of the complex64 kernels
+
+// shared memory of k4_fwd: gates and two sets of tiles (state[, tangent][, phi])
+inline size_t k4_fwd_smem(int NB, bool tan, bool with_phi)
+{
+	(void)NB;
+	const size_t A = AMAX4;
+	const int ns = (tan ? 2 : 1) + (with_phi ? 1 : 0);
+	return 32 * MAXK * sizeof(float2) + 2 * ns * A * sizeof(float2);
+}
+
+// Forward pass (complex64).  Same contract as k2_fwd.  The next tile streams into a
+// second set of shared-memory buffers with cp.async while the current one is processed.
+template <bool TAN, int IN, int OUT>
+__global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+                                                 float2* __restrict__ psi_o, float2* __restrict__ dpsi_o,
+                                                 const float2* __restrict__ phi, PassGeom pg, PassGates<float> gates,
+                                                 double2* __restrict__ fpart)
+{
+	constexpr int NS = (TAN ? 2 : 1) + (OUT == 2 ? 1 : 0);
+	constexpr int CPT = (1 << MAXNB) * 4 / NT4F;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, K = pg.K;
+	float2* sg = reinterpret_cast<float2*>(smem_raw);
+	float2* tiles = sg + 32 * MAXK;
+	auto stage = [&](int buf, int st) { return tiles + (buf * NS + st) * AMAX4; };
+	gates_to_smem<float>(gates, K, TAN, sg);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const int units = R / 8;
+	int ro[CPT];
+#pragma unroll
+	for (int i = 0; i < CPT; i++) {
+		const int r = (threadIdx.x + i * NT4F) >> 2;
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		ro[i] = o;
+	}
+	int E0[MAXK], LA[MAXK], LB[MAXK], LS[MAXK], LO[MAXK], HI[MAXK];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) {
+		const Lane4 ln(pg.gi[k < K ? k : 0], pg.gj[k < K ? k : 0], lane);
+		E0[k] = ln.E0;
+		LA[k] = ln.LA;
+		LB[k] = ln.LB;
+		LS[k] = ln.LS;
+		LO[k] = ln.lo;
+		HI[k] = ln.hi;
+	}
+	double fx = 0, fy = 0;
+	auto fetch = [&](int64_t tile, int buf) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT; i++) {
+			const int e = threadIdx.x + i * NT4F;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			if (IN == 0) {
+				cp_async16(stage(buf, 0) + pe, psi + a);
+				if (TAN) cp_async16(stage(buf, 1) + pe, dpsi + a);
+			} else {
+				const int64_t row = rowbase + ro[i], col = colbase + c2i;
+				*reinterpret_cast<float4*>(stage(buf, 0) + pe) =
+				    make_float4(row == pg.b0 + col ? 1.f : 0.f, 0.f, row == pg.b0 + col + 1 ? 1.f : 0.f, 0.f);
+				if (TAN) *reinterpret_cast<float4*>(stage(buf, 1) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+			}
+			if (OUT == 2) cp_async16(stage(buf, NS - 1) + pe, phi + a);
+		}
+		cp_async_commit();
+	};
+	__syncthreads();
+	if (blockIdx.x < pg.ntiles) fetch(blockIdx.x, 0);
+	int buf = 0;
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x, buf ^= 1) {
+		cp_async_wait_all();
+		__syncthreads();
+		if (tile + gridDim.x < pg.ntiles) fetch(tile + gridDim.x, buf ^ 1);
+		float* S = reinterpret_cast<float*>(stage(buf, 0));
+		float* dS = TAN ? reinterpret_cast<float*>(stage(buf, 1)) : nullptr;
+#pragma unroll
+		for (int k = 0; k < MAXK; k++) {
+			if (k >= K) break;
+			uint32_t gb[2], gs[2], zb[2] = {0, 0}, zs[2] = {0, 0};
+			bfrag4(sg + 32 * k, true, lane, gb, gs);
+			if (TAN) bfrag4(sg + 32 * k + 16, true, lane, zb, zs);
+#pragma unroll 2
+			for (int j = 0; j < UPW4; j++) {
+				const int u = warp + j * nwarps;
+				if (u >= units) break;
+				const int b = insert2(2 * u, LO[k], HI[k]);
+				const int B0 = (b ^ ((__popc(u) ^ b) & 1)) << 4;
+				apply_unit4o<TAN>(S, dS, S, dS, B0, E0[k], LA[k], LB[k], LS[k], gb, gs, zb, zs, IN == 1 && k == 0, true);
+			}
+			__syncthreads();
+		}
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT; i++) {
+			const int e = threadIdx.x + i * NT4F;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			const float4 v = *reinterpret_cast<const float4*>(stage(buf, 0) + pe);
+			if (OUT == 2) {
+				const float4 p = *reinterpret_cast<const float4*>(stage(buf, NS - 1) + pe);
+				fx += (double)p.x * v.x - (double)p.y * v.y + (double)p.z * v.z - (double)p.w * v.w;
+				fy += (double)p.x * v.y + (double)p.y * v.x + (double)p.z * v.w + (double)p.w * v.z;
+			} else if (OUT == 1) {
+				*reinterpret_cast<float4*>(psi_o + a) = make_float4(-v.x, v.y, -v.z, v.w);
+			} else {
+				*reinterpret_cast<float4*>(psi_o + a) = v;
+				if (TAN) *reinterpret_cast<float4*>(dpsi_o + a) = *reinterpret_cast<const float4*>(stage(buf, 1) + pe);
+			}
+		}
+	}
+	if (OUT == 2) {
+		__shared__ double red[2][NT4F / 32];
+		fx = warp_sum(fx);
+		fy = warp_sum(fy);
+		if (lane == 0) { red[0][warp] = fx; red[1][warp] = fy; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double sx = 0, sy = 0;
+			for (int w = 0; w < nwarps; w++) { sx += red[0][w]; sy += red[1][w]; }
+			fpart[blockIdx.x].x += sx;
+			fpart[blockIdx.x].y += sy;
+		}
+	}
+}
+
+// shared memory of k4_rev: gates, two sets of staged input tiles (psi, phi[, dpsi, dphi])
+// and the K-1 recomputed intermediate states (and their tangents)
+inline size_t k4_rev_smem(int NB, int K, bool tan)
+{
+	(void)NB;
+	(void)K;
+	const int ns = tan ? 4 : 2;
+	return 32 * MAXK * sizeof(float2) + (2 * ns + (tan ? 2 : 1) * (MAXK - 1)) * (size_t)AMAX4 * sizeof(float2);
+}
+
+
+// Reverse pass (complex64).  Same contract as k2_rev; partials are raw sums
+// (part + k * nblk * NRAW4 + blockIdx.x * NRAW4 + lane * 4 + v).
+// scratch: per-block FP64 lane sums, blockIdx.x * (NT4R/32 * 32 * MAXK * 4) doubles.
+// The next tile's inputs stream into a second set of shared-memory buffers with
+// cp.async while the current tile is processed.  Lane offsets, unit bases and the
+// split gate fragments of every gate of the pass stay in registers for the whole launch.
+template <bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT4R, 1) k4_rev(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+                                                  const float2* __restrict__ phi, const float2* __restrict__ dphi,
+                                                  float2* __restrict__ phi_o, float2* __restrict__ dphi_o, PassGeom pg,
+                                                  PassGates<float> gates, double* __restrict__ part, int nblk,
+                                                  double* __restrict__ scratch)
+{
+	constexpr int NS = TAN ? 4 : 2;            // staged streams: psi, phi, dpsi, dphi
+	constexpr int CPT = (1 << MAXNB) * 4 / NT4R; // 16-byte chunks per thread and stream
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, K = pg.K;
+	float2* sg = reinterpret_cast<float2*>(smem_raw);
+	float2* tiles = sg + 32 * MAXK;
+	auto stage = [&](int buf, int st) { return tiles + (buf * NS + st) * AMAX4; };
+	float2* Mid = tiles + 2 * NS * AMAX4;                        // Psi[1..K-1]
+	float2* dMid = TAN ? Mid + (MAXK - 1) * AMAX4 : nullptr;     // dPsi[1..K-1]
+	gates_to_smem<float>(gates, K, TAN, sg);
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const int units = R / 8;
+	// chunks of this thread: row r = e >> 2, columns 2(e & 3), 2(e & 3) + 1
+	int ro[CPT];
+#pragma unroll
+	for (int i = 0; i < CPT; i++) {
+		const int r = (threadIdx.x + i * NT4R) >> 2;
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		ro[i] = o;
+	}
+	__syncthreads();
+	// per-gate constants
+	int E0[MAXK], LA[MAXK], LB[MAXK], LS[MAXK], LO[MAXK], GL[MAXK], GH[MAXK];
+	uint32_t rgb[MAXK][2], rgs[MAXK][2], rzb[MAXK][2], rzs[MAXK][2];   // G, Z (reverse)
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) {
+		const int kk = k < K ? k : 0;
+		const Lane4 ln(pg.gi[kk], pg.gj[kk], lane);
+		E0[k] = ln.E0;
+		LA[k] = ln.LA;
+		LB[k] = ln.LB;
+		LS[k] = ln.LS;
+		LO[k] = ln.LO;
+		GL[k] = ln.lo;
+		GH[k] = ln.hi;
+		rzb[k][0] = rzb[k][1] = rzs[k][0] = rzs[k][1] = 0;
+		bfrag4(sg + 32 * kk, false, lane, rgb[k], rgs[k]);
+		if (TAN) bfrag4(sg + 32 * kk + 16, false, lane, rzb[k], rzs[k]);
+	}
+	double* scr = scratch + ((size_t)blockIdx.x * nwarps + warp) * 32 * MAXK * 4 + (size_t)lane * MAXK * 4;
+#pragma unroll
+	for (int v = 0; v < MAXK * 4; v++) scr[v] = 0;
+	// outer sums: cx = [P; dP]^T X (rows 0-7 dG, rows 8-15 dP^T X), cd = [P; dP]^T dX (rows 0-7 P^T dX)
+	float cx[MAXK][4], cd[MAXK][4];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++)
+#pragma unroll
+		for (int v = 0; v < 4; v++) { cx[k][v] = 0; cd[k][v] = 0; }
+	auto flush = [&]() {
+#pragma unroll
+		for (int k = 0; k < MAXK; k++) {
+			scr[k * 4 + 0] += (double)cx[k][0];
+			scr[k * 4 + 1] += (double)cx[k][1];
+			scr[k * 4 + 2] += (double)cx[k][2] + (double)cd[k][0];
+			scr[k * 4 + 3] += (double)cx[k][3] + (double)cd[k][1];
+#pragma unroll
+			for (int v = 0; v < 4; v++) { cx[k][v] = 0; cd[k][v] = 0; }
+		}
+	};
+	// stage the inputs of tile `tile` into buffer set `buf`
+	auto fetch = [&](int64_t tile, int buf) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT; i++) {
+			const int e = threadIdx.x + i * NT4R;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			if (LAST) {
+				const int64_t row = rowbase + ro[i], col = colbase + c2i;
+				*reinterpret_cast<float4*>(stage(buf, 0) + pe) =
+				    make_float4(row == pg.b0 + col ? 1.f : 0.f, 0.f, row == pg.b0 + col + 1 ? 1.f : 0.f, 0.f);
+				if (TAN) *reinterpret_cast<float4*>(stage(buf, 2) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+			} else {
+				cp_async16(stage(buf, 0) + pe, psi + a);
+				if (TAN) cp_async16(stage(buf, 2) + pe, dpsi + a);
+			}
+			cp_async16(stage(buf, 1) + pe, phi + a);
+			if (TAN) {
+				if (FIRST)
+					*reinterpret_cast<float4*>(stage(buf, 3) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+				else
+					cp_async16(stage(buf, 3) + pe, dphi + a);
+			}
+		}
+		cp_async_commit();
+	};
+	if (blockIdx.x < pg.ntiles) fetch(blockIdx.x, 0);
+	int ntile = 0, buf = 0;
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x, buf ^= 1) {
+		cp_async_wait_all();
+		__syncthreads();
+		if (tile + gridDim.x < pg.ntiles) fetch(tile + gridDim.x, buf ^ 1);
+		float2* Psi0 = stage(buf, 0);
+		float2* Phi = stage(buf, 1);
+		float2* dPsi0 = TAN ? stage(buf, 2) : nullptr;
+		float2* dPhi = TAN ? stage(buf, 3) : nullptr;
+		auto psi_at = [&](int k) { return k == 0 ? Psi0 : Mid + (k - 1) * AMAX4; };
+		auto dpsi_at = [&](int k) { return k == 0 ? dPsi0 : dMid + (k - 1) * AMAX4; };
+		// recompute the states entering gates 1..K-1
+#pragma unroll
+		for (int k = 0; k < MAXK - 1; k++) {
+			if (k + 1 >= K) break;
+			const float* in = reinterpret_cast<const float*>(psi_at(k));
+			const float* din = TAN ? reinterpret_cast<const float*>(dpsi_at(k)) : nullptr;
+			float* out = reinterpret_cast<float*>(psi_at(k + 1));
+			float* dout = TAN ? reinterpret_cast<float*>(dpsi_at(k + 1)) : nullptr;
+			uint32_t fgb[2], fgs[2], fzb[2] = {0, 0}, fzs[2] = {0, 0};   // G^T, Z^T
+			bfrag4(sg + 32 * k, true, lane, fgb, fgs);
+			if (TAN) bfrag4(sg + 32 * k + 16, true, lane, fzb, fzs);
+#pragma unroll 2
+			for (int j = 0; j < UPW4; j++) {
+				const int u = warp + j * nwarps;
+				if (u >= units) break;
+				const int b = insert2(2 * u, GL[k], GH[k]);
+				apply_unit4o<TAN>(in, din, out, dout, (b ^ ((__popc(u) ^ b) & 1)) << 4, E0[k], LA[k], LB[k], LS[k], fgb,
+				                  fgs, fzb, fzs, LAST && k == 0, false);
+			}
+			__syncthreads();
+		}
+		// reverse through the pass
+		const float* P = reinterpret_cast<const float*>(Phi);
+		const float* dP = TAN ? reinterpret_cast<const float*>(dPhi) : nullptr;
+#pragma unroll
+		for (int k = MAXK - 1; k >= 0; k--) {
+			if (k >= K) continue;
+			const bool first_gate = FIRST && k == K - 1;
+			const bool last_gate = LAST && k == 0;
+			const float* X = reinterpret_cast<const float*>(psi_at(k));
+			const float* dX = TAN ? reinterpret_cast<const float*>(dpsi_at(k)) : nullptr;
+#pragma unroll 2
+			for (int j = 0; j < UPW4; j++) {
+				const int u = warp + j * nwarps;
+				if (u >= units) break;
+				const int b = insert2(2 * u, GL[k], GH[k]);
+				const int B0 = (b ^ ((__popc(u) ^ b) & 1)) << 4;
+				// outer products over the two sets (b6 = 2u, 2u+1) of eight groups (cc = 0..7);
+				// this lane's operands sit in columns t and t + 4
+#pragma unroll
+				for (int sset = 0; sset < 2; sset++) {
+					const int j0 = (sset ? B0 ^ E0[k] : B0) ^ LO[k], j1 = j0 + 8;
+					const float a[4] = { P[j0], (TAN && !first_gate) ? dP[j0] : 0.f, P[j1],
+					                     (TAN && !first_gate) ? dP[j1] : 0.f };
+					uint32_t ab[4], as[4];
+					split4(a, ab, as);
+					uint32_t xb[2], xs[2];
+					tf32_split(X[j0], xb[0], xs[0]);
+					tf32_split(X[j1], xb[1], xs[1]);
+					mma3(cx[k], ab, as, xb, xs);
+					if (TAN && !last_gate) {
+						uint32_t db[2], ds[2];
+						tf32_split(dX[j0], db[0], ds[0]);
+						tf32_split(dX[j1], db[1], ds[1]);
+						mma3(cd[k], ab, as, db, ds);   // rows 0-7: P^T dX (rows 8-15 unused)
+					}
+				}
+				if (last_gate) continue;
+				// adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place)
+				apply_unit4o<TAN>(P, dP, reinterpret_cast<float*>(Phi), TAN ? reinterpret_cast<float*>(dPhi) : nullptr,
+				                  B0, E0[k], LA[k], LB[k], LS[k], rgb[k], rgs[k], rzb[k], rzs[k], first_gate, true);
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+			const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+			const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cgp * CW4;
+#pragma unroll
+			for (int i = 0; i < CPT; i++) {
+				const int e = threadIdx.x + i * NT4R;
+				if (e >= 4 * R) continue;
+				const int r = e >> 2, c2i = 2 * (e & 3);
+				const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+				const int pe = prow(r) * CW4 + c2i;
+				*reinterpret_cast<float4*>(phi_o + a) = *reinterpret_cast<const float4*>(Phi + pe);
+				if (TAN) *reinterpret_cast<float4*>(dphi_o + a) = *reinterpret_cast<const float4*>(dPhi + pe);
+			}
+		}
+		if (++ntile == FLUSH4) {
+			ntile = 0;
+			flush();
+		}
+	}
+	flush();
+	__syncthreads();
+	// sum over warps: (k, lane, v) -> part
+	for (int idx = threadIdx.x; idx < K * NRAW4; idx += blockDim.x) {
+		const int k = idx / NRAW4, rem = idx % NRAW4, ln = rem / 4, v = rem % 4;
+		double s2 = 0;
+		for (int w = 0; w < nwarps; w++)
+			s2 += scratch[((size_t)blockIdx.x * nwarps + w) * 32 * MAXK * 4 + (size_t)ln * MAXK * 4 + k * 4 + v];
+		part[(size_t)k * nblk * NRAW4 + (size_t)blockIdx.x * NRAW4 + rem] += s2;
+	}
+}
+
+// Sum the complex64 engine's raw partials over blocks and fold them into complex dG, HZ.
+// Lane (g, t) of an outer-sum MMA holds C[g][2t..2t+1] (v 0,1) and C[g+8][2t..2t+1]
+// (v 2,3): dG raw R[g][2t+i] = v_i, HZ raw R[g][2t+i] = v_{2+i}.
+__global__ void k4_reduce(const double* __restrict__ part, int nslots, int nblk, const double2* __restrict__ fpart,
+                          int nblk_f, int with_hvp, double2* __restrict__ out)
+{
+	__shared__ double raw[NRAW4];
+	__shared__ double R[2][64];
+	const int s = blockIdx.x, t = threadIdx.x;
+	if (s < nslots) {
+		for (int v = t; v < NRAW4; v += blockDim.x) {
+			double sum = 0, comp = 0;
+			for (int b = 0; b < nblk; b++) {
+				const double y = part[((size_t)s * nblk + b) * NRAW4 + v] - comp;
+				const double u = sum + y;
+				comp = (u - sum) - y;
+				sum = u;
+			}
+			raw[v] = sum;
+		}
+		__syncthreads();
+		if (t < 64) {
+			const int ln = t >> 1, i = t & 1, gg = ln >> 2, tt = ln & 3;
+			R[0][gg * 8 + 2 * tt + i] = raw[ln * 4 + i];
+			R[1][gg * 8 + 2 * tt + i] = raw[ln * 4 + 2 + i];
+		}
+		__syncthreads();
+		if (t < 32) {
+			const int which = t >> 4, e = t & 15, r = e >> 2, c = e & 3;
+			if (which == 1 && !with_hvp) return;
+			const double* X = R[which];
+			const double re = X[(2 * r) * 8 + 2 * c] - X[(2 * r + 1) * 8 + 2 * c + 1];
+			const double im = X[(2 * r) * 8 + 2 * c + 1] + X[(2 * r + 1) * 8 + 2 * c];
+			out[1 + 16 * (size_t)(which ? nslots + s : s) + e] = make_double2(re, im);
+		}
+	} else if (t < 2) {
+		double sum = 0, comp = 0;
+		for (int b = 0; b < nblk_f; b++) {
+			const double y = (t == 0 ? fpart[b].x : fpart[b].y) - comp;
+			const double u = sum + y;
+			comp = (u - sum) - y;
+			sum = u;
+		}
+		reinterpret_cast<double*>(out)[t] = sum;
+	}
+}
+
 // -conj of host columns [Cc][N] (complex128) into the interleaved chunk [N][C]
 template <typename T>
 __global__ void k2_target_from_host(const double2* __restrict__ in, cplx<T>* __restrict__ out, int64_t N, int64_t Cc,
@@ -952,6 +1525,7 @@ size_t fwd_smem(int NB)
 template <typename T>
 size_t rev_smem(int NB, int K, bool tan)
 {
+	if (!std::is_same<T, double>::value) return k4_rev_smem(NB, K, tan);
 	const size_t A = ((size_t)1 << NB) * ColsPer<T>::v;
 	const size_t tiles = (tan ? 2 * K + 2 : K + 1) * A * sizeof(cplx<T>);
 	const size_t red = std::is_same<T, double>::value ? (size_t)(NTR / 32) * MAXK * NPART3 * sizeof(double)
@@ -1009,18 +1583,20 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
 	} else {
 		if (!per_sm) {
-			int ret = prepare(k2_fwd<T, TAN, IN, OUT>, fwd_smem<T>(MAXNB), &per_sm);
+			int ret = prepare(k4_fwd<TAN, IN, OUT>, k4_fwd_smem(MAXNB, TAN, OUT == 2), &per_sm, NT4F);
 			if (ret) return ret;
 		}
 		const int grid = OUT == 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
-		RQC_LAUNCH2(rt, KC_FUSED, (k2_fwd<T, TAN, IN, OUT>), grid, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
+		RQC_LAUNCH3(rt, KC_FUSED, (k4_fwd<TAN, IN, OUT>), grid, NT4F, k4_fwd_smem(pg.NB, TAN, OUT == 2), psi, dpsi, psi_o,
+		            dpsi_o, phi, pg, gates, fpart);
 	}
 	return OK;
 }
 
 template <typename T, bool TAN, bool FIRST, bool LAST>
 int launch_rev(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<T>* phi, const cplx<T>* dphi,
-               cplx<T>* phi_o, cplx<T>* dphi_o, const PassGeom& pg, const PassGates<T>& gates, double* part, int nblk)
+               cplx<T>* phi_o, cplx<T>* dphi_o, const PassGeom& pg, const PassGates<T>& gates, double* part, int nblk,
+               double* scratch)
 {
 	const size_t smem = rev_smem<T>(pg.NB, pg.K, TAN);
 	static bool ready = false;
@@ -1036,12 +1612,12 @@ int launch_rev(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<
 	} else {
 		if (!ready) {
 			int per_sm;
-			int ret = prepare(k2_rev<T, TAN, FIRST, LAST>, rev_smem<T>(MAXNB, MAXK, TAN), &per_sm);
+			int ret = prepare(k4_rev<TAN, FIRST, LAST>, rev_smem<T>(MAXNB, MAXK, TAN), &per_sm, NT4R);
 			if (ret) return ret;
 			ready = true;
 		}
-		RQC_LAUNCH2(rt, KC_REVERSE, (k2_rev<T, TAN, FIRST, LAST>), nblk, smem, psi, dpsi, phi, dphi, phi_o, dphi_o, pg,
-		            gates, part, nblk);
+		RQC_LAUNCH3(rt, KC_REVERSE, (k4_rev<TAN, FIRST, LAST>), nblk, NT4R, smem, psi, dpsi, phi, dphi, phi_o, dphi_o, pg,
+		            gates, part, nblk, scratch);
 	}
 	return OK;
 }
@@ -1049,12 +1625,15 @@ int launch_rev(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<
 template <typename T, bool TAN>
 int launch_rev_any(Runtime& rt, bool first, bool last, const cplx<T>* psi, const cplx<T>* dpsi, const cplx<T>* phi,
                    const cplx<T>* dphi, cplx<T>* phi_o, cplx<T>* dphi_o, const PassGeom& pg, const PassGates<T>& gates,
-                   double* part, int nblk)
+                   double* part, int nblk, double* scratch)
 {
-	if (first && last) return launch_rev<T, TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
-	if (first) return launch_rev<T, TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
-	if (last) return launch_rev<T, TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
-	return launch_rev<T, TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk);
+	if (first && last)
+		return launch_rev<T, TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk, scratch);
+	if (first)
+		return launch_rev<T, TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk, scratch);
+	if (last)
+		return launch_rev<T, TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk, scratch);
+	return launch_rev<T, TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk, scratch);
 }
 
 // grid of the partial-sum kernels: one resident wave of the reverse kernel
@@ -1068,8 +1647,8 @@ int rev_grid(Runtime& rt, bool tan)
 		ret = tan ? prepare(k3_rev<true, false, false>, smem, &per_sm, NTR)
 		          : prepare(k3_rev<false, false, false>, smem, &per_sm, NTR);
 	else
-		ret = tan ? prepare(k2_rev<T, true, false, false>, smem, &per_sm)
-		          : prepare(k2_rev<T, false, false, false>, smem, &per_sm);
+		ret = tan ? prepare(k4_rev<true, false, false>, smem, &per_sm, NT4R)
+		          : prepare(k4_rev<false, false, false>, smem, &per_sm, NT4R);
 	if (ret) per_sm = 1;
 	return rt.num_sms * per_sm;
 }
@@ -1125,12 +1704,19 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	auto dck_at = [&](int p) { return dck + (int64_t)(p - 1) * C * N; };
 
 	const int nblk = rev_grid<T>(rt, tan);
-	const int nps = std::is_same<T, double>::value ? NPART3 : NPART2;   // partial doubles per gate and block
-	const size_t part_doubles = (size_t)G * nblk * nps + 2 * (size_t)nblk;
+	// blocks of the forward launches that sum f (one FP64 partial each)
+	const int nfb = std::is_same<T, double>::value ? nblk : 2 * rt.num_sms;
+	const int nps = std::is_same<T, double>::value ? NPART3 : NRAW4;   // partial doubles per gate and block
+	const size_t part_doubles = (size_t)G * nblk * nps + 2 * (size_t)nfb;
 	if ((ret = ensure_device(rt.partials, part_doubles * sizeof(double)))) return ret;
 	double* part = reinterpret_cast<double*>(rt.partials.ptr);
 	double2* fpart = reinterpret_cast<double2*>(part + (size_t)G * nblk * nps);
 	if ((ret = RQC_CUDA(cudaMemsetAsync(part, 0, part_doubles * sizeof(double), rt.stream)))) return ret;
+	double* scratch = nullptr;
+	if (!std::is_same<T, double>::value) {
+		if ((ret = ensure_device(rt.scratch, (size_t)nblk * (NT4R / 32) * 32 * MAXK * 4 * sizeof(double)))) return ret;
+		scratch = reinterpret_cast<double*>(rt.scratch.ptr);
+	}
 
 	double2* hcols = nullptr;
 	double2* hbasis = nullptr;
@@ -1196,26 +1782,26 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 			if (mode == EVAL_F) {
 				const V* in = first ? nullptr : Pb[(p - 1) & 1];
 				V* out = last ? nullptr : Pb[p & 1];
-				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 			} else if (!tan) {
 				const V* in = first ? nullptr : ck_at(p);
 				V* out = last ? nullptr : ck_at(p + 1);
-				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
-				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nblk);
+				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 			} else {
 				const V* in = first ? nullptr : ck_at(p);
 				const V* din = first ? nullptr : dck_at(p);
 				V* out = last ? nullptr : ck_at(p + 1);
 				V* dout = last ? nullptr : dck_at(p + 1);
-				if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
-				else if (first) ret = launch_fwd<T, true, 1, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
-				else if (last) ret = launch_fwd<T, true, 0, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
-				else ret = launch_fwd<T, true, 0, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nblk);
+				if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+				else if (first) ret = launch_fwd<T, true, 1, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+				else if (last) ret = launch_fwd<T, true, 0, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+				else ret = launch_fwd<T, true, 0, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 			}
 			if (ret) return ret;
 		}
@@ -1231,18 +1817,19 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 			double* pp = part + (size_t)passes[p].first * nblk * nps;
 			if (tan)
 				ret = launch_rev_any<T, true>(rt, first, last, last ? nullptr : ck_at(p), last ? nullptr : dck_at(p), ph, dph,
-				                              last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pp, nblk);
+				                              last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pp, nblk,
+				                              scratch);
 			else
 				ret = launch_rev_any<T, false>(rt, first, last, last ? nullptr : ck_at(p), nullptr, ph, nullptr,
-				                               last ? nullptr : Pb[nxt], nullptr, g, pgates[p], pp, nblk);
+				                               last ? nullptr : Pb[nxt], nullptr, g, pgates[p], pp, nblk, scratch);
 			if (ret) return ret;
 		}
 	}
 
 	if (std::is_same<T, double>::value)
-		k3_reduce<<<G + 1, NPART3, 0, rt.stream>>>(part, G, nblk, fpart, nblk, tan ? 1 : 0, d_out);
+		k3_reduce<<<G + 1, NPART3, 0, rt.stream>>>(part, G, nblk, fpart, nfb, tan ? 1 : 0, d_out);
 	else
-		k2_reduce<<<G + 1, 64, 0, rt.stream>>>(part, G, nblk, fpart, nblk, tan ? 1 : 0, d_out);
+		k4_reduce<<<G + 1, NRAW4, 0, rt.stream>>>(part, G, nblk, fpart, nfb, tan ? 1 : 0, d_out);
 	rt.launches++;
 	return RQC_CUDA(cudaGetLastError());
 }

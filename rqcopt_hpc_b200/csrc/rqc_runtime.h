@@ -33,6 +33,7 @@ struct Runtime
 	Buffer small;         // inputs of the exported calls (gates, directions)
 	Buffer result;        // reduction results of the engine and single-gate passes
 	Buffer opt;           // optimiser vectors
+	Buffer scratch;       // FP64 per-lane sums of the complex64 reverse passes
 	Buffer stage[4];      // staging of host statevectors
 	Buffer hpin;          // pinned host scratch
 
