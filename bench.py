@@ -7,7 +7,12 @@ over all 65,536 basis columns (random tangent direction, seed 12).  Inputs are
 seeded synthetic data; the working set is many GB, far larger than L2.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision c128|c64] [--L 16 --depth 9 --tdepth 5]
+                    [--precision mixed|c64|c128] [--L 16 --depth 9 --tdepth 5]
+
+The default arm is the mixed-precision evaluation (complex64 passes on the tensor
+cores with FP64 sums); the same run times the plain complex128 evaluation, reports
+the error of one against the other, and runs a short trust-region optimisation in
+both modes to compare time at equal final error.
 
 One JSON line on rank 0.  `value` is device-timed throughput with the inputs
 resident in HBM (CUDA events on the library stream); `e2e` is the same metric
@@ -33,7 +38,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
-METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns)"
+METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns; mixed vs FP64)"
 
 
 def haar(rng):
@@ -223,6 +228,52 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
     return res
 
 
+# ----------------------------------------------------------------------------- mixed vs plain
+
+def _relerr(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def compare_plain(gpu, torch, stream, step, res_mixed, steps):
+    """The same evaluation with plain complex128 passes (one warm-up, `steps` timed), and
+    the error of the complex64-pass result against it."""
+    gpu.set_precision(gpu.PRECISION_C128)
+    ref = step()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"evals_per_s": 1e3 / ms, "ms_per_step": ms,
+            "mixed_rel_err": {"f": _relerr(res_mixed[0], ref[0]), "grad": _relerr(res_mixed[1], ref[1]),
+                              "hvp": _relerr(res_mixed[2], ref[2])}}
+
+
+def rtr_equal_error(gpu, L=10, depth=5, tdepth=3, niter=12):
+    """Riemannian trust region (reference defaults) from the same start in plain complex128 and
+    in mixed precision (complex64 HVPs until the gradient norm falls below the refinement
+    threshold, complex128 f, gradient and refinement): wall time and the final f of each."""
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, seed=0, tseed=1, dseed=2)
+    target = gpu.Target(brickwall=(tvlist, tperms))
+    out = {"workload": f"brickwall L={L} depth={depth} vs brickwall target depth={tdepth}, {niter} RTR iterations"}
+    runs = {}
+    for name, p in (("plain_c128", gpu.PRECISION_C128), ("mixed", gpu.PRECISION_MIXED)):
+        gpu.set_precision(p)
+        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, 1)   # warm-up
+        t0 = time.perf_counter()
+        f_iter, vopt = gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)
+        runs[name] = (time.perf_counter() - t0, f_iter)
+        out[name] = {"seconds": runs[name][0], "f_final": float(f_iter[-1])}
+    fp, fm = runs["plain_c128"][1][-1], runs["mixed"][1][-1]
+    out["f_final_rel_diff"] = abs(fm - fp) / max(abs(fp), 1e-300)
+    out["speedup"] = runs["plain_c128"][0] / runs["mixed"][0]
+    return out
+
+
 # ----------------------------------------------------------------------------- main
 
 def main():
@@ -231,7 +282,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="c128", choices=["c128", "c64"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "c64", "c128"],
+                    help="mixed / c64: complex64 passes with FP64 sums; c128: plain complex128")
     ap.add_argument("--L", type=int, default=16)
     ap.add_argument("--depth", type=int, default=9)
     ap.add_argument("--tdepth", type=int, default=5)
@@ -239,6 +291,7 @@ def main():
     ap.add_argument("--gates-per-pass", type=int, default=4, help="gates fused per HBM round trip (1-4)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate-throughput", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the complex128 comparison and the RTR runs")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -283,7 +336,7 @@ def main():
 
     from rqcopt_hpc_b200 import gpu
     lib = gpu.lib()
-    prec = gpu.PRECISION_C128 if a.precision == "c128" else gpu.PRECISION_C64
+    prec = {"c128": gpu.PRECISION_C128, "c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED}[a.precision]
     gpu.set_precision(prec)
     gpu.set_gates_per_pass(a.gates_per_pass)
     config["gates_per_pass"] = a.gates_per_pass
@@ -337,6 +390,8 @@ def main():
 
     if rank == 0:
         itemsize = 16 if prec == gpu.PRECISION_C128 else 8
+        rev_kernel = ("k3_rev (complex128 FP64-MMA gradient/HVP pass" if itemsize == 16
+                      else "k4_rev (complex64 3xTF32-MMA gradient/HVP pass")
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
@@ -351,13 +406,17 @@ def main():
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128 (f64)" if itemsize == 16 else "c64 (f32, f64 sums)",
+            "vs_baseline": None,
+            "dtype": "c128 (f64)" if itemsize == 16 else "c64 (f32 passes on 3xTF32 MMA, f64 sums)",
+            "precision": a.precision,
             "data": "synthetic (seeded Haar gates)", "config": config,
             "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "evals/s",
                     "h2d_bytes_per_step": int(vlist.nbytes + vdirs.nbytes + tvlist.nbytes + perms.nbytes + tperms.nbytes),
                     "d2h_bytes_per_step": int(16 + 2 * 16 * depth * 8)},
             "roofline": {"kernel": ("k_reverse (gradient/HVP pass of one gate over a column chunk)" if a.gates_per_pass == 1
-                                    else f"k2_rev (gradient/HVP pass of {a.gates_per_pass} fused gates over a column chunk)"),
+                                    else f"{rev_kernel} of {a.gates_per_pass} fused gates over a column chunk)"),
+                         "bytes_model": "(6P-5) * 2^L * 2^L * itemsize per evaluation (P passes): reads of "
+                                        "phi, dphi, psi, dpsi and writes of phi', dphi' per pass",
                          "bound": "hbm",
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak if achieved else None,
@@ -368,6 +427,11 @@ def main():
             "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
             "clocks": clk.summary(), "gpu_launches": int(launches),
         }
+        if not a.no_compare and world == 1 and prec != gpu.PRECISION_C128:
+            line["plain_c128"] = compare_plain(gpu, torch, stream, step, res, a.steps)
+            line["mixed_over_plain"] = line["plain_c128"]["ms_per_step"] / line["ms_per_step"]
+            line["rtr_equal_error"] = rtr_equal_error(gpu)
+            gpu.set_precision(prec)
         if not a.no_gate_throughput:
             line["gate_throughput"] = gate_throughput(gpu, torch)
         if not a.no_cpu_baseline and world == 1:

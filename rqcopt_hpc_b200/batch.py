@@ -1,0 +1,142 @@
+"""Batched brickwall evaluation and optimisation (include/rqcopt_batch.h).
+
+A problem is ``(L, vlist, perms, target_vlist, target_perms)``: a brickwall
+circuit of ``len(vlist)`` layer gates on the pairs of ``perms[l]`` fitted to a
+brickwall target applied matrix-free, the objective of the reference's
+``brickwall_unitary_target*`` functions (src/target.c:467-678) and of
+``optimize_brickwall_circuit_hvp`` (src/brickwall_opt.c:107-149).  Many such
+problems run together on one GPU; see :class:`Batch` for the slot interface a
+request loop uses.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import gpu
+from .abi import RTRParams, cplx, default_rtr_params, perm_pointers
+
+EVAL_F, EVAL_GRAD, EVAL_HVP = 0, 1, 2
+
+
+class BatchProblem(C.Structure):
+    _fields_ = [("nqubits", C.c_int), ("nlayers", C.c_int), ("vlist", C.c_void_p), ("perms", C.c_void_p),
+                ("target_nlayers", C.c_int), ("target_vlist", C.c_void_p), ("target_perms", C.c_void_p)]
+
+
+def _pack(problems):
+    """ctypes problem array plus the numpy arrays it points into (kept alive by the caller)."""
+    keep = []
+    arr = (BatchProblem * len(problems))()
+    for k, (L, vlist, perms, tvlist, tperms) in enumerate(problems):
+        v, tv = cplx(vlist), cplx(tvlist)
+        pp, k1 = perm_pointers(perms)
+        tp, k2 = perm_pointers(tperms)
+        keep += [v, tv, pp, k1, tp, k2]
+        arr[k] = BatchProblem(int(L), v.shape[0], v.ctypes.data, C.cast(pp, C.c_void_p).value, tv.shape[0],
+                              tv.ctypes.data, C.cast(tp, C.c_void_p).value)
+    return arr, keep
+
+
+def _check(fn, ret):
+    if ret < 0:
+        raise gpu.RqcError(fn, ret)
+    return ret
+
+
+def evaluate(problems, vdirs=None, mode=EVAL_HVP, precision=gpu.PRECISION_C64):
+    """f (complex), projected gradients and projected HVPs of every problem in one batched pass."""
+    arr, keep = _pack(problems)
+    n = [16 * len(p[1]) for p in problems]
+    f = np.zeros(2 * len(problems))
+    grad = np.zeros(sum(n))
+    hvp = np.zeros(sum(n))
+    dptr = None
+    if mode == EVAL_HVP:
+        dl = [cplx(d) for d in vdirs]
+        keep += dl
+        dptr = (C.c_void_p * len(dl))(*[d.ctypes.data for d in dl])
+    _check("rqcopt_brickwall_batch_evaluate",
+           gpu.lib().rqcopt_brickwall_batch_evaluate(C.byref(arr), len(problems), dptr, mode, precision,
+                                                     f.ctypes.data, grad.ctypes.data, hvp.ctypes.data))
+    off = np.cumsum([0] + n)
+    fc = f[0::2] + 1j * f[1::2]
+    return fc, [grad[off[k]:off[k + 1]] for k in range(len(n))], [hvp[off[k]:off[k + 1]] for k in range(len(n))]
+
+
+def optimize(problems, niter, precision=gpu.PRECISION_C64, params=None):
+    """optimize_brickwall_circuit_hvp for every problem at once: (f_iter [count][niter+1], [vlist_opt])."""
+    arr, keep = _pack(problems)
+    nl = [len(p[1]) for p in problems]
+    f_iter = np.zeros((len(problems), niter + 1))
+    vopt = np.zeros((sum(nl), 4, 4), np.complex128)
+    pa = None
+    if params is not None:
+        pa = (RTRParams * len(problems))(*params)
+    _check("rqcopt_optimize_brickwall_batch",
+           gpu.lib().rqcopt_optimize_brickwall_batch(C.byref(arr), len(problems), pa, niter, precision,
+                                                     f_iter.ctypes.data, vopt.ctypes.data))
+    off = np.cumsum([0] + nl)
+    return f_iter, [vopt[off[k]:off[k + 1]] for k in range(len(nl))]
+
+
+def footprint(L, nlayers):
+    """Device bytes one problem holds in a batch."""
+    return int(gpu.lib().rqcopt_batch_footprint(L, nlayers))
+
+
+class Batch:
+    """Slots of a running batch: problems join (add) and leave (result + release)
+    between rounds; run(k) advances every active problem by up to k evaluations."""
+
+    def __init__(self, capacity, max_iterations):
+        self.h = gpu.lib().rqcopt_batch_create(capacity, max_iterations)
+        if not self.h:
+            raise gpu.RqcError("rqcopt_batch_create", gpu.lib().rqcopt_gpu_last_error())
+        self.capacity = capacity
+        self._nl = {}
+        self._niter = {}
+
+    def add(self, problem, niter, precision=gpu.PRECISION_C64, params=None):
+        arr, keep = _pack([problem])
+        p = C.byref(params) if params is not None else None
+        slot = _check("rqcopt_batch_add", gpu.lib().rqcopt_batch_add(self.h, C.byref(arr), p, niter, precision))
+        self._nl[slot] = len(problem[1])
+        self._niter[slot] = niter
+        return slot
+
+    def run(self, rounds):
+        return _check("rqcopt_batch_run", gpu.lib().rqcopt_batch_run(self.h, rounds))
+
+    def finished(self, max_slots=None):
+        m = max_slots or self.capacity
+        buf = np.zeros(m, np.int32)
+        k = _check("rqcopt_batch_finished", gpu.lib().rqcopt_batch_finished(self.h, buf.ctypes.data, m))
+        return [int(x) for x in buf[:k]]
+
+    def result(self, slot):
+        f = np.zeros(self._niter[slot] + 1)
+        v = np.zeros((self._nl[slot], 4, 4), np.complex128)
+        r = _check("rqcopt_batch_result", gpu.lib().rqcopt_batch_result(self.h, slot, f.ctypes.data, v.ctypes.data))
+        return (f, v) if r == 1 else None
+
+    def release(self, slot):
+        _check("rqcopt_batch_release", gpu.lib().rqcopt_batch_release(self.h, slot))
+        self._nl.pop(slot, None)
+        self._niter.pop(slot, None)
+
+    @property
+    def rounds(self):
+        return int(gpu.lib().rqcopt_batch_rounds(self.h))
+
+    def close(self):
+        if self.h:
+            gpu.lib().rqcopt_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -91,6 +91,17 @@ _SIGS = {
     "rqcopt_gpu_enable_kernel_timing": (None, [I]),
     "rqcopt_gpu_kernel_time": (I, [I, PD, C.POINTER(C.c_long)]),
     "rqcopt_gpu_stream": (VP, []),
+    "rqcopt_brickwall_batch_evaluate": (I, [VP, I, VP, I, I, VP, VP, VP]),
+    "rqcopt_optimize_brickwall_batch": (I, [VP, I, VP, I, I, VP, VP]),
+    "rqcopt_batch_create": (VP, [I, I]),
+    "rqcopt_batch_destroy": (None, [VP]),
+    "rqcopt_batch_add": (I, [VP, VP, VP, I, I]),
+    "rqcopt_batch_run": (I, [VP, I]),
+    "rqcopt_batch_finished": (I, [VP, VP, I]),
+    "rqcopt_batch_result": (I, [VP, I, VP, VP]),
+    "rqcopt_batch_release": (I, [VP, I]),
+    "rqcopt_batch_rounds": (C.c_long, [VP]),
+    "rqcopt_batch_footprint": (C.c_size_t, [I, I]),
 }
 
 PRECISION_C128, PRECISION_MIXED, PRECISION_C64 = 0, 1, 2
