@@ -41,16 +41,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns; mixed vs FP64)"
 
 
-def haar(rng):
-    z = (rng.standard_normal((4, 4)) + 1j * rng.standard_normal((4, 4))) / np.sqrt(2)
-    q, r = np.linalg.qr(z)
-    d = np.diagonal(r)
-    return q * (d / np.abs(d))
-
-
-def perms_for(L, nlayers):
-    even, odd = np.arange(L), np.roll(np.arange(L), -1)
-    return np.stack([even if l % 2 == 0 else odd for l in range(nlayers)]).astype(np.int32)
+from rqcopt_hpc_b200.workloads import haar, perms_for  # noqa: E402
 
 
 def antisymm(r):

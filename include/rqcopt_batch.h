@@ -62,19 +62,29 @@ int rqcopt_optimize_brickwall_batch(const struct rqcopt_batch_problem* problems,
 struct rqcopt_batch;
 struct rqcopt_batch* rqcopt_batch_create(int capacity, int max_iterations);
 void rqcopt_batch_destroy(struct rqcopt_batch* batch);
-/* admit a problem: returns its slot */
+/* admit a problem: returns its slot; it stops after niter trust-region iterations
+ * or, with grad_tol > 0, at the first iteration whose gradient norm is at most
+ * grad_tol (f_iter then ends at that iteration) */
 int rqcopt_batch_add(struct rqcopt_batch* batch, const struct rqcopt_batch_problem* problem,
-                     const struct rtr_params* params, int niter, int precision);
+                     const struct rtr_params* params, int niter, int precision, double grad_tol);
 /* run up to max_rounds rounds (fewer if every slot finishes): active slots left */
 int rqcopt_batch_run(struct rqcopt_batch* batch, int max_rounds);
 /* slots that finished since the last call (at most max_slots) */
 int rqcopt_batch_finished(struct rqcopt_batch* batch, int* slots, int max_slots);
-/* 1 and the results of a finished slot, 0 while it runs */
-int rqcopt_batch_result(struct rqcopt_batch* batch, int slot, double* f_iter, struct mat4x4* vlist_opt);
+/* 1 and the results of a finished slot, 0 while it runs; iterations: trust-region
+ * iterations completed (f_iter holds iterations + 1 values) */
+int rqcopt_batch_result(struct rqcopt_batch* batch, int slot, double* f_iter, struct mat4x4* vlist_opt,
+                        int* iterations);
 /* free a slot */
 int rqcopt_batch_release(struct rqcopt_batch* batch, int slot);
+/* cost-weighted sharing for problems added from now on: a problem is evaluated
+ * only every p-th round, p growing with its cost per evaluation (off by default) */
+int rqcopt_batch_set_sharing(struct rqcopt_batch* batch, int on);
 /* rounds run so far */
 long rqcopt_batch_rounds(const struct rqcopt_batch* batch);
+/* evaluations run so far (one per active problem and round), and of them the
+ * Hessian-vector products */
+long rqcopt_batch_evaluations(const struct rqcopt_batch* batch, long* hvp_evaluations);
 /* device bytes held for one problem of this size (admission accounting) */
 size_t rqcopt_batch_footprint(int nqubits, int nlayers);
 

@@ -90,18 +90,21 @@ class Batch:
     """Slots of a running batch: problems join (add) and leave (result + release)
     between rounds; run(k) advances every active problem by up to k evaluations."""
 
-    def __init__(self, capacity, max_iterations):
+    def __init__(self, capacity, max_iterations, sharing=False):
         self.h = gpu.lib().rqcopt_batch_create(capacity, max_iterations)
         if not self.h:
             raise gpu.RqcError("rqcopt_batch_create", gpu.lib().rqcopt_gpu_last_error())
+        if sharing:
+            gpu.lib().rqcopt_batch_set_sharing(self.h, 1)
         self.capacity = capacity
         self._nl = {}
         self._niter = {}
 
-    def add(self, problem, niter, precision=gpu.PRECISION_C64, params=None):
+    def add(self, problem, niter, precision=gpu.PRECISION_C64, params=None, grad_tol=0.0):
         arr, keep = _pack([problem])
         p = C.byref(params) if params is not None else None
-        slot = _check("rqcopt_batch_add", gpu.lib().rqcopt_batch_add(self.h, C.byref(arr), p, niter, precision))
+        slot = _check("rqcopt_batch_add",
+                      gpu.lib().rqcopt_batch_add(self.h, C.byref(arr), p, niter, precision, float(grad_tol)))
         self._nl[slot] = len(problem[1])
         self._niter[slot] = niter
         return slot
@@ -116,10 +119,15 @@ class Batch:
         return [int(x) for x in buf[:k]]
 
     def result(self, slot):
+        """(f_iter, vlist_opt) of a finished slot (f_iter ends at the last iteration run), else None."""
         f = np.zeros(self._niter[slot] + 1)
         v = np.zeros((self._nl[slot], 4, 4), np.complex128)
-        r = _check("rqcopt_batch_result", gpu.lib().rqcopt_batch_result(self.h, slot, f.ctypes.data, v.ctypes.data))
-        return (f, v) if r == 1 else None
+        it = C.c_int(0)
+        r = _check("rqcopt_batch_result",
+                   gpu.lib().rqcopt_batch_result(self.h, slot, f.ctypes.data, v.ctypes.data, C.byref(it)))
+        if r != 1:
+            return None
+        return f[:it.value + 1], v
 
     def release(self, slot):
         _check("rqcopt_batch_release", gpu.lib().rqcopt_batch_release(self.h, slot))
@@ -129,6 +137,12 @@ class Batch:
     @property
     def rounds(self):
         return int(gpu.lib().rqcopt_batch_rounds(self.h))
+
+    def evaluations(self):
+        """(evaluations, of them Hessian-vector products) run so far."""
+        h = C.c_long(0)
+        n = _check("rqcopt_batch_evaluations", gpu.lib().rqcopt_batch_evaluations(self.h, C.byref(h)))
+        return int(n), int(h.value)
 
     def close(self):
         if self.h:

@@ -21,7 +21,10 @@
 // Optimisation.  Every instance carries a trust-region state machine on the
 // device; one round evaluates every active instance once (gradient, HVP or f,
 // whichever its state needs next), projects, and advances each state machine.
-// A round is five launches, captured once as a CUDA graph and replayed.
+// A round is six launches, captured once as a CUDA graph and replayed.  With
+// sharing on, an instance joins only every period-th round, the period growing
+// with its cost per evaluation, so that every instance gets a similar share of
+// the GPU and small instances finish without waiting on large ones.
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -45,6 +48,10 @@ constexpr int MAXTU = 16;        // target layers per instance
 constexpr int MAXL = 14;         // qubits per instance
 constexpr int MAXN = 16 * MAXU;  // real parameters per instance
 constexpr int NACC = 2 + 64 * MAXU;   // FP64 accumulators per item: f (re, im), dG and HZ per layer
+constexpr double ITEM_WORK = 4194304.0;   // amplitude x gate updates per work item (about)
+constexpr int TSTR = 20;               // shared-memory stride of a 4x4 gate table (rows padded to 5)
+constexpr int NTABS = (MAXU * 3 + MAXTU) * TSTR;
+constexpr int SWIRES = (MAXU + MAXTU) * MAXL + 4;   // wire ints in shared memory (16-byte multiple)
 
 enum Phase { PH_GRAD = 0, PH_TCG = 1, PH_HETA = 2, PH_FNEXT = 3, PH_FINAL = 4, PH_DONE = 5, PH_EVAL = 6 };
 
@@ -72,6 +79,8 @@ struct BInst
 	int item0, item1;          // this instance's work items
 	int niter, maxiter;        // RTR iterations, tCG iteration limit
 	double radius_init, maxradius, rho_trust, abstol, reltol;
+	double gtol;               // stop once the gradient norm is at most gtol (0: run niter iterations)
+	int period;                // evaluated in rounds r with (r + slot) % period == 0 (cost-weighted sharing)
 };
 
 struct BOpt
@@ -149,6 +158,282 @@ __device__ __forceinline__ void kahan_add(double* s, double* c, double v)
 
 // ------------------------------------------------------------------ evaluation kernel
 
+// One work item: columns item.y .. item.z - 1 of instance item.x, with the four
+// state tiles in shared memory (SMEM) or in this CTA's global scratch.
+template <typename T, bool SMEM>
+__device__ __forceinline__ void beval_item(const BInst& in, const int4& item, int it, const int* __restrict__ wires,
+                                           const typename BTr<T>::E* __restrict__ tabs, double* __restrict__ partial,
+                                           typename BTr<T>::V* __restrict__ gscratch, unsigned char* smem)
+{
+	using V = typename BTr<T>::V;
+	using E = typename BTr<T>::E;
+	constexpr int NTAB = (MAXU * 3 + MAXTU) * 16;
+	E* stab = reinterpret_cast<E*>(smem);
+	double* acc = reinterpret_cast<double*>(stab + NTABS);          // [NACC] sums
+	double* cmp = acc + NACC;                                        // [NACC] Kahan compensations
+	V* red = reinterpret_cast<V*>(cmp + NACC);                       // [BT/32][32]
+	double* fred = reinterpret_cast<double*>(red + BT);              // [2][BT/32]
+	int* sw = reinterpret_cast<int*>(fred + 2 * (BT / 32));          // [(MAXU + MAXTU) * MAXL] wires
+	V* sstates = reinterpret_cast<V*>(sw + SWIRES);
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	const int L = in.L, N = 1 << L, nl = in.nl, tnl = in.tnl, per = in.per;
+	const int CW = N >= BTr<T>::AMP ? 1 : BTr<T>::AMP >> L;
+	const int lcw = __ffs(CW) - 1;
+	const int amps = N * CW, ngc = amps >> 2;
+	V* base = SMEM ? sstates : gscratch + (size_t)blockIdx.x * 4 * ((size_t)1 << MAXL);
+	V* S = base;
+	V* dS = base + amps;
+	V* P = base + 2 * amps;
+	V* dP = base + 3 * amps;
+	const int mode = in.mode;
+	const bool tan = mode == EVAL_HVP;
+	// gate tables with rows padded to 5 entries (rows 2h and 2h + 1 of a thread pair
+	// fall in different banks)
+	const E* gt = tabs + (size_t)item.x * NTAB;
+	for (int e = tid; e < nl * 3 * 16; e += BT) stab[(e >> 4) * TSTR + 5 * ((e >> 2) & 3) + (e & 3)] = gt[e];
+	for (int e = tid; e < tnl * 16; e += BT)
+		stab[(MAXU * 3 + (e >> 4)) * TSTR + 5 * ((e >> 2) & 3) + (e & 3)] = gt[MAXU * 3 * 16 + e];
+	for (int e = tid; e < (MAXU + MAXTU) * MAXL; e += BT) sw[e] = wires[(size_t)item.x * (MAXU + MAXTU) * MAXL + e];
+	const int nacc = 2 + 64 * nl;
+	for (int e = tid; e < nacc; e += BT) { acc[e] = 0; cmp[e] = 0; }
+	const int* w = sw;
+	double fx = 0, fy = 0;
+	__syncthreads();
+
+	// Group-columns are split over thread pairs: thread h of a pair computes the
+	// output rows 2h, 2h + 1 of every product of its group-column.
+	const int h = tid & 1, pr = tid >> 1;
+	constexpr int NPAIR = BT / 2;
+	auto group = [&](int gc, int wi, int wj, int idx[4]) {
+		const int c = gc & (CW - 1), g = gc >> lcw;
+		const int pi = L - 1 - wi, pj = L - 1 - wj;
+		const int b = ins2(g, min(pi, pj), max(pi, pj));
+		idx[0] = (b << lcw) | c;
+		idx[1] = ((b | (1 << pj)) << lcw) | c;
+		idx[2] = ((b | (1 << pi)) << lcw) | c;
+		idx[3] = ((b | (1 << pi) | (1 << pj)) << lcw) | c;
+	};
+	// rows 2h, 2h + 1 of M x (TR: M^T x)
+	auto rows2 = [&](const E* m, const V x[4], V y[2], bool tr, bool accum) {
+#pragma unroll
+		for (int q = 0; q < 2; q++) {
+			const int r = 2 * h + q;
+			V a2 = accum ? y[q] : vzero<V>();
+#pragma unroll
+			for (int c = 0; c < 4; c++) a2 = cmac(a2, m[tr ? 5 * c + r : 5 * r + c], x[c]);
+			y[q] = a2;
+		}
+	};
+	// full vector from this thread's two rows and the partner's
+	auto share = [&](const V own[2], V full[4]) {
+		V o0, o1;
+		o0.x = __shfl_xor_sync(0xffffffffu, own[0].x, 1);
+		o0.y = __shfl_xor_sync(0xffffffffu, own[0].y, 1);
+		o1.x = __shfl_xor_sync(0xffffffffu, own[1].x, 1);
+		o1.y = __shfl_xor_sync(0xffffffffu, own[1].y, 1);
+		full[0] = h ? o0 : own[0];
+		full[1] = h ? o1 : own[1];
+		full[2] = h ? own[0] : o0;
+		full[3] = h ? own[1] : o1;
+	};
+	// one gate on X (and the tangent dX += Zm X): in place
+	auto apply = [&](V* X, V* dX, const E* m, const E* zm, int wi, int wj) {
+		for (int gc = pr; gc < ngc; gc += NPAIR) {
+			int idx[4];
+			group(gc, wi, wj, idx);
+			const V x[4] = { X[idx[0]], X[idx[1]], X[idx[2]], X[idx[3]] };
+			V y[2], dy[2];
+			rows2(m, x, y, false, false);
+			if (dX) {
+				const V dx[4] = { dX[idx[0]], dX[idx[1]], dX[idx[2]], dX[idx[3]] };
+				rows2(m, dx, dy, false, false);
+				rows2(zm, x, dy, false, true);
+			}
+			const int o0 = h ? idx[2] : idx[0], o1 = h ? idx[3] : idx[1];
+			__syncwarp();
+			X[o0] = y[0];
+			X[o1] = y[1];
+			if (dX) {
+				dX[o0] = dy[0];
+				dX[o1] = dy[1];
+			}
+		}
+		__syncthreads();
+	};
+
+	for (int b0 = item.y; b0 < item.z; b0 += CW) {
+		// phi = -conj(W e_b) for the columns b0 .. b0 + CW - 1
+		for (int e = tid; e < amps; e += BT) {
+			const int row = e >> lcw, c = e & (CW - 1);
+			P[e] = vzero<V>();
+			if (row == b0 + c) P[e].x = 1;
+		}
+		__syncthreads();
+		for (int l = 0; l < tnl; l++)
+			for (int p = 0; p < per; p++)
+				apply(P, nullptr, stab + (MAXU * 3 + l) * TSTR, nullptr, w[(MAXU + l) * MAXL + 2 * p],
+				      w[(MAXU + l) * MAXL + 2 * p + 1]);
+		for (int e = tid; e < amps; e += BT) {
+			const V v = P[e];
+			P[e].x = -v.x;
+			P[e].y = v.y;
+			const int row = e >> lcw, c = e & (CW - 1);
+			S[e] = vzero<V>();
+			if (row == b0 + c) S[e].x = 1;
+			if (tan) dS[e] = vzero<V>();
+		}
+		__syncthreads();
+		// forward: psi <- G psi, dpsi <- G dpsi + Z psi
+		for (int l = 0; l < nl; l++)
+			for (int p = 0; p < per; p++)
+				apply(S, tan ? dS : nullptr, stab + (3 * l) * TSTR, stab + (3 * l + 2) * TSTR, w[l * MAXL + 2 * p],
+				      w[l * MAXL + 2 * p + 1]);
+		// f contribution: sum phi . psi (unconjugated)
+		for (int e = tid; e < amps; e += BT) {
+			const V pp = P[e], ss = S[e];
+			fx += (double)pp.x * ss.x - (double)pp.y * ss.y;
+			fy += (double)pp.x * ss.y + (double)pp.y * ss.x;
+		}
+		if (mode == EVAL_F) {
+			__syncthreads();
+			continue;
+		}
+		if (tan)
+			for (int e = tid; e < amps; e += BT) dP[e] = vzero<V>();
+		__syncthreads();
+		// reverse
+		for (int l = nl - 1; l >= 0; l--) {
+			const E* G = stab + (3 * l) * TSTR;
+			const E* Gc = stab + (3 * l + 1) * TSTR;
+			const E* Z = stab + (3 * l + 2) * TSTR;
+			// a[0..15]: dG rows 2h, 2h+1 (re, im), a[16..31]: HZ rows 2h, 2h+1
+			T a[32];
+#pragma unroll
+			for (int e = 0; e < 32; e++) a[e] = 0;
+			for (int p = per - 1; p >= 0; p--) {
+				const int wi = w[l * MAXL + 2 * p], wj = w[l * MAXL + 2 * p + 1];
+				for (int gc = pr; gc < ngc; gc += NPAIR) {
+					int idx[4];
+					group(gc, wi, wj, idx);
+					const V x[4] = { S[idx[0]], S[idx[1]], S[idx[2]], S[idx[3]] };
+					const V ph[4] = { P[idx[0]], P[idx[1]], P[idx[2]], P[idx[3]] };
+					V xo[2], xk[4], np[2];
+					rows2(Gc, x, xo, true, false);     // psi_k = G^+ psi_{k+1}
+					share(xo, xk);
+					rows2(G, ph, np, true, false);     // phi_k = G^T phi_{k+1}
+					const int o0 = h ? idx[2] : idx[0], o1 = h ? idx[3] : idx[1];
+					E pe[2];
+					pe[0] = entry_of(h ? ph[2] : ph[0]);
+					pe[1] = entry_of(h ? ph[3] : ph[1]);
+#pragma unroll
+					for (int q = 0; q < 2; q++)
+#pragma unroll
+						for (int c = 0; c < 4; c++) {
+							V v = make_v(a[2 * (4 * q + c)], a[2 * (4 * q + c) + 1]);
+							v = cmac(v, pe[q], xk[c]);
+							a[2 * (4 * q + c)] = v.x;
+							a[2 * (4 * q + c) + 1] = v.y;
+						}
+					V dxo[2], ndp[2];
+					if (tan) {
+						const V dph[4] = { dP[idx[0]], dP[idx[1]], dP[idx[2]], dP[idx[3]] };
+						const V dx2[2] = { dS[o0], dS[o1] };
+						V zx[2], to[2], t4[4], dxk[4];
+						rows2(Z, xk, zx, false, false);
+						to[0] = vsub(dx2[0], zx[0]);
+						to[1] = vsub(dx2[1], zx[1]);
+						share(to, t4);
+						rows2(Gc, t4, dxo, true, false);   // dpsi_k = G^+ (dpsi_{k+1} - Z psi_k)
+						share(dxo, dxk);
+						rows2(G, dph, ndp, true, false);   // dphi_k = G^T dphi_{k+1} + Z^T phi_{k+1}
+						rows2(Z, ph, ndp, true, true);
+						E dpe[2];
+						dpe[0] = entry_of(h ? dph[2] : dph[0]);
+						dpe[1] = entry_of(h ? dph[3] : dph[1]);
+#pragma unroll
+						for (int q = 0; q < 2; q++)
+#pragma unroll
+							for (int c = 0; c < 4; c++) {
+								V v = make_v(a[16 + 2 * (4 * q + c)], a[16 + 2 * (4 * q + c) + 1]);
+								v = cmac(v, pe[q], dxk[c]);
+								v = cmac(v, dpe[q], xk[c]);
+								a[16 + 2 * (4 * q + c)] = v.x;
+								a[16 + 2 * (4 * q + c) + 1] = v.y;
+							}
+					}
+					__syncwarp();
+					S[o0] = xo[0];
+					S[o1] = xo[1];
+					P[o0] = np[0];
+					P[o1] = np[1];
+					if (tan) {
+						dS[o0] = dxo[0];
+						dS[o1] = dxo[1];
+						dP[o0] = ndp[0];
+						dP[o1] = ndp[1];
+					}
+				}
+				__syncthreads();
+			}
+			// layer sums over the 16 lanes of each parity: lane (h, j = lane >> 1) ends with
+			// complex entry j of its parity (j < 8: dG[2h + j/4][j%4], else HZ[2h + (j-8)/4][(j-8)%4])
+#pragma unroll
+			for (int st = 0; st < 4; st++) {
+				const int hh = 16 >> st, m = 16 >> st;
+				const bool up = (lane & m) != 0;
+#pragma unroll
+				for (int i2 = 0; i2 < 16; i2++) {
+					if (i2 >= hh) break;
+					const T send = up ? a[i2] : a[i2 + hh];
+					const T keep = up ? a[i2 + hh] : a[i2];
+					a[i2] = keep + __shfl_xor_sync(0xffffffffu, send, m);
+				}
+			}
+			red[warp * 32 + lane] = make_v(a[0], a[1]);
+			__syncthreads();
+			if (tid < 32) {
+				const int hp = tid & 1, j = tid >> 1;
+				if (tan || j < 8) {
+					double sx = 0, sy = 0;
+					for (int ww = 0; ww < BT / 32; ww++) {
+						sx += (double)red[ww * 32 + tid].x;
+						sy += (double)red[ww * 32 + tid].y;
+					}
+					const int which = j >> 3, r = 2 * hp + ((j & 7) >> 2), c = j & 3, e = 4 * r + c;
+					const int off = which == 0 ? 2 + 32 * l + 2 * e : 2 + 32 * nl + 32 * l + 2 * e;
+					kahan_add(acc + off, cmp + off, sx);
+					kahan_add(acc + off + 1, cmp + off + 1, sy);
+				}
+			}
+			__syncthreads();
+		}
+	}
+	// f of this item
+	fx = warp_sum(fx);
+	fy = warp_sum(fy);
+	if (lane == 0) {
+		fred[warp] = fx;
+		fred[BT / 32 + warp] = fy;
+	}
+	__syncthreads();
+	if (tid == 0) {
+		double sx = 0, sy = 0;
+		for (int ww = 0; ww < BT / 32; ww++) {
+			sx += fred[ww];
+			sy += fred[BT / 32 + ww];
+		}
+		acc[0] = sx;
+		acc[1] = sy;
+		cmp[0] = 0;
+		cmp[1] = 0;
+	}
+	__syncthreads();
+	double* out = partial + (size_t)it * NACC;
+	for (int e = tid; e < nacc; e += BT) out[e] = acc[e] - cmp[e];
+	__syncthreads();
+
+}
+
 template <typename T>
 __global__ void __launch_bounds__(BT, 1)
 k_beval(const BInst* __restrict__ insts, const int4* __restrict__ items, int nitems, int* __restrict__ queue,
@@ -156,18 +441,9 @@ k_beval(const BInst* __restrict__ insts, const int4* __restrict__ items, int nit
         typename BTr<T>::V* __restrict__ gscratch, int prec)
 {
 	using V = typename BTr<T>::V;
-	using E = typename BTr<T>::E;
-	constexpr int NTAB = (MAXU * 3 + MAXTU) * 16;
 	extern __shared__ __align__(16) unsigned char smem[];
-	E* stab = reinterpret_cast<E*>(smem);
-	double* acc = reinterpret_cast<double*>(stab + NTAB);           // [NACC] sums
-	double* cmp = acc + NACC;                                        // [NACC] Kahan compensations
-	V* red = reinterpret_cast<V*>(cmp + NACC);                       // [BT/32][32]
-	double* fred = reinterpret_cast<double*>(red + BT);              // [2][BT/32]
-	V* sstates = reinterpret_cast<V*>(fred + 2 * (BT / 32));
 	__shared__ int s_item;
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-
+	const int tid = threadIdx.x;
 	for (;;) {
 		if (tid == 0) s_item = atomicAdd(queue, 1);
 		__syncthreads();
@@ -177,259 +453,12 @@ k_beval(const BInst* __restrict__ insts, const int4* __restrict__ items, int nit
 		const int4 item = items[it];
 		const BInst in = insts[item.x];
 		if (!in.active || in.prec != prec) continue;
-		const int L = in.L, N = 1 << L, nl = in.nl, tnl = in.tnl, per = in.per;
-		const int CW = N >= BTr<T>::AMP ? 1 : BTr<T>::AMP >> L;
-		const int lcw = __ffs(CW) - 1;
-		const int amps = N * CW, ngc = amps >> 2;
-		V* base = (size_t)4 * amps * sizeof(V) <= STATE_SMEM
-		              ? sstates
-		              : gscratch + (size_t)blockIdx.x * 4 * ((size_t)1 << MAXL);
-		V* S = base;
-		V* dS = base + amps;
-		V* P = base + 2 * amps;
-		V* dP = base + 3 * amps;
-		const int mode = in.mode;
-		const bool tan = mode == EVAL_HVP;
-		const E* gt = tabs + (size_t)item.x * NTAB;
-		for (int e = tid; e < nl * 3 * 16; e += BT) stab[e] = gt[e];
-		for (int e = tid; e < tnl * 16; e += BT) stab[MAXU * 3 * 16 + e] = gt[MAXU * 3 * 16 + e];
-		const int nacc = 2 + 64 * nl;
-		for (int e = tid; e < nacc; e += BT) { acc[e] = 0; cmp[e] = 0; }
-		const int* w = wires + (size_t)item.x * (MAXU + MAXTU) * MAXL;
-		double fx = 0, fy = 0;
-		__syncthreads();
-
-		// Group-columns are split over thread pairs: thread h of a pair computes the
-		// output rows 2h, 2h + 1 of every product of its group-column.
-		const int h = tid & 1, pr = tid >> 1;
-		constexpr int NPAIR = BT / 2;
-		auto group = [&](int gc, int wi, int wj, int idx[4]) {
-			const int c = gc & (CW - 1), g = gc >> lcw;
-			const int pi = L - 1 - wi, pj = L - 1 - wj;
-			const int b = ins2(g, min(pi, pj), max(pi, pj));
-			idx[0] = (b << lcw) | c;
-			idx[1] = ((b | (1 << pj)) << lcw) | c;
-			idx[2] = ((b | (1 << pi)) << lcw) | c;
-			idx[3] = ((b | (1 << pi) | (1 << pj)) << lcw) | c;
-		};
-		// rows 2h, 2h + 1 of M x (TR: M^T x)
-		auto rows2 = [&](const E* m, const V x[4], V y[2], bool tr, bool accum) {
-#pragma unroll
-			for (int q = 0; q < 2; q++) {
-				const int r = 2 * h + q;
-				V a2 = accum ? y[q] : vzero<V>();
-#pragma unroll
-				for (int c = 0; c < 4; c++) a2 = cmac(a2, m[tr ? 4 * c + r : 4 * r + c], x[c]);
-				y[q] = a2;
-			}
-		};
-		// full vector from this thread's two rows and the partner's
-		auto share = [&](const V own[2], V full[4]) {
-			V o0, o1;
-			o0.x = __shfl_xor_sync(0xffffffffu, own[0].x, 1);
-			o0.y = __shfl_xor_sync(0xffffffffu, own[0].y, 1);
-			o1.x = __shfl_xor_sync(0xffffffffu, own[1].x, 1);
-			o1.y = __shfl_xor_sync(0xffffffffu, own[1].y, 1);
-			full[0] = h ? o0 : own[0];
-			full[1] = h ? o1 : own[1];
-			full[2] = h ? own[0] : o0;
-			full[3] = h ? own[1] : o1;
-		};
-		// one gate on X (and the tangent dX += Zm X): in place
-		auto apply = [&](V* X, V* dX, const E* m, const E* zm, int wi, int wj) {
-			for (int gc = pr; gc < ngc; gc += NPAIR) {
-				int idx[4];
-				group(gc, wi, wj, idx);
-				const V x[4] = { X[idx[0]], X[idx[1]], X[idx[2]], X[idx[3]] };
-				V y[2], dy[2];
-				rows2(m, x, y, false, false);
-				if (dX) {
-					const V dx[4] = { dX[idx[0]], dX[idx[1]], dX[idx[2]], dX[idx[3]] };
-					rows2(m, dx, dy, false, false);
-					rows2(zm, x, dy, false, true);
-				}
-				const int o0 = h ? idx[2] : idx[0], o1 = h ? idx[3] : idx[1];
-				__syncwarp();
-				X[o0] = y[0];
-				X[o1] = y[1];
-				if (dX) {
-					dX[o0] = dy[0];
-					dX[o1] = dy[1];
-				}
-			}
-			__syncthreads();
-		};
-
-		for (int b0 = item.y; b0 < item.z; b0 += CW) {
-			// phi = -conj(W e_b) for the columns b0 .. b0 + CW - 1
-			for (int e = tid; e < amps; e += BT) {
-				const int row = e >> lcw, c = e & (CW - 1);
-				P[e] = vzero<V>();
-				if (row == b0 + c) P[e].x = 1;
-			}
-			__syncthreads();
-			for (int l = 0; l < tnl; l++)
-				for (int p = 0; p < per; p++)
-					apply(P, nullptr, stab + (MAXU * 3 + l) * 16, nullptr, w[(MAXU + l) * MAXL + 2 * p],
-					      w[(MAXU + l) * MAXL + 2 * p + 1]);
-			for (int e = tid; e < amps; e += BT) {
-				const V v = P[e];
-				P[e].x = -v.x;
-				P[e].y = v.y;
-				const int row = e >> lcw, c = e & (CW - 1);
-				S[e] = vzero<V>();
-				if (row == b0 + c) S[e].x = 1;
-				if (tan) dS[e] = vzero<V>();
-			}
-			__syncthreads();
-			// forward: psi <- G psi, dpsi <- G dpsi + Z psi
-			for (int l = 0; l < nl; l++)
-				for (int p = 0; p < per; p++)
-					apply(S, tan ? dS : nullptr, stab + (3 * l) * 16, stab + (3 * l + 2) * 16, w[l * MAXL + 2 * p],
-					      w[l * MAXL + 2 * p + 1]);
-			// f contribution: sum phi . psi (unconjugated)
-			for (int e = tid; e < amps; e += BT) {
-				const V pp = P[e], ss = S[e];
-				fx += (double)pp.x * ss.x - (double)pp.y * ss.y;
-				fy += (double)pp.x * ss.y + (double)pp.y * ss.x;
-			}
-			if (mode == EVAL_F) {
-				__syncthreads();
-				continue;
-			}
-			if (tan)
-				for (int e = tid; e < amps; e += BT) dP[e] = vzero<V>();
-			__syncthreads();
-			// reverse
-			for (int l = nl - 1; l >= 0; l--) {
-				const E* G = stab + (3 * l) * 16;
-				const E* Gc = stab + (3 * l + 1) * 16;
-				const E* Z = stab + (3 * l + 2) * 16;
-				// a[0..15]: dG rows 2h, 2h+1 (re, im), a[16..31]: HZ rows 2h, 2h+1
-				T a[32];
-#pragma unroll
-				for (int e = 0; e < 32; e++) a[e] = 0;
-				for (int p = per - 1; p >= 0; p--) {
-					const int wi = w[l * MAXL + 2 * p], wj = w[l * MAXL + 2 * p + 1];
-					for (int gc = pr; gc < ngc; gc += NPAIR) {
-						int idx[4];
-						group(gc, wi, wj, idx);
-						const V x[4] = { S[idx[0]], S[idx[1]], S[idx[2]], S[idx[3]] };
-						const V ph[4] = { P[idx[0]], P[idx[1]], P[idx[2]], P[idx[3]] };
-						V xo[2], xk[4], np[2];
-						rows2(Gc, x, xo, true, false);     // psi_k = G^+ psi_{k+1}
-						share(xo, xk);
-						rows2(G, ph, np, true, false);     // phi_k = G^T phi_{k+1}
-						const int o0 = h ? idx[2] : idx[0], o1 = h ? idx[3] : idx[1];
-						E pe[2];
-						pe[0] = entry_of(h ? ph[2] : ph[0]);
-						pe[1] = entry_of(h ? ph[3] : ph[1]);
-#pragma unroll
-						for (int q = 0; q < 2; q++)
-#pragma unroll
-							for (int c = 0; c < 4; c++) {
-								V v = make_v(a[2 * (4 * q + c)], a[2 * (4 * q + c) + 1]);
-								v = cmac(v, pe[q], xk[c]);
-								a[2 * (4 * q + c)] = v.x;
-								a[2 * (4 * q + c) + 1] = v.y;
-							}
-						V dxo[2], ndp[2];
-						if (tan) {
-							const V dph[4] = { dP[idx[0]], dP[idx[1]], dP[idx[2]], dP[idx[3]] };
-							const V dx2[2] = { dS[o0], dS[o1] };
-							V zx[2], to[2], t4[4], dxk[4];
-							rows2(Z, xk, zx, false, false);
-							to[0] = vsub(dx2[0], zx[0]);
-							to[1] = vsub(dx2[1], zx[1]);
-							share(to, t4);
-							rows2(Gc, t4, dxo, true, false);   // dpsi_k = G^+ (dpsi_{k+1} - Z psi_k)
-							share(dxo, dxk);
-							rows2(G, dph, ndp, true, false);   // dphi_k = G^T dphi_{k+1} + Z^T phi_{k+1}
-							rows2(Z, ph, ndp, true, true);
-							E dpe[2];
-							dpe[0] = entry_of(h ? dph[2] : dph[0]);
-							dpe[1] = entry_of(h ? dph[3] : dph[1]);
-#pragma unroll
-							for (int q = 0; q < 2; q++)
-#pragma unroll
-								for (int c = 0; c < 4; c++) {
-									V v = make_v(a[16 + 2 * (4 * q + c)], a[16 + 2 * (4 * q + c) + 1]);
-									v = cmac(v, pe[q], dxk[c]);
-									v = cmac(v, dpe[q], xk[c]);
-									a[16 + 2 * (4 * q + c)] = v.x;
-									a[16 + 2 * (4 * q + c) + 1] = v.y;
-								}
-						}
-						__syncwarp();
-						S[o0] = xo[0];
-						S[o1] = xo[1];
-						P[o0] = np[0];
-						P[o1] = np[1];
-						if (tan) {
-							dS[o0] = dxo[0];
-							dS[o1] = dxo[1];
-							dP[o0] = ndp[0];
-							dP[o1] = ndp[1];
-						}
-					}
-					__syncthreads();
-				}
-				// layer sums over the 16 lanes of each parity: lane (h, j = lane >> 1) ends with
-				// complex entry j of its parity (j < 8: dG[2h + j/4][j%4], else HZ[2h + (j-8)/4][(j-8)%4])
-#pragma unroll
-				for (int st = 0; st < 4; st++) {
-					const int hh = 16 >> st, m = 16 >> st;
-					const bool up = (lane & m) != 0;
-#pragma unroll
-					for (int i2 = 0; i2 < 16; i2++) {
-						if (i2 >= hh) break;
-						const T send = up ? a[i2] : a[i2 + hh];
-						const T keep = up ? a[i2 + hh] : a[i2];
-						a[i2] = keep + __shfl_xor_sync(0xffffffffu, send, m);
-					}
-				}
-				red[warp * 32 + lane] = make_v(a[0], a[1]);
-				__syncthreads();
-				if (tid < 32) {
-					const int hp = tid & 1, j = tid >> 1;
-					if (tan || j < 8) {
-						double sx = 0, sy = 0;
-						for (int ww = 0; ww < BT / 32; ww++) {
-							sx += (double)red[ww * 32 + tid].x;
-							sy += (double)red[ww * 32 + tid].y;
-						}
-						const int which = j >> 3, r = 2 * hp + ((j & 7) >> 2), c = j & 3, e = 4 * r + c;
-						const int off = which == 0 ? 2 + 32 * l + 2 * e : 2 + 32 * nl + 32 * l + 2 * e;
-						kahan_add(acc + off, cmp + off, sx);
-						kahan_add(acc + off + 1, cmp + off + 1, sy);
-					}
-				}
-				__syncthreads();
-			}
-		}
-		// f of this item
-		fx = warp_sum(fx);
-		fy = warp_sum(fy);
-		if (lane == 0) {
-			fred[warp] = fx;
-			fred[BT / 32 + warp] = fy;
-		}
-		__syncthreads();
-		if (tid == 0) {
-			double sx = 0, sy = 0;
-			for (int ww = 0; ww < BT / 32; ww++) {
-				sx += fred[ww];
-				sy += fred[BT / 32 + ww];
-			}
-			acc[0] = sx;
-			acc[1] = sy;
-			cmp[0] = 0;
-			cmp[1] = 0;
-		}
-		__syncthreads();
-		double* out = partial + (size_t)it * NACC;
-		for (int e = tid; e < nacc; e += BT) out[e] = acc[e] - cmp[e];
-		__syncthreads();
+		const int N = 1 << in.L;
+		const int amps = N * (N >= BTr<T>::AMP ? 1 : BTr<T>::AMP >> in.L);
+		if ((size_t)4 * amps * sizeof(V) <= STATE_SMEM)
+			beval_item<T, true>(in, item, it, wires, tabs, partial, gscratch, smem);
+		else
+			beval_item<T, false>(in, item, it, wires, tabs, partial, gscratch, smem);
 	}
 }
 
@@ -437,23 +466,31 @@ k_beval(const BInst* __restrict__ insts, const int4* __restrict__ items, int nit
 
 __device__ __forceinline__ float4 fmt32(double2 v) { return make_float4((float)v.x, (float)v.x, (float)-v.y, (float)v.y); }
 
+// Start of a round: reset the work queues and the live count, advance the round number.
+__global__ void k_bround(int* counters)
+{
+	counters[0] = 0;   // work queue of the complex64 kernel
+	counters[1] = 0;   // work queue of the complex128 kernel
+	counters[2] = 0;   // slots not finished at the start of this round
+	counters[8]++;     // round number
+}
+
 // Per slot: pick the evaluation of this round from the state machine, build the
 // gates (and, for HVPs, the tangent directions) and write the gate tables.
 __global__ void k_bprepare(Slots s, int* counters)
 {
 	const int i = blockIdx.x, t = threadIdx.x;
-	if (i == 0 && t == 0) {
-		counters[0] = 0;   // work queue of the complex64 kernel
-		counters[1] = 0;   // work queue of the complex128 kernel
-		counters[2] = 0;   // active slots after this round
-	}
 	BInst& in = s.inst[i];
 	const BOpt& op = s.opt[i];
 	const int ph = op.phase;
 	const bool live = in.L > 0 && ph != PH_DONE;
+	const bool turn = live && (in.period <= 1 || (counters[8] + i) % in.period == 0);
 	__syncthreads();
-	if (t == 0) in.active = live ? 1 : 0;
-	if (!live) return;
+	if (t == 0) {
+		in.active = turn ? 1 : 0;
+		if (live) atomicAdd(&counters[2], 1);
+	}
+	if (!turn) return;
 	const int nl = in.nl;
 	double* vec = s.vec + (size_t)i * 7 * MAXN;
 	double2* x = s.x + (size_t)i * MAXU * 16;
@@ -579,6 +616,8 @@ __global__ void k_badvance(Slots s, int cap, int fiter_cap, double refine_thresh
 	const BInst in = s.inst[i];
 	if (!in.active) return;
 	BOpt& op = s.opt[i];
+	atomicAdd(reinterpret_cast<unsigned long long*>(counters + 4), 1ull);
+	if (in.mode == EVAL_HVP) atomicAdd(reinterpret_cast<unsigned long long*>(counters + 6), 1ull);
 	const int n = 16 * in.nl;
 	double* vec = s.vec + (size_t)i * 7 * MAXN;
 	double *r = vec, *d = vec + MAXN, *hd = vec + 2 * MAXN, *z = vec + 3 * MAXN, *grad = vec + 4 * MAXN,
@@ -589,6 +628,10 @@ __global__ void k_badvance(Slots s, int cap, int fiter_cap, double refine_thresh
 		op.rtr.fx = op.fval;
 		fiter[op.iter] = op.fval;
 		tcg_init_dev(n, grad, r, d, z, &op.tcg, op.rtr.radius, in.abstol, in.reltol);
+		if (in.gtol > 0 && sqrt(op.tcg.rsq) <= in.gtol) {   // converged: f_iter[iter] is f at the final point
+			op.phase = PH_DONE;
+			break;
+		}
 		if (op.refine && op.hvp_prec != PREC_C128 && sqrt(op.tcg.rsq) < refine_threshold) op.hvp_prec = PREC_C128;
 		op.tcg_it = 0;
 		op.boundary = 0;
@@ -622,8 +665,6 @@ __global__ void k_badvance(Slots s, int cap, int fiter_cap, double refine_thresh
 	if (op.phase == PH_DONE) {
 		const int k = atomicAdd(&counters[3], 1);
 		done_ring[k % ring_cap] = i;
-	} else {
-		atomicAdd(&counters[2], 1);
 	}
 }
 
@@ -645,12 +686,14 @@ struct Batch
 	size_t partial_cap = 0;
 	float2* gs32 = nullptr;
 	double2* gs64 = nullptr;
-	int* counters = nullptr;               // [0] queue c64, [1] queue c128, [2] active, [3] done count
+	int* counters = nullptr;               // [0] queue c64, [1] queue c128, [2] live slots, [3] done count,
+	                                       // [4..5] evaluations, [6..7] HVP evaluations (64-bit), [8] round
 	int* ring = nullptr;
 	int ring_cap = 0;
 	int done_read = 0;
 	int grid = 0;
 	double refine_threshold = 1e-5;
+	bool sharing = false;
 	cudaGraphExec_t graph = nullptr;
 	bool dirty = true;
 	size_t smem32 = 0, smem64 = 0;
@@ -661,8 +704,8 @@ namespace {
 
 size_t eval_smem(size_t elem)
 {
-	constexpr int NTAB = (MAXU * 3 + MAXTU) * 16;
-	return NTAB * elem + 2 * NACC * sizeof(double) + BT * 16 + 2 * (BT / 32) * sizeof(double) + STATE_SMEM;
+	return NTABS * elem + 2 * NACC * sizeof(double) + BT * 16 + 2 * (BT / 32) * sizeof(double) + SWIRES * sizeof(int) +
+	       STATE_SMEM;
 }
 
 int batch_init(Runtime& rt, Batch& b, int cap, int fiter_cap)
@@ -678,7 +721,7 @@ int batch_init(Runtime& rt, Batch& b, int cap, int fiter_cap)
 	             o_t = take(sizeof(double2) * cap * MAXTU * 16), o_t32 = take(sizeof(float4) * cap * NTAB),
 	             o_t64 = take(sizeof(double2) * cap * NTAB), o_v = take(sizeof(double) * cap * 7 * MAXN),
 	             o_f = take(sizeof(double) * cap * (fiter_cap + 1)), o_e = take(sizeof(double) * cap * (2 + 2 * MAXN)),
-	             o_c = take(sizeof(int) * 8), o_r = take(sizeof(int) * cap);
+	             o_c = take(sizeof(int) * 16), o_r = take(sizeof(int) * cap);
 	if (cudaMalloc(&b.mem, off) != cudaSuccess) { cudaGetLastError(); return E_ALLOC; }
 	char* m = static_cast<char*>(b.mem);
 	b.d.inst = reinterpret_cast<BInst*>(m + o_inst);
@@ -725,7 +768,10 @@ int rebuild_items(Runtime& rt, Batch& b)
 			total += per_col * (1 << in.L);
 		}
 	std::sort(live.begin(), live.end(), [](const W& a, const W& c) { return a.cost > c.cost || (a.cost == c.cost && a.slot < c.slot); });
-	const double target = std::max(total / (8.0 * b.grid), 1.0);
+	// item size from the instance alone, so that its partial sums (and results) do not
+	// depend on what else is in the batch
+	const double target = ITEM_WORK;
+	(void)total;
 	b.hitems.clear();
 	bool big = false;
 	for (const W& wv : live) {
@@ -774,6 +820,7 @@ int rebuild_items(Runtime& rt, Batch& b)
 int launch_round(Runtime& rt, Batch& b)
 {
 	const int ni = (int)b.hitems.size();
+	k_bround<<<1, 1, 0, rt.stream>>>(b.counters);
 	k_bprepare<<<b.cap, 64, 0, rt.stream>>>(b.d, b.counters);
 	k_beval<float><<<b.grid, BT, b.smem32, rt.stream>>>(b.d.inst, b.ditems, ni, b.counters + 0, b.d.wires, b.d.tab32,
 	                                                     b.partial, b.gs32, PREC_C64);
@@ -807,7 +854,7 @@ int run_rounds(Runtime& rt, Batch& b, int max_rounds, int check_every)
 	for (int r = 0; r < max_rounds; r++) {
 		if ((ret = RQC_CUDA(cudaGraphLaunch(b.graph, rt.stream)))) return ret;
 		b.rounds++;
-		rt.launches += 5;
+		rt.launches += 6;
 		if ((r + 1) % check_every == 0 || r + 1 == max_rounds) {
 			if ((ret = RQC_CUDA(cudaMemcpyAsync(&active, b.counters + 2, sizeof(int), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
 			if ((ret = sync(rt))) return ret;
@@ -819,7 +866,7 @@ int run_rounds(Runtime& rt, Batch& b, int max_rounds, int check_every)
 
 // Write one problem into a slot (host arrays -> device) with the given phase.
 int load_slot(Runtime& rt, Batch& b, int i, const struct rqcopt_batch_problem* p, const struct rtr_params* params,
-              int niter, int precision, int phase)
+              int niter, int precision, int phase, double gtol = 0)
 {
 	const int L = p->nqubits, nl = p->nlayers, tnl = p->target_nlayers;
 	BInst in{};
@@ -839,6 +886,14 @@ int load_slot(Runtime& rt, Batch& b, int i, const struct rqcopt_batch_problem* p
 	in.maxradius = pp->maxradius;
 	in.rho_trust = pp->rho_trust;
 	in.prec = precision == PREC_C128 ? PREC_C128 : PREC_C64;
+	in.gtol = gtol;
+	in.period = 1;
+	if (b.sharing) {
+		// cost of one evaluation relative to a 10-qubit, 5-layer instance
+		const double cost = std::ldexp(1.0, 2 * L) * (nl + tnl) * (L / 2);
+		const double ref = std::ldexp(1.0, 20) * 8 * 5;
+		in.period = (int)std::min(1024.0, std::max(1.0, std::round(cost / ref)));
+	}
 	BOpt op{};
 	op.phase = phase;
 	op.fprec = precision == PREC_C64 ? PREC_C64 : PREC_C128;
@@ -938,18 +993,19 @@ void rqcopt_batch_destroy(struct rqcopt_batch* h)
 }
 
 int rqcopt_batch_add(struct rqcopt_batch* h, const struct rqcopt_batch_problem* p, const struct rtr_params* params,
-                     int niter, int precision)
+                     int niter, int precision, double grad_tol)
 {
 	Runtime* rt = runtime();
 	if (!rt) return E_CUDA;
-	if (!h || !problem_ok(p) || niter < 0 || niter > h->b.fiter_cap || precision < PREC_C128 || precision > PREC_C64)
+	if (!h || !problem_ok(p) || niter < 0 || niter > h->b.fiter_cap || precision < PREC_C128 || precision > PREC_C64 ||
+	    !(grad_tol >= 0))
 		return E_ARG;
 	Batch& b = h->b;
 	int slot = -1;
 	for (int i = 0; i < b.cap; i++)
 		if (!b.used[i]) { slot = i; break; }
 	if (slot < 0) return E_ALLOC;
-	int ret = load_slot(*rt, b, slot, p, params, niter, precision, PH_GRAD);
+	int ret = load_slot(*rt, b, slot, p, params, niter, precision, PH_GRAD, grad_tol);
 	if (ret) return ret;
 	b.used[slot] = 1;
 	if ((ret = rebuild_items(*rt, b))) return ret;
@@ -984,7 +1040,7 @@ int rqcopt_batch_finished(struct rqcopt_batch* h, int* slots, int max_slots)
 	return avail;
 }
 
-int rqcopt_batch_result(struct rqcopt_batch* h, int slot, double* f_iter, struct mat4x4* vlist_opt)
+int rqcopt_batch_result(struct rqcopt_batch* h, int slot, double* f_iter, struct mat4x4* vlist_opt, int* iterations)
 {
 	Runtime* rt = runtime();
 	if (!rt) return E_CUDA;
@@ -996,6 +1052,7 @@ int rqcopt_batch_result(struct rqcopt_batch* h, int slot, double* f_iter, struct
 	if (ret) return ret;
 	if (op.phase != PH_DONE) return 0;
 	const BInst& in = b.hinst[slot];
+	if (iterations) *iterations = op.iter;
 	if (f_iter)
 		ret = RQC_CUDA(cudaMemcpyAsync(f_iter, b.d.fiter + (size_t)slot * (b.fiter_cap + 1), (in.niter + 1) * sizeof(double),
 		                               cudaMemcpyDeviceToHost, rt->stream));
@@ -1021,6 +1078,25 @@ int rqcopt_batch_release(struct rqcopt_batch* h, int slot)
 }
 
 long rqcopt_batch_rounds(const struct rqcopt_batch* h) { return h ? h->b.rounds : 0; }
+
+int rqcopt_batch_set_sharing(struct rqcopt_batch* h, int on)
+{
+	if (!h) return E_ARG;
+	h->b.sharing = on != 0;   // applies to problems added from now on
+	return 0;
+}
+
+long rqcopt_batch_evaluations(const struct rqcopt_batch* h, long* hvp_evaluations)
+{
+	Runtime* rt = runtime();
+	if (!rt || !h) return E_ARG;
+	unsigned long long c[2] = {0, 0};
+	if (RQC_CUDA(cudaMemcpyAsync(&c[0], h->b.counters + 4, sizeof(c[0]), cudaMemcpyDeviceToHost, rt->stream)) ||
+	    RQC_CUDA(cudaMemcpyAsync(&c[1], h->b.counters + 6, sizeof(c[1]), cudaMemcpyDeviceToHost, rt->stream)) || sync(*rt))
+		return E_CUDA;
+	if (hvp_evaluations) *hvp_evaluations = (long)c[1];
+	return (long)c[0];
+}
 
 size_t rqcopt_batch_footprint(int nqubits, int nlayers)
 {
@@ -1060,7 +1136,7 @@ int rqcopt_brickwall_batch_evaluate(const struct rqcopt_batch_problem* problems,
 	}
 	if (!ret) ret = rebuild_items(*rt, *b);
 	if (!ret) ret = launch_round(*rt, *b);
-	rt->launches += 5;
+	rt->launches += 6;
 	std::vector<double> ev((size_t)count * (2 + 2 * MAXN));
 	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(ev.data(), b->d.evout, ev.size() * sizeof(double), cudaMemcpyDeviceToHost, rt->stream));
 	if (!ret) ret = sync(*rt);

@@ -95,12 +95,14 @@ _SIGS = {
     "rqcopt_optimize_brickwall_batch": (I, [VP, I, VP, I, I, VP, VP]),
     "rqcopt_batch_create": (VP, [I, I]),
     "rqcopt_batch_destroy": (None, [VP]),
-    "rqcopt_batch_add": (I, [VP, VP, VP, I, I]),
+    "rqcopt_batch_add": (I, [VP, VP, VP, I, I, D]),
     "rqcopt_batch_run": (I, [VP, I]),
     "rqcopt_batch_finished": (I, [VP, VP, I]),
-    "rqcopt_batch_result": (I, [VP, I, VP, VP]),
+    "rqcopt_batch_result": (I, [VP, I, VP, VP, VP]),
     "rqcopt_batch_release": (I, [VP, I]),
     "rqcopt_batch_rounds": (C.c_long, [VP]),
+    "rqcopt_batch_set_sharing": (I, [VP, I]),
+    "rqcopt_batch_evaluations": (C.c_long, [VP, C.POINTER(C.c_long)]),
     "rqcopt_batch_footprint": (C.c_size_t, [I, I]),
 }
 

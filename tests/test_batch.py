@@ -138,3 +138,26 @@ def test_batch_slots_admit_and_retire(gpu):
     assert sorted(results) == [0, 1, 2, 3]
     for k in range(4):
         assert np.max(np.abs(results[k] - alone[k])) <= 1e-12 * np.max(np.abs(alone[k])), k
+
+
+def test_serving_mix_equals_alone(gpu):
+    """Requests admitted into a running batch as they arrive: every result is
+    bit-identical to the same request run alone."""
+    from rqcopt_hpc_b200 import batch, serving
+    from rqcopt_hpc_b200.workloads import brickwall_problem
+    reqs = [serving.Request(k, brickwall_problem(L, d, 3, 500 + k, 600 + k), 6, 1e-8, 0.002 * k,
+                            gpu.PRECISION_MIXED)
+            for k, (L, d) in enumerate([(6, 3), (8, 5), (4, 3), (10, 3), (6, 7), (8, 3), (12, 3), (4, 5)])]
+    b = batch.Batch(capacity=4, max_iterations=6, sharing=True)
+    srv = serving.Server(b, capacity=4, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=3)
+    done, left = serving.run_arrivals(srv, reqs, wall_limit=300.0)
+    b.close()
+    assert not left and len(done) == len(reqs)
+    for r in done:
+        alone = batch.Batch(capacity=1, max_iterations=6)
+        s = alone.add(r.problem, r.niter, r.precision, grad_tol=r.grad_tol)
+        while alone.run(8) > 0:
+            pass
+        f_alone, _ = alone.result(s)
+        alone.close()
+        assert np.array_equal(r.f_iter, f_alone), (r.rid, r.f_iter, f_alone)
