@@ -38,6 +38,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
+# DRAM traffic / algorithmic bytes of the reverse-pass kernel, from ncu
+# (complex64 k4_rev: 789.9 MB measured for 805.3 MB algorithmic at L=12)
+TRAFFIC_RATIO = {8: 0.981}
+
 METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns; mixed vs FP64)"
 
 
@@ -174,49 +178,123 @@ def cpu_baseline(L, depth, tdepth, seconds=15.0, cores=None):
 
 def gate_throughput(gpu, torch, L=28, G=256, seed=20):
     """Forward through G Haar gates on uniformly random distinct qubit pairs, then the
-    adjoint gates in reverse order, on one L-qubit complex128 state resident in HBM,
-    with 1 and with 4 gates per HBM round trip; DRAM GB/s counts one read and one write
-    of the state per round trip."""
+    adjoint gates in reverse order, on one L-qubit state resident in HBM (complex128,
+    then complex64), with 1 and with 4 gates per HBM round trip; DRAM GB/s counts one
+    read and one write of the state per round trip."""
+    import ctypes
+    from rqcopt_hpc_b200.abi import Statevector
     rng = np.random.default_rng(seed)
     gates = np.stack([haar(rng) for _ in range(G)])
     wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
     adj = np.ascontiguousarray(np.conj(np.transpose(gates[::-1], (0, 2, 1))))
     wires_rev = np.ascontiguousarray(wires[::-1])
-    gen = torch.Generator(device="cuda").manual_seed(seed)
-    psi = torch.randn(1 << L, dtype=torch.complex128, device="cuda", generator=gen)
-    psi /= torch.linalg.vector_norm(psi)
-    out, back = torch.empty_like(psi), torch.empty_like(psi)
     lib = gpu.lib()
-    from rqcopt_hpc_b200.abi import Statevector
-    import ctypes
-    sv = lambda t: ctypes.byref(Statevector(t.data_ptr(), L))
     stream = torch.cuda.ExternalStream(lib.rqcopt_gpu_stream())
-    state_bytes = (1 << L) * 16
-    res = {"workload": f"one L={L} complex128 state ({state_bytes / 2**30:.0f} GiB), {G} Haar gates on random "
-                       f"distinct pairs, forward then adjoint backward"}
-    for gpp in (1, 4):
-        gpu.set_gates_per_pass(gpp)
-        lib.apply_quantum_circuit(gates.ctypes.data, G, wires.ctypes.data, sv(psi), sv(out))   # warm-up
-        torch.cuda.synchronize()
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-        e[0].record(stream)
-        lib.apply_quantum_circuit(gates.ctypes.data, G, wires.ctypes.data, sv(psi), sv(out))
-        e[1].record(stream)
-        lib.apply_quantum_circuit(adj.ctypes.data, G, wires_rev.ctypes.data, sv(out), sv(back))
-        e[2].record(stream)
-        torch.cuda.synchronize()
-        t_f, t_b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
-        trips = G if gpp == 1 else -(-G // gpp)
-        err = float(torch.max(torch.abs(back - psi)))
-        res[f"gates_per_round_trip_{gpp}"] = {
-            "forward_ms": t_f, "backward_ms": t_b, "round_trips": trips,
-            "dram_gbs": 2 * trips * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
-            "gate_equivalent_gbs": 2 * G * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
-            "recovery_max_abs_err": err}
+    res = {"workload": f"one L={L} state, {G} Haar gates on random distinct pairs, forward then adjoint backward"}
+    for dtype, name, tol in ((torch.complex128, "c128", 1e-12), (torch.complex64, "c64", 1e-5)):
+        gen = torch.Generator(device="cuda").manual_seed(seed)
+        psi = torch.randn(1 << L, dtype=dtype, device="cuda", generator=gen)
+        psi /= torch.linalg.vector_norm(psi)
+        out, back = torch.empty_like(psi), torch.empty_like(psi)
+        state_bytes = (1 << L) * psi.element_size()
+        if name == "c128":
+            sv = lambda t: ctypes.byref(Statevector(t.data_ptr(), L))
+            run = lambda g, w, a, b: lib.apply_quantum_circuit(g.ctypes.data, G, w.ctypes.data, sv(a), sv(b))
+        else:
+            run = lambda g, w, a, b: lib.rqcopt_apply_quantum_circuit_c64(g.ctypes.data, G, w.ctypes.data, a.data_ptr(),
+                                                                          b.data_ptr(), L)
+        r = {"state_gib": state_bytes / 2 ** 30, "recovery_tolerance": tol}
+        for gpp in (1, 4):
+            gpu.set_gates_per_pass(gpp)
+            run(gates, wires, psi, out)   # warm-up
+            torch.cuda.synchronize()
+            e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+            e[0].record(stream)
+            run(gates, wires, psi, out)
+            e[1].record(stream)
+            run(adj, wires_rev, out, back)
+            e[2].record(stream)
+            torch.cuda.synchronize()
+            t_f, t_b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
+            trips = G if gpp == 1 else -(-G // gpp)
+            err = float(torch.max(torch.abs(back - psi)))
+            r[f"gates_per_round_trip_{gpp}"] = {
+                "forward_ms": t_f, "backward_ms": t_b, "round_trips": trips,
+                "dram_gbs": 2 * trips * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
+                "gate_equivalent_gbs": 2 * G * 2 * state_bytes / ((t_f + t_b) * 1e-3) / 1e9,
+                "recovery_max_abs_err": err, "recovered": err <= tol}
+        res[name] = r
+        del psi, out, back
+        torch.cuda.empty_cache()
     gpu.set_gates_per_pass(4)
-    del psi, out, back
-    torch.cuda.empty_cache()
     return res
+
+
+# ----------------------------------------------------------------------------- batched and serving
+
+def batched_c4(gpu, torch, count=512, niter=2):
+    """512 independent brickwall instances (even L uniform over 6..12, depth over
+    {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), niter trust-region iterations
+    each: the batched complex64 path (one persistent kernel per round, CUDA-graph
+    rounds) against the plain per-instance complex128 optimiser loop."""
+    from rqcopt_hpc_b200 import batch
+    from rqcopt_hpc_b200.workloads import batched_instances
+    probs = batched_instances(count)
+    out = {"workload": f"{count} brickwall instances, L in {{6,8,10,12}}, depth in {{3,5,7,9}}, {niter} RTR iterations"}
+    b = batch.Batch(count, niter)
+    for p in probs:
+        b.add(p, niter, gpu.PRECISION_C64)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    while b.run(32) > 0:
+        pass
+    torch.cuda.synchronize()
+    tb = time.perf_counter() - t0
+    ev, hv = b.evaluations()
+    fb = np.array([b.result(s)[0][-1] for s in range(count)])
+    b.close()
+    gpu.set_precision(gpu.PRECISION_C128)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fp = []
+    for (L, vl, pm, tv, tp) in probs:
+        f, _ = gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, niter)
+        fp.append(f[-1])
+    torch.cuda.synchronize()
+    tp_ = time.perf_counter() - t0
+    fp = np.array(fp)
+    out["batched_c64"] = {"seconds": tb, "evaluations": ev, "hvp_evaluations": hv, "evals_per_s": ev / tb,
+                          "instance_iterations_per_s": count * niter / tb}
+    out["per_instance_c128"] = {"seconds": tp_, "instance_iterations_per_s": count * niter / tp_}
+    out["speedup"] = tp_ / tb
+    out["f_final_max_rel_diff"] = float(np.max(np.abs(fb - fp) / np.abs(fp)))
+    return out
+
+
+def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-8):
+    """Poisson arrivals (seed 40) of brickwall optimisation requests (even L in 8..14,
+    P(L) ~ 2^(-(L-8)/2), depth in {3,5,7,9}, target depth 3), each stopping at gradient
+    norm grad_tol or after niter iterations, admitted into a running batch within a
+    150 GB device budget; p50 / p99 time from arrival to completion of the requests
+    completed within `wall` seconds (the offered load far exceeds one GPU, so the
+    latencies are queue-dominated and the rest is reported as still running)."""
+    from rqcopt_hpc_b200 import batch, serving
+    reqs = serving.c5_requests(rate=rate, duration=duration, niter=niter, grad_tol=grad_tol,
+                               precision=gpu.PRECISION_MIXED)
+    b = batch.Batch(capacity=4096, max_iterations=niter, sharing=True)
+    srv = serving.Server(b, capacity=4096, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=4)
+    t0 = time.perf_counter()
+    done, left = serving.run_arrivals(srv, reqs, wall_limit=wall)
+    el = time.perf_counter() - t0
+    ev, hv = b.evaluations()
+    b.close()
+    out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s ({len(reqs)} requests), measured for {wall:g} s",
+           "precision": "mixed", "wall_s": el, "completed": len(done), "still_running_or_queued": len(left),
+           "completed_per_s": len(done) / el, "evaluations": ev, "rounds": srv.rounds}
+    out.update(serving.latency_stats(done))
+    if done:
+        out["mean_iterations"] = float(np.mean([r.iterations for r in done]))
+    return out
 
 
 # ----------------------------------------------------------------------------- mixed vs plain
@@ -283,6 +361,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate-throughput", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the complex128 comparison and the RTR runs")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 512-instance batched measurement")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--serving-wall", type=float, default=45.0)
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -393,6 +474,13 @@ def main():
         rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
         achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
         value = world * a.steps / (dev_ms * 1e-3)
+        # DRAM bytes per launch: the algorithmic bytes per launch times the traffic /
+        # algorithmic ratio measured by ncu on a smaller case of the same kernel
+        # (dram__bytes_read + dram__bytes_write of one middle pass at L=12)
+        ratio = TRAFFIC_RATIO.get(itemsize) if a.gates_per_pass > 1 else None
+        traffic = rbytes / max(rev_n, 1) * ratio if ratio else None
+        traffic_src = (f"ncu capture of one middle pass at L=12 (traffic / algorithmic = {ratio}), "
+                       "scaled to the bytes of an average launch here") if ratio else None
         flops = flops_per_eval(L, G, Gt)
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": a.steps,
@@ -412,7 +500,8 @@ def main():
                          "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                          "frac": achieved / hbm_peak if achieved else None,
                          "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650",
-                         "traffic": None, "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)},
+                         "traffic": traffic, "traffic_source": traffic_src,
+                         "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)},
             "kernel_share": {"reverse_ms": rev_ms, "forward_ms": fwd_ms, "apply_ms": app_ms,
                              "fused_forward_ms": fus_ms, "device_ms": dev_ms},
             "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
@@ -425,6 +514,12 @@ def main():
             gpu.set_precision(prec)
         if not a.no_gate_throughput:
             line["gate_throughput"] = gate_throughput(gpu, torch)
+        if not a.no_batched and world == 1:
+            line["batched"] = batched_c4(gpu, torch)
+            gpu.set_precision(prec)
+        if not a.no_serving and world == 1:
+            line["serving"] = serving_c5(gpu, wall=a.serving_wall)
+            gpu.set_precision(prec)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)
         print(json.dumps(line))

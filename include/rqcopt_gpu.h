@@ -337,6 +337,14 @@ int  rqcopt_gpu_kernel_time(int kernel_class, double* total_ms, long* launches);
 /* the CUDA stream (cudaStream_t) all library work is issued on */
 void* rqcopt_gpu_stream(void);
 
+/* Addition (no counterpart in the reference): apply_quantum_circuit
+ * (src/quantum_circuit.h:7, src/quantum_circuit.c:13-35) on complex64 states
+ * already in device memory (psi, psi_out: 2^nqubits float2 each, distinct);
+ * gates are complex128 host matrices, rounded to complex64 for the passes.
+ * Returns 0, or -5 (CUDA) / -6 (invalid argument, host pointers). */
+int rqcopt_apply_quantum_circuit_c64(const struct mat4x4 gates[], int ngates, const int wires[], const void* psi,
+                                     void* psi_out, int nqubits);
+
 /*
  * Allocation-free gate backward pass.  No counterpart in the reference; it
  * computes what apply_gate_backward (src/gate.h:9-10) computes, without any

@@ -154,3 +154,36 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def _main():
+    """python -m rqcopt_hpc_b200.batch: optimise `count` seeded brickwall instances together."""
+    import argparse
+    import time
+    from .workloads import batched_instances, brickwall_problem
+    ap = argparse.ArgumentParser(description=_main.__doc__)
+    ap.add_argument("--count", type=int, default=512)
+    ap.add_argument("--L", type=int, default=0, help="fixed qubit count (default: even L uniform over 6..12)")
+    ap.add_argument("--niter", type=int, default=2)
+    ap.add_argument("--precision", default="c64", choices=["c64", "mixed", "c128"])
+    a = ap.parse_args()
+    prec = {"c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED, "c128": gpu.PRECISION_C128}[a.precision]
+    if a.L:
+        probs = [brickwall_problem(a.L, (3, 5, 7, 9)[i % 4], 3, 30 + i, 10000 + i) for i in range(a.count)]
+    else:
+        probs = batched_instances(a.count)
+    b = Batch(a.count, a.niter)
+    for p in probs:
+        b.add(p, a.niter, prec)
+    t0 = time.perf_counter()
+    while b.run(8) > 0:
+        pass
+    el = time.perf_counter() - t0
+    ev, hv = b.evaluations()
+    print(f"{a.count} instances x {a.niter} iterations ({a.precision}): {el:.3f} s, {b.rounds} rounds, "
+          f"{ev} evaluations ({hv} HVP), {ev / el:.1f} evaluations/s")
+    b.close()
+
+
+if __name__ == "__main__":
+    _main()

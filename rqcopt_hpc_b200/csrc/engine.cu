@@ -629,6 +629,27 @@ int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, c
 	return OK;
 }
 
+int apply_circuit_device_c64(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const float2* d_in,
+                             float2* d_out)
+{
+	if (rt.gates_per_pass > 1 && L >= 10)
+		return apply_circuit_fused_device_c64(rt, L, ngates, gates, wires, d_in, d_out, rt.gates_per_pass);
+	const size_t bytes = ((size_t)1 << L) * sizeof(float2);
+	int ret;
+	if (ngates > 1 && (ret = ensure_device(rt.stage[3], bytes))) return ret;
+	float2* tmp = reinterpret_cast<float2*>(rt.stage[3].ptr);
+	const float2* src = d_in;
+	const int64_t ngroups = (int64_t)1 << (L - 2);
+	for (int k = 0; k < ngates; k++) {
+		float2* dst = ((ngates - 1 - k) % 2 == 0) ? d_out : tmp;
+		if ((ret = launch_apply<float>(rt, 0, 0, src, dst, nullptr, to_gate<float>(gates + 16 * k),
+		                               make_pair_(L, wires[2 * k], wires[2 * k + 1]), L, ngroups, 0, nullptr, 0)))
+			return ret;
+		src = dst;
+	}
+	return OK;
+}
+
 int gate_backward_device(Runtime& rt, int L, const double2* gate, int i, int j, const double2* d_psi,
                          const double2* d_dout, double2* d_dpsi, double2* d_dgate)
 {

@@ -48,6 +48,12 @@ int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, c
 // (shared-memory tiles over the gates' qubits plus the lowest amplitude bits).
 int apply_circuit_fused_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
                                const double2* d_in, double2* d_out, int maxk);
+int apply_circuit_fused_device_c64(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
+                                   const float2* d_in, float2* d_out, int maxk);
+// out = C in for one complex64 statevector (per-gate passes, or fused passes of
+// up to gates_per_pass gates for L >= 10)
+int apply_circuit_device_c64(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const float2* d_in,
+                             float2* d_out);
 
 // Single-gate kernels on device statevectors (ncols states one after another).
 int gate_apply_device(Runtime& rt, int L, const double2* gate, int i, int j,

@@ -14,6 +14,7 @@
 
 #include "engine.h"
 #include "rqc_common.cuh"
+#include "rqcopt_gpu.h"
 
 namespace rqc {
 
@@ -127,27 +128,31 @@ std::vector<SvPass> sv_schedule(int L, int G, const int* wires, int maxk)
 
 }  // namespace
 
-// out = C in for one statevector (complex128), maxk gates per pass; in and out may not alias.
-int apply_circuit_fused_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
-                               const double2* d_in, double2* d_out, int maxk)
+template <typename T>
+int apply_circuit_fused_t(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const cplx<T>* d_in,
+                          cplx<T>* d_out, int maxk)
 {
 	maxk = std::max(1, std::min(SV_MAXK, maxk));
 	std::vector<SvPass> passes = sv_schedule(L, ngates, wires, maxk);
 	const int P = (int)passes.size();
-	const size_t bytes = ((size_t)1 << L) * sizeof(double2);
+	const size_t bytes = ((size_t)1 << L) * sizeof(cplx<T>);
 	int ret;
 	if (P > 1 && (ret = ensure_device(rt.stage[3], bytes))) return ret;
-	double2* tmp = reinterpret_cast<double2*>(rt.stage[3].ptr);
-	const double2* src = d_in;
+	cplx<T>* tmp = reinterpret_cast<cplx<T>*>(rt.stage[3].ptr);
+	const cplx<T>* src = d_in;
 	for (int p = 0; p < P; p++) {
-		double2* dst = ((P - 1 - p) % 2 == 0) ? d_out : tmp;
-		SvGates<double> sg;
+		cplx<T>* dst = ((P - 1 - p) % 2 == 0) ? d_out : tmp;
+		SvGates<T> sg;
 		for (int k = 0; k < passes[p].K; k++)
-			for (int e = 0; e < 16; e++) sg.g[k].m[e] = gates[16 * (passes[p].first + k) + e];
+			for (int e = 0; e < 16; e++) {
+				const double2 g = gates[16 * (passes[p].first + k) + e];
+				sg.g[k].m[e].x = (T)g.x;
+				sg.g[k].m[e].y = (T)g.y;
+			}
 		const int grid = (int)std::min<int64_t>(passes[p].ntiles, (int64_t)rt.num_sms * 8);
 		cudaEvent_t ev;
 		launch_begin(rt, KC_FUSED, &ev);
-		k_sv_pass<double><<<grid, SV_TPB, 0, rt.stream>>>(src, dst, passes[p], sg);
+		k_sv_pass<T><<<grid, SV_TPB, 0, rt.stream>>>(src, dst, passes[p], sg);
 		launch_end(rt, KC_FUSED, ev);
 		if ((ret = RQC_CUDA(cudaGetLastError()))) return ret;
 		src = dst;
@@ -155,4 +160,39 @@ int apply_circuit_fused_device(Runtime& rt, int L, int ngates, const double2* ga
 	return OK;
 }
 
+// out = C in for one statevector (complex128), maxk gates per pass; in and out may not alias.
+int apply_circuit_fused_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
+                               const double2* d_in, double2* d_out, int maxk)
+{
+	return apply_circuit_fused_t<double>(rt, L, ngates, gates, wires, d_in, d_out, maxk);
+}
+
+int apply_circuit_fused_device_c64(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,
+                                   const float2* d_in, float2* d_out, int maxk)
+{
+	return apply_circuit_fused_t<float>(rt, L, ngates, gates, wires, d_in, d_out, maxk);
+}
+
 }  // namespace rqc
+
+using namespace rqc;
+
+// The complex64 form of apply_quantum_circuit (src/quantum_circuit.c:13-35) on
+// device-resident complex64 states; gates stay complex128 on the host and are
+// rounded to complex64 for the passes.
+extern "C" int rqcopt_apply_quantum_circuit_c64(const struct mat4x4 gates[], int ngates, const int wires[],
+                                                const void* psi, void* psi_out, int nqubits)
+{
+	if (nqubits < 2 || nqubits > 34 || ngates < 1 || !gates || !wires || !psi || !psi_out || psi == psi_out) return E_ARG;
+	for (int k = 0; k < ngates; k++)
+		if (wires[2 * k] < 0 || wires[2 * k] >= nqubits || wires[2 * k + 1] < 0 || wires[2 * k + 1] >= nqubits ||
+		    wires[2 * k] == wires[2 * k + 1])
+			return E_ARG;
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	if (!is_device_pointer(psi) || !is_device_pointer(psi_out)) return E_ARG;
+	int ret = apply_circuit_device_c64(*rt, nqubits, ngates, reinterpret_cast<const double2*>(gates), wires,
+	                                   static_cast<const float2*>(psi), static_cast<float2*>(psi_out));
+	if (!ret) ret = sync(*rt);
+	return ret;
+}

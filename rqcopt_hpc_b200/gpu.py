@@ -91,6 +91,7 @@ _SIGS = {
     "rqcopt_gpu_enable_kernel_timing": (None, [I]),
     "rqcopt_gpu_kernel_time": (I, [I, PD, C.POINTER(C.c_long)]),
     "rqcopt_gpu_stream": (VP, []),
+    "rqcopt_apply_quantum_circuit_c64": (I, [VP, I, VP, VP, VP, I]),
     "rqcopt_brickwall_batch_evaluate": (I, [VP, I, VP, I, I, VP, VP, VP]),
     "rqcopt_optimize_brickwall_batch": (I, [VP, I, VP, I, I, VP, VP]),
     "rqcopt_batch_create": (VP, [I, I]),

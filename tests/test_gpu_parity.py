@@ -189,3 +189,39 @@ def test_single_state_fused_passes(gpu, oracle, per_pass):
     gpu.set_gates_per_pass(4)
     ref = oracle.apply_quantum_circuit(gates, wires, psi)
     assert rel_err(out, ref) <= 1e-12
+
+
+@pytest.mark.parametrize("gpp", [1, 4])
+def test_complex64_circuit_matches_complex128(gpu, gpp):
+    """rqcopt_apply_quantum_circuit_c64 against apply_quantum_circuit (complex128) on
+    random pairs, per-gate and fused passes; the adjoint circuit recovers the input."""
+    import ctypes
+    import torch
+    from rqcopt_hpc_b200.abi import Statevector
+    L, G = 12, 24
+    rng = np.random.default_rng(77)
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    adj = np.ascontiguousarray(np.conj(np.transpose(gates[::-1], (0, 2, 1))))
+    wrev = np.ascontiguousarray(wires[::-1])
+    psi = crandn(1 << L, rng)
+    psi /= np.linalg.norm(psi)
+    gpu.set_gates_per_pass(gpp)
+    try:
+        ref = np.empty_like(psi)
+        assert gpu.lib().apply_quantum_circuit(gates.ctypes.data, G, wires.ctypes.data,
+                                               ctypes.byref(Statevector(psi.ctypes.data, L)),
+                                               ctypes.byref(Statevector(ref.ctypes.data, L))) == 0
+        x = torch.from_numpy(psi.astype(np.complex64)).cuda()
+        y, z = torch.empty_like(x), torch.empty_like(x)
+        assert gpu.lib().rqcopt_apply_quantum_circuit_c64(gates.ctypes.data, G, wires.ctypes.data, x.data_ptr(),
+                                                          y.data_ptr(), L) == 0
+        assert gpu.lib().rqcopt_apply_quantum_circuit_c64(adj.ctypes.data, G, wrev.ctypes.data, y.data_ptr(),
+                                                          z.data_ptr(), L) == 0
+        assert np.max(np.abs(y.cpu().numpy() - ref)) <= 1e-5 * np.max(np.abs(ref))
+        assert np.max(np.abs(z.cpu().numpy() - psi)) <= 1e-5 * np.max(np.abs(psi))
+        # host pointers are rejected
+        assert gpu.lib().rqcopt_apply_quantum_circuit_c64(gates.ctypes.data, G, wires.ctypes.data, psi.ctypes.data,
+                                                          ref.ctypes.data, L) == -6
+    finally:
+        gpu.set_gates_per_pass(4)
