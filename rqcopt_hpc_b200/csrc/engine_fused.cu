@@ -66,6 +66,8 @@ struct PassGeom
 };
 
 template <typename T> struct PassGates { Gate4<T> g[MAXK]; Gate4<T> z[MAXK]; };
+// W_k = G_k^+ Z_k G_k^+ of each gate of a pass (adjoint reconstruction of the tangent state)
+template <typename T> struct PassW { Gate4<T> w[MAXK]; };
 
 // deposit the bits of v into the positions set in mask (ascending)
 __device__ __forceinline__ int64_t deposit(int64_t v, uint32_t mask)
@@ -1024,7 +1026,8 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
                                                  const float2* __restrict__ phi, PassGeom pg, PassGates<float> gates,
                                                  double2* __restrict__ fpart)
 {
-	constexpr int NS = (TAN ? 2 : 1) + (OUT == 2 ? 1 : 0);
+	constexpr bool FSUM = OUT >= 2;            // sum f = phi . psi (OUT 2: only that; OUT 3: also write psi)
+	constexpr int NS = (TAN ? 2 : 1) + (FSUM ? 1 : 0);
 	constexpr int CPT = (1 << MAXNB) * 4 / NT4F;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int R = 1 << pg.NB, K = pg.K;
@@ -1074,7 +1077,7 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 				    make_float4(row == pg.b0 + col ? 1.f : 0.f, 0.f, row == pg.b0 + col + 1 ? 1.f : 0.f, 0.f);
 				if (TAN) *reinterpret_cast<float4*>(stage(buf, 1) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
 			}
-			if (OUT == 2) cp_async16(stage(buf, NS - 1) + pe, phi + a);
+			if (FSUM) cp_async16(stage(buf, NS - 1) + pe, phi + a);
 		}
 		cp_async_commit();
 	};
@@ -1113,10 +1116,12 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
 			const int pe = prow(r) * CW4 + c2i;
 			const float4 v = *reinterpret_cast<const float4*>(stage(buf, 0) + pe);
-			if (OUT == 2) {
+			if (FSUM) {
 				const float4 p = *reinterpret_cast<const float4*>(stage(buf, NS - 1) + pe);
 				fx += (double)p.x * v.x - (double)p.y * v.y + (double)p.z * v.z - (double)p.w * v.w;
 				fy += (double)p.x * v.y + (double)p.y * v.x + (double)p.z * v.w + (double)p.w * v.z;
+			}
+			if (OUT == 2) {
 			} else if (OUT == 1) {
 				*reinterpret_cast<float4*>(psi_o + a) = make_float4(-v.x, v.y, -v.z, v.w);
 			} else {
@@ -1125,7 +1130,7 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 			}
 		}
 	}
-	if (OUT == 2) {
+	if (FSUM) {
 		__shared__ double red[2][NT4F / 32];
 		fx = warp_sum(fx);
 		fy = warp_sum(fy);
@@ -1362,6 +1367,239 @@ __global__ void __launch_bounds__(NT4R, 1) k4_rev(const float2* __restrict__ psi
 	}
 }
 
+// B fragment of the embedding of m (tr: m^T; conj: conj(m); neg: -m), split:
+// f[0..1] big, f[2..3] small parts (rows t, t+4; column g).
+__device__ __forceinline__ void bfrag4x(const float2* m, bool tr, bool conj, bool neg, int lane, uint32_t f[4])
+{
+	const int t = lane & 3, g = lane >> 2;
+#pragma unroll
+	for (int h = 0; h < 2; h++) {
+		const int rowk = t + 4 * h, coln = g;
+		const int r = rowk >> 1, a = rowk & 1, c = coln >> 1, b = coln & 1;
+		float2 v = tr ? m[4 * c + r] : m[4 * r + c];
+		if (conj) v.y = -v.y;
+		if (neg) { v.x = -v.x; v.y = -v.y; }
+		const float x = a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
+		tf32_split(x, f[h], f[2 + h]);
+	}
+}
+
+constexpr int NT5 = 256;   // threads of the reconstructing complex64 reverse kernel (two blocks per SM)
+
+// shared memory of k5_rev: gate matrices (G, Z, W), per-lane fragment and offset
+// tables of every gate, unit bases, and the four state tiles (two without tangents)
+inline size_t k5_rev_smem(bool tan)
+{
+	return 48 * MAXK * sizeof(float2) + MAXK * 32 * 16 * sizeof(uint32_t) + MAXK * 5 * 32 * sizeof(int) +
+	       MAXK * 32 * sizeof(int) + (tan ? 4 : 2) * (size_t)AMAX4 * sizeof(float2);
+}
+
+// Reverse pass (complex64) for unitary gates: starts from the state at the OUTPUT of
+// the pass (psi, dpsi = the next pass's checkpoint) and walks back through the pass,
+// rebuilding the state entering each gate with the adjoint gate,
+//   psi_k = G^+ psi_{k+1},  dpsi_k = G^+ dpsi_{k+1} - (G^+ Z G^+) psi_{k+1},
+// so no state inside the pass is recomputed or kept: four tiles, updated in place.
+// Partial sums, scratch and the other arguments as in k4_rev.
+template <bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT5, 2) k5_rev(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+                                                 const float2* __restrict__ phi, const float2* __restrict__ dphi,
+                                                 float2* __restrict__ phi_o, float2* __restrict__ dphi_o, PassGeom pg,
+                                                 PassGates<float> gates, PassW<float> wg, double* __restrict__ part,
+                                                 int nblk, double* __restrict__ scratch)
+{
+	constexpr int CPT = (1 << MAXNB) * 4 / NT5;   // 16-byte chunks per thread and state
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, K = pg.K, units = R / 8;
+	float2* sg = reinterpret_cast<float2*>(smem_raw);                       // [MAXK][48]: G, Z, W
+	uint4* sfr = reinterpret_cast<uint4*>(sg + 48 * MAXK);                  // [MAXK][4][32] fragments
+	int* slc = reinterpret_cast<int*>(sfr + MAXK * 4 * 32);                 // [MAXK][5][32] lane offsets
+	int* sub = slc + MAXK * 5 * 32;                                          // [MAXK][32] unit bases
+	float2* Psi = reinterpret_cast<float2*>(sub + MAXK * 32);
+	float2* Phi = Psi + AMAX4;
+	float2* dPsi = TAN ? Phi + AMAX4 : nullptr;
+	float2* dPhi = TAN ? Phi + 2 * AMAX4 : nullptr;
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	for (int e = threadIdx.x; e < 48 * MAXK; e += blockDim.x) {
+		const int k = e / 48, w = e % 48;
+		if (k >= K) continue;
+		float2 v = make_float2(0.f, 0.f);
+		if (w < 16) v = gates.g[k].m[w];
+		else if (TAN && w < 32) v = gates.z[k].m[w - 16];
+		else if (TAN) v = wg.w[k].m[w - 32];
+		sg[e] = v;
+	}
+	__syncthreads();
+	if (warp < K) {   // one warp per gate builds its lane tables
+		const int k = warp;
+		const Lane4 ln(pg.gi[k], pg.gj[k], lane);
+		uint32_t f[16];
+		bfrag4x(sg + 48 * k, false, true, false, lane, f);            // G^+ (row-vector operand conj(G))
+		bfrag4x(sg + 48 * k + 32, true, false, true, lane, f + 4);    // -W
+		bfrag4x(sg + 48 * k, false, false, false, lane, f + 8);       // G^T (operand G)
+		bfrag4x(sg + 48 * k + 16, false, false, false, lane, f + 12); // Z^T (operand Z)
+#pragma unroll
+		for (int q = 0; q < 4; q++) sfr[(k * 4 + q) * 32 + lane] = make_uint4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+		slc[(k * 5 + 0) * 32 + lane] = ln.E0;
+		slc[(k * 5 + 1) * 32 + lane] = ln.LA;
+		slc[(k * 5 + 2) * 32 + lane] = ln.LB;
+		slc[(k * 5 + 3) * 32 + lane] = ln.LS;
+		slc[(k * 5 + 4) * 32 + lane] = ln.LO;
+		for (int u = lane; u < units; u += 32) sub[k * 32 + u] = ln.unit_base(u);
+	}
+	int ro[CPT];
+#pragma unroll
+	for (int i = 0; i < CPT; i++) {
+		const int r = (threadIdx.x + i * NT5) >> 2;
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		ro[i] = o;
+	}
+	double* scr = scratch + ((size_t)blockIdx.x * nwarps + warp) * 32 * MAXK * 4 + (size_t)lane * MAXK * 4;
+#pragma unroll
+	for (int v = 0; v < MAXK * 4; v++) scr[v] = 0;
+	// outer sums: cx = [P; dP]^T X (rows 0-7 dG, rows 8-15 dP^T X), cd = [P; dP]^T dX (rows 0-7 P^T dX)
+	float cx[MAXK][4], cd[MAXK][4];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++)
+#pragma unroll
+		for (int v = 0; v < 4; v++) { cx[k][v] = 0; cd[k][v] = 0; }
+	auto flush = [&]() {
+#pragma unroll
+		for (int k = 0; k < MAXK; k++) {
+			scr[k * 4 + 0] += (double)cx[k][0];
+			scr[k * 4 + 1] += (double)cx[k][1];
+			scr[k * 4 + 2] += (double)cx[k][2] + (double)cd[k][0];
+			scr[k * 4 + 3] += (double)cx[k][3] + (double)cd[k][1];
+#pragma unroll
+			for (int v = 0; v < 4; v++) { cx[k][v] = 0; cd[k][v] = 0; }
+		}
+	};
+	__syncthreads();
+	float* fPsi = reinterpret_cast<float*>(Psi);
+	float* fdPsi = reinterpret_cast<float*>(dPsi);
+	float* fPhi = reinterpret_cast<float*>(Phi);
+	float* fdPhi = reinterpret_cast<float*>(dPhi);
+	int ntile = 0;
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cgp * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT; i++) {
+			const int e = threadIdx.x + i * NT5;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			cp_async16(Psi + pe, psi + a);
+			cp_async16(Phi + pe, phi + a);
+			if (TAN) {
+				cp_async16(dPsi + pe, dpsi + a);
+				if (FIRST) *reinterpret_cast<float4*>(dPhi + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+				else cp_async16(dPhi + pe, dphi + a);
+			}
+		}
+		cp_async_commit();
+		cp_async_wait_all();
+		__syncthreads();
+#pragma unroll
+		for (int k = MAXK - 1; k >= 0; k--) {
+			if (k >= K) continue;
+			const uint4 q0 = sfr[(k * 4 + 0) * 32 + lane], q1 = sfr[(k * 4 + 1) * 32 + lane];
+			const uint4 q2 = sfr[(k * 4 + 2) * 32 + lane], q3 = sfr[(k * 4 + 3) * 32 + lane];
+			const uint32_t rcb[2] = { q0.x, q0.y }, rcs[2] = { q0.z, q0.w };
+			const uint32_t wb[2] = { q1.x, q1.y }, ws[2] = { q1.z, q1.w };
+			const uint32_t gb[2] = { q2.x, q2.y }, gs[2] = { q2.z, q2.w };
+			const uint32_t zb[2] = { q3.x, q3.y }, zs[2] = { q3.z, q3.w };
+			const int E0 = slc[(k * 5 + 0) * 32 + lane], LA = slc[(k * 5 + 1) * 32 + lane];
+			const int LB = slc[(k * 5 + 2) * 32 + lane], LS = slc[(k * 5 + 3) * 32 + lane];
+			const int LO = slc[(k * 5 + 4) * 32 + lane];
+			const bool first_gate = FIRST && k == K - 1;
+			const bool last_gate = LAST && k == 0;
+#pragma unroll 2
+			for (int j = 0; j < UPW4; j++) {
+				const int u = warp + j * nwarps;
+				if (u >= units) break;
+				const int B0 = sub[k * 32 + u], B1 = B0 ^ E0;
+				// 1. the state (and tangent) entering gate k, in place
+				{
+					const int i0 = B0 ^ LA, i1 = B1 ^ LA, i2 = B0 ^ LB, i3 = B1 ^ LB;
+					const float a[4] = { fPsi[i0], fPsi[i1], fPsi[i2], fPsi[i3] };
+					uint32_t ab[4], as[4];
+					split4(a, ab, as);
+					float y[4] = {0, 0, 0, 0}, z[4] = {0, 0, 0, 0};
+					mma3(y, ab, as, rcb, rcs);
+					const bool dt = TAN && !last_gate;
+					if (dt) {
+						mma3(z, ab, as, wb, ws);
+						const float da[4] = { fdPsi[i0], fdPsi[i1], fdPsi[i2], fdPsi[i3] };
+						split4(da, ab, as);
+						mma3(z, ab, as, rcb, rcs);
+					}
+					__syncwarp();
+					const int s0 = B0 ^ LS, s1 = B1 ^ LS;
+					*reinterpret_cast<float2*>(fPsi + s0) = make_float2(y[0], y[1]);
+					*reinterpret_cast<float2*>(fPsi + s1) = make_float2(y[2], y[3]);
+					if (dt) {
+						*reinterpret_cast<float2*>(fdPsi + s0) = make_float2(z[0], z[1]);
+						*reinterpret_cast<float2*>(fdPsi + s1) = make_float2(z[2], z[3]);
+					}
+					__syncwarp();
+				}
+				// 2. outer products over the two sets (b6 = 2u, 2u+1) of eight groups
+#pragma unroll
+				for (int sset = 0; sset < 2; sset++) {
+					const int j0 = (sset ? B1 : B0) ^ LO, j1 = j0 + 8;
+					const float a[4] = { fPhi[j0], (TAN && !first_gate) ? fdPhi[j0] : 0.f, fPhi[j1],
+					                     (TAN && !first_gate) ? fdPhi[j1] : 0.f };
+					uint32_t ab[4], as[4];
+					split4(a, ab, as);
+					uint32_t xb[2], xs[2];
+					tf32_split(fPsi[j0], xb[0], xs[0]);
+					tf32_split(fPsi[j1], xb[1], xs[1]);
+					mma3(cx[k], ab, as, xb, xs);
+					if (TAN && !last_gate) {
+						uint32_t db[2], ds[2];
+						tf32_split(fdPsi[j0], db[0], ds[0]);
+						tf32_split(fdPsi[j1], db[1], ds[1]);
+						mma3(cd[k], ab, as, db, ds);   // rows 0-7: P^T dX (rows 8-15 unused)
+					}
+				}
+				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place)
+				if (!last_gate)
+					apply_unit4o<TAN>(fPhi, fdPhi, fPhi, fdPhi, B0, E0, LA, LB, LS, gb, gs, zb, zs, first_gate, true);
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+#pragma unroll
+			for (int i = 0; i < CPT; i++) {
+				const int e = threadIdx.x + i * NT5;
+				if (e >= 4 * R) continue;
+				const int r = e >> 2, c2i = 2 * (e & 3);
+				const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+				const int pe = prow(r) * CW4 + c2i;
+				*reinterpret_cast<float4*>(phi_o + a) = *reinterpret_cast<const float4*>(Phi + pe);
+				if (TAN) *reinterpret_cast<float4*>(dphi_o + a) = *reinterpret_cast<const float4*>(dPhi + pe);
+			}
+		}
+		if (++ntile == FLUSH4) {
+			ntile = 0;
+			flush();
+		}
+		__syncthreads();
+	}
+	flush();
+	__syncthreads();
+	for (int idx = threadIdx.x; idx < K * NRAW4; idx += blockDim.x) {
+		const int k = idx / NRAW4, rem = idx % NRAW4, ln = rem / 4, v = rem % 4;
+		double s2 = 0;
+		for (int w = 0; w < nwarps; w++)
+			s2 += scratch[((size_t)blockIdx.x * nwarps + w) * 32 * MAXK * 4 + (size_t)ln * MAXK * 4 + k * 4 + v];
+		part[(size_t)k * nblk * NRAW4 + (size_t)blockIdx.x * NRAW4 + rem] += s2;
+	}
+}
+
 // Sum the complex64 engine's raw partials over blocks and fold them into complex dG, HZ.
 // Lane (g, t) of an outer-sum MMA holds C[g][2t..2t+1] (v 0,1) and C[g+8][2t..2t+1]
 // (v 2,3): dG raw R[g][2t+i] = v_i, HZ raw R[g][2t+i] = v_{2+i}.
@@ -1583,11 +1821,11 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
 	} else {
 		if (!per_sm) {
-			int ret = prepare(k4_fwd<TAN, IN, OUT>, k4_fwd_smem(MAXNB, TAN, OUT == 2), &per_sm, NT4F);
+			int ret = prepare(k4_fwd<TAN, IN, OUT>, k4_fwd_smem(MAXNB, TAN, OUT >= 2), &per_sm, NT4F);
 			if (ret) return ret;
 		}
-		const int grid = OUT == 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
-		RQC_LAUNCH3(rt, KC_FUSED, (k4_fwd<TAN, IN, OUT>), grid, NT4F, k4_fwd_smem(pg.NB, TAN, OUT == 2), psi, dpsi, psi_o,
+		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
+		RQC_LAUNCH3(rt, KC_FUSED, (k4_fwd<TAN, IN, OUT>), grid, NT4F, k4_fwd_smem(pg.NB, TAN, OUT >= 2), psi, dpsi, psi_o,
 		            dpsi_o, phi, pg, gates, fpart);
 	}
 	return OK;
@@ -1636,6 +1874,97 @@ int launch_rev_any(Runtime& rt, bool first, bool last, const cplx<T>* psi, const
 	return launch_rev<T, TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, part, nblk, scratch);
 }
 
+template <bool TAN, bool FIRST, bool LAST>
+int launch_rev5(Runtime& rt, const float2* psi, const float2* dpsi, const float2* phi, const float2* dphi, float2* phi_o,
+                float2* dphi_o, const PassGeom& pg, const PassGates<float>& gates, const PassW<float>& wg, double* part,
+                int nblk, double* scratch)
+{
+	static bool ready = false;
+	if (!ready) {
+		int per_sm;
+		int ret = prepare(k5_rev<TAN, FIRST, LAST>, k5_rev_smem(TAN), &per_sm, NT5);
+		if (ret) return ret;
+		ready = true;
+	}
+	RQC_LAUNCH3(rt, KC_REVERSE, (k5_rev<TAN, FIRST, LAST>), nblk, NT5, k5_rev_smem(TAN), psi, dpsi, phi, dphi, phi_o,
+	            dphi_o, pg, gates, wg, part, nblk, scratch);
+	return OK;
+}
+
+template <bool TAN>
+int launch_rev5_any(Runtime& rt, bool first, bool last, const float2* psi, const float2* dpsi, const float2* phi,
+                    const float2* dphi, float2* phi_o, float2* dphi_o, const PassGeom& pg, const PassGates<float>& gates,
+                    const PassW<float>& wg, double* part, int nblk, double* scratch)
+{
+	if (first && last)
+		return launch_rev5<TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk, scratch);
+	if (first)
+		return launch_rev5<TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk, scratch);
+	if (last)
+		return launch_rev5<TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk, scratch);
+	return launch_rev5<TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk, scratch);
+}
+
+int rev_grid5(Runtime& rt, bool tan)
+{
+	int per_sm = 1;
+	const int ret = tan ? prepare(k5_rev<true, false, false>, k5_rev_smem(true), &per_sm, NT5)
+	                    : prepare(k5_rev<false, false, false>, k5_rev_smem(false), &per_sm, NT5);
+	if (ret) per_sm = 1;
+	return rt.num_sms * per_sm;
+}
+
+// every gate unitary to 1e-10 (max |G^+ G - I|): the reverse pass may then rebuild
+// states with adjoint gates
+bool gates_unitary(const double2* gates, int G)
+{
+	for (int k = 0; k < G; k++) {
+		const double2* g = gates + 16 * (size_t)k;
+		for (int r = 0; r < 4; r++)
+			for (int c = 0; c < 4; c++) {
+				double re = 0, im = 0;
+				for (int q = 0; q < 4; q++) {   // (G^+ G)[r][c] = sum_q conj(G[q][r]) G[q][c]
+					const double2 a = g[4 * q + r], b = g[4 * q + c];
+					re += a.x * b.x + a.y * b.y;
+					im += a.x * b.y - a.y * b.x;
+				}
+				if (fabs(re - (r == c ? 1.0 : 0.0)) > 1e-10 || fabs(im) > 1e-10) return false;
+			}
+	}
+	return true;
+}
+
+// W = G^+ Z G^+ of every gate of a pass
+PassW<float> pass_w(const Pass& p, const double2* gates, const double2* dirs)
+{
+	PassW<float> pw;
+	memset(&pw, 0, sizeof(pw));
+	for (int k = 0; k < p.K; k++) {
+		const double2* g = gates + 16 * (size_t)(p.first + k);
+		const double2* z = dirs + 16 * (size_t)(p.first + k);
+		double2 gh[16], t[16];
+		for (int r = 0; r < 4; r++)
+			for (int c = 0; c < 4; c++) gh[4 * r + c] = make_double2(g[4 * c + r].x, -g[4 * c + r].y);
+		auto mul = [](const double2* a, const double2* b, double2* o) {
+			for (int r = 0; r < 4; r++)
+				for (int c = 0; c < 4; c++) {
+					double re = 0, im = 0;
+					for (int q = 0; q < 4; q++) {
+						const double2 x = a[4 * r + q], y = b[4 * q + c];
+						re += x.x * y.x - x.y * y.y;
+						im += x.x * y.y + x.y * y.x;
+					}
+					o[4 * r + c] = make_double2(re, im);
+				}
+		};
+		mul(gh, z, t);
+		double2 w[16];
+		mul(t, gh, w);
+		for (int e = 0; e < 16; e++) pw.w[k].m[e] = make_float2((float)w[e].x, (float)w[e].y);
+	}
+	return pw;
+}
+
 // grid of the partial-sum kernels: one resident wave of the reverse kernel
 template <typename T>
 int rev_grid(Runtime& rt, bool tan)
@@ -1680,8 +2009,16 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	for (int p = 0; p < P; p++) pgates[p] = pass_gates<T>(passes[p], c.gates, tan ? c.dirs : nullptr);
 	for (int p = 0; p < Pt; p++) tgates[p] = pass_gates<T>(tpasses[p], t.gates, nullptr);
 
+	// complex64 with unitary gates: the reverse passes start from each pass's output
+	// (the next checkpoint, or the final state) and rebuild states with adjoint gates
+	bool recon = false;
+	if constexpr (!std::is_same<T, double>::value) recon = mode != EVAL_F && gates_unitary(c.gates, G);
+	std::vector<PassW<float>> pw(recon && tan ? P : 0);
+	for (int p = 0; p < (int)pw.size(); p++) pw[p] = pass_w(passes[p], c.gates, c.dirs);
+	const int64_t nck = recon ? P : P - 1;   // checkpoints (recon: also the final state)
+
 	// states per column: PHI, P0, P1 (+ D0, D1) and the pass checkpoints
-	const int64_t nstates = mode == EVAL_F ? 3 : (mode == EVAL_GRAD ? 3 + (P - 1) : 5 + 2 * (int64_t)(P - 1));
+	const int64_t nstates = mode == EVAL_F ? 3 : (mode == EVAL_GRAD ? 3 + nck : 5 + 2 * nck);
 	const size_t col_bytes = (size_t)nstates * N * sizeof(V);
 	const int64_t C_mem = (int64_t)(workspace_limit2(rt) / col_bytes);
 	int64_t C = C_mem;
@@ -1698,12 +2035,12 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	V* PHI = reinterpret_cast<V*>(rt.work.ptr);
 	V* Pb[2] = { PHI + C * N, PHI + 2 * C * N };
 	V* Db[2] = { tan ? PHI + 3 * C * N : nullptr, tan ? PHI + 4 * C * N : nullptr };
-	V* ck = PHI + (tan ? 5 : 3) * C * N;                             // psi at the input of pass p = 1..P-1
-	V* dck = tan ? ck + (int64_t)(P - 1) * C * N : nullptr;          // dpsi at the input of pass p
+	V* ck = PHI + (tan ? 5 : 3) * C * N;                             // psi at the input of pass p = 1..nck
+	V* dck = tan ? ck + nck * C * N : nullptr;                       // dpsi at the input of pass p
 	auto ck_at = [&](int p) { return ck + (int64_t)(p - 1) * C * N; };
 	auto dck_at = [&](int p) { return dck + (int64_t)(p - 1) * C * N; };
 
-	const int nblk = rev_grid<T>(rt, tan);
+	const int nblk = recon ? rev_grid5(rt, tan) : rev_grid<T>(rt, tan);
 	// blocks of the forward launches that sum f (one FP64 partial each)
 	const int nfb = std::is_same<T, double>::value ? nblk : 2 * rt.num_sms;
 	const int nps = std::is_same<T, double>::value ? NPART3 : NRAW4;   // partial doubles per gate and block
@@ -1788,17 +2125,27 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 			} else if (!tan) {
 				const V* in = first ? nullptr : ck_at(p);
-				V* out = last ? nullptr : ck_at(p + 1);
-				if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+				V* out = (last && !recon) ? nullptr : ck_at(p + 1);
+				if (recon && last) {
+					if constexpr (!std::is_same<T, double>::value) {
+						if (first) ret = launch_fwd<T, false, 1, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+						else ret = launch_fwd<T, false, 0, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+					}
+				} else if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				else ret = launch_fwd<T, false, 0, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 			} else {
 				const V* in = first ? nullptr : ck_at(p);
 				const V* din = first ? nullptr : dck_at(p);
-				V* out = last ? nullptr : ck_at(p + 1);
-				V* dout = last ? nullptr : dck_at(p + 1);
-				if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+				V* out = (last && !recon) ? nullptr : ck_at(p + 1);
+				V* dout = (last && !recon) ? nullptr : dck_at(p + 1);
+				if (recon && last) {
+					if constexpr (!std::is_same<T, double>::value) {
+						if (first) ret = launch_fwd<T, true, 1, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+						else ret = launch_fwd<T, true, 0, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+					}
+				} else if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				else if (first) ret = launch_fwd<T, true, 1, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				else if (last) ret = launch_fwd<T, true, 0, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				else ret = launch_fwd<T, true, 0, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
@@ -1815,6 +2162,20 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 			const V* ph = first ? PHI : Pb[cur];
 			const V* dph = (first || !tan) ? nullptr : Db[cur];
 			double* pp = part + (size_t)passes[p].first * nblk * nps;
+			if constexpr (!std::is_same<T, double>::value) {
+				if (recon) {
+					if (tan)
+						ret = launch_rev5_any<true>(rt, first, last, ck_at(p + 1), dck_at(p + 1), ph, dph,
+						                            last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pw[p],
+						                            pp, nblk, scratch);
+					else
+						ret = launch_rev5_any<false>(rt, first, last, ck_at(p + 1), nullptr, ph, nullptr,
+						                             last ? nullptr : Pb[nxt], nullptr, g, pgates[p], PassW<float>{}, pp,
+						                             nblk, scratch);
+					if (ret) return ret;
+					continue;
+				}
+			}
 			if (tan)
 				ret = launch_rev_any<T, true>(rt, first, last, last ? nullptr : ck_at(p), last ? nullptr : dck_at(p), ph, dph,
 				                              last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pp, nblk,

@@ -225,3 +225,36 @@ def test_complex64_circuit_matches_complex128(gpu, gpp):
                                                           ref.ctypes.data, L) == -6
     finally:
         gpu.set_gates_per_pass(4)
+
+
+@pytest.mark.parametrize("L,depth,per_pass", [(6, 3, 4), (9, 4, 3), (12, 5, 4), (12, 5, 2)])
+@pytest.mark.parametrize("unitary", [True, False])
+def test_complex64_reverse_paths_match_complex128(gpu, L, depth, per_pass, unitary):
+    """complex64 passes against complex128 (1e-5): unitary gates take the reverse pass
+    that rebuilds states with adjoint gates, perturbed (non-unitary) gates the one that
+    recomputes them; gradient and HVP modes of a general circuit."""
+    rng = np.random.default_rng(2000 + L + 10 * per_pass)
+    G = 3 * depth
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    if not unitary:
+        gates = gates + 0.05 * crandn((G, 4, 4), rng)
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    dirs = 0.3 * crandn((G, 4, 4), rng)
+    tg = np.stack([haar_unitary(rng) for _ in range(6)])
+    tw = np.array([rng.choice(L, 2, replace=False) for _ in range(6)], np.int32)
+    t = gpu.Target(circuit=(tg, tw))
+    gpu.set_gates_per_pass(per_pass)
+    try:
+        gpu.set_precision(gpu.PRECISION_C128)
+        ref_h = gpu.circuit_unitary_target_hessian_vector_product(t, gates, dirs, wires, L)
+        ref_g = gpu.circuit_unitary_target_and_gradient(t, gates, wires, L)
+        gpu.set_precision(gpu.PRECISION_C64)
+        got_h = gpu.circuit_unitary_target_hessian_vector_product(t, gates, dirs, wires, L)
+        got_g = gpu.circuit_unitary_target_and_gradient(t, gates, wires, L)
+    finally:
+        gpu.set_precision(gpu.PRECISION_C128)
+        gpu.set_gates_per_pass(4)
+    for a, b in zip(got_h, ref_h):
+        assert rel_err(a, b) <= 1e-5
+    for a, b in zip(got_g, ref_g):
+        assert rel_err(a, b) <= 1e-5
