@@ -901,6 +901,23 @@ __device__ __forceinline__ void bfrag4(const float2* m, bool tr, int lane, uint3
 	}
 }
 
+// B fragment of the embedding of m (tr: m^T; conj: conj(m); neg: -m), split:
+// f[0..1] big, f[2..3] small parts (rows t, t+4; column g).
+__device__ __forceinline__ void bfrag4x(const float2* m, bool tr, bool conj, bool neg, int lane, uint32_t f[4])
+{
+	const int t = lane & 3, g = lane >> 2;
+#pragma unroll
+	for (int h = 0; h < 2; h++) {
+		const int rowk = t + 4 * h, coln = g;
+		const int r = rowk >> 1, a = rowk & 1, c = coln >> 1, b = coln & 1;
+		float2 v = tr ? m[4 * c + r] : m[4 * r + c];
+		if (conj) v.y = -v.y;
+		if (neg) { v.x = -v.x; v.y = -v.y; }
+		const float x = a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
+		tf32_split(x, f[h], f[2 + h]);
+	}
+}
+
 // Float index of (row, column cc, part) in a swizzled complex64 tile of 8 columns is
 // 16 prow(row) + 2 cc + part.  prow(r) = r ^ (parity of r >> 1), so for disjoint bit
 // sets 16 prow(x | y) = roff(x) ^ roff(y): every operand address of a gate step is the
@@ -1002,7 +1019,7 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
-constexpr int NT4F = 256;   // threads of the complex64 forward kernel (two blocks per SM)
+constexpr int NT4F = 256;   // threads of the complex64 forward kernel (up to three blocks per SM)
 constexpr int NT4R = 256;   // threads of the complex64 reverse kernel
 constexpr int UPW4 = (1 << MAXNB) / 8 / (NT4R / 32); // units per warp and gate step (full tiles)
 static_assert(NT4F == NT4R, "the unit tables assume equal block sizes");
@@ -1015,13 +1032,15 @@ inline size_t k4_fwd_smem(int NB, bool tan, bool with_phi)
 	(void)NB;
 	const size_t A = AMAX4;
 	const int ns = (tan ? 2 : 1) + (with_phi ? 1 : 0);
-	return 32 * MAXK * sizeof(float2) + 2 * ns * A * sizeof(float2);
+	// gates, per-gate lane tables (fragments of G^T and Z^T, lane offsets, unit bases), tiles
+	return 32 * MAXK * sizeof(float2) + MAXK * 2 * 32 * sizeof(uint4) + MAXK * 4 * 32 * sizeof(int) +
+	       MAXK * 32 * sizeof(int) + 2 * ns * A * sizeof(float2);
 }
 
 // Forward pass (complex64).  Same contract as k2_fwd.  The next tile streams into a
 // second set of shared-memory buffers with cp.async while the current one is processed.
 template <bool TAN, int IN, int OUT>
-__global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+__global__ void __launch_bounds__(NT4F, 3) k4_fwd(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
                                                  float2* __restrict__ psi_o, float2* __restrict__ dpsi_o,
                                                  const float2* __restrict__ phi, PassGeom pg, PassGates<float> gates,
                                                  double2* __restrict__ fpart)
@@ -1032,11 +1051,29 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const int R = 1 << pg.NB, K = pg.K;
 	float2* sg = reinterpret_cast<float2*>(smem_raw);
-	float2* tiles = sg + 32 * MAXK;
+	uint4* sfr = reinterpret_cast<uint4*>(sg + 32 * MAXK);              // [MAXK][2][32] fragments of G^T, Z^T
+	int* slc = reinterpret_cast<int*>(sfr + MAXK * 2 * 32);             // [MAXK][4][32] E0, LA, LB, LS
+	int* sub = slc + MAXK * 4 * 32;                                      // [MAXK][32] unit bases
+	float2* tiles = reinterpret_cast<float2*>(sub + MAXK * 32);
 	auto stage = [&](int buf, int st) { return tiles + (buf * NS + st) * AMAX4; };
 	gates_to_smem<float>(gates, K, TAN, sg);
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	const int units = R / 8;
+	__syncthreads();
+	if (warp < K) {   // one warp per gate builds its lane tables
+		const int k = warp;
+		const Lane4 ln(pg.gi[k], pg.gj[k], lane);
+		uint32_t f[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+		bfrag4x(sg + 32 * k, true, false, false, lane, f);
+		if (TAN) bfrag4x(sg + 32 * k + 16, true, false, false, lane, f + 4);
+		sfr[(k * 2 + 0) * 32 + lane] = make_uint4(f[0], f[1], f[2], f[3]);
+		sfr[(k * 2 + 1) * 32 + lane] = make_uint4(f[4], f[5], f[6], f[7]);
+		slc[(k * 4 + 0) * 32 + lane] = ln.E0;
+		slc[(k * 4 + 1) * 32 + lane] = ln.LA;
+		slc[(k * 4 + 2) * 32 + lane] = ln.LB;
+		slc[(k * 4 + 3) * 32 + lane] = ln.LS;
+		for (int u = lane; u < units; u += 32) sub[k * 32 + u] = ln.unit_base(u);
+	}
 	int ro[CPT];
 #pragma unroll
 	for (int i = 0; i < CPT; i++) {
@@ -1045,17 +1082,6 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 		for (int b = 0; b < pg.NB; b++)
 			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
 		ro[i] = o;
-	}
-	int E0[MAXK], LA[MAXK], LB[MAXK], LS[MAXK], LO[MAXK], HI[MAXK];
-#pragma unroll
-	for (int k = 0; k < MAXK; k++) {
-		const Lane4 ln(pg.gi[k < K ? k : 0], pg.gj[k < K ? k : 0], lane);
-		E0[k] = ln.E0;
-		LA[k] = ln.LA;
-		LB[k] = ln.LB;
-		LS[k] = ln.LS;
-		LO[k] = ln.lo;
-		HI[k] = ln.hi;
 	}
 	double fx = 0, fy = 0;
 	auto fetch = [&](int64_t tile, int buf) {
@@ -1093,16 +1119,16 @@ __global__ void __launch_bounds__(NT4F, 2) k4_fwd(const float2* __restrict__ psi
 #pragma unroll
 		for (int k = 0; k < MAXK; k++) {
 			if (k >= K) break;
-			uint32_t gb[2], gs[2], zb[2] = {0, 0}, zs[2] = {0, 0};
-			bfrag4(sg + 32 * k, true, lane, gb, gs);
-			if (TAN) bfrag4(sg + 32 * k + 16, true, lane, zb, zs);
+			const uint4 q0 = sfr[(k * 2 + 0) * 32 + lane], q1 = sfr[(k * 2 + 1) * 32 + lane];
+			const uint32_t gb[2] = { q0.x, q0.y }, gs[2] = { q0.z, q0.w };
+			const uint32_t zb[2] = { q1.x, q1.y }, zs[2] = { q1.z, q1.w };
+			const int E0 = slc[(k * 4 + 0) * 32 + lane], LA = slc[(k * 4 + 1) * 32 + lane];
+			const int LB = slc[(k * 4 + 2) * 32 + lane], LS = slc[(k * 4 + 3) * 32 + lane];
 #pragma unroll 2
 			for (int j = 0; j < UPW4; j++) {
 				const int u = warp + j * nwarps;
 				if (u >= units) break;
-				const int b = insert2(2 * u, LO[k], HI[k]);
-				const int B0 = (b ^ ((__popc(u) ^ b) & 1)) << 4;
-				apply_unit4o<TAN>(S, dS, S, dS, B0, E0[k], LA[k], LB[k], LS[k], gb, gs, zb, zs, IN == 1 && k == 0, true);
+				apply_unit4o<TAN>(S, dS, S, dS, sub[k * 32 + u], E0, LA, LB, LS, gb, gs, zb, zs, IN == 1 && k == 0, true);
 			}
 			__syncthreads();
 		}
@@ -1364,23 +1390,6 @@ __global__ void __launch_bounds__(NT4R, 1) k4_rev(const float2* __restrict__ psi
 		for (int w = 0; w < nwarps; w++)
 			s2 += scratch[((size_t)blockIdx.x * nwarps + w) * 32 * MAXK * 4 + (size_t)ln * MAXK * 4 + k * 4 + v];
 		part[(size_t)k * nblk * NRAW4 + (size_t)blockIdx.x * NRAW4 + rem] += s2;
-	}
-}
-
-// B fragment of the embedding of m (tr: m^T; conj: conj(m); neg: -m), split:
-// f[0..1] big, f[2..3] small parts (rows t, t+4; column g).
-__device__ __forceinline__ void bfrag4x(const float2* m, bool tr, bool conj, bool neg, int lane, uint32_t f[4])
-{
-	const int t = lane & 3, g = lane >> 2;
-#pragma unroll
-	for (int h = 0; h < 2; h++) {
-		const int rowk = t + 4 * h, coln = g;
-		const int r = rowk >> 1, a = rowk & 1, c = coln >> 1, b = coln & 1;
-		float2 v = tr ? m[4 * c + r] : m[4 * r + c];
-		if (conj) v.y = -v.y;
-		if (neg) { v.x = -v.x; v.y = -v.y; }
-		const float x = a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
-		tf32_split(x, f[h], f[2 + h]);
 	}
 }
 
