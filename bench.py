@@ -241,6 +241,12 @@ def batched_c4(gpu, torch, count=512, niter=2):
     from rqcopt_hpc_b200.workloads import batched_instances
     probs = batched_instances(count)
     out = {"workload": f"{count} brickwall instances, L in {{6,8,10,12}}, depth in {{3,5,7,9}}, {niter} RTR iterations"}
+    warm = batch.Batch(16, niter)   # kernel set-up outside the timed run
+    for p in probs[:16]:
+        warm.add(p, niter, gpu.PRECISION_C64)
+    while warm.run(32) > 0:
+        pass
+    warm.close()
     b = batch.Batch(count, niter)
     for p in probs:
         b.add(p, niter, gpu.PRECISION_C64)
@@ -254,6 +260,13 @@ def batched_c4(gpu, torch, count=512, niter=2):
     fb = np.array([b.result(s)[0][-1] for s in range(count)])
     b.close()
     gpu.set_precision(gpu.PRECISION_C128)
+    # warm-up: one instance of every (L, depth) class, so that workspace growth and
+    # kernel set-up fall outside the timed loop
+    seen = set()
+    for (L, vl, pm, tv, tp) in probs:
+        if (L, len(vl)) not in seen:
+            seen.add((L, len(vl)))
+            gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, niter)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     fp = []
@@ -271,7 +284,7 @@ def batched_c4(gpu, torch, count=512, niter=2):
     return out
 
 
-def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-8):
+def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-8, sizes=(8, 10, 12, 14)):
     """Poisson arrivals (seed 40) of brickwall optimisation requests (even L in 8..14,
     P(L) ~ 2^(-(L-8)/2), depth in {3,5,7,9}, target depth 3), each stopping at gradient
     norm grad_tol or after niter iterations, admitted into a running batch within a
@@ -280,7 +293,7 @@ def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-
     latencies are queue-dominated and the rest is reported as still running)."""
     from rqcopt_hpc_b200 import batch, serving
     reqs = serving.c5_requests(rate=rate, duration=duration, niter=niter, grad_tol=grad_tol,
-                               precision=gpu.PRECISION_MIXED)
+                               precision=gpu.PRECISION_MIXED, sizes=sizes)
     b = batch.Batch(capacity=4096, max_iterations=niter, sharing=True)
     srv = serving.Server(b, capacity=4096, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=4)
     t0 = time.perf_counter()
@@ -288,7 +301,8 @@ def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-
     el = time.perf_counter() - t0
     ev, hv = b.evaluations()
     b.close()
-    out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s ({len(reqs)} requests), measured for {wall:g} s",
+    out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s ({len(reqs)} requests, L in {set(sizes)}), "
+                       f"measured for {wall:g} s",
            "precision": "mixed", "wall_s": el, "completed": len(done), "still_running_or_queued": len(left),
            "completed_per_s": len(done) / el, "evaluations": ev, "rounds": srv.rounds}
     out.update(serving.latency_stats(done))
@@ -322,17 +336,18 @@ def compare_plain(gpu, torch, stream, step, res_mixed, steps):
                               "hvp": _relerr(res_mixed[2], ref[2])}}
 
 
-def rtr_equal_error(gpu, L=10, depth=5, tdepth=3, niter=12):
+def rtr_equal_error(gpu, L=12, depth=5, tdepth=3, niter=12):
     """Riemannian trust region (reference defaults) from the same start in plain complex128 and
     in mixed precision (complex64 HVPs until the gradient norm falls below the refinement
-    threshold, complex128 f, gradient and refinement): wall time and the final f of each."""
+    threshold, complex128 f, gradient and refinement): wall time and the final f of each
+    (each mode runs once untimed first, so that its workspace and kernels are set up)."""
     vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, seed=0, tseed=1, dseed=2)
     target = gpu.Target(brickwall=(tvlist, tperms))
     out = {"workload": f"brickwall L={L} depth={depth} vs brickwall target depth={tdepth}, {niter} RTR iterations"}
     runs = {}
     for name, p in (("plain_c128", gpu.PRECISION_C128), ("mixed", gpu.PRECISION_MIXED)):
         gpu.set_precision(p)
-        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, 1)   # warm-up
+        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)   # warm-up
         t0 = time.perf_counter()
         f_iter, vopt = gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)
         runs[name] = (time.perf_counter() - t0, f_iter)
@@ -519,6 +534,8 @@ def main():
             gpu.set_precision(prec)
         if not a.no_serving and world == 1:
             line["serving"] = serving_c5(gpu, wall=a.serving_wall)
+            # a load one GPU sustains: 2 req/s of the two smallest size classes
+            line["serving_sustainable"] = serving_c5(gpu, rate=2.0, duration=10.0, wall=40.0, sizes=(8, 10))
             gpu.set_precision(prec)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)

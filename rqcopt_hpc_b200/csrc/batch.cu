@@ -48,7 +48,11 @@ constexpr int MAXTU = 16;        // target layers per instance
 constexpr int MAXL = 14;         // qubits per instance
 constexpr int MAXN = 16 * MAXU;  // real parameters per instance
 constexpr int NACC = 2 + 64 * MAXU;   // FP64 accumulators per item: f (re, im), dG and HZ per layer
-constexpr double ITEM_WORK = 4194304.0;   // amplitude x gate updates per work item (about)
+// Work items of an instance: at least ITEM_WORK amplitude x gate updates each (to amortise
+// their set-up) and at most MAX_ITEMS per instance; more items let a single instance
+// spread over the SMs, which shortens its rounds when few instances are in flight.
+constexpr double ITEM_WORK = 262144.0;
+constexpr int MAX_ITEMS = 128;
 constexpr int TSTR = 20;               // shared-memory stride of a 4x4 gate table (rows padded to 5)
 constexpr int NTABS = (MAXU * 3 + MAXTU) * TSTR;
 constexpr int SWIRES = (MAXU + MAXTU) * MAXL + 4;   // wire ints in shared memory (16-byte multiple)
@@ -778,7 +782,7 @@ int rebuild_items(Runtime& rt, Batch& b)
 		BInst& in = b.hinst[wv.slot];
 		const int N = 1 << in.L, cw = tile_cols(in.L);
 		int cols = cw;
-		while (cols < N && (double)(2 * cols) * wv.cost <= target) cols *= 2;
+		while (cols < N && (N / cols > MAX_ITEMS || (double)cols * wv.cost < target)) cols *= 2;
 		in.item0 = (int)b.hitems.size();
 		for (int c0 = 0; c0 < N; c0 += cols) b.hitems.push_back(make_int4(wv.slot, c0, std::min(N, c0 + cols), 0));
 		in.item1 = (int)b.hitems.size();
@@ -1104,9 +1108,9 @@ size_t rqcopt_batch_footprint(int nqubits, int nlayers)
 	constexpr int NTAB = (MAXU * 3 + MAXTU) * 16;
 	const size_t slot = sizeof(BInst) + sizeof(BOpt) + sizeof(int) * (MAXU + MAXTU) * MAXL + sizeof(double2) * (3 * MAXU + MAXTU) * 16 +
 	                    (sizeof(float4) + sizeof(double2)) * NTAB + sizeof(double) * (7 * MAXN + 2 + 2 * MAXN);
-	// partial sums of its work items (at most one item per tile of columns)
+	// partial sums of its work items (at most MAX_ITEMS, at most one per tile of columns)
 	const size_t cols = (size_t)1 << nqubits;
-	const size_t items = (cols + tile_cols(nqubits) - 1) / tile_cols(nqubits);
+	const size_t items = std::min<size_t>(MAX_ITEMS, (cols + tile_cols(nqubits) - 1) / tile_cols(nqubits));
 	return slot + items * (sizeof(int4) + NACC * sizeof(double));
 }
 
