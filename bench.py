@@ -39,8 +39,8 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 # DRAM traffic / algorithmic bytes of the reverse-pass kernel, from ncu
-# (complex64 k4_rev: 789.9 MB measured for 805.3 MB algorithmic at L=12)
-TRAFFIC_RATIO = {8: 0.981}
+# (complex64 k5_rev: 541.2 + 312.7 MB measured for 805.3 MB algorithmic at L=12)
+TRAFFIC_RATIO = {8: 1.060}
 
 METRIC = "grad+HVP evals/s (f + projected gradient + projected HVP, all basis columns; mixed vs FP64)"
 
@@ -478,7 +478,7 @@ def main():
     if rank == 0:
         itemsize = 16 if prec == gpu.PRECISION_C128 else 8
         rev_kernel = ("k3_rev (complex128 FP64-MMA gradient/HVP pass" if itemsize == 16
-                      else "k4_rev (complex64 3xTF32-MMA gradient/HVP pass")
+                      else "k5_rev (complex64 3xTF32-MMA gradient/HVP pass rebuilding states with adjoint gates")
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
