@@ -470,10 +470,8 @@ def main():
     barrier()
     e2e_ms = (time.perf_counter() - t0) * 1e3
 
-    t = torch.tensor([dev_ms, e2e_ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    dev_ms, e2e_ms = float(t[0]), float(t[1])
+    from rqcopt_hpc_b200.replicas import max_over_ranks, whole_job_rate
+    dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_ms], device="cuda")
 
     if rank == 0:
         itemsize = 16 if prec == gpu.PRECISION_C128 else 8
@@ -488,7 +486,7 @@ def main():
         npass = G if a.gates_per_pass == 1 else -(-G // a.gates_per_pass)
         rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
         achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
-        value = world * a.steps / (dev_ms * 1e-3)
+        value = whole_job_rate(world, a.steps, dev_ms)
         # DRAM bytes per launch: the algorithmic bytes per launch times the traffic /
         # algorithmic ratio measured by ncu on a smaller case of the same kernel
         # (dram__bytes_read + dram__bytes_write of one middle pass at L=12)
@@ -504,7 +502,7 @@ def main():
             "dtype": "c128 (f64)" if itemsize == 16 else "c64 (f32 passes on 3xTF32 MMA, f64 sums)",
             "precision": a.precision,
             "data": "synthetic (seeded Haar gates)", "config": config,
-            "e2e": {"value": world * a.steps / (e2e_ms * 1e-3), "unit": "evals/s",
+            "e2e": {"value": whole_job_rate(world, a.steps, e2e_ms), "unit": "evals/s",
                     "h2d_bytes_per_step": int(vlist.nbytes + vdirs.nbytes + tvlist.nbytes + perms.nbytes + tperms.nbytes),
                     "d2h_bytes_per_step": int(16 + 2 * 16 * depth * 8)},
             "roofline": {"kernel": ("k_reverse (gradient/HVP pass of one gate over a column chunk)" if a.gates_per_pass == 1

@@ -684,6 +684,7 @@ struct Batch
 	std::vector<int> used;                 // slot -> 0 free, 1 in use
 	std::vector<BInst> hinst;
 	std::vector<int4> hitems;
+	std::vector<int> hranges;              // (item0, item1) per slot, staged for the device table
 	int4* ditems = nullptr;
 	size_t items_cap = 0;
 	double* partial = nullptr;
@@ -788,10 +789,16 @@ int rebuild_items(Runtime& rt, Batch& b)
 		in.item1 = (int)b.hitems.size();
 		if (in.L >= 12) big = true;
 	}
-	// item ranges live in the device instance table
+	// item ranges live in the device instance table: one strided copy of (item0, item1)
+	// into every slot (free slots get empty ranges)
+	b.hranges.assign(2 * (size_t)b.cap, 0);
 	for (const W& wv : live) {
-		const BInst& in = b.hinst[wv.slot];
-		int ret = RQC_CUDA(cudaMemcpyAsync(&b.d.inst[wv.slot].item0, &in.item0, 2 * sizeof(int), cudaMemcpyHostToDevice, rt.stream));
+		b.hranges[2 * (size_t)wv.slot] = b.hinst[wv.slot].item0;
+		b.hranges[2 * (size_t)wv.slot + 1] = b.hinst[wv.slot].item1;
+	}
+	{
+		int ret = RQC_CUDA(cudaMemcpy2DAsync(&b.d.inst[0].item0, sizeof(BInst), b.hranges.data(), 2 * sizeof(int),
+		                                     2 * sizeof(int), b.cap, cudaMemcpyHostToDevice, rt.stream));
 		if (ret) return ret;
 	}
 	const size_t ni = std::max<size_t>(b.hitems.size(), 1);
@@ -1035,11 +1042,17 @@ int rqcopt_batch_finished(struct rqcopt_batch* h, int* slots, int max_slots)
 	if (!ret) ret = sync(*rt);
 	if (ret) return ret;
 	const int avail = std::min(total - b.done_read, max_slots);
-	for (int k = 0; k < avail; k++) {
-		int v;
-		if ((ret = RQC_CUDA(cudaMemcpy(&v, b.ring + (b.done_read + k) % b.ring_cap, sizeof(int), cudaMemcpyDeviceToHost)))) return ret;
-		slots[k] = v;
-	}
+	// the ring range [done_read, done_read + avail), in at most two pieces
+	const int start = b.done_read % b.ring_cap;
+	const int first = std::min(avail, b.ring_cap - start);
+	if (first > 0 &&
+	    (ret = RQC_CUDA(cudaMemcpyAsync(slots, b.ring + start, first * sizeof(int), cudaMemcpyDeviceToHost, rt->stream))))
+		return ret;
+	if (avail > first &&
+	    (ret = RQC_CUDA(cudaMemcpyAsync(slots + first, b.ring, (avail - first) * sizeof(int), cudaMemcpyDeviceToHost,
+	                                    rt->stream))))
+		return ret;
+	if ((ret = sync(*rt))) return ret;
 	b.done_read += avail;
 	return avail;
 }
