@@ -166,6 +166,8 @@ def _main():
     ap.add_argument("--L", type=int, default=0, help="fixed qubit count (default: even L uniform over 6..12)")
     ap.add_argument("--niter", type=int, default=2)
     ap.add_argument("--precision", default="c64", choices=["c64", "mixed", "c128"])
+    ap.add_argument("--plain", action="store_true",
+                    help="also run the per-instance complex128 optimiser on every instance and compare")
     a = ap.parse_args()
     prec = {"c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED, "c128": gpu.PRECISION_C128}[a.precision]
     if a.L:
@@ -182,7 +184,21 @@ def _main():
     ev, hv = b.evaluations()
     print(f"{a.count} instances x {a.niter} iterations ({a.precision}): {el:.3f} s, {b.rounds} rounds, "
           f"{ev} evaluations ({hv} HVP), {ev / el:.1f} evaluations/s")
+    fb = np.array([b.result(s)[0][-1] for s in range(a.count)])
     b.close()
+    if a.plain:
+        gpu.set_precision(gpu.PRECISION_C128)
+        seen = set()
+        for (L, vl, pm, tv, tp) in probs:   # set-up of every size class outside the timed loop
+            if (L, len(vl)) not in seen:
+                seen.add((L, len(vl)))
+                gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, a.niter)
+        t0 = time.perf_counter()
+        fp = np.array([gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, a.niter)[0][-1]
+                       for (L, vl, pm, tv, tp) in probs])
+        ep = time.perf_counter() - t0
+        print(f"per-instance complex128 loop: {ep:.3f} s; batched speed-up {ep / el:.2f}x; "
+              f"max relative difference of the final f {np.max(np.abs(fb - fp) / np.abs(fp)):.2e}")
 
 
 if __name__ == "__main__":
