@@ -55,6 +55,14 @@ struct statevector
 	int nqubits;
 };
 
+/* src/statevector.h:39-44 -- states interleaved: amplitude a of state s at data[a*nstates + s] */
+struct statevector_array
+{
+	numeric* data;
+	int nqubits;
+	int nstates;
+};
+
 /* src/quantum_circuit.h:16-21 */
 struct quantum_circuit_cache
 {
@@ -74,6 +82,10 @@ int allocate_statevector(int nqubits, struct statevector* psi);
 void free_statevector(struct statevector* psi);
 /* src/statevector.h:32 */
 void add_statevectors(const struct statevector* psi1, const struct statevector* psi2, struct statevector* psi_sum);
+/* src/statevector.h:47 -- returns CUDA managed memory */
+int allocate_statevector_array(int nqubits, int nstates, struct statevector_array* psi_list);
+/* src/statevector.h:49 */
+void free_statevector_array(struct statevector_array* psi_list);
 
 /* ------------------------------------------------------------------ gate.h */
 
@@ -83,6 +95,13 @@ void apply_gate(const struct mat4x4* gate, const int i, const int j,
 /* src/gate.h:9-10 */
 void apply_gate_backward(const struct mat4x4* gate, const int i, const int j, const struct statevector* psi,
 	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4* dgate);
+/* src/gate.h:13 */
+void apply_gate_to_array(const struct mat4x4* gate, const int i, const int j, const struct statevector_array* psi, struct statevector_array* psi_out);
+/* src/gate.h:15-16 */
+void apply_gate_backward_array(const struct mat4x4* gate, const int i, const int j, const struct statevector_array* psi,
+	const struct statevector* dpsi_out, struct mat4x4* dgates);
+/* src/gate.h:19 -- psi_out->nstates must be 16 */
+void apply_gate_placeholder(const int i, const int j, const struct statevector* psi, struct statevector_array* psi_out);
 
 /* ------------------------------------------------------------------ quantum_circuit.h */
 
@@ -115,6 +134,12 @@ int brickwall_unitary_forward(const struct mat4x4 vlist[], int nlayers, const in
 /* src/brickwall_circuit.h:14-15 */
 int brickwall_unitary_backward(const struct mat4x4 vlist[], int nlayers, const int* perms[], const struct quantum_circuit_cache* cache,
 	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4 dvlist[]);
+/* src/brickwall_circuit.h:17-18 -- hess: (16 nlayers)^2 row-major, entry ((i*16 + x)*nlayers + j)*16 + y */
+int brickwall_unitary_backward_hessian(const struct mat4x4 vlist[], int nlayers, const int* perms[], const struct quantum_circuit_cache* cache,
+	const struct statevector* dpsi_out, struct statevector* dpsi, struct mat4x4 dvlist[], numeric* hess);
+/* src/brickwall_circuit.h:21-22 */
+int apply_brickwall_unitary_gate_placeholder(const struct mat4x4 vlist[], int nlayers, const int* perms[], int l,
+	const struct quantum_circuit_cache* cache, struct statevector_array* psi_out);
 
 /* ------------------------------------------------------------------ target.h */
 
@@ -159,6 +184,15 @@ int brickwall_unitary_target_projected_hessian_vector_product(linear_func ufunc,
 	const struct mat4x4 vlist[], const struct mat4x4 vdirs[], const int nlayers, const int* perms[], const int nqubits,
 	numeric* fval, double* grad_vec, double* hvp_vec);
 
+/* src/target.h:70-72 -- complex (16 nlayers)^2 Hessian, layout as brickwall_unitary_backward_hessian */
+int brickwall_unitary_target_gradient_hessian(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval, struct mat4x4 dvlist[], numeric* hess);
+/* src/target.h:81-83 -- real symmetric (16 nlayers)^2 Riemannian Hessian H */
+int brickwall_unitary_target_gradient_vector_hessian_matrix(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval, double* grad_vec, double* H);
+
 /* ------------------------------------------------------------------ trust_region.h */
 
 /* src/trust_region.h:10-16 */
@@ -177,12 +211,17 @@ static inline void set_truncated_cg_default_params(int n, struct truncated_cg_pa
 	params->reltol  = 1e-6;
 }
 
+/* src/trust_region.h:31 */
+bool truncated_cg_hmat(const double* grad, const double* hess, int n, double radius, const struct truncated_cg_params* params, double* z);
+
 /* src/trust_region.h:34 */
 typedef void (*hessian_vector_product_func)(const double* x, void* fdata, double* vec, double* hvp);
 /* src/trust_region.h:39 */
 typedef double (*target_func)(const double* x, void* fdata);
 /* src/trust_region.h:41 */
 typedef double (*target_gradient_func)(const double* x, void* fdata, double* grad);
+/* src/trust_region.h:43 */
+typedef double (*target_gradient_hessian_func)(const double* x, void* fdata, double* grad, double* hess);
 /* src/trust_region.h:45 */
 typedef void (*retract_func)(const double* x, const double* eta, void* rdata, double* xs);
 
@@ -213,6 +252,9 @@ static inline void set_rtr_default_params(int n, struct rtr_params* params)
 /* src/trust_region.h:36 */
 bool truncated_cg_hvp(const double* x, const double* grad, const hessian_vector_product_func f_hvp, void* fdata,
 	const int n, const double radius, const struct truncated_cg_params* params, double* z);
+/* src/trust_region.h:80-81 */
+void riemannian_trust_region_optimize_hmat(target_func f, target_gradient_hessian_func f_deriv_hess, void* fdata, retract_func retract, void* rdata,
+	const int n, const double* x_init, const int m, const struct rtr_params* params, const int niter, double* f_iter, double* x_final);
 /* src/trust_region.h:83-85 */
 void riemannian_trust_region_optimize_hvp(const target_func f, const target_gradient_func f_deriv,
 	const hessian_vector_product_func f_hvp, void* fdata, retract_func retract, void* rdata,
@@ -223,6 +265,10 @@ void riemannian_trust_region_optimize_hvp(const target_func f, const target_grad
 
 /* src/brickwall_opt.h:8-10 */
 void optimize_brickwall_circuit_hvp(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist_start[], const int nlayers, const int nqubits, const int* perms[],
+	struct rtr_params* params, const int niter, double* f_iter, struct mat4x4 vlist_opt[]);
+/* src/brickwall_opt.h:15-17 -- complex128 regardless of rqcopt_gpu_set_precision */
+void optimize_brickwall_circuit_hmat(linear_func ufunc, void* udata,
 	const struct mat4x4 vlist_start[], const int nlayers, const int nqubits, const int* perms[],
 	struct rtr_params* params, const int niter, double* f_iter, struct mat4x4 vlist_opt[]);
 /* src/circuit_opt.h:8 */
@@ -329,7 +375,8 @@ void rqcopt_gpu_reset_launch_count(void);
  * enabled, each launch of a kernel class is bracketed by events; the totals
  * are read with rqcopt_gpu_kernel_time (milliseconds summed over launches and
  * number of launches).  Kernel classes: 0 gate apply, 1 forward tangent pass,
- * 2 reverse (gradient/HVP) pass, 3 fused multi-gate apply.
+ * 2 reverse (gradient/HVP) pass, 3 fused multi-gate apply, 4 full-Hessian
+ * tangent sweep.
  */
 void rqcopt_gpu_enable_kernel_timing(int enable);
 int  rqcopt_gpu_kernel_time(int kernel_class, double* total_ms, long* launches);

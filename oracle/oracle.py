@@ -324,6 +324,103 @@ class Oracle:
         return f_iter, gopt, acc, bnd
 
 
+    # full-Hessian path (arrays: amplitude-major, [2^L, nstates])
+    def apply_gate_to_array(self, V, i, j, psi):
+        V, psi = _c(V), _c(psi)
+        L = _nq(psi)
+        out = np.empty_like(psi)
+        self.lib.orc_apply_gate_to_array(_p(V), i, j, L, psi.shape[1], _p(psi), _p(out))
+        return out
+
+    def apply_gate_backward_array(self, V, i, j, psi, dpsi_out):
+        psi, dpsi_out = _c(psi), _c(dpsi_out)
+        L = _nq(psi)
+        dg = np.empty((psi.shape[1], 4, 4), np.complex128)
+        self.lib.orc_apply_gate_backward_array(i, j, L, psi.shape[1], _p(psi), _p(dpsi_out), _p(dg))
+        return dg
+
+    def apply_gate_placeholder(self, i, j, psi):
+        psi = _c(psi)
+        L = _nq(psi)
+        out = np.empty((psi.shape[0], 16), np.complex128)
+        self.lib.orc_apply_gate_placeholder(i, j, L, _p(psi), _p(out))
+        return out
+
+    def brickwall_unitary_forward(self, vlist, perms, psi):
+        vlist, perms, psi = _c(vlist), _i(perms), _c(psi)
+        L = _nq(psi)
+        arr, states = self._cache(L, vlist.shape[0] * (L // 2))
+        out = np.empty_like(psi)
+        self.lib.orc_brickwall_forward(_p(vlist), vlist.shape[0], _p(perms), C.byref(SV(psi.ctypes.data, L)), arr,
+                                       C.byref(SV(out.ctypes.data, L)))
+        return out, states
+
+    def brickwall_unitary_backward_hessian(self, vlist, perms, states, dpsi_out):
+        vlist, perms, dpsi_out = _c(vlist), _i(perms), _c(dpsi_out)
+        L, nl = _nq(dpsi_out), vlist.shape[0]
+        states = [_c(s) for s in states]
+        arr = (SV * len(states))(*[SV(s.ctypes.data, L) for s in states])
+        dpsi = np.empty_like(dpsi_out)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        self.lib.orc_brickwall_backward_hessian(_p(vlist), nl, _p(perms), arr, C.byref(SV(dpsi_out.ctypes.data, L)),
+                                                C.byref(SV(dpsi.ctypes.data, L)), _p(dv), _p(hess))
+        return dpsi, dv, hess
+
+    def apply_brickwall_unitary_gate_placeholder(self, vlist, perms, l, states):
+        vlist, perms = _c(vlist), _i(perms)
+        states = [_c(s) for s in states]
+        L = _nq(states[0])
+        arr = (SV * len(states))(*[SV(s.ctypes.data, L) for s in states])
+        out = np.empty((1 << L, 16), np.complex128)
+        ret = self.lib.orc_apply_brickwall_placeholder(_p(vlist), vlist.shape[0], _p(perms), l, arr, _p(out))
+        assert ret == 0
+        return out
+
+    def brickwall_unitary_target_gradient_hessian(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1, np.complex128)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        ret = self.lib.orc_brickwall_target_gradient_hessian(tgt.ufunc, tgt.udata, _p(vlist), nl, L, _p(perms), _p(f),
+                                                             _p(dv), _p(hess))
+        assert ret == 0
+        return f[0], dv, hess
+
+    def brickwall_unitary_target_gradient_vector_hessian_matrix(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * nl)
+        H = np.empty((16 * nl, 16 * nl))
+        ret = self.lib.orc_brickwall_target_gradient_vector_hessian_matrix(tgt.ufunc, tgt.udata, _p(vlist), nl, L,
+                                                                           _p(perms), _p(f), _p(g), _p(H))
+        assert ret == 0
+        return f[0], g, H
+
+    def truncated_cg_hmat(self, grad, hess, radius):
+        grad, hess = np.ascontiguousarray(grad, np.float64), np.ascontiguousarray(hess, np.float64)
+        n = grad.shape[0]
+        z = np.empty(n)
+        params = TcgParams(2 * n, 1e-8, 1e-6)
+        self.lib.orc_truncated_cg_hmat.restype = C.c_bool
+        b = self.lib.orc_truncated_cg_hmat(_p(grad), _p(hess), n, D(radius), C.byref(params), _p(z))
+        return z, bool(b)
+
+    def optimize_brickwall_circuit_hmat(self, tgt, vstart, perms, L, niter):
+        vstart, perms = _c(vstart), _i(perms)
+        nl = vstart.shape[0]
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        acc = np.zeros(niter, np.int32)
+        bnd = np.zeros(niter, np.int32)
+        params = default_rtr(16 * nl)
+        self.lib.orc_optimize_brickwall_hmat(tgt.ufunc, tgt.udata, _p(vstart), nl, L, _p(perms), C.byref(params),
+                                             niter, _p(f_iter), _p(vopt), _p(acc), _p(bnd))
+        return f_iter, vopt, acc, bnd
+
+
 class Reference:
     """The reference's own C sources compiled in _ref/ (built only where the sources exist)."""
 
@@ -378,3 +475,48 @@ class Reference:
         self.lib.truncated_cg_hvp.restype = C.c_bool
         b = self.lib.truncated_cg_hvp(None, _p(grad), C.cast(f, VP), None, n, D(radius), C.byref(params), _p(z))
         return z, bool(b)
+
+    # full-Hessian path of the reference
+    def gradient_vector_hessian_matrix(self, vlist, perms, L, tvlist, tperms):
+        vlist, perms, tvlist, tperms = _c(vlist), _i(perms), _c(tvlist), _i(tperms)
+        nl = vlist.shape[0]
+        f = np.zeros(2)
+        g = np.empty(16 * nl)
+        H = np.empty((16 * nl, 16 * nl))
+        ret = self.lib.refdrv_gradient_vector_hessian_matrix(_p(vlist), nl, _p(perms), L, _p(tvlist), tvlist.shape[0],
+                                                             _p(tperms), _p(f), _p(g), _p(H))
+        assert ret == 0
+        return f[0] + 1j * f[1], g, H
+
+    def gradient_hessian(self, vlist, perms, L, tvlist, tperms):
+        vlist, perms, tvlist, tperms = _c(vlist), _i(perms), _c(tvlist), _i(tperms)
+        nl = vlist.shape[0]
+        f = np.zeros(2)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        ret = self.lib.refdrv_gradient_hessian(_p(vlist), nl, _p(perms), L, _p(tvlist), tvlist.shape[0], _p(tperms),
+                                               _p(f), _p(dv), _p(hess))
+        assert ret == 0
+        return f[0] + 1j * f[1], dv, hess
+
+    def optimize_brickwall_hmat(self, vstart, perms, L, tvlist, tperms, niter):
+        vstart, perms, tvlist, tperms = _c(vstart), _i(perms), _c(tvlist), _i(tperms)
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        self.lib.refdrv_optimize_brickwall_hmat(_p(vstart), vstart.shape[0], L, _p(perms), _p(tvlist),
+                                                tvlist.shape[0], _p(tperms), niter, _p(f_iter), _p(vopt))
+        return f_iter, vopt
+
+    def forward_backward_hessian(self, vlist, perms, psi, dpsi_out):
+        """One brickwall_unitary_forward + brickwall_unitary_backward_hessian of a single
+        state (the 16-qubit benchmark of the reference's examples)."""
+        vlist, perms, psi, dpsi_out = _c(vlist), _i(perms), _c(psi), _c(dpsi_out)
+        L, nl = _nq(psi), vlist.shape[0]
+        psi_out = np.empty_like(psi)
+        dpsi = np.empty_like(psi)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        ret = self.lib.refdrv_forward_backward_hessian(_p(vlist), nl, _p(perms), L, _p(psi), _p(dpsi_out),
+                                                       _p(psi_out), _p(dpsi), _p(dv), _p(hess))
+        assert ret == 0
+        return psi_out, dpsi, dv, hess

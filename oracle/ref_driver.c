@@ -138,3 +138,79 @@ void refdrv_optimize_brickwall(const struct mat4x4* vstart, int nlayers, int L, 
 	optimize_brickwall_circuit_hvp(refdrv_brickwall_ufunc, &target, vstart, nlayers, L, p, &params, niter, f_iter, vopt);
 	free(p); free(tp);
 }
+
+/* f, projected gradient and projected Hessian matrix with a brickwall target
+ * (src/target.c:996-1035) */
+int refdrv_gradient_vector_hessian_matrix(const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                                          const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                                          double* fval, double* grad_vec, double* H)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	numeric f;
+	int ret = brickwall_unitary_target_gradient_vector_hessian_matrix(refdrv_brickwall_ufunc, &target, vlist, nlayers,
+		L, p, &f, grad_vec, H);
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free(p); free(tp);
+	return ret;
+}
+
+/* f, gradients and complex Hessian with a brickwall target (src/target.c:687-806) */
+int refdrv_gradient_hessian(const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                            const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                            double* fval, struct mat4x4* dvlist, numeric* hess)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	numeric f;
+	int ret = brickwall_unitary_target_gradient_hessian(refdrv_brickwall_ufunc, &target, vlist, nlayers, L, p, &f,
+		dvlist, hess);
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free(p); free(tp);
+	return ret;
+}
+
+/* the full-Hessian driver with a brickwall target and default RTR parameters */
+void refdrv_optimize_brickwall_hmat(const struct mat4x4* vstart, int nlayers, int L, const int* perms_flat,
+                                    const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                                    int niter, double* f_iter, struct mat4x4* vopt)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	struct rtr_params params;
+	set_rtr_default_params(nlayers * num_tangent_params, &params);
+	optimize_brickwall_circuit_hmat(refdrv_brickwall_ufunc, &target, vstart, nlayers, L, p, &params, niter, f_iter, vopt);
+	free(p); free(tp);
+}
+
+/* one forward pass and one backward pass with Hessian of a single state, as in
+ * examples/benchmark/benchmark_16_qubits.c:66-80 */
+int refdrv_forward_backward_hessian(const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                                    const numeric* psi_in, const numeric* dpsi_out_in, numeric* psi_out_o,
+                                    numeric* dpsi_o, struct mat4x4* dvlist, numeric* hess)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const intqs n = (intqs)1 << L;
+	struct statevector psi, psi_out, dpsi_out, dpsi;
+	allocate_statevector(L, &psi);
+	allocate_statevector(L, &psi_out);
+	allocate_statevector(L, &dpsi_out);
+	allocate_statevector(L, &dpsi);
+	memcpy(psi.data, psi_in, n * sizeof(numeric));
+	memcpy(dpsi_out.data, dpsi_out_in, n * sizeof(numeric));
+	struct quantum_circuit_cache cache;
+	int ret = allocate_quantum_circuit_cache(L, nlayers * (L / 2), &cache);
+	if (!ret) ret = brickwall_unitary_forward(vlist, nlayers, p, &psi, &cache, &psi_out);
+	if (!ret) ret = brickwall_unitary_backward_hessian(vlist, nlayers, p, &cache, &dpsi_out, &dpsi, dvlist, hess);
+	memcpy(psi_out_o, psi_out.data, n * sizeof(numeric));
+	memcpy(dpsi_o, dpsi.data, n * sizeof(numeric));
+	free_quantum_circuit_cache(&cache);
+	free_statevector(&psi); free_statevector(&psi_out); free_statevector(&dpsi_out); free_statevector(&dpsi);
+	free(p);
+	return ret;
+}

@@ -854,3 +854,331 @@ int orc_dense_ufunc(const orc_sv* psi, void* udata, orc_sv* psi_out)
 	}
 	return 0;
 }
+
+/* ------------------------------------------------------------ full-Hessian path */
+
+/* src/gate.c:195-262: the gate on wires (i, j) of each of the ns states of an
+ * interleaved array, amplitude a of state s at data[a*ns + s] */
+void orc_apply_gate_to_array(const orc_mat4* g, int i, int j, int L, int ns, const orc_cplx* psi, orc_cplx* out)
+{
+	const long ngroups = 1L << (L - 2);
+	for (long r = 0; r < ngroups; r++) {
+		long idx[4];
+		group_indices(r, L, i, j, idx);
+		for (int s = 0; s < ns; s++) {
+			orc_cplx x[4];
+			for (int c = 0; c < 4; c++) x[c] = psi[idx[c]*ns + s];
+			for (int k = 0; k < 4; k++) {
+				orc_cplx acc = 0;
+				for (int c = 0; c < 4; c++) acc += g->data[4*k + c] * x[c];
+				out[idx[k]*ns + s] = acc;
+			}
+		}
+	}
+}
+
+/* src/gate.c:269-377: dgates[s] = sum over groups of dpsi_out (x) psi_s (no conjugation) */
+void orc_apply_gate_backward_array(int i, int j, int L, int ns, const orc_cplx* psi, const orc_cplx* dpsi_out,
+                                   orc_mat4* dgates)
+{
+	const long ngroups = 1L << (L - 2);
+	memset(dgates, 0, ns * sizeof(orc_mat4));
+	for (long r = 0; r < ngroups; r++) {
+		long idx[4];
+		group_indices(r, L, i, j, idx);
+		orc_cplx d[4];
+		for (int c = 0; c < 4; c++) d[c] = dpsi_out[idx[c]];
+		for (int s = 0; s < ns; s++)
+			for (int a = 0; a < 4; a++)
+				for (int c = 0; c < 4; c++) dgates[s].data[4*a + c] += d[a] * psi[idx[c]*ns + s];
+	}
+}
+
+/* src/gate.c:386-460: 16 states, state e = 4 r + c is E_rc psi (the unit gate with
+ * entry (r, c)): at group member r it holds psi's member c, zero elsewhere */
+void orc_apply_gate_placeholder(int i, int j, int L, const orc_cplx* psi, orc_cplx* out)
+{
+	const long ngroups = 1L << (L - 2);
+	memset(out, 0, ((size_t)16 << L) * sizeof(orc_cplx));
+	for (long r = 0; r < ngroups; r++) {
+		long idx[4];
+		group_indices(r, L, i, j, idx);
+		for (int row = 0; row < 4; row++)
+			for (int c = 0; c < 4; c++) out[idx[row]*16 + 4*row + c] = psi[idx[c]];
+	}
+}
+
+/* flat row-major (m x m) index of Hessian entry (layer a, entry x), (layer b, entry y) */
+static inline long hidx(int nlayers, int a, int x, int b, int y)
+{
+	return ((long)(a*16 + x)*nlayers + b)*16 + y;
+}
+
+/* src/brickwall_circuit.c:134-255.  cache[k] is the input state of sequential gate
+ * k (layer-major order); returns dpsi, the per-layer gradients and the symmetric
+ * (16 nlayers)^2 complex Hessian of psi_out . dpsi_out in the gate entries. */
+int orc_brickwall_backward_hessian(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* cache,
+                                   const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dvlist, orc_cplx* hess)
+{
+	const int L = dpsi->nqubits, per = L / 2, G = nlayers * per, m = 16 * nlayers;
+	const long N = 1L << L;
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, NULL, perms, NULL, wires);
+	/* adjoint states at each gate output: phi[k] for gate k */
+	orc_cplx* phi = (orc_cplx*)malloc((size_t)G * N * sizeof(orc_cplx));
+	memcpy(phi + (size_t)(G - 1) * N, dpsi_out->data, N * sizeof(orc_cplx));
+	for (int l = 0; l < nlayers; l++) memset(&dvlist[l], 0, sizeof(orc_mat4));
+	for (int k = G - 1; k >= 0; k--) {
+		orc_sv in = { phi + (size_t)k * N, L };
+		orc_sv o = { k > 0 ? phi + (size_t)(k - 1) * N : dpsi->data, L };
+		orc_mat4 dv;
+		orc_apply_gate_backward(&vlist[k / per], wires[2*k], wires[2*k + 1], &cache[k], &in, &o, &dv);
+		for (int e = 0; e < 16; e++) dvlist[k / per].data[e] += dv.data[e];
+	}
+	memset(hess, 0, (size_t)m * m * sizeof(orc_cplx));
+	orc_cplx* t[2];
+	t[0] = (orc_cplx*)malloc((size_t)16 * N * sizeof(orc_cplx));
+	t[1] = (orc_cplx*)malloc((size_t)16 * N * sizeof(orc_cplx));
+	orc_mat4 h[16];
+	for (int k = 0; k < G; k++) {
+		const int a = k / per;
+		orc_apply_gate_placeholder(wires[2*k], wires[2*k + 1], L, cache[k].data, t[0]);
+		int cur = 0;
+		for (int q = k + 1; q < G; q++) {
+			const int b = q / per;
+			orc_apply_gate_backward_array(wires[2*q], wires[2*q + 1], L, 16, t[cur], phi + (size_t)q * N, h);
+			for (int x = 0; x < 16; x++)
+				for (int y = 0; y < 16; y++) hess[hidx(nlayers, a, x, b, y)] += h[x].data[y];
+			if (q < G - 1) {
+				orc_apply_gate_to_array(&vlist[b], wires[2*q], wires[2*q + 1], L, 16, t[cur], t[1 - cur]);
+				cur = 1 - cur;
+			}
+		}
+	}
+	/* diagonal blocks: both orders of a pair of gates of the same layer */
+	for (int a = 0; a < nlayers; a++)
+		for (int x = 0; x < 16; x++)
+			for (int y = 0; y <= x; y++) {
+				const orc_cplx s = hess[hidx(nlayers, a, x, a, y)] + hess[hidx(nlayers, a, y, a, x)];
+				hess[hidx(nlayers, a, x, a, y)] = s;
+				hess[hidx(nlayers, a, y, a, x)] = s;
+			}
+	/* blocks below the diagonal from the ones above */
+	for (int a = 0; a < nlayers; a++)
+		for (int b = 0; b < a; b++)
+			for (int x = 0; x < 16; x++)
+				for (int y = 0; y < 16; y++) hess[hidx(nlayers, a, x, b, y)] = hess[hidx(nlayers, b, y, a, x)];
+	free(t[0]); free(t[1]); free(phi); free(wires);
+	return 0;
+}
+
+/* src/brickwall_circuit.c:264-315: sum over the gate positions s of layer l of the
+ * circuit with the gate at (l, s) replaced by the 16 unit placeholders */
+int orc_apply_brickwall_placeholder(const orc_mat4* vlist, int nlayers, const int* perms, int l, const orc_sv* cache,
+                                    orc_cplx* out)
+{
+	const int L = cache[0].nqubits, per = L / 2, G = nlayers * per;
+	const long N = 1L << L;
+	if (l < 0 || l >= nlayers) return -1;
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, NULL, perms, NULL, wires);
+	orc_cplx* t[2];
+	t[0] = (orc_cplx*)malloc((size_t)16 * N * sizeof(orc_cplx));
+	t[1] = (orc_cplx*)malloc((size_t)16 * N * sizeof(orc_cplx));
+	memset(out, 0, (size_t)16 * N * sizeof(orc_cplx));
+	for (int p = 0; p < per; p++) {
+		const int k = l * per + p;
+		orc_apply_gate_placeholder(wires[2*k], wires[2*k + 1], L, cache[k].data, t[0]);
+		int cur = 0;
+		for (int q = k + 1; q < G; q++) {
+			orc_apply_gate_to_array(&vlist[q / per], wires[2*q], wires[2*q + 1], L, 16, t[cur], t[1 - cur]);
+			cur = 1 - cur;
+		}
+		for (long e = 0; e < 16 * N; e++) out[e] += t[cur][e];
+	}
+	free(t[0]); free(t[1]); free(wires);
+	return 0;
+}
+
+/* src/target.c:687-806: f, per-layer gradients and the complex Hessian summed over
+ * all basis columns (one forward pass and one backward_hessian per column) */
+int orc_brickwall_target_gradient_hessian(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int L,
+                                          const int* perms, orc_cplx* fval, orc_mat4* dvlist, orc_cplx* hess)
+{
+	const int per = L / 2, G = nlayers * per, m = 16 * nlayers;
+	const long N = 1L << L;
+	orc_sv psi = { sv_alloc(L), L }, upsi = { sv_alloc(L), L }, wpsi = { sv_alloc(L), L };
+	orc_sv* cache = (orc_sv*)malloc(G * sizeof(orc_sv));
+	for (int k = 0; k < G; k++) { cache[k].data = sv_alloc(L); cache[k].nqubits = L; }
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* hu = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	for (int l = 0; l < nlayers; l++) memset(&dvlist[l], 0, sizeof(orc_mat4));
+	memset(hess, 0, (size_t)m * m * sizeof(orc_cplx));
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = 0; b < N && !ret; b++) {
+		if (target_column(uf, ud, b, &psi, &upsi) < 0) { ret = -2; break; }
+		memset(psi.data, 0, N * sizeof(orc_cplx));
+		psi.data[b] = 1;
+		orc_brickwall_forward(vlist, nlayers, perms, &psi, cache, &wpsi);
+		for (long a = 0; a < N; a++) f += upsi.data[a] * wpsi.data[a];
+		orc_brickwall_backward_hessian(vlist, nlayers, perms, cache, &upsi, &psi, dv, hu);
+		for (int l = 0; l < nlayers; l++)
+			for (int e = 0; e < 16; e++) dvlist[l].data[e] += dv[l].data[e];
+		for (long e = 0; e < (long)m * m; e++) hess[e] += hu[e];
+	}
+	*fval = f;
+	for (int k = 0; k < G; k++) free(cache[k].data);
+	free(cache); free(dv); free(hu);
+	free(psi.data); free(upsi.data); free(wpsi.data);
+	return ret;
+}
+
+/* src/target.c:937-987: real (16 nlayers)^2 Riemannian Hessian from the complex one;
+ * dvlist holds the conjugated gradients.  Column (b, k) is the Hessian applied to
+ * the tangent direction real_to_tangent(e_k, V_b); rows of layers a <= b are
+ * computed, the rest mirrored. */
+static void project_hessian_matrix(int nlayers, const orc_mat4* vlist, const orc_mat4* dvlist, const orc_cplx* hess,
+                                   double* H)
+{
+	const int m = 16 * nlayers;
+	for (int a = 0; a < nlayers; a++)
+		for (int b = a; b < nlayers; b++)
+			for (int k = 0; k < 16; k++) {
+				double r[16] = { 0 };
+				r[k] = 1;
+				orc_mat4 z, g;
+				orc_real_to_tangent(r, &vlist[b], &z);
+				for (int x = 0; x < 16; x++) {
+					orc_cplx s = 0;
+					for (int y = 0; y < 16; y++) s += hess[hidx(nlayers, a, x, b, y)] * z.data[y];
+					g.data[x] = conj(s);
+				}
+				if (a == b) {
+					orc_mat4 p, gh, t;
+					orc_project_tangent(&vlist[a], &g, &p);
+					orc_adjoint(&dvlist[a], &gh);
+					orc_symmetric_triple_product(&z, &gh, &vlist[a], &t);
+					for (int e = 0; e < 16; e++) g.data[e] = p.data[e] - t.data[e];
+				}
+				orc_tangent_to_real(&vlist[a], &g, r);
+				for (int x = 0; x < 16; x++) H[hidx(nlayers, a, x, b, k)] = r[x];
+			}
+	for (int row = 0; row < m; row++)
+		for (int col = 0; col < row; col++) H[(long)row * m + col] = H[(long)col * m + row];
+}
+
+/* src/target.c:996-1035 */
+int orc_brickwall_target_gradient_vector_hessian_matrix(orc_linear_func uf, void* ud, const orc_mat4* vlist,
+                                                        int nlayers, int L, const int* perms, orc_cplx* fval,
+                                                        double* grad_vec, double* H)
+{
+	const int m = 16 * nlayers;
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* hess = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	int ret = orc_brickwall_target_gradient_hessian(uf, ud, vlist, nlayers, L, perms, fval, dv, hess);
+	if (!ret) {
+		for (int l = 0; l < nlayers; l++) {
+			for (int e = 0; e < 16; e++) dv[l].data[e] = conj(dv[l].data[e]);
+			orc_tangent_to_real(&vlist[l], &dv[l], &grad_vec[16*l]);
+		}
+		project_hessian_matrix(nlayers, vlist, dv, hess, H);
+	}
+	free(dv); free(hess);
+	return ret;
+}
+
+/* row-major y = A x with sequential row sums (cblas_dgemv, alpha 1, beta 0) */
+static void gemv_rows(int n, const double* a, const double* x, double* y)
+{
+	for (int r = 0; r < n; r++) y[r] = dot(n, a + (long)r * n, x);
+}
+
+/* src/trust_region.c:83-141 */
+bool orc_truncated_cg_hmat(const double* grad, const double* hess, int n, double radius,
+                           const orc_tcg_params* params, double* z)
+{
+	double* r = (double*)malloc(n * sizeof(double));
+	double* d = (double*)malloc(n * sizeof(double));
+	double* hd = (double*)malloc(n * sizeof(double));
+	memcpy(r, grad, n * sizeof(double));
+	double rsq = dot(n, r, r);
+	const double stoptol = fmax(params->abstol, params->reltol * sqrt(rsq));
+	memset(z, 0, n * sizeof(double));
+	for (int k = 0; k < n; k++) d[k] = -r[k];
+	bool boundary = false;
+	for (int it = 0; it < params->maxiter; it++) {
+		gemv_rows(n, hess, d, hd);
+		const double dhd = dot(n, d, hd);
+		const double t = to_boundary(z, d, n, radius);
+		const double alpha = rsq / dhd;
+		if (dhd <= 0 || alpha > t) {
+			for (int k = 0; k < n; k++) z[k] += t * d[k];
+			boundary = true;
+			break;
+		}
+		for (int k = 0; k < n; k++) r[k] += alpha * hd[k];
+		for (int k = 0; k < n; k++) z[k] += alpha * d[k];
+		const double rsq_next = dot(n, r, r);
+		if (sqrt(rsq_next) <= stoptol) break;
+		const double beta = rsq_next / rsq;
+		for (int k = 0; k < n; k++) d[k] = beta * d[k] - r[k];
+		rsq = rsq_next;
+	}
+	free(r); free(d); free(hd);
+	return boundary;
+}
+
+/* src/trust_region.c:230-293 */
+void orc_rtr_optimize_hmat(orc_target_func f, orc_target_grad_hess_func f_deriv_hess, void* fdata,
+                           orc_retract_func retract, void* rdata, int n, const double* x_init, int m,
+                           const orc_rtr_params* params, int niter, double* f_iter, double* x_final,
+                           int* accepted, int* on_boundary)
+{
+	double* x = (double*)malloc(m * sizeof(double));
+	double* xn = (double*)malloc(m * sizeof(double));
+	double* grad = (double*)malloc(n * sizeof(double));
+	double* hess = (double*)malloc((size_t)n * n * sizeof(double));
+	double* eta = (double*)malloc(n * sizeof(double));
+	double* heta = (double*)malloc(n * sizeof(double));
+	memcpy(x, x_init, m * sizeof(double));
+	double radius = params->radius_init;
+	for (int k = 0; k < niter; k++) {
+		const double fx = f_deriv_hess(x, fdata, grad, hess);
+		const bool bnd = orc_truncated_cg_hmat(grad, hess, n, radius, &params->tcg, eta);
+		retract(x, eta, rdata, xn);
+		f_iter[k] = fx;
+		gemv_rows(n, hess, eta, heta);
+		const double rho = (f(xn, fdata) - fx) / (dot(n, grad, eta) + 0.5 * dot(n, eta, heta));
+		if (rho < 0.25) radius *= 0.25;
+		else if (rho > 0.75 && bnd) radius = fmin(2 * radius, params->maxradius);
+		const int acc = rho > params->rho_trust;
+		if (acc) { double* t = x; x = xn; xn = t; }
+		if (accepted) accepted[k] = acc;
+		if (on_boundary) on_boundary[k] = bnd;
+	}
+	memcpy(x_final, x, m * sizeof(double));
+	f_iter[niter] = f(x_final, fdata);
+	free(x); free(xn); free(grad); free(hess); free(eta); free(heta);
+}
+
+/* src/brickwall_opt.c:85-100 */
+static double glue_fdh(const double* x, void* fd, double* grad, double* hess)
+{
+	const glue* g = (const glue*)fd;
+	orc_cplx f;
+	int ret = orc_brickwall_target_gradient_vector_hessian_matrix(g->uf, g->ud, (const orc_mat4*)x,
+		g->ngates_or_layers, g->L, g->perms_or_wires, &f, grad, hess);
+	return ret < 0 ? -1 : creal(f);
+}
+
+/* src/brickwall_opt.c:159-186 */
+void orc_optimize_brickwall_hmat(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int L,
+                                 const int* perms, const orc_rtr_params* params, int niter,
+                                 double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary)
+{
+	glue g = { uf, ud, perms, nlayers, L, 1 };
+	int k = nlayers;
+	orc_rtr_optimize_hmat(glue_f, glue_fdh, &g, glue_retract, &k, 16 * nlayers, (const double*)vstart,
+	                      32 * nlayers, params, niter, f_iter, (double*)vopt, accepted, on_boundary);
+}

@@ -30,6 +30,7 @@ typedef void (*orc_hvp_func)(const double* x, void* fdata, double* vec, double* 
 typedef double (*orc_target_func)(const double* x, void* fdata);
 typedef double (*orc_target_grad_func)(const double* x, void* fdata, double* grad);
 typedef void (*orc_retract_func)(const double* x, const double* eta, void* rdata, double* xs);
+typedef double (*orc_target_grad_hess_func)(const double* x, void* fdata, double* grad, double* hess);
 
 typedef struct { int maxiter; double abstol; double reltol; } orc_tcg_params;
 typedef struct { orc_tcg_params tcg; double rho_trust, radius_init, maxradius; } orc_rtr_params;
@@ -109,6 +110,35 @@ void orc_optimize_brickwall_hvp(orc_linear_func uf, void* ud, const orc_mat4* vs
 void orc_optimize_circuit_hvp(orc_linear_func uf, void* ud, const orc_mat4* gstart, int ngates, int nqubits,
                               const int* wires, const orc_rtr_params* params, int niter,
                               double* f_iter, orc_mat4* gopt, int* accepted, int* on_boundary);
+
+/* ---- full-Hessian path (src/gate.c:195-460, src/brickwall_circuit.c:134-315,
+ *      src/target.c:687-1035, src/trust_region.c:83-141, 230-293, src/brickwall_opt.c:85-186) ----
+ * Arrays of ns states are interleaved: amplitude a of state s at data[a*ns + s].
+ * Hessians are row-major (16 nlayers)^2, entry ((a*16 + x)*nlayers + b)*16 + y for
+ * gate entry x of layer a and gate entry y of layer b. */
+void orc_apply_gate_to_array(const orc_mat4* g, int i, int j, int nqubits, int ns, const orc_cplx* psi, orc_cplx* out);
+void orc_apply_gate_backward_array(int i, int j, int nqubits, int ns, const orc_cplx* psi, const orc_cplx* dpsi_out,
+                                   orc_mat4* dgates);
+void orc_apply_gate_placeholder(int i, int j, int nqubits, const orc_cplx* psi, orc_cplx* out /* 16 states */);
+int  orc_brickwall_backward_hessian(const orc_mat4* vlist, int nlayers, const int* perms, const orc_sv* cache,
+                                    const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dvlist, orc_cplx* hess);
+int  orc_apply_brickwall_placeholder(const orc_mat4* vlist, int nlayers, const int* perms, int l, const orc_sv* cache,
+                                     orc_cplx* out /* 16 states */);
+int  orc_brickwall_target_gradient_hessian(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                           int nqubits, const int* perms, orc_cplx* fval, orc_mat4* dvlist,
+                                           orc_cplx* hess);
+int  orc_brickwall_target_gradient_vector_hessian_matrix(orc_linear_func uf, void* ud, const orc_mat4* vlist,
+                                                         int nlayers, int nqubits, const int* perms, orc_cplx* fval,
+                                                         double* grad_vec, double* H);
+bool orc_truncated_cg_hmat(const double* grad, const double* hess, int n, double radius,
+                           const orc_tcg_params* params, double* z);
+void orc_rtr_optimize_hmat(orc_target_func f, orc_target_grad_hess_func f_deriv_hess, void* fdata,
+                           orc_retract_func retract, void* rdata, int n, const double* x_init, int m,
+                           const orc_rtr_params* params, int niter, double* f_iter, double* x_final,
+                           int* accepted, int* on_boundary);
+void orc_optimize_brickwall_hmat(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int nqubits,
+                                 const int* perms, const orc_rtr_params* params, int niter,
+                                 double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary);
 
 /* ---- targets used by tests and benchmarks ---- */
 /* matrix-free brickwall target U: udata points to orc_brickwall_udata */

@@ -16,6 +16,11 @@ class Statevector(C.Structure):
     _fields_ = [("data", C.c_void_p), ("nqubits", C.c_int)]
 
 
+class StatevectorArray(C.Structure):
+    """struct statevector_array: 2^nqubits x nstates amplitudes, states interleaved."""
+    _fields_ = [("data", C.c_void_p), ("nqubits", C.c_int), ("nstates", C.c_int)]
+
+
 class QuantumCircuitCache(C.Structure):
     _fields_ = [("psi_list", C.POINTER(Statevector)), ("nqubits", C.c_int), ("ngates", C.c_int)]
 
@@ -26,6 +31,8 @@ class TruncatedCGParams(C.Structure):
 
 TARGET_FUNC = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
 TARGET_GRAD_FUNC = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double))
+TARGET_GRAD_HESS_FUNC = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double),
+                                   C.POINTER(C.c_double))
 HVP_FUNC = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double))
 RETRACT_FUNC = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double))
 LINEAR_FUNC = C.CFUNCTYPE(C.c_int, C.POINTER(Statevector), C.c_void_p, C.POINTER(Statevector))

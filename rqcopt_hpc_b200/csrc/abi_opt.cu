@@ -1,6 +1,6 @@
 // Truncated CG, Riemannian trust region and the circuit optimisers
-// (src/trust_region.c:14-65, 159-217, 306-368; src/brickwall_opt.c:22-149;
-// src/circuit_opt.c:22-124).
+// (src/trust_region.c:14-65, 83-141, 159-217, 230-293, 306-368;
+// src/brickwall_opt.c:22-186; src/circuit_opt.c:22-124).
 //
 // The vector algebra and every scalar decision of tCG and of the ratio test run
 // in FP64 on the device, in single-thread kernels whose dot products and axpys
@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "engine.h"
+#include "hess.h"
 #include "manifold.cuh"
 #include "rqc_runtime.h"
 #include "rqcopt_gpu.h"
@@ -201,6 +202,95 @@ extern "C" void riemannian_trust_region_optimize_hvp(const target_func f, const 
 	f_iter[niter] = f(x_final, fdata);
 }
 
+// ----------------------------------------------------------------------------- dense Hessian
+
+extern "C" bool truncated_cg_hmat(const double* grad, const double* hess, int n, double radius,
+                                  const struct truncated_cg_params* params, double* z)
+{
+	Runtime* rt = runtime();
+	if (!rt || n < 1 || !grad || !hess || !params || !z) {
+		if (rt) fail_arg("truncated_cg_hmat", "invalid arguments");
+		else set_last_error(E_CUDA);
+		return false;
+	}
+	// device: grad n | hess n^2 | work 3n | z n | status
+	const size_t nd = (size_t)n * n + 5 * (size_t)n;
+	int ret = ensure_device(rt->opt, nd * sizeof(double) + 64);
+	double* d_grad = static_cast<double*>(rt->opt.ptr);
+	double* d_hess = d_grad + n;
+	double* d_work = d_hess + (size_t)n * n;
+	double* d_z = d_work + 3 * (size_t)n;
+	int* d_status = reinterpret_cast<int*>(d_z + n);
+	int status = 0;
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(d_grad, grad, n * sizeof(double), cudaMemcpyHostToDevice, rt->stream));
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(d_hess, hess, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, rt->stream));
+	if (!ret) ret = tcg_hmat_device(*rt, n, d_grad, d_hess, radius, params->maxiter, params->abstol, params->reltol, d_work,
+	                                d_z, d_status);
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(z, d_z, n * sizeof(double), cudaMemcpyDeviceToHost, rt->stream));
+	if (!ret) ret = RQC_CUDA(cudaMemcpyAsync(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost, rt->stream));
+	if (!ret) ret = sync(*rt);
+	if (ret) set_last_error(ret);
+	return status != 0;
+}
+
+extern "C" void riemannian_trust_region_optimize_hmat(target_func f, target_gradient_hessian_func f_deriv_hess, void* fdata,
+                                                      retract_func retract_fn, void* rdata, const int n,
+                                                      const double* x_init, const int m, const struct rtr_params* params,
+                                                      const int niter, double* f_iter, double* x_final)
+{
+	Runtime* rt = runtime();
+	if (!rt || n < 1 || m < 1 || !f || !f_deriv_hess || !retract_fn || !params ||
+	    !(params->rho_trust >= 0 && params->rho_trust < 0.25)) {
+		if (rt) fail_arg("riemannian_trust_region_optimize_hmat", "invalid arguments");
+		else set_last_error(E_CUDA);
+		return;
+	}
+	DevVecs v;
+	int ret = alloc_vecs(*rt, n, v, rt->opt);
+	// dense Hessian, tCG work and status
+	if (!ret) ret = ensure_device(rt->arrays, ((size_t)n * n + 3 * (size_t)n) * sizeof(double) + 64);
+	double* d_hess = static_cast<double*>(rt->arrays.ptr);
+	double* d_work = d_hess + (size_t)n * n;
+	int* d_status = reinterpret_cast<int*>(d_work + 3 * (size_t)n);
+	std::vector<double> x(x_init, x_init + m), xn(m), hgrad(n), hhess((size_t)n * n), heta(n);
+	RtrState rs = {};
+	rs.radius = params->radius_init;
+	rs.maxradius = params->maxradius;
+	rs.rho_trust = params->rho_trust;
+	if (params->g_func) params->g_iter[0] = params->g_func(x.data(), params->g_data);
+	for (int k = 0; k < niter && !ret; k++) {
+		const double fx = f_deriv_hess(x.data(), fdata, hgrad.data(), hhess.data());
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.grad, hgrad.data(), n * sizeof(double), cudaMemcpyHostToDevice, rt->stream)))) break;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(d_hess, hhess.data(), (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice,
+		                                    rt->stream))))
+			break;
+		if ((ret = tcg_hmat_device(*rt, n, v.grad, d_hess, rs.radius, params->tcg_params.maxiter, params->tcg_params.abstol,
+		                           params->tcg_params.reltol, d_work, v.z, d_status)))
+			break;
+		int boundary = 0;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(heta.data(), v.z, n * sizeof(double), cudaMemcpyDeviceToHost, rt->stream)))) break;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(&boundary, d_status, sizeof(int), cudaMemcpyDeviceToHost, rt->stream)))) break;
+		if ((ret = gemv_device(*rt, n, d_hess, v.z, v.heta))) break;
+		if ((ret = sync(*rt))) break;
+		retract_fn(x.data(), heta.data(), rdata, xn.data());
+		f_iter[k] = fx;
+		rs.fx = fx;
+		rs.fnext = f(xn.data(), fdata);
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.rtr, &rs, sizeof(rs), cudaMemcpyHostToDevice, rt->stream)))) break;
+		k_rtr_rho<<<1, 1, 0, rt->stream>>>(n, v.grad, v.z, v.heta, nullptr, nullptr, v.rtr, boundary);
+		if ((ret = launched(*rt))) break;
+		if ((ret = read_state(*rt, v.rtr, &rs))) break;
+		if (rs.accept) x.swap(xn);
+		if (params->g_func) params->g_iter[k + 1] = params->g_func(x.data(), params->g_data);
+	}
+	if (ret) {
+		set_last_error(ret);
+		return;
+	}
+	memcpy(x_final, x.data(), m * sizeof(double));
+	f_iter[niter] = f(x_final, fdata);
+}
+
 // ----------------------------------------------------------------------------- device-resident optimiser
 
 namespace rqc {
@@ -354,6 +444,67 @@ struct DeviceOptimizer
 		f_iter[niter] = ff.x;
 		return OK;
 	}
+
+	// Trust region with the dense Riemannian Hessian of a brickwall (src/trust_region.c:230-293,
+	// src/brickwall_opt.c:85-100, 159-186): every evaluation in complex128.
+	int run_hmat(const struct rtr_params* params, int niter, double* f_iter, double2* x_final)
+	{
+		const int nl = pb.nunits;
+		const size_t nrec = hess_record_count(nl);
+		// record | dense Hessian | tCG work | fx | status
+		int ret = ensure_device(rt.arrays, nrec * sizeof(double2) + ((size_t)n * n + 3 * (size_t)n + 2) * sizeof(double) + 64);
+		if (ret) return ret;
+		double2* rec = static_cast<double2*>(rt.arrays.ptr);
+		double* d_hess = reinterpret_cast<double*>(rec + nrec);
+		double* d_work = d_hess + (size_t)n * n;
+		double* fx_slot = d_work + 3 * (size_t)n;
+		int* d_status = reinterpret_cast<int*>(fx_slot + 2);
+		RtrState rs = {};
+		rs.radius = params->radius_init;
+		rs.maxradius = params->maxradius;
+		rs.rho_trust = params->rho_trust;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(v.rtr, &rs, sizeof(rs), cudaMemcpyHostToDevice, rt.stream)))) return ret;
+		HessCircuit c;
+		c.L = pb.L;
+		c.nlayers = nl;
+		c.wires = pb.wires.data();
+		const int threads = 64, blocks = (nl + threads - 1) / threads;
+		for (int k = 0; k < niter && !ret; k++) {
+			// f, gradient vector and Hessian matrix at x (src/trust_region.c:263)
+			if ((ret = load_gates(x))) break;
+			c.ugates = hx.data();
+			if ((ret = hessian_target_device(rt, c, th.spec, rec))) break;
+			if ((ret = project_hessian_device(rt, nl, ug, rec, v.grad, d_hess))) break;
+			if ((ret = RQC_CUDA(cudaMemcpyAsync(fx_slot, rec, sizeof(double), cudaMemcpyDeviceToDevice, rt.stream)))) break;
+			// tCG on the dense Hessian (src/trust_region.c:264)
+			if ((ret = tcg_hmat_device(rt, n, v.grad, d_hess, rs.radius, params->tcg_params.maxiter,
+			                           params->tcg_params.abstol, params->tcg_params.reltol, d_work, v.z, d_status)))
+				break;
+			int boundary = 0;
+			if ((ret = RQC_CUDA(cudaMemcpyAsync(&boundary, d_status, sizeof(int), cudaMemcpyDeviceToHost, rt.stream)))) break;
+			// candidate, model decrease and ratio test (src/trust_region.c:265-281)
+			k_retract<<<blocks, threads, 0, rt.stream>>>(nl, x, v.z, xn);
+			if ((ret = launched(rt))) break;
+			if ((ret = gemv_device(rt, n, d_hess, v.z, v.heta))) break;
+			if ((ret = load_gates(xn))) break;   // synchronises: boundary is valid after this
+			if ((ret = eval_f(PREC_C128))) break;
+			k_rtr_rho<<<1, 1, 0, rt.stream>>>(n, v.grad, v.z, v.heta, fx_slot, reinterpret_cast<const double*>(res), v.rtr,
+			                                   boundary);
+			if ((ret = launched(rt))) break;
+			if ((ret = read_state(rt, v.rtr, &rs))) break;
+			f_iter[k] = rs.fx;
+			if (rs.accept) std::swap(x, xn);
+		}
+		if (ret) return ret;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(x_final, x, hx.size() * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
+		if ((ret = load_gates(x))) return ret;
+		if ((ret = eval_f(PREC_C128))) return ret;
+		double2 ff;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(&ff, res, sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
+		if ((ret = sync(rt))) return ret;
+		f_iter[niter] = ff.x;
+		return OK;
+	}
 };
 
 }  // namespace rqc
@@ -361,7 +512,7 @@ struct DeviceOptimizer
 namespace {
 
 void run_optimizer(const char* fn, Problem& pb, linear_func ufunc, void* udata, struct rtr_params* params, int niter,
-                   double* f_iter, const struct mat4x4* start, struct mat4x4* out)
+                   double* f_iter, const struct mat4x4* start, struct mat4x4* out, bool hmat = false)
 {
 	TargetHolder th;
 	if (!th.set(ufunc, udata, pb.L)) {
@@ -376,7 +527,9 @@ void run_optimizer(const char* fn, Problem& pb, linear_func ufunc, void* udata, 
 	params->g_iter = NULL;
 	DeviceOptimizer opt(*rt, pb, th);
 	int ret = opt.init(reinterpret_cast<const double2*>(start));
-	if (!ret) ret = opt.run(params, niter, f_iter, reinterpret_cast<double2*>(out), rt->precision);
+	if (!ret)
+		ret = hmat ? opt.run_hmat(params, niter, f_iter, reinterpret_cast<double2*>(out))
+		           : opt.run(params, niter, f_iter, reinterpret_cast<double2*>(out), rt->precision);
 	if (ret) set_last_error(ret);
 }
 
@@ -405,4 +558,17 @@ extern "C" void optimize_quantum_circuit(linear_func ufunc, void* udata, const s
 		return;
 	}
 	run_optimizer("optimize_quantum_circuit", pb, ufunc, udata, params, niter, f_iter, gates_start, gates_opt);
+}
+
+extern "C" void optimize_brickwall_circuit_hmat(linear_func ufunc, void* udata, const struct mat4x4 vlist_start[],
+                                                const int nlayers, const int nqubits, const int* perms[],
+                                                struct rtr_params* params, const int niter, double* f_iter,
+                                                struct mat4x4 vlist_opt[])
+{
+	Problem pb;
+	if (!params || !f_iter || !vlist_opt || !pb.set_brickwall(nqubits, nlayers, vlist_start, nullptr, perms)) {
+		fail_arg("optimize_brickwall_circuit_hmat", "invalid arguments");
+		return;
+	}
+	run_optimizer("optimize_brickwall_circuit_hmat", pb, ufunc, udata, params, niter, f_iter, vlist_start, vlist_opt, true);
 }

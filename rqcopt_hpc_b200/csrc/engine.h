@@ -68,6 +68,11 @@ int gate_backward_device(Runtime& rt, int L, const double2* gate, int i, int j, 
 int column_passes_device(Runtime& rt, int L, int ngates, const double2* gates, const double2* dirs, const int* wires,
                          const double2* d_psi, const double2* d_phi, double2* d_psi_out, double2* d_dgates,
                          double2* d_hess);
+// Target columns of one chunk: phi[c] = -conj(U e_{b0 + c}) for c < ncols (states of
+// 2^L amplitudes one after another), through the device circuit of t or its host
+// callback; p0 and p1 are two chunk-sized scratch arrays.
+int target_columns_device(Runtime& rt, const TargetSpec& t, int L, int64_t b0, int64_t ncols, double2* phi,
+                          double2* p0, double2* p1);
 // c = a + b elementwise, n complex entries
 int add_device(Runtime& rt, const double2* a, const double2* b, double2* c, long n);
 

@@ -13,7 +13,7 @@ namespace rqc {
 
 enum ErrorCode { OK = 0, E_ALLOC = -1, E_UFUNC = -2, E_PASS = -3, E_PASS2 = -4, E_CUDA = -5, E_ARG = -6 };
 
-enum KernelClass { KC_APPLY = 0, KC_FORWARD = 1, KC_REVERSE = 2, KC_FUSED = 3, KC_COUNT = 4 };
+enum KernelClass { KC_APPLY = 0, KC_FORWARD = 1, KC_REVERSE = 2, KC_FUSED = 3, KC_HESS = 4, KC_COUNT = 5 };
 
 struct Buffer
 {
@@ -35,6 +35,7 @@ struct Runtime
 	Buffer opt;           // optimiser vectors
 	Buffer scratch;       // FP64 per-lane sums of the complex64 reverse passes
 	Buffer stage[4];      // staging of host statevectors
+	Buffer arrays;        // statevector arrays and gate-input caches of the full-Hessian calls
 	Buffer hpin;          // pinned host scratch
 
 	// configuration
@@ -47,8 +48,8 @@ struct Runtime
 	// instrumentation
 	unsigned long long launches = 0;
 	bool timing = false;
-	double time_ms[KC_COUNT] = {0, 0, 0, 0};
-	long time_count[KC_COUNT] = {0, 0, 0, 0};
+	double time_ms[KC_COUNT] = {0, 0, 0, 0, 0};
+	long time_count[KC_COUNT] = {0, 0, 0, 0, 0};
 	std::vector<cudaEvent_t> event_pool;
 	struct Pending { cudaEvent_t a, b; int cls; };
 	std::vector<Pending> pending;

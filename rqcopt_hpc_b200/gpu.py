@@ -19,9 +19,10 @@ import os
 
 import numpy as np
 
-from .abi import (HVP_FUNC, LINEAR_FUNC, RETRACT_FUNC, TARGET_FUNC, TARGET_GRAD_FUNC, BrickwallTarget,
-                  CircuitTarget, QuantumCircuitCache, RTRParams, Statevector, TruncatedCGParams, cplx,
-                  default_rtr_params, default_tcg_params, ints, perm_pointers, ptr, wrap_ufunc)
+from .abi import (HVP_FUNC, LINEAR_FUNC, RETRACT_FUNC, TARGET_FUNC, TARGET_GRAD_FUNC, TARGET_GRAD_HESS_FUNC,
+                  BrickwallTarget, CircuitTarget, QuantumCircuitCache, RTRParams, Statevector, StatevectorArray,
+                  TruncatedCGParams, cplx, default_rtr_params, default_tcg_params, ints, perm_pointers, ptr,
+                  wrap_ufunc)
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "librqcopt_gpu.so")
 
@@ -77,6 +78,19 @@ _SIGS = {
     "multiply_matrices": (None, [VP, VP, VP]),
     "inverse_matrix": (I, [VP, VP]),
     "symmetric_triple_matrix_product": (None, [VP, VP, VP, VP]),
+    "allocate_statevector_array": (I, [I, I, C.POINTER(StatevectorArray)]),
+    "free_statevector_array": (None, [C.POINTER(StatevectorArray)]),
+    "apply_gate_to_array": (None, [VP, I, I, C.POINTER(StatevectorArray), C.POINTER(StatevectorArray)]),
+    "apply_gate_backward_array": (None, [VP, I, I, C.POINTER(StatevectorArray), PSV, VP]),
+    "apply_gate_placeholder": (None, [I, I, PSV, C.POINTER(StatevectorArray)]),
+    "brickwall_unitary_backward_hessian": (I, [VP, I, VP, C.POINTER(QuantumCircuitCache), PSV, PSV, VP, VP]),
+    "apply_brickwall_unitary_gate_placeholder": (I, [VP, I, VP, I, C.POINTER(QuantumCircuitCache),
+                                                     C.POINTER(StatevectorArray)]),
+    "brickwall_unitary_target_gradient_hessian": (I, [VP, VP, VP, I, I, VP, VP, VP, VP]),
+    "brickwall_unitary_target_gradient_vector_hessian_matrix": (I, [VP, VP, VP, I, I, VP, VP, VP, VP]),
+    "truncated_cg_hmat": (C.c_bool, [VP, VP, I, D, C.POINTER(TruncatedCGParams), VP]),
+    "riemannian_trust_region_optimize_hmat": (None, [VP, VP, VP, VP, VP, I, VP, I, C.POINTER(RTRParams), I, VP, VP]),
+    "optimize_brickwall_circuit_hmat": (None, [VP, VP, VP, I, I, VP, C.POINTER(RTRParams), I, VP, VP]),
     "rqcopt_brickwall_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_circuit_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_gpu_set_precision": (I, [I]),
@@ -108,7 +122,7 @@ _SIGS = {
 }
 
 PRECISION_C128, PRECISION_MIXED, PRECISION_C64 = 0, 1, 2
-KC_APPLY, KC_FORWARD, KC_REVERSE, KC_FUSED = 0, 1, 2, 3
+KC_APPLY, KC_FORWARD, KC_REVERSE, KC_FUSED, KC_HESS = 0, 1, 2, 3, 4
 
 
 def lib():
@@ -268,6 +282,76 @@ def brickwall_unitary_backward(vlist, perms, cache, dpsi_out):
     return dpsi, dv
 
 
+# ------------------------------------------------------------------------ full-Hessian primitives
+# Statevector arrays are numpy complex128 arrays of shape (2^L, nstates), amplitude-major
+# (the reference's interleaved layout).
+
+def _sva(a, L):
+    return StatevectorArray(a.ctypes.data, L, a.shape[1])
+
+
+def apply_gate_to_array(V, i, j, psi):
+    V, psi = cplx(V), cplx(psi)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    lib().apply_gate_to_array(ptr(V), i, j, C.byref(_sva(psi, L)), C.byref(_sva(out, L)))
+    _check_void("apply_gate_to_array")
+    return out
+
+
+def apply_gate_backward_array(V, i, j, psi, dpsi_out):
+    V, psi, dpsi_out = cplx(V), cplx(psi), cplx(dpsi_out)
+    L = _nq(psi)
+    dg = np.empty((psi.shape[1], 4, 4), np.complex128)
+    lib().apply_gate_backward_array(ptr(V), i, j, C.byref(_sva(psi, L)), C.byref(_sv(dpsi_out, L)), ptr(dg))
+    _check_void("apply_gate_backward_array")
+    return dg
+
+
+def apply_gate_placeholder(i, j, psi):
+    psi = cplx(psi)
+    L = _nq(psi)
+    out = np.empty((psi.shape[0], 16), np.complex128)
+    lib().apply_gate_placeholder(i, j, C.byref(_sv(psi, L)), C.byref(_sva(out, L)))
+    _check_void("apply_gate_placeholder")
+    return out
+
+
+def _host_cache(states):
+    """quantum_circuit_cache over host arrays (kept alive by the returned tuple)."""
+    states = [cplx(s) for s in states]
+    L = _nq(states[0])
+    arr = (Statevector * len(states))(*[Statevector(s.ctypes.data, L) for s in states])
+    c = QuantumCircuitCache(C.cast(arr, C.POINTER(Statevector)), L, len(states))
+    return c, (arr, states)
+
+
+def brickwall_unitary_backward_hessian(vlist, perms, cache, dpsi_out):
+    """cache: a Cache from brickwall_unitary_forward or a list of the gate input states."""
+    vlist, dpsi_out = cplx(vlist), cplx(dpsi_out)
+    L, nl = _nq(dpsi_out), vlist.shape[0]
+    pp, keep = perm_pointers(perms)
+    c, hold = (cache.c, None) if isinstance(cache, Cache) else _host_cache(cache)
+    dpsi = np.empty_like(dpsi_out)
+    dv = np.empty((nl, 4, 4), np.complex128)
+    hess = np.empty((16 * nl, 16 * nl), np.complex128)
+    _check("brickwall_unitary_backward_hessian",
+           lib().brickwall_unitary_backward_hessian(ptr(vlist), nl, C.cast(pp, VP), C.byref(c), C.byref(_sv(dpsi_out, L)),
+                                                    C.byref(_sv(dpsi, L)), ptr(dv), ptr(hess)))
+    return dpsi, dv, hess
+
+
+def apply_brickwall_unitary_gate_placeholder(vlist, perms, l, cache):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    c, hold = (cache.c, None) if isinstance(cache, Cache) else _host_cache(cache)
+    out = np.empty((1 << c.nqubits, 16), np.complex128)
+    _check("apply_brickwall_unitary_gate_placeholder",
+           lib().apply_brickwall_unitary_gate_placeholder(ptr(vlist), vlist.shape[0], C.cast(pp, VP), l, C.byref(c),
+                                                          C.byref(_sva(out, c.nqubits))))
+    return out
+
+
 # ------------------------------------------------------------------------ targets
 
 class Target:
@@ -407,7 +491,88 @@ def brickwall_unitary_target_projected_hessian_vector_product(target, vlist, vdi
     return f[0], g, h
 
 
+def brickwall_unitary_target_gradient_hessian(target, vlist, perms, nqubits):
+    """f, per-layer gradients and the complex (16 nlayers)^2 Hessian."""
+    vlist = cplx(vlist)
+    nl = vlist.shape[0]
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    dv = np.empty((nl, 4, 4), np.complex128)
+    hess = np.empty((16 * nl, 16 * nl), np.complex128)
+    _check("brickwall_unitary_target_gradient_hessian",
+           lib().brickwall_unitary_target_gradient_hessian(target.ufunc, target.udata, ptr(vlist), nl, nqubits,
+                                                           C.cast(pp, VP), ptr(f), ptr(dv), ptr(hess)))
+    return f[0], dv, hess
+
+
+def brickwall_unitary_target_gradient_vector_hessian_matrix(target, vlist, perms, nqubits):
+    """f, the Riemannian gradient vector and the real symmetric Hessian matrix."""
+    vlist = cplx(vlist)
+    nl = vlist.shape[0]
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * nl)
+    H = np.empty((16 * nl, 16 * nl))
+    _check("brickwall_unitary_target_gradient_vector_hessian_matrix",
+           lib().brickwall_unitary_target_gradient_vector_hessian_matrix(target.ufunc, target.udata, ptr(vlist), nl,
+                                                                         nqubits, C.cast(pp, VP), ptr(f), ptr(g), ptr(H)))
+    return f[0], g, H
+
+
 # ------------------------------------------------------------------------ trust region and optimisers
+
+def truncated_cg_hmat(grad, hess, radius, params=None):
+    grad = np.ascontiguousarray(grad, dtype=np.float64)
+    hess = np.ascontiguousarray(hess, dtype=np.float64)
+    n = grad.shape[0]
+    params = params or default_tcg_params(n)
+    z = np.empty(n)
+    b = lib().truncated_cg_hmat(ptr(grad), ptr(hess), n, radius, C.byref(params), ptr(z))
+    _check_void("truncated_cg_hmat")
+    return z, bool(b)
+
+
+def riemannian_trust_region_optimize_hmat(f, f_deriv_hess, retract_fn, n, x_init, niter, params=None):
+    """RTR with Python callbacks f(x) -> float, f_deriv_hess(x) -> (f, grad, hess) and
+    retract_fn(x, eta) -> x_new over real vectors x of length m."""
+    x_init = np.ascontiguousarray(x_init, dtype=np.float64)
+    m = x_init.shape[0]
+    params = params or default_rtr_params(n)
+
+    def cf(xp, fd):
+        return float(f(np.ctypeslib.as_array(xp, shape=(m,)).copy()))
+
+    def cfdh(xp, fd, g, h):
+        fx, gv, hv = f_deriv_hess(np.ctypeslib.as_array(xp, shape=(m,)).copy())
+        np.ctypeslib.as_array(g, shape=(n,))[:] = gv
+        np.ctypeslib.as_array(h, shape=(n * n,))[:] = np.asarray(hv).ravel()
+        return float(fx)
+
+    def cr(xp, eta, rd, xs):
+        np.ctypeslib.as_array(xs, shape=(m,))[:] = retract_fn(np.ctypeslib.as_array(xp, shape=(m,)).copy(),
+                                                             np.ctypeslib.as_array(eta, shape=(n,)).copy())
+
+    fcb, dcb, rcb = TARGET_FUNC(cf), TARGET_GRAD_HESS_FUNC(cfdh), RETRACT_FUNC(cr)
+    f_iter = np.empty(niter + 1)
+    x_final = np.empty(m)
+    lib().riemannian_trust_region_optimize_hmat(C.cast(fcb, VP), C.cast(dcb, VP), None, C.cast(rcb, VP), None, n,
+                                                ptr(x_init), m, C.byref(params), niter, ptr(f_iter), ptr(x_final))
+    _check_void("riemannian_trust_region_optimize_hmat")
+    return f_iter, x_final
+
+
+def optimize_brickwall_circuit_hmat(target, vlist_start, perms, nqubits, niter, params=None):
+    vlist_start = cplx(vlist_start)
+    nl = vlist_start.shape[0]
+    pp, keep = perm_pointers(perms)
+    params = params or default_rtr_params(16 * nl)
+    f_iter = np.empty(niter + 1)
+    vopt = np.empty_like(vlist_start)
+    lib().optimize_brickwall_circuit_hmat(target.ufunc, target.udata, ptr(vlist_start), nl, nqubits, C.cast(pp, VP),
+                                          C.byref(params), niter, ptr(f_iter), ptr(vopt))
+    _check_void("optimize_brickwall_circuit_hmat")
+    return f_iter, vopt
+
 
 def truncated_cg_hvp(grad, hvp_fn, radius, params=None, x=None):
     """Steihaug tCG with a Python Hessian-vector product `hvp_fn(vec) -> H vec`."""
@@ -488,6 +653,14 @@ def multiply_matrices(a, b):
     c = np.empty((4, 4), np.complex128)
     lib().multiply_matrices(ptr(a), ptr(b), ptr(c))
     return c
+
+
+def retract(u, eta):
+    """Polar retraction of the unitary u along the tangent vector given by 16 reals (src/matrix.c:517-531)."""
+    u, eta = cplx(u), np.ascontiguousarray(eta, dtype=np.float64)
+    v = np.empty((4, 4), np.complex128)
+    lib().retract(ptr(u), ptr(eta), ptr(v))
+    return v
 
 
 def inverse_matrix(a):

@@ -26,6 +26,9 @@ FIXTURES = [
     "brickwall_unitary_target_and_projected_gradient", "brickwall_unitary_target_hessian_vector_product",
     "brickwall_unitary_target_projected_hessian_vector_product",
     "real_to_tangent", "project_tangent", "polar_factor", "multiply",
+    # full-Hessian path
+    "apply_gate_to_array", "apply_gate_placeholder", "brickwall_unitary_backward_hessian",
+    "brickwall_unitary_target_gradient_hessian", "brickwall_unitary_target_gradient_vector_hessian_matrix",
 ]
 
 

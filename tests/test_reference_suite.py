@@ -253,3 +253,75 @@ def test_truncated_cg_hvp(impl):
     z, on_boundary = impl.truncated_cg_hvp(grad, lambda v: hess @ v, 1.5)
     assert np.max(np.abs(z - d["z"])) <= 1e-14
     assert on_boundary == bool(d["on_boundary"])
+
+
+# ------------------------------------------------------------------ full-Hessian path
+# test_gate.c:203-330, test_brickwall_circuit.c:297-460, test_target.c:1139-1285, 1391-1484,
+# test_trust_region.c:88-145
+
+def test_apply_gate_to_array(impl):
+    d = golden("apply_gate_to_array")
+    for k, (i, j) in enumerate([(2, 5), (4, 1), (3, 4)]):
+        chi = impl.apply_gate_to_array(d["V"], i, j, d["psi"])
+        assert udist(chi, d[f"chi{k + 1}"]) <= 1e-12
+
+
+def test_apply_gate_placeholder(impl):
+    d = golden("apply_gate_placeholder")
+    assert udist(impl.apply_gate_placeholder(2, 5, d["psi"]).ravel(), d["psi_out1"]) <= 1e-12
+    assert udist(impl.apply_gate_placeholder(5, 1, d["psi"]).ravel(), d["psi_out2"]) <= 1e-12
+
+
+def test_brickwall_unitary_backward_hessian(impl):
+    d = golden("brickwall_unitary_backward_hessian")
+    V, Z, P = stack(d, "V", 4), stack(d, "Z", 4), stack(d, "perm", 4)
+    psi, dout = d["psi"], d["dpsi_out"]
+    for nl in (3, 4):
+        v, z, p = V[:nl], Z[:nl], P[:nl]
+        out, cache = impl.brickwall_unitary_forward(v, p, psi)
+        assert udist(out, d[f"psi_out{nl - 3}"]) <= 1e-12
+        dpsi, dv, hess = impl.brickwall_unitary_backward_hessian(v, p, cache, dout)
+        assert udist(hess, hess.T) <= 1e-12
+        num_psi = num_grad_backward(lambda x: impl.apply_brickwall_unitary(v, p, x), psi, dout)
+        assert udist(dpsi, num_psi) <= 1e-8
+        num_v = num_grad_backward(lambda w: impl.apply_brickwall_unitary(w, p, psi), v, dout)
+        assert udist(dv, num_v) <= 1e-8
+
+        def grad_of(w):
+            _, c = impl.brickwall_unitary_forward(w, p, psi)
+            return impl.brickwall_unitary_backward_hessian(w, p, c, dout)[1]
+
+        num_h = num_grad_backward(grad_of, v, z)
+        assert udist((hess @ z.ravel()).reshape(nl, 4, 4), num_h) <= 1e-8
+
+
+def test_brickwall_unitary_target_gradient_hessian(impl):
+    d = golden("brickwall_unitary_target_gradient_hessian")
+    t = impl.target("fixture")
+    V, Z, P = stack(d, "V", 5), stack(d, "Z", 5), stack(d, "perm", 5)
+    for k, nl in enumerate([4, 5]):
+        v, z, p = V[:nl], Z[:nl], P[:nl]
+        f, dv, hess = impl.brickwall_unitary_target_gradient_hessian(t, v, p, 6)
+        assert udist(hess, hess.T) <= 1e-12
+        assert abs(f - d[f"f{k}"]) <= 1e-12
+        assert udist(dv, d[f"dVlist{k}"]) <= 1e-12
+        assert udist(hess, d[f"hess{k}"]) <= 1e-12
+        num_h = num_grad_wirtinger(lambda w: impl.brickwall_unitary_target_and_gradient(t, w, p, 6)[1], v, z)
+        assert udist((hess @ z.ravel()).reshape(nl, 4, 4), num_h) <= 1e-7
+
+
+def test_brickwall_unitary_target_gradient_vector_hessian_matrix(impl):
+    d = golden("brickwall_unitary_target_gradient_vector_hessian_matrix")
+    t = impl.target("fixture")
+    f, g, H = impl.brickwall_unitary_target_gradient_vector_hessian_matrix(t, stack(d, "V", 5), stack(d, "perm", 5), 6)
+    assert abs(f - d["f"]) <= 1e-12
+    assert np.max(np.abs(g - d["grad"])) <= 1e-14
+    assert np.max(np.abs(H - H.T)) <= 1e-14
+    assert np.max(np.abs(H - d["H"])) <= 1e-13
+
+
+def test_truncated_cg_hmat(impl):
+    d = golden("truncated_cg")
+    z, on_boundary = impl.truncated_cg_hmat(d["grad"], d["hess"], 1.5)
+    assert np.max(np.abs(z - d["z"])) <= 1e-14
+    assert on_boundary == bool(d["on_boundary"])
