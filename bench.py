@@ -230,6 +230,218 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
     return res
 
 
+# ----------------------------------------------------------------------------- full-Hessian path
+
+def hess_model(L, nlayers, single):
+    """Algorithmic HBM transfers (state-sized reads + writes) and complex multiply-adds
+    per basis column of the full-Hessian sweep kernels of one evaluation.
+
+    L <= 12 runs k_hlayer, one launch per layer with the tangents' column tiles in
+    shared memory: per layer a the tangents of the earlier layers (16 a) are read once
+    and all 16 (a + 1) written once (not after the last layer), phi_q and psi_q of the
+    layer's gates are read once (psi_0 of a basis column is generated).  Larger L runs
+    k_hsweep, one launch per gate: per gate q of layer a, phi_q is read, the tangents of
+    the earlier layers are read and written, the 16 tangents of layer a are read (not
+    at the layer's first gate) and written (not at the last gate), and psi_q is read
+    (and, in target sums, the next psi written).  Complex multiply-adds: 16 for the
+    contraction with phi_q and 16 for G_q per group of 4 amplitudes and active state."""
+    per = L // 2
+    G = nlayers * per
+    layered = L <= 12
+    transfers = 0
+    cmacs = 0
+    for q in range(G):
+        a, pos = divmod(q, per)
+        last = q == G - 1
+        # multiply-adds: psi (contraction, G at the last gate), earlier layers, own layer
+        cmacs += 16 + (16 if last else 0)
+        cmacs += 16 * a * (16 + (0 if last else 16))
+        cmacs += 0 if pos == 0 else 16 * (16 + (0 if last else 16))
+        if layered:
+            continue
+        t_read = 16 * a + (0 if pos == 0 else 16)
+        t_write = 0 if last else 16 * (a + 1)
+        psi = 1 if single else (1 if q > 0 else 0) + (0 if last else 1)
+        transfers += 1 + psi + t_read + t_write
+    if layered:
+        for a in range(nlayers):
+            transfers += 16 * a + (16 * (a + 1) if a < nlayers - 1 else 0) + per + per
+        if not single:
+            transfers -= 1          # psi_0 is the basis column
+    groups = (1 << L) // 4
+    return {"kernel": ("k_hlayer (one brickwall layer of the full-Hessian tangent sweep, column tiles in shared memory)"
+                       if layered else "k_hsweep (one gate of the full-Hessian tangent sweep)"),
+            "launches": nlayers if layered else G, "transfers": transfers, "cmacs": cmacs * groups}
+
+
+def _ref_hessian_worker(args):
+    L, depth, tdepth, b0, b1 = args
+    from oracle.oracle import Reference
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth)
+    t0 = time.perf_counter()
+    Reference().hessian_columns(vlist, perms, L, tvlist, tperms, b0, b1)
+    return time.perf_counter() - t0
+
+
+def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
+    """Full-Hessian ("hmat") path.  (1) The reference's own Hessian benchmark
+    (examples/benchmark/benchmark_16_qubits.c): brickwall_unitary_forward plus
+    brickwall_unitary_backward_hessian of one L=16 state through 8 layers.
+    (2) f + gradient vector + real Hessian matrix of the brickwall target summed over
+    all basis columns (brickwall_unitary_target_gradient_vector_hessian_matrix) at
+    L=8 depth 5 and L=12 depth 9.  (3) optimize_brickwall_circuit_hmat at L=8 depth 5.
+    GPU numbers go through the C ABI with host buffers (e2e) and, per kernel, CUDA
+    events on the library stream; the reference's C code runs on the host cores."""
+    import multiprocessing as mp
+    from rqcopt_hpc_b200.workloads import perms_for as pf
+    from oracle.oracle import Reference
+    have_ref = with_reference and Reference.available()
+    out = {}
+
+    def timed(fn, n):
+        gpu.enable_kernel_timing(True)
+        gpu.reset_launch_count()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        for _ in range(n):
+            r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        wall = (time.perf_counter() - t0) / n
+        hs_ms, hs_n = gpu.kernel_time(gpu.KC_HESS)
+        gpu.enable_kernel_timing(False)
+        return r, wall, e0.elapsed_time(e1) / n, hs_ms / n, hs_n // n, gpu.launch_count() // n
+
+    def roofline(model, columns, L, ms, launches):
+        """HBM roofline for the per-gate sweep; the layer kernel moves ~L/2 times fewer
+        bytes and is bound by FP64 arithmetic instead (no measured FP64 peak exists for
+        this pool: the nominal 37 TFLOP/s of B200 is used and labelled as such)."""
+        state_bytes = columns * (16 << L)
+        per_launch = model["transfers"] * state_bytes / launches
+        gbs = per_launch / (ms / launches * 1e-3) / 1e9
+        tflops = 8.0 * model["cmacs"] * columns / (ms * 1e-3) / 1e12
+        out = {"kernel": model["kernel"], "avg_launch_ms": ms / launches, "launches": launches,
+               "bytes_per_launch": per_launch,
+               "bytes_model": "algorithmic state transfers of the sweep (bench.hess_model) x columns x 2^L x 16 B",
+               "hbm_gbs": gbs, "hbm_frac": gbs / hbm_peak, "fp64_tflops": tflops}
+        if "k_hlayer" in model["kernel"]:
+            out.update({"bound": "fp64", "achieved": tflops, "peak": 37.0, "unit": "TFLOP/s",
+                        "frac": tflops / 37.0, "peak_source": "nominal B200 FP64 (no measured FP64 peak)"})
+        else:
+            out.update({"bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s", "frac": gbs / hbm_peak,
+                        "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)"})
+        return out
+
+    # GPU legs first, the reference's CPU legs after them (no CPU load during GPU timing)
+    # (1) single state, L = 16, 8 layers
+    L, nl = 16, 8
+    rng = np.random.default_rng(16)
+    vlist = np.stack([haar(rng) for _ in range(nl)])
+    perms = pf(L, nl)
+    psi = (rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)) / np.sqrt(2 << L)
+    dout = (rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)) / np.sqrt(2 << L)
+    cache = gpu.Cache(L, nl * (L // 2))
+
+    def single():
+        gpu.brickwall_unitary_forward(vlist, perms, psi, cache)
+        return gpu.brickwall_unitary_backward_hessian(vlist, perms, cache, dout)
+
+    for _ in range(2):
+        single()
+    (dpsi, dv, hess), wall, dev_ms, hs_ms, hs_n, launches = timed(single, steps)
+    r1 = {"workload": "brickwall_unitary_forward + brickwall_unitary_backward_hessian, one L=16 state, 8 layers "
+                      "(examples/benchmark/benchmark_16_qubits.c)",
+          "e2e_ms": wall * 1e3, "device_ms": dev_ms, "sweep_ms": hs_ms, "gpu_launches": launches,
+          "roofline": roofline(hess_model(L, nl, True), 1, L, hs_ms, hs_n)}
+    single_case = (vlist, perms, psi, dout, dpsi, dv, hess, wall)
+    out["single_state_L16"] = r1
+    del cache
+
+    # (2) target sums
+    target_cases = []
+    for L, depth, tdepth, seed, tseed in [(8, 5, 3, 0, 1), (12, 9, 5, 10, 11)]:
+        vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, seed, tseed)
+        tg = gpu.Target(brickwall=(tvlist, tperms))
+
+        def target():
+            return gpu.brickwall_unitary_target_gradient_vector_hessian_matrix(tg, vlist, perms, L)
+
+        target()
+        (f, g, H), wall, dev_ms, hs_ms, hs_n, launches = timed(target, steps)
+        N = 1 << L
+        r2 = {"workload": f"f + gradient vector + Hessian matrix, brickwall L={L} depth {depth} vs brickwall target "
+                          f"depth {tdepth}, all {N} basis columns", "evals_per_s_e2e": 1.0 / wall,
+              "evals_per_s_device": 1e3 / dev_ms, "sweep_ms": hs_ms, "gpu_launches": launches,
+              "roofline": roofline(hess_model(L, depth, False), N, L, hs_ms, hs_n)}
+        out[f"target_L{L}_depth{depth}"] = r2
+        target_cases.append((r2, L, depth, tdepth, vlist, perms, tvlist, tperms, g, H, wall))
+
+    # (3) optimiser
+    L, depth, tdepth, niter = 8, 5, 3, 10
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, 0, 1)
+    tg = gpu.Target(brickwall=(tvlist, tperms))
+    gpu.optimize_brickwall_circuit_hmat(tg, vlist, perms, L, 1)
+    t0 = time.perf_counter()
+    f_iter, _ = gpu.optimize_brickwall_circuit_hmat(tg, vlist, perms, L, niter)
+    tg_s = time.perf_counter() - t0
+    r3 = {"workload": f"optimize_brickwall_circuit_hmat, L={L} depth {depth}, target depth {tdepth}, {niter} iterations",
+          "seconds": tg_s, "seconds_per_iteration": tg_s / niter, "f_first": float(f_iter[0]),
+          "f_final": float(f_iter[-1])}
+    out["optimize_hmat_L8"] = r3
+    if not have_ref:
+        return out
+
+    # reference legs
+    vlist, perms, psi, dout, dpsi, dv, hess, wall = single_case
+    t0 = time.perf_counter()
+    _, dpr, dvr, hr = Reference().forward_backward_hessian(vlist, perms, psi, dout)
+    tref = time.perf_counter() - t0
+    r1["cpu_baseline"] = {"value": tref * 1e3, "unit": "ms per call", "cores": 1, "kind": "reference",
+                          "sample": "one full call of the reference (single-threaded C)"}
+    r1["speedup_e2e"] = tref / wall
+    r1["max_rel_diff_vs_reference"] = {
+        "hess": float(np.max(np.abs(hess - hr)) / np.max(np.abs(hr))),
+        "dvlist": float(np.max(np.abs(dv - dvr)) / np.max(np.abs(dvr))),
+        "dpsi": float(np.max(np.abs(dpsi - dpr)) / np.max(np.abs(dpr)))}
+    for r2, L, depth, tdepth, vlist, perms, tvlist, tperms, g, H, wall in target_cases:
+        N = 1 << L
+        if L <= 8:
+            t0 = time.perf_counter()
+            fr, gr, Hr = Reference().gradient_vector_hessian_matrix(vlist, perms, L, tvlist, tperms)
+            tref = time.perf_counter() - t0
+            r2["cpu_baseline"] = {"value": 1.0 / tref, "unit": "evals/s", "cores": 1, "kind": "reference",
+                                  "sample": "one full evaluation of the reference (single-threaded C)"}
+            r2["speedup_e2e"] = tref / wall
+            r2["max_rel_diff_vs_reference"] = {"H": float(np.max(np.abs(H - Hr)) / np.max(np.abs(Hr))),
+                                               "grad": float(np.max(np.abs(g - gr)) / np.max(np.abs(gr)))}
+        else:
+            cores = os.cpu_count() or 1
+            jobs = [(L, depth, tdepth, k, k + 1) for k in range(cores)]
+            with mp.get_context("spawn").Pool(cores) as pool:
+                t0 = time.perf_counter()
+                pool.map(_ref_hessian_worker, jobs)
+                tref = time.perf_counter() - t0
+            v = (cores / N) / tref
+            r2["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "reference",
+                                  "sample": f"{cores} of {N} basis columns (one per core) through the reference's "
+                                            f"forward + backward_hessian column loop, {tref:.1f} s wall; "
+                                            f"evals/s = sampled fraction / wall time"}
+            r2["speedup_e2e"] = (1.0 / wall) / v
+    L, depth, tdepth = 8, 5, 3
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, 0, 1)
+    nref = 2
+    t0 = time.perf_counter()
+    fr, _ = Reference().optimize_brickwall_hmat(vlist, perms, L, tvlist, tperms, nref)
+    tref = time.perf_counter() - t0
+    r3["cpu_baseline"] = {"value": tref / nref, "unit": "s per iteration", "cores": 1, "kind": "reference",
+                          "sample": f"{nref} iterations of the reference driver"}
+    r3["speedup_per_iteration"] = (tref / nref) / r3["seconds_per_iteration"]
+    r3["f_iter_max_rel_diff_vs_reference"] = float(np.max(np.abs(f_iter[:nref] - fr[:nref]) / np.abs(fr[:nref])))
+    return out
+
+
 # ----------------------------------------------------------------------------- batched and serving
 
 def batched_c4(gpu, torch, count=512, niter=2):
@@ -378,6 +590,12 @@ def main():
     ap.add_argument("--no-compare", action="store_true", help="skip the complex128 comparison and the RTR runs")
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-instance batched measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
+    ap.add_argument("--no-hmat", action="store_true", help="skip the full-Hessian path measurement")
+    ap.add_argument("--hmat-case", choices=["target", "single"],
+                    help="run one full-Hessian evaluation at --L/--depth/--tdepth and exit (a small case for "
+                         "profilers): 'target' sums over all basis columns, 'single' is one state's "
+                         "forward + backward_hessian")
+    ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
     ap.add_argument("--serving-wall", type=float, default=45.0)
     a = ap.parse_args()
 
@@ -411,6 +629,22 @@ def main():
                           "scaling": "weak", "vs_baseline": None, "dtype": "c128 (f64)", "data": "synthetic (seeded)",
                           "config": config, "cpu_baseline": base,
                           "e2e": {"value": v, "unit": "evals/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+        return
+
+    if a.hmat_case:
+        from rqcopt_hpc_b200 import gpu
+        gpu.set_column_chunk(a.column_chunk)
+        vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth)
+        if a.hmat_case == "target":
+            f, g, H = gpu.brickwall_unitary_target_gradient_vector_hessian_matrix(
+                gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L)
+            print(json.dumps({"hmat_case": "target", "L": L, "depth": depth, "f": f.real, "H_norm": float(np.abs(H).max())}))
+        else:
+            rng = np.random.default_rng(16)
+            psi = (rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)) / np.sqrt(2 << L)
+            out, cache = gpu.brickwall_unitary_forward(vlist, perms, psi)
+            _, dv, hess = gpu.brickwall_unitary_backward_hessian(vlist, perms, cache, np.conj(out))
+            print(json.dumps({"hmat_case": "single", "L": L, "depth": depth, "hess_norm": float(np.abs(hess).max())}))
         return
 
     import torch
@@ -534,6 +768,9 @@ def main():
             line["serving"] = serving_c5(gpu, wall=a.serving_wall)
             # a load one GPU sustains: 2 req/s of the two smallest size classes
             line["serving_sustainable"] = serving_c5(gpu, rate=2.0, duration=10.0, wall=40.0, sizes=(8, 10))
+            gpu.set_precision(prec)
+        if not a.no_hmat and world == 1:
+            line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
             gpu.set_precision(prec)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)

@@ -520,3 +520,15 @@ class Reference:
                                                        _p(psi_out), _p(dpsi), _p(dv), _p(hess))
         assert ret == 0
         return psi_out, dpsi, dv, hess
+
+    def hessian_columns(self, vlist, perms, L, tvlist, tperms, b0, b1):
+        """Sums of f, gradients and complex Hessian over basis columns [b0, b1)."""
+        vlist, perms, tvlist, tperms = _c(vlist), _i(perms), _c(tvlist), _i(tperms)
+        nl = vlist.shape[0]
+        f = np.zeros(2)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        ret = self.lib.refdrv_hessian_columns(_p(vlist), nl, _p(perms), L, _p(tvlist), tvlist.shape[0], _p(tperms),
+                                              L_(b0), L_(b1), _p(f), _p(dv), _p(hess))
+        assert ret == 0
+        return f[0] + 1j * f[1], dv, hess

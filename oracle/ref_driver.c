@@ -214,3 +214,50 @@ int refdrv_forward_backward_hessian(const struct mat4x4* vlist, int nlayers, con
 	free(p);
 	return ret;
 }
+
+/*
+ * The basis-column loop of brickwall_unitary_target_gradient_hessian
+ * (src/target.c:733-790) restricted to columns [b0, b1), with a brickwall target,
+ * through the reference's brickwall_unitary_forward and
+ * brickwall_unitary_backward_hessian, so that a bounded sample of a large
+ * evaluation can be timed.  Outputs are the sums over the sampled columns.
+ */
+int refdrv_hessian_columns(const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                           const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                           long b0, long b1, double* fval, struct mat4x4* dvlist, numeric* hess)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	const int m = 16 * nlayers;
+	const intqs n = (intqs)1 << L;
+	struct statevector psi, upsi, wpsi;
+	allocate_statevector(L, &psi);
+	allocate_statevector(L, &upsi);
+	allocate_statevector(L, &wpsi);
+	struct quantum_circuit_cache cache;
+	int ret = allocate_quantum_circuit_cache(L, nlayers * (L / 2), &cache);
+	struct mat4x4* dv = malloc(nlayers * sizeof(struct mat4x4));
+	numeric* hu = malloc((size_t)m * m * sizeof(numeric));
+	memset(dvlist, 0, nlayers * sizeof(struct mat4x4));
+	memset(hess, 0, (size_t)m * m * sizeof(numeric));
+	numeric f = 0;
+	for (long b = b0; b < b1 && !ret; b++) {
+		memset(psi.data, 0, n * sizeof(numeric));
+		psi.data[b] = 1;
+		refdrv_brickwall_ufunc(&psi, &target, &upsi);
+		for (intqs a = 0; a < n; a++) upsi.data[a] = -conj(upsi.data[a]);
+		if ((ret = brickwall_unitary_forward(vlist, nlayers, p, &psi, &cache, &wpsi)) < 0) break;
+		for (intqs a = 0; a < n; a++) f += upsi.data[a] * wpsi.data[a];
+		if ((ret = brickwall_unitary_backward_hessian(vlist, nlayers, p, &cache, &upsi, &psi, dv, hu)) < 0) break;
+		for (int i = 0; i < nlayers; i++) add_matrix(&dvlist[i], &dv[i]);
+		for (long i = 0; i < (long)m * m; i++) hess[i] += hu[i];
+	}
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free(dv); free(hu);
+	free_quantum_circuit_cache(&cache);
+	free_statevector(&psi); free_statevector(&upsi); free_statevector(&wpsi);
+	free(p); free(tp);
+	return ret;
+}

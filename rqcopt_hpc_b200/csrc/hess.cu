@@ -190,6 +190,150 @@ k_hsweep(const double2* __restrict__ psi_in, int64_t basis_b0, double2* __restri
 	}
 }
 
+constexpr int HTILE = 4096;   // amplitudes per shared-memory tile of the layer kernel (64 KB)
+constexpr int HMAXPER = 6;    // gates per layer of the layer kernel (L <= 12)
+
+// The wire pairs of one brickwall layer (every position holds the layer gate).
+struct LayerGates
+{
+	WirePair w[HMAXPER];
+	int q0, per;
+};
+
+// One whole layer of the forward sweep with each tangent's column tiles held in
+// shared memory (L <= 12): the gates of a brickwall layer act on disjoint wires,
+// so a block loads HTILE amplitudes of a tangent (cb = HTILE / 2^L columns) once,
+// runs the layer's L/2 gates on them -- contraction with phi_q, G_q, placeholder --
+// and writes them back once; one thread per amplitude group and gate.  Block
+// (s, bx): state s as in k_hsweep, column blocks bx, bx + nbx, ...  psi_q comes
+// from the forward cache psi + q * sstride, except psi_0 of a basis-column sum
+// (basis_b0 >= 0), which is the basis column basis_b0 + c.  The tangents of
+// `layer` start at zero (they are created at its first gate).  last: the layer
+// holds the circuit's last gate (no G at that gate, no store of the tiles, f
+// summed by the psi blocks).
+__global__ void __launch_bounds__(HT, 2)
+k_hlayer(const double2* __restrict__ psi, int64_t basis_b0, const double2* __restrict__ phi, double2* __restrict__ tan,
+         Gate4<double> g, LayerGates lgts, int L, int64_t ncols, int64_t sstride, int layer, int last,
+         double* __restrict__ part, int S, double2* __restrict__ fpart)
+{
+	extern __shared__ double2 tile[];
+	__shared__ WirePair sw[HMAXPER];
+	if (threadIdx.x < lgts.per) sw[threadIdx.x] = lgts.w[threadIdx.x];
+	__syncthreads();
+	const int s = blockIdx.x, bx = blockIdx.y, nbx = gridDim.y;
+	const int t = s - 1;
+	const bool own = s > 0 && (t >> 4) == layer;
+	const int er = (t & 15) >> 2, ec = t & 3;
+	double2* __restrict__ T = s > 0 ? tan + (int64_t)t * sstride : nullptr;
+	const int lg = L - 2;
+	const int64_t gmask = ((int64_t)1 << lg) - 1;
+	const int cb = HTILE >> L;                               // columns per tile
+	const int64_t nblk = (ncols + cb - 1) / cb;
+	double acc[32];
+#pragma unroll
+	for (int k = 0; k < 32; k++) acc[k] = 0;
+	double fx = 0, fy = 0;
+	for (int64_t blk = bx; blk < nblk; blk += nbx) {
+		const int64_t col0 = blk * cb;
+		const int cbn = (int)min((int64_t)cb, ncols - col0);
+		const int n = cbn << L;                               // amplitudes of this tile
+		const int64_t gofs = col0 << L;
+		if (s > 0 && !own) {
+			for (int e = threadIdx.x; e < n; e += HT) tile[e] = T[gofs + e];
+			__syncthreads();
+		}
+		const int ngr = n >> 2;
+		for (int k = 0; k < lgts.per; k++) {
+			const int q = lgts.q0 + k;
+			const WirePair w = sw[k];
+			int64_t off[4];
+			group_offsets(w, off);
+			const bool final_gate = last && k == lgts.per - 1;
+			const double2* __restrict__ ph = phi + (int64_t)q * sstride + gofs;
+			const double2* __restrict__ ps = psi + (int64_t)q * sstride + gofs;
+			const bool zero_in = own && k == 0;
+			const bool basis = q == 0 && basis_b0 >= 0;
+			const int64_t offc = ((ec & 2) ? w.si : 0) + ((ec & 1) ? w.sj : 0);
+			for (int gi = threadIdx.x; gi < ngr; gi += HT) {
+				const int cc = gi >> lg;
+				const int64_t loc = group_base(gi & gmask, w);
+				const int64_t li = ((int64_t)cc << L) + loc;      // index within the tile
+				double2 p[4], x[4];
+#pragma unroll
+				for (int m = 0; m < 4; m++) p[m] = ph[li + off[m]];
+				if (s == 0) {
+#pragma unroll
+					for (int m = 0; m < 4; m++)
+						x[m] = basis ? make_double2(loc + off[m] == basis_b0 + col0 + cc ? 1.0 : 0.0, 0.0) : ps[li + off[m]];
+				} else if (zero_in) {
+#pragma unroll
+					for (int m = 0; m < 4; m++) x[m] = make_double2(0, 0);
+				} else {
+#pragma unroll
+					for (int m = 0; m < 4; m++) x[m] = tile[li + off[m]];
+				}
+				if (!zero_in) {
+#pragma unroll
+					for (int r = 0; r < 4; r++)
+#pragma unroll
+						for (int c = 0; c < 4; c++) {
+							acc[2 * (4 * r + c)] = fma(p[r].x, x[c].x, fma(-p[r].y, x[c].y, acc[2 * (4 * r + c)]));
+							acc[2 * (4 * r + c) + 1] = fma(p[r].x, x[c].y, fma(p[r].y, x[c].x, acc[2 * (4 * r + c) + 1]));
+						}
+				}
+				if (s == 0) {
+					if (final_gate) {
+						double2 y[4];
+						gate_apply(g, x, y);
+#pragma unroll
+						for (int m = 0; m < 4; m++) {
+							fx += p[m].x * y[m].x - p[m].y * y[m].y;
+							fy += p[m].x * y[m].y + p[m].y * y[m].x;
+						}
+					}
+				} else if (!final_gate) {
+					double2 y[4];
+					if (zero_in) {
+#pragma unroll
+						for (int m = 0; m < 4; m++) y[m] = make_double2(0, 0);
+					} else {
+						gate_apply(g, x, y);
+					}
+					if (own) {
+						const double2 v = basis ? make_double2(loc + offc == basis_b0 + col0 + cc ? 1.0 : 0.0, 0.0)
+						                        : ps[li + offc];
+						y[er].x += v.x;
+						y[er].y += v.y;
+					}
+#pragma unroll
+					for (int m = 0; m < 4; m++) tile[li + off[m]] = y[m];
+				}
+			}
+			__syncthreads();
+		}
+		if (s > 0 && !last) {
+			for (int e = threadIdx.x; e < n; e += HT) T[gofs + e] = tile[e];
+			__syncthreads();
+		}
+	}
+	const size_t slot = (size_t)layer * S + s;
+	block_add32(acc, part + slot * 32 * nbx + bx, nbx, true);
+	if (s == 0 && fpart) {
+		__shared__ double fr[2][HT / 32];
+		fx = warp_sum(fx);
+		fy = warp_sum(fy);
+		const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+		if (lane == 0) { fr[0][warp] = fx; fr[1][warp] = fy; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double sx = 0, sy = 0;
+			for (int k = 0; k < HT / 32; k++) { sx += fr[0][k]; sy += fr[1][k]; }
+			fpart[bx].x += sx;
+			fpart[bx].y += sy;
+		}
+	}
+}
+
 // Sum over the blocks of partial slot (slot, entry e)
 __device__ __forceinline__ double2 slot_sum(const double* __restrict__ part, int nbx, size_t slot, int e)
 {
@@ -234,18 +378,21 @@ __global__ void k_hassemble(const double* __restrict__ part, int nbx, int nl, in
 }
 
 // out = G in over `ngroups` groups of consecutive 2^L-amplitude states
+//   basis_b0 >= 0: `in` is the basis column basis_b0 + c of column c
 __global__ void __launch_bounds__(HT) k_happly(const double2* __restrict__ in, double2* __restrict__ out, Gate4<double> g,
-                                               WirePair w, int L, int64_t ngroups)
+                                               WirePair w, int L, int64_t ngroups, int64_t basis_b0 = -1)
 {
 	const int lg = L - 2;
 	const int64_t gmask = ((int64_t)1 << lg) - 1;
 	int64_t off[4];
 	group_offsets(w, off);
 	for (int64_t gi = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; gi < ngroups; gi += (int64_t)gridDim.x * blockDim.x) {
-		const int64_t base = ((gi >> lg) << L) + group_base(gi & gmask, w);
+		const int64_t c = gi >> lg, loc = group_base(gi & gmask, w);
+		const int64_t base = (c << L) + loc;
 		double2 x[4], y[4];
 #pragma unroll
-		for (int m = 0; m < 4; m++) x[m] = in[base + off[m]];
+		for (int m = 0; m < 4; m++)
+			x[m] = basis_b0 >= 0 ? make_double2(loc + off[m] == basis_b0 + c ? 1.0 : 0.0, 0.0) : in[base + off[m]];
 		gate_apply(g, x, y);
 #pragma unroll
 		for (int m = 0; m < 4; m++) out[base + off[m]] = y[m];
@@ -447,9 +594,10 @@ struct Sweep
 	Sweep(Runtime& r, const HessCircuit& hc) : rt(r), c(hc), L(hc.L), nl(hc.nlayers), per(hc.L / 2),
 	                                           G(hc.nlayers * (hc.L / 2)), S(1 + 16 * hc.nlayers), nbx(1) {}
 
-	int init(int64_t ngroups_per_state)
+	// blocks per state: by groups for the per-gate kernel, by column tiles for the layer kernel
+	int init(int64_t ngroups_per_state, int64_t layer_tiles = 0)
 	{
-		nbx = blocks_per_state(ngroups_per_state);
+		nbx = layer_tiles > 0 ? (int)std::min<int64_t>(HMAXBX, layer_tiles) : blocks_per_state(ngroups_per_state);
 		gg.resize(nl);
 		gt.resize(nl);
 		for (int l = 0; l < nl; l++) {
@@ -476,8 +624,8 @@ struct Sweep
 			cudaEvent_t ev;
 			launch_begin(rt, KC_APPLY, &ev);
 			k_happly<<<grid, HT, 0, rt.stream>>>(phi_at(q), phi_at(q - 1), gt[q / per], gw[q], L, ngroups);
-			launch_end(rt, KC_APPLY, ev);
-			if (int e = checked(rt)) return e;
+			launch_end(rt, KC_APPLY, ev);   // launch_begin counted the launch
+			if (int e = RQC_CUDA(cudaGetLastError())) return e;
 		}
 		if (dpsi_in) {
 			k_happly<<<grid, HT, 0, rt.stream>>>(phi_at(0), dpsi_in, gt[0], gw[0], L, ngroups);
@@ -499,7 +647,49 @@ struct Sweep
 		                                     ngroups, sstride, a, q % per == 0 ? 1 : 0, last ? 0 : 1, part, S,
 		                                     (with_f && last) ? fpart : nullptr);
 		launch_end(rt, KC_HESS, ev);
-		return checked(rt);
+		return RQC_CUDA(cudaGetLastError());
+	}
+
+	// psi_q = G_{q-1} psi_{q-1} for q = 1 .. G-1 into psi_at(q); psi_0 the basis columns from basis_b0
+	template <typename PsiAt>
+	int forward_chain(PsiAt psi_at, int64_t ngroups, int64_t basis_b0)
+	{
+		const int grid = grid_of(rt, ngroups, 8);
+		for (int q = 1; q < G; q++) {
+			cudaEvent_t ev;
+			launch_begin(rt, KC_APPLY, &ev);
+			k_happly<<<grid, HT, 0, rt.stream>>>(psi_at(q - 1), psi_at(q), gg[(q - 1) / per], gw[q - 1], L, ngroups,
+			                                     q == 1 ? basis_b0 : -1);
+			launch_end(rt, KC_APPLY, ev);
+			if (int e = RQC_CUDA(cudaGetLastError())) return e;
+		}
+		return OK;
+	}
+
+	// one layer with shared-memory tiles (L <= 12)
+	int layer(int a, const double2* psi, int64_t basis_b0, const double2* phi, double2* tan, int64_t ncols,
+	          int64_t sstride, bool with_f)
+	{
+		static bool smem_set = false;
+		if (!smem_set) {
+			if (int e = RQC_CUDA(cudaFuncSetAttribute(k_hlayer, cudaFuncAttributeMaxDynamicSharedMemorySize,
+			                                          (int)(HTILE * sizeof(double2)))))
+				return e;
+			smem_set = true;
+		}
+		LayerGates lgts;
+		lgts.q0 = a * per;
+		lgts.per = per;
+		for (int k = 0; k < per; k++) lgts.w[k] = gw[a * per + k];
+		const bool last = a == nl - 1;
+		const dim3 grid(1 + 16 * (a + 1), nbx);
+		cudaEvent_t ev;
+		launch_begin(rt, KC_HESS, &ev);
+		k_hlayer<<<grid, HT, HTILE * sizeof(double2), rt.stream>>>(psi, basis_b0, phi, tan, gg[a], lgts, L, ncols, sstride, a,
+		                                                             last ? 1 : 0, part, S,
+		                                                             (with_f && last) ? fpart : nullptr);
+		launch_end(rt, KC_HESS, ev);
+		return RQC_CUDA(cudaGetLastError());
 	}
 
 	int assemble(double2* d_rec)
@@ -521,8 +711,11 @@ int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t
 	if (L < 2 || L % 2 || nl < 1) return E_ARG;
 	const int per = L / 2, G = nl * per;
 	const int64_t N = (int64_t)1 << L;
-	// states per column: phi_q of every gate, two psi buffers, 16 tangents per layer
-	const int64_t nstates = G + 2 + 16 * (int64_t)nl;
+	// layer kernel (shared-memory tiles) up to L = 12, one kernel per gate beyond
+	const bool layered = L <= 12 && per <= HMAXPER;
+	// states per column: phi_q of every gate, psi_q of every gate (layered) or two psi
+	// buffers, 16 tangents per layer
+	const int64_t nstates = G + (layered ? G : 2) + 16 * (int64_t)nl;
 	const size_t col_bytes = (size_t)nstates * N * sizeof(double2);
 	int64_t C = (int64_t)(hess_workspace_limit(rt) / col_bytes);
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, rt.column_chunk);
@@ -538,16 +731,24 @@ int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t
 	double2* phi = reinterpret_cast<double2*>(rt.work.ptr);
 	const int64_t cs = C * N;   // elements per chunk state
 	double2* P[2] = { phi + (int64_t)G * cs, phi + (int64_t)(G + 1) * cs };
-	double2* tan = phi + (int64_t)(G + 2) * cs;
+	double2* psi = phi + (int64_t)G * cs;                              // layered: psi_q at psi + q cs
+	double2* tan = phi + (int64_t)(G + (layered ? G : 2)) * cs;
 	auto phi_at = [&](int q) { return phi + (int64_t)q * cs; };
+	auto psi_at = [&](int q) { return psi + (int64_t)q * cs; };
 
 	Sweep sw(rt, c);
-	if ((ret = sw.init(cs / 4))) return ret;
+	if ((ret = sw.init(cs / 4, layered ? (C + (HTILE >> L) - 1) / (HTILE >> L) : 0))) return ret;
 	for (int64_t b0 = 0; b0 < N; b0 += C) {
 		const int64_t Cc = std::min(C, N - b0);
 		const int64_t ngroups = Cc * (N / 4);
 		if ((ret = target_columns_device(rt, t, L, b0, Cc, phi_at(G - 1), P[0], P[1]))) return ret;
 		if ((ret = sw.reverse_chain(phi_at, ngroups, nullptr))) return ret;
+		if (layered) {
+			if ((ret = sw.forward_chain(psi_at, ngroups, b0))) return ret;
+			for (int a = 0; a < nl; a++)
+				if ((ret = sw.layer(a, psi, b0, phi, tan, Cc, cs, true))) return ret;
+			continue;
+		}
 		for (int q = 0; q < G; q++) {
 			const double2* in = q == 0 ? nullptr : P[(q - 1) & 1];
 			if ((ret = sw.gate(q, in, q == 0 ? b0 : -1, P[q & 1], phi_at(q), tan, ngroups, cs, true))) return ret;
@@ -563,18 +764,26 @@ int hessian_single_device(Runtime& rt, const HessCircuit& c, const double2* d_ca
 	if (L < 2 || L % 2 || nl < 1) return E_ARG;
 	const int per = L / 2, G = nl * per;
 	const int64_t N = (int64_t)1 << L;
-	// phi_0 .. phi_{G-2} (phi_{G-1} is d_dout) and 16 tangents per layer
-	const int64_t nstates = (G - 1) + 16 * (int64_t)nl;
+	const bool layered = L <= 12 && per <= HMAXPER;
+	// phi_0 .. phi_{G-1} (the last a copy of d_dout) and 16 tangents per layer
+	const int64_t nstates = G + 16 * (int64_t)nl;
 	int ret = ensure_device(rt.work, (size_t)nstates * N * sizeof(double2));
 	if (ret) return ret;
 	double2* phi = reinterpret_cast<double2*>(rt.work.ptr);
-	double2* tan = phi + (int64_t)(G - 1) * N;
-	auto phi_at = [&](int q) { return q == G - 1 ? const_cast<double2*>(d_dout) : phi + (int64_t)q * N; };
+	double2* tan = phi + (int64_t)G * N;
+	auto phi_at = [&](int q) { return phi + (int64_t)q * N; };
+	if ((ret = RQC_CUDA(cudaMemcpyAsync(phi_at(G - 1), d_dout, N * sizeof(double2), cudaMemcpyDeviceToDevice, rt.stream))))
+		return ret;
 	Sweep sw(rt, c);
-	if ((ret = sw.init(N / 4))) return ret;
+	if ((ret = sw.init(N / 4, layered ? 1 : 0))) return ret;
 	if ((ret = sw.reverse_chain(phi_at, N / 4, d_dpsi))) return ret;
-	for (int q = 0; q < G; q++)
-		if ((ret = sw.gate(q, d_cache + (int64_t)q * N, -1, nullptr, phi_at(q), tan, N / 4, N, false))) return ret;
+	if (layered) {
+		for (int a = 0; a < nl; a++)
+			if ((ret = sw.layer(a, d_cache, -1, phi, tan, 1, N, false))) return ret;
+	} else {
+		for (int q = 0; q < G; q++)
+			if ((ret = sw.gate(q, d_cache + (int64_t)q * N, -1, nullptr, phi_at(q), tan, N / 4, N, false))) return ret;
+	}
 	return sw.assemble(d_rec);
 }
 

@@ -258,11 +258,11 @@ def apply_brickwall_unitary(vlist, perms, psi):
     return out
 
 
-def brickwall_unitary_forward(vlist, perms, psi):
+def brickwall_unitary_forward(vlist, perms, psi, cache=None):
     vlist, psi = cplx(vlist), cplx(psi)
     L = _nq(psi)
     pp, keep = perm_pointers(perms)
-    cache = Cache(L, vlist.shape[0] * (L // 2))
+    cache = cache or Cache(L, vlist.shape[0] * (L // 2))
     out = np.empty_like(psi)
     _check("brickwall_unitary_forward", lib().brickwall_unitary_forward(ptr(vlist), vlist.shape[0], C.cast(pp, VP),
                                                                        C.byref(_sv(psi, L)), C.byref(cache.c),
