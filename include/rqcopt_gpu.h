@@ -38,6 +38,7 @@ typedef double complex numeric;
 #endif
 
 #include <stddef.h>
+#include <stdint.h>
 
 /* src/config.h:62 */
 typedef long int intqs;
@@ -63,6 +64,25 @@ struct statevector_array
 	int nstates;
 };
 
+/* src/pcg_basic.h:32-36 -- the PCG32 generator (state, stream) */
+struct pcg32_random
+{
+	uint64_t state;
+	uint64_t inc;
+};
+
+/* src/pcg_basic.h:50-53 */
+struct pcg32x2_random
+{
+	struct pcg32_random gen[2];
+};
+
+/* src/rng.h:15-18 */
+struct rng_state
+{
+	struct pcg32x2_random pcgstate;
+};
+
 /* src/quantum_circuit.h:16-21 */
 struct quantum_circuit_cache
 {
@@ -82,6 +102,10 @@ int allocate_statevector(int nqubits, struct statevector* psi);
 void free_statevector(struct statevector* psi);
 /* src/statevector.h:32 */
 void add_statevectors(const struct statevector* psi1, const struct statevector* psi2, struct statevector* psi_sum);
+/* src/rng.h:21 */
+void seed_rng_state(const uint64_t seed, struct rng_state* state);
+/* src/statevector.h:29 -- generated on the GPU; advances rng exactly as the reference does */
+void haar_random_statevector(struct statevector* psi, struct rng_state* rng);
 /* src/statevector.h:47 -- returns CUDA managed memory */
 int allocate_statevector_array(int nqubits, int nstates, struct statevector_array* psi_list);
 /* src/statevector.h:49 */
@@ -147,6 +171,11 @@ int apply_brickwall_unitary_gate_placeholder(const struct mat4x4 vlist[], int nl
 int circuit_unitary_target(linear_func ufunc, void* udata,
 	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
 	numeric* fval);
+/* src/target.h:14-17 -- Haar-random sample states drawn on the GPU from rng's stream */
+int circuit_unitary_target_sampling(linear_func ufunc, void* udata,
+	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
+	const long nsamples, struct rng_state* rng,
+	numeric* fval);
 /* src/target.h:20-22 */
 int circuit_unitary_target_and_gradient(linear_func ufunc, void* udata,
 	const struct mat4x4 gates[], const int ngates, const int wires[], const int nqubits,
@@ -166,6 +195,11 @@ int circuit_unitary_target_projected_hessian_vector_product(linear_func ufunc, v
 /* src/target.h:42-44 */
 int brickwall_unitary_target(linear_func ufunc, void* udata,
 	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval);
+/* src/target.h:46-49 */
+int brickwall_unitary_target_sampling(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	const long nsamples, struct rng_state* rng,
 	numeric* fval);
 /* src/target.h:52-54 */
 int brickwall_unitary_target_and_gradient(linear_func ufunc, void* udata,
@@ -191,6 +225,16 @@ int brickwall_unitary_target_gradient_hessian(linear_func ufunc, void* udata,
 /* src/target.h:81-83 -- real symmetric (16 nlayers)^2 Riemannian Hessian H */
 int brickwall_unitary_target_gradient_vector_hessian_matrix(linear_func ufunc, void* udata,
 	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	numeric* fval, double* grad_vec, double* H);
+/* src/target.h:74-77 */
+int brickwall_unitary_target_gradient_hessian_sampling(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	const long nsamples, struct rng_state* rng,
+	numeric* fval, struct mat4x4 dvlist[], numeric* hess);
+/* src/target.h:85-88 */
+int brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	const long nsamples, struct rng_state* rng,
 	numeric* fval, double* grad_vec, double* H);
 
 /* ------------------------------------------------------------------ trust_region.h */
@@ -270,6 +314,11 @@ void optimize_brickwall_circuit_hvp(linear_func ufunc, void* udata,
 /* src/brickwall_opt.h:15-17 -- complex128 regardless of rqcopt_gpu_set_precision */
 void optimize_brickwall_circuit_hmat(linear_func ufunc, void* udata,
 	const struct mat4x4 vlist_start[], const int nlayers, const int nqubits, const int* perms[],
+	struct rtr_params* params, const int niter, double* f_iter, struct mat4x4 vlist_opt[]);
+/* src/brickwall_opt.h:19-22 */
+void optimize_brickwall_circuit_hmat_sampling(linear_func ufunc, void* udata,
+	const struct mat4x4 vlist_start[], const int nlayers, const int nqubits, const int* perms[],
+	const long nsamples, struct rng_state* rng,
 	struct rtr_params* params, const int niter, double* f_iter, struct mat4x4 vlist_opt[]);
 /* src/circuit_opt.h:8 */
 void optimize_quantum_circuit(linear_func ufunc, void* udata, const struct mat4x4 gates_start[], const int ngates,

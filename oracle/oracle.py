@@ -32,6 +32,18 @@ class RtrParams(C.Structure):
     _fields_ = [("tcg", TcgParams), ("rho_trust", C.c_double), ("radius_init", C.c_double), ("maxradius", C.c_double)]
 
 
+class Pcg32(C.Structure):
+    _fields_ = [("state", C.c_uint64), ("inc", C.c_uint64)]
+
+
+class RngState(C.Structure):
+    """struct rng_state (src/rng.h:15-18): two PCG32 generators."""
+    _fields_ = [("gen", Pcg32 * 2)]
+
+    def tuple(self):
+        return tuple((g.state, g.inc) for g in self.gen)
+
+
 class BrickwallUdata(C.Structure):
     _fields_ = [("vlist", C.c_void_p), ("nlayers", C.c_int), ("perms", C.c_void_p)]
 
@@ -421,6 +433,68 @@ class Oracle:
         return f_iter, vopt, acc, bnd
 
 
+    # sampling estimator
+    def seed_rng_state(self, seed):
+        r = RngState()
+        self.lib.orc_seed_rng(C.c_uint64(seed), C.byref(r))
+        return r
+
+    def haar_random_statevector(self, L, rng):
+        out = np.empty(1 << L, np.complex128)
+        self.lib.orc_haar_statevector(C.byref(SV(out.ctypes.data, L)), C.byref(rng))
+        return out
+
+    def brickwall_unitary_target_sampling(self, tgt, vlist, perms, L, nsamples, rng):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1, np.complex128)
+        ret = self.lib.orc_brickwall_target_sampling(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L, _p(perms),
+                                                     L_(nsamples), C.byref(rng), _p(f))
+        assert ret == 0
+        return f[0]
+
+    def circuit_unitary_target_sampling(self, tgt, gates, wires, L, nsamples, rng):
+        gates, wires = _c(gates), _i(wires)
+        f = np.zeros(1, np.complex128)
+        ret = self.lib.orc_circuit_target_sampling(tgt.ufunc, tgt.udata, _p(gates), gates.shape[0], _p(wires), L,
+                                                   L_(nsamples), C.byref(rng), _p(f))
+        assert ret == 0
+        return f[0]
+
+    def brickwall_unitary_target_gradient_hessian_sampling(self, tgt, vlist, perms, L, nsamples, rng):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1, np.complex128)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        hess = np.empty((16 * nl, 16 * nl), np.complex128)
+        ret = self.lib.orc_brickwall_target_gradient_hessian_sampling(tgt.ufunc, tgt.udata, _p(vlist), nl, L,
+                                                                      _p(perms), L_(nsamples), C.byref(rng), _p(f),
+                                                                      _p(dv), _p(hess))
+        assert ret == 0
+        return f[0], dv, hess
+
+    def brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(self, tgt, vlist, perms, L, nsamples, rng):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1, np.complex128)
+        g = np.empty(16 * nl)
+        H = np.empty((16 * nl, 16 * nl))
+        ret = self.lib.orc_brickwall_target_gradient_vector_hessian_matrix_sampling(
+            tgt.ufunc, tgt.udata, _p(vlist), nl, L, _p(perms), L_(nsamples), C.byref(rng), _p(f), _p(g), _p(H))
+        assert ret == 0
+        return f[0], g, H
+
+    def optimize_brickwall_circuit_hmat_sampling(self, tgt, vstart, perms, L, nsamples, rng, niter):
+        vstart, perms = _c(vstart), _i(perms)
+        nl = vstart.shape[0]
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        params = default_rtr(16 * nl)
+        self.lib.orc_optimize_brickwall_hmat_sampling(tgt.ufunc, tgt.udata, _p(vstart), nl, L, _p(perms),
+                                                      L_(nsamples), C.byref(rng), C.byref(params), niter,
+                                                      _p(f_iter), _p(vopt), None, None)
+        return f_iter, vopt
+
+
 class Reference:
     """The reference's own C sources compiled in _ref/ (built only where the sources exist)."""
 
@@ -532,3 +606,47 @@ class Reference:
                                               L_(b0), L_(b1), _p(f), _p(dv), _p(hess))
         assert ret == 0
         return f[0] + 1j * f[1], dv, hess
+
+
+    # sampling estimator of the reference
+    def seed_rng_state(self, seed):
+        r = RngState()
+        self.lib.seed_rng_state(C.c_uint64(seed), C.byref(r))
+        return r
+
+    def haar_random_statevector(self, L, rng):
+        out = np.empty(1 << L, np.complex128)
+        self.lib.haar_random_statevector(C.byref(SV(out.ctypes.data, L)), C.byref(rng))
+        return out
+
+    def sampling(self, mode, vlist, perms, L, target, nsamples, rng):
+        """mode 0: f; 1: f, dvlist, complex hess; 2: f, grad_vec, H.  target: (tvlist, tperms)
+        for a brickwall target or a dense matrix."""
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        if isinstance(target, tuple):
+            tv, tp, td = _c(target[0]), _i(target[1]), None
+        else:
+            tv, tp, td = None, None, _c(target)
+        f = np.zeros(2)
+        o1 = o2 = None
+        if mode == 1:
+            o1, o2 = np.empty((nl, 4, 4), np.complex128), np.empty((16 * nl, 16 * nl), np.complex128)
+        elif mode == 2:
+            o1, o2 = np.empty(16 * nl), np.empty((16 * nl, 16 * nl))
+        ret = self.lib.refdrv_sampling(mode, _p(vlist), nl, _p(perms), L, _p(tv) if tv is not None else None,
+                                       tv.shape[0] if tv is not None else 0, _p(tp) if tp is not None else None,
+                                       _p(td) if td is not None else None, L_(nsamples), C.byref(rng), _p(f),
+                                       _p(o1) if o1 is not None else None, _p(o2) if o2 is not None else None)
+        assert ret == 0
+        fc = f[0] + 1j * f[1]
+        return fc if mode == 0 else (fc, o1, o2)
+
+    def optimize_brickwall_hmat_sampling(self, vstart, perms, L, tvlist, tperms, nsamples, rng, niter):
+        vstart, perms, tvlist, tperms = _c(vstart), _i(perms), _c(tvlist), _i(tperms)
+        f_iter = np.empty(niter + 1)
+        vopt = np.empty_like(vstart)
+        self.lib.refdrv_optimize_brickwall_hmat_sampling(_p(vstart), vstart.shape[0], L, _p(perms), _p(tvlist),
+                                                         tvlist.shape[0], _p(tperms), L_(nsamples), C.byref(rng),
+                                                         niter, _p(f_iter), _p(vopt))
+        return f_iter, vopt

@@ -20,6 +20,7 @@
 #include "trust_region.h"
 #include "brickwall_opt.h"
 #include "circuit_opt.h"
+#include "rng.h"
 
 struct refdrv_brickwall
 {
@@ -260,4 +261,56 @@ int refdrv_hessian_columns(const struct mat4x4* vlist, int nlayers, const int* p
 	free_statevector(&psi); free_statevector(&upsi); free_statevector(&wpsi);
 	free(p); free(tp);
 	return ret;
+}
+
+/* dense row-major target matrix U as a linear_func (udata: the 2^L x 2^L matrix) */
+int refdrv_dense_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out)
+{
+	const numeric* u = udata;
+	const intqs n = (intqs)1 << psi->nqubits;
+	for (intqs r = 0; r < n; r++) {
+		numeric s = 0;
+		for (intqs c = 0; c < n; c++) s += u[r*n + c] * psi->data[c];
+		psi_out->data[r] = s;
+	}
+	return 0;
+}
+
+/* sampling estimator with a brickwall target (tvlist, tperms) or, if tvlist is NULL,
+ * the dense target matrix tdense: f only (mode 0), f + gradients + complex Hessian
+ * (mode 1) or f + gradient vector + real Hessian (mode 2) */
+int refdrv_sampling(int mode, const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                    const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat, const numeric* tdense,
+                    long nsamples, struct rng_state* rng, double* fval, void* out1, void* out2)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = tvlist ? perm_ptrs(tperms_flat, tnlayers, L) : NULL;
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	linear_func uf = tvlist ? refdrv_brickwall_ufunc : refdrv_dense_ufunc;
+	void* ud = tvlist ? (void*)&target : (void*)tdense;
+	numeric f = 0;
+	int ret;
+	if (mode == 0) ret = brickwall_unitary_target_sampling(uf, ud, vlist, nlayers, L, p, nsamples, rng, &f);
+	else if (mode == 1) ret = brickwall_unitary_target_gradient_hessian_sampling(uf, ud, vlist, nlayers, L, p, nsamples, rng, &f, out1, out2);
+	else ret = brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(uf, ud, vlist, nlayers, L, p, nsamples, rng, &f, out1, out2);
+	fval[0] = creal(f);
+	fval[1] = cimag(f);
+	free(p); free(tp);
+	return ret;
+}
+
+/* the sampling full-Hessian driver with default RTR parameters */
+void refdrv_optimize_brickwall_hmat_sampling(const struct mat4x4* vstart, int nlayers, int L, const int* perms_flat,
+                                             const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
+                                             long nsamples, struct rng_state* rng, int niter, double* f_iter,
+                                             struct mat4x4* vopt)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** tp = perm_ptrs(tperms_flat, tnlayers, L);
+	struct refdrv_brickwall target = { tvlist, tnlayers, tp };
+	struct rtr_params params;
+	set_rtr_default_params(nlayers * num_tangent_params, &params);
+	optimize_brickwall_circuit_hmat_sampling(refdrv_brickwall_ufunc, &target, vstart, nlayers, L, p, nsamples, rng,
+		&params, niter, f_iter, vopt);
+	free(p); free(tp);
 }

@@ -1182,3 +1182,207 @@ void orc_optimize_brickwall_hmat(orc_linear_func uf, void* ud, const orc_mat4* v
 	orc_rtr_optimize_hmat(glue_f, glue_fdh, &g, glue_retract, &k, 16 * nlayers, (const double*)vstart,
 	                      32 * nlayers, params, niter, f_iter, (double*)vopt, accepted, on_boundary);
 }
+
+/* ------------------------------------------------------------ sampling estimator */
+
+/* PCG32 (O'Neill 2014, the XSH-RR output of a 64-bit LCG; the reference vendors it as
+ * src/pcg_basic.c): one step, returning the output of the old state */
+static uint32_t pcg32_step(orc_pcg32* g)
+{
+	const uint64_t old = g->state;
+	g->state = old * 6364136223846793005ULL + g->inc;
+	const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+	const uint32_t rot = (uint32_t)(old >> 59u);
+	return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+
+/* src/pcg_basic.c:31-38 */
+static void pcg32_seed(orc_pcg32* g, uint64_t initstate, uint64_t initseq)
+{
+	g->state = 0;
+	g->inc = (initseq << 1u) | 1u;
+	pcg32_step(g);
+	g->state += initstate;
+	pcg32_step(g);
+}
+
+/* src/rng.c:13-25 with src/pcg_basic.c:112-121 */
+void orc_seed_rng(uint64_t seed, orc_rng* rng)
+{
+	orc_pcg32 s;
+	pcg32_seed(&s, seed, 6364136223846793005ULL * seed + 1442695040888963407ULL);
+	uint64_t v[4];
+	for (int k = 0; k < 4; k++) {
+		const uint64_t hi = pcg32_step(&s);
+		v[k] = (hi << 32) | pcg32_step(&s);
+	}
+	uint64_t seq2 = v[3];
+	const uint64_t mask = ~0ull >> 1;
+	if ((v[2] & mask) == (seq2 & mask)) seq2 = ~seq2;
+	pcg32_seed(&rng->gen[0], v[0], v[2]);
+	pcg32_seed(&rng->gen[1], v[1], seq2);
+}
+
+/* src/pcg_basic.c:128-132 */
+static uint64_t rng_u64(orc_rng* rng)
+{
+	const uint64_t hi = pcg32_step(&rng->gen[0]);
+	return (hi << 32) | pcg32_step(&rng->gen[1]);
+}
+
+/* src/rng.c:100-123, 146-157: Box-Muller normals, complex normal / sqrt(2) */
+static double rng_randn(orc_rng* rng)
+{
+	double u1 = ldexp((double)rng_u64(rng), -64);
+	const double u2 = ldexp((double)rng_u64(rng), -64);
+	if (u1 == 0) u1 = 1;
+	return sqrt(-2 * log(u1)) * sin(6.2831853071795864769 * u2);
+}
+
+static orc_cplx rng_crandn(orc_rng* rng)
+{
+	const double x = rng_randn(rng);
+	const double y = rng_randn(rng);
+	return x / sqrt(2.0) + I * (y / sqrt(2.0));
+}
+
+/* src/statevector.c:47-66, 102-125 */
+void orc_haar_statevector(orc_sv* psi, orc_rng* rng)
+{
+	const long n = 1L << psi->nqubits;
+	for (long j = 0; j < n; j++) psi->data[j] = rng_crandn(rng);
+	double s = 0;
+	for (long j = 0; j < n; j++) s += creal(psi->data[j]) * creal(psi->data[j]) + cimag(psi->data[j]) * cimag(psi->data[j]);
+	const double nrm = sqrt(s);
+	if (nrm > 0) {
+		const double a = 1. / nrm;
+		for (long j = 0; j < n; j++) psi->data[j] *= a;
+	}
+}
+
+/* src/target.c:85-149 */
+int orc_circuit_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates, const int* wires,
+                                int L, long nsamples, orc_rng* rng, orc_cplx* fval)
+{
+	const long n = 1L << L;
+	orc_sv psi = { sv_alloc(L), L }, upsi = { sv_alloc(L), L }, cpsi = { sv_alloc(L), L };
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = 0; b < nsamples && !ret; b++) {
+		orc_haar_statevector(&psi, rng);
+		if (uf(&psi, ud, &upsi) < 0) { ret = -2; break; }
+		for (long a = 0; a < n; a++) upsi.data[a] = -conj(upsi.data[a]);
+		orc_apply_circuit(gates, ngates, wires, &psi, &cpsi);
+		for (long a = 0; a < n; a++) f += upsi.data[a] * cpsi.data[a];
+	}
+	*fval = f * ((double)n / nsamples);
+	free(psi.data); free(upsi.data); free(cpsi.data);
+	return ret;
+}
+
+/* src/target.c:491-505 */
+int orc_brickwall_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int L,
+                                  const int* perms, long nsamples, orc_rng* rng, orc_cplx* fval)
+{
+	const int G = nlayers * (L / 2);
+	orc_mat4* gates = (orc_mat4*)malloc(G * sizeof(orc_mat4));
+	int* wires = (int*)malloc(2 * G * sizeof(int));
+	brickwall_expand(L, nlayers, vlist, perms, gates, wires);
+	int ret = orc_circuit_target_sampling(uf, ud, gates, G, wires, L, nsamples, rng, fval);
+	free(gates); free(wires);
+	return ret;
+}
+
+/* src/target.c:807-928 */
+int orc_brickwall_target_gradient_hessian_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                                   int L, const int* perms, long nsamples, orc_rng* rng,
+                                                   orc_cplx* fval, orc_mat4* dvlist, orc_cplx* hess)
+{
+	const int per = L / 2, G = nlayers * per, m = 16 * nlayers;
+	const long N = 1L << L;
+	orc_sv psi = { sv_alloc(L), L }, upsi = { sv_alloc(L), L }, wpsi = { sv_alloc(L), L };
+	orc_sv* cache = (orc_sv*)malloc(G * sizeof(orc_sv));
+	for (int k = 0; k < G; k++) { cache[k].data = sv_alloc(L); cache[k].nqubits = L; }
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* hu = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	for (int l = 0; l < nlayers; l++) memset(&dvlist[l], 0, sizeof(orc_mat4));
+	memset(hess, 0, (size_t)m * m * sizeof(orc_cplx));
+	orc_cplx f = 0;
+	int ret = 0;
+	for (long b = 0; b < nsamples && !ret; b++) {
+		orc_haar_statevector(&psi, rng);
+		if (uf(&psi, ud, &upsi) < 0) { ret = -2; break; }
+		for (long a = 0; a < N; a++) upsi.data[a] = -conj(upsi.data[a]);
+		orc_brickwall_forward(vlist, nlayers, perms, &psi, cache, &wpsi);
+		for (long a = 0; a < N; a++) f += upsi.data[a] * wpsi.data[a];
+		orc_brickwall_backward_hessian(vlist, nlayers, perms, cache, &upsi, &psi, dv, hu);
+		for (int l = 0; l < nlayers; l++)
+			for (int e = 0; e < 16; e++) dvlist[l].data[e] += dv[l].data[e];
+		for (long e = 0; e < (long)m * m; e++) hess[e] += hu[e];
+	}
+	const double scale = (double)N / nsamples;
+	*fval = f * scale;
+	for (int l = 0; l < nlayers; l++)
+		for (int e = 0; e < 16; e++) dvlist[l].data[e] *= scale;
+	for (long e = 0; e < (long)m * m; e++) hess[e] *= scale;
+	for (int k = 0; k < G; k++) free(cache[k].data);
+	free(cache); free(dv); free(hu);
+	free(psi.data); free(upsi.data); free(wpsi.data);
+	return ret;
+}
+
+/* src/target.c:1050-1088 */
+int orc_brickwall_target_gradient_vector_hessian_matrix_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist,
+                                                                 int nlayers, int L, const int* perms, long nsamples,
+                                                                 orc_rng* rng, orc_cplx* fval, double* grad_vec,
+                                                                 double* H)
+{
+	const int m = 16 * nlayers;
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* hess = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	int ret = orc_brickwall_target_gradient_hessian_sampling(uf, ud, vlist, nlayers, L, perms, nsamples, rng, fval, dv,
+	                                                         hess);
+	if (!ret) {
+		for (int l = 0; l < nlayers; l++) {
+			for (int e = 0; e < 16; e++) dv[l].data[e] = conj(dv[l].data[e]);
+			orc_tangent_to_real(&vlist[l], &dv[l], &grad_vec[16*l]);
+		}
+		project_hessian_matrix(nlayers, vlist, dv, hess, H);
+	}
+	free(dv); free(hess);
+	return ret;
+}
+
+typedef struct { glue g; long nsamples; orc_rng* rng; } glue_sampling;
+
+/* src/brickwall_opt.c:205-217 */
+static double glue_f_sampling(const double* x, void* fd)
+{
+	const glue_sampling* s = (const glue_sampling*)fd;
+	orc_cplx f;
+	int ret = orc_brickwall_target_sampling(s->g.uf, s->g.ud, (const orc_mat4*)x, s->g.ngates_or_layers, s->g.L,
+	                                        s->g.perms_or_wires, s->nsamples, s->rng, &f);
+	return ret < 0 ? -1 : creal(f);
+}
+
+/* src/brickwall_opt.c:224-236 */
+static double glue_fdh_sampling(const double* x, void* fd, double* grad, double* hess)
+{
+	const glue_sampling* s = (const glue_sampling*)fd;
+	orc_cplx f;
+	int ret = orc_brickwall_target_gradient_vector_hessian_matrix_sampling(s->g.uf, s->g.ud, (const orc_mat4*)x,
+		s->g.ngates_or_layers, s->g.L, s->g.perms_or_wires, s->nsamples, s->rng, &f, grad, hess);
+	return ret < 0 ? -1 : creal(f);
+}
+
+/* src/brickwall_opt.c:244-265 */
+void orc_optimize_brickwall_hmat_sampling(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int L,
+                                          const int* perms, long nsamples, orc_rng* rng, const orc_rtr_params* params,
+                                          int niter, double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary)
+{
+	glue_sampling s = { { uf, ud, perms, nlayers, L, 1 }, nsamples, rng };
+	int k = nlayers;
+	orc_rtr_optimize_hmat(glue_f_sampling, glue_fdh_sampling, &s, glue_retract, &k, 16 * nlayers,
+	                      (const double*)vstart, 32 * nlayers, params, niter, f_iter, (double*)vopt, accepted,
+	                      on_boundary);
+}

@@ -16,6 +16,7 @@
 
 #include <complex.h>
 #include <stdbool.h>
+#include <stdint.h>
 
 typedef double complex orc_cplx;
 
@@ -139,6 +140,29 @@ void orc_rtr_optimize_hmat(orc_target_func f, orc_target_grad_hess_func f_deriv_
 void orc_optimize_brickwall_hmat(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers, int nqubits,
                                  const int* perms, const orc_rtr_params* params, int niter,
                                  double* f_iter, orc_mat4* vopt, int* accepted, int* on_boundary);
+
+/* ---- sampling estimator (src/rng.c, src/pcg_basic.c, src/statevector.c:102-125,
+ *      src/target.c:85-149, 491-505, 807-928, 1050-1088, src/brickwall_opt.c:189-267) ----
+ * Layout-identical to the reference's struct pcg32_random / struct rng_state. */
+typedef struct { uint64_t state, inc; } orc_pcg32;
+typedef struct { orc_pcg32 gen[2]; } orc_rng;
+void orc_seed_rng(uint64_t seed, orc_rng* rng);
+void orc_haar_statevector(orc_sv* psi, orc_rng* rng);
+int  orc_circuit_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates, const int* wires,
+                                 int nqubits, long nsamples, orc_rng* rng, orc_cplx* fval);
+int  orc_brickwall_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int nqubits,
+                                   const int* perms, long nsamples, orc_rng* rng, orc_cplx* fval);
+int  orc_brickwall_target_gradient_hessian_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers,
+                                                    int nqubits, const int* perms, long nsamples, orc_rng* rng,
+                                                    orc_cplx* fval, orc_mat4* dvlist, orc_cplx* hess);
+int  orc_brickwall_target_gradient_vector_hessian_matrix_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist,
+                                                                  int nlayers, int nqubits, const int* perms,
+                                                                  long nsamples, orc_rng* rng, orc_cplx* fval,
+                                                                  double* grad_vec, double* H);
+void orc_optimize_brickwall_hmat_sampling(orc_linear_func uf, void* ud, const orc_mat4* vstart, int nlayers,
+                                          int nqubits, const int* perms, long nsamples, orc_rng* rng,
+                                          const orc_rtr_params* params, int niter, double* f_iter, orc_mat4* vopt,
+                                          int* accepted, int* on_boundary);
 
 /* ---- targets used by tests and benchmarks ---- */
 /* matrix-free brickwall target U: udata points to orc_brickwall_udata */

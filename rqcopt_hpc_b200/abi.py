@@ -21,6 +21,19 @@ class StatevectorArray(C.Structure):
     _fields_ = [("data", C.c_void_p), ("nqubits", C.c_int), ("nstates", C.c_int)]
 
 
+class Pcg32(C.Structure):
+    """struct pcg32_random: one PCG32 generator (state, stream)."""
+    _fields_ = [("state", C.c_uint64), ("inc", C.c_uint64)]
+
+
+class RngState(C.Structure):
+    """struct rng_state: the two PCG32 generators of the reference's rng_state."""
+    _fields_ = [("gen", Pcg32 * 2)]
+
+    def tuple(self):
+        return tuple((g.state, g.inc) for g in self.gen)
+
+
 class QuantumCircuitCache(C.Structure):
     _fields_ = [("psi_list", C.POINTER(Statevector)), ("nqubits", C.c_int), ("ngates", C.c_int)]
 

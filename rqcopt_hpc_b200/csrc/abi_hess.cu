@@ -1,8 +1,10 @@
 // Exported functions of the full-Hessian path with the reference's signatures:
 // statevector arrays (src/statevector.h:39-49), the array gate kernels
 // (src/gate.h:13-19), the brickwall backward pass with Hessian and the gate
-// placeholder circuit (src/brickwall_circuit.h:17-22) and the Hessian targets
-// (src/target.h:70-83).  Host buffers are staged through HBM; every call
+// placeholder circuit (src/brickwall_circuit.h:17-22), the Hessian targets
+// (src/target.h:70-83) and the random-state sampling estimators with their
+// generator (src/target.h:14-17, 46-49, 74-77, 85-88; src/rng.h:21;
+// src/statevector.h:29).  Host buffers are staged through HBM; every call
 // synchronises before returning.
 #include <stdio.h>
 #include <string.h>
@@ -11,6 +13,7 @@
 #include "hess.h"
 #include "rqc_runtime.h"
 #include "rqcopt_gpu.h"
+#include "sampling.h"
 #include "target_problem.h"
 
 using namespace rqc;
@@ -255,7 +258,7 @@ namespace {
 
 int hessian_target(const char* fn, linear_func ufunc, void* udata, const struct mat4x4 vlist[], int nlayers,
                    int nqubits, const int* perms[], numeric* fval, struct mat4x4* dvlist, numeric* hess,
-                   double* grad_vec, double* H)
+                   double* grad_vec, double* H, const SampleSpec* samp = nullptr)
 {
 	Runtime* rt = runtime();
 	if (!rt) return E_CUDA;
@@ -278,7 +281,7 @@ int hessian_target(const char* fn, linear_func ufunc, void* udata, const struct 
 	c.nlayers = nlayers;
 	c.ugates = ug.data();
 	c.wires = wires.data();
-	if ((ret = hessian_target_device(*rt, c, th.spec, rec))) return ret;
+	if ((ret = hessian_target_device(*rt, c, th.spec, rec, samp))) return ret;
 	if (H) {
 		if ((ret = RQC_CUDA(cudaMemcpyAsync(d_ug, ug.data(), 16 * (size_t)nlayers * sizeof(double2), cudaMemcpyHostToDevice,
 		                                    rt->stream))))
@@ -313,4 +316,143 @@ extern "C" int brickwall_unitary_target_gradient_vector_hessian_matrix(linear_fu
 	if (!fval || !grad_vec || !H) return fail("brickwall_unitary_target_gradient_vector_hessian_matrix", E_ARG);
 	return hessian_target("brickwall_unitary_target_gradient_vector_hessian_matrix", ufunc, udata, vlist, nlayers,
 	                      nqubits, perms, fval, nullptr, nullptr, grad_vec, H);
+}
+
+extern "C" int brickwall_unitary_target_gradient_hessian_sampling(linear_func ufunc, void* udata,
+                                                                  const struct mat4x4 vlist[], const int nlayers,
+                                                                  const int nqubits, const int* perms[],
+                                                                  const long nsamples, struct rng_state* rng,
+                                                                  numeric* fval, struct mat4x4 dvlist[], numeric* hess)
+{
+	const char* fn = "brickwall_unitary_target_gradient_hessian_sampling";
+	if (!fval || !dvlist || !hess || !rng || nsamples < 1) return fail(fn, E_ARG);
+	const SampleSpec sp = sample_spec(rng, nsamples);
+	const int ret = hessian_target(fn, ufunc, udata, vlist, nlayers, nqubits, perms, fval, dvlist, hess, nullptr,
+	                               nullptr, &sp);
+	if (!ret) advance_rng(rng, nsamples, nqubits);
+	return ret;
+}
+
+extern "C" int brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(linear_func ufunc, void* udata,
+                                                                                const struct mat4x4 vlist[],
+                                                                                const int nlayers, const int nqubits,
+                                                                                const int* perms[], const long nsamples,
+                                                                                struct rng_state* rng, numeric* fval,
+                                                                                double* grad_vec, double* H)
+{
+	const char* fn = "brickwall_unitary_target_gradient_vector_hessian_matrix_sampling";
+	if (!fval || !grad_vec || !H || !rng || nsamples < 1) return fail(fn, E_ARG);
+	const SampleSpec sp = sample_spec(rng, nsamples);
+	const int ret = hessian_target(fn, ufunc, udata, vlist, nlayers, nqubits, perms, fval, nullptr, nullptr, grad_vec, H,
+	                               &sp);
+	if (!ret) advance_rng(rng, nsamples, nqubits);
+	return ret;
+}
+
+// ------------------------------------------------------------------ generator and sampled target values
+
+namespace {
+
+uint32_t pcg32_next(struct pcg32_random* g)
+{
+	const uint64_t old = g->state;
+	g->state = old * 6364136223846793005ULL + g->inc;
+	const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+	const uint32_t rot = (uint32_t)(old >> 59u);
+	return (xs >> rot) | (xs << ((32u - rot) & 31u));
+}
+
+// PCG32 seeding with a state and a stream (src/pcg_basic.c:31-38)
+void pcg32_seed(struct pcg32_random* g, uint64_t initstate, uint64_t initseq)
+{
+	g->state = 0;
+	g->inc = (initseq << 1u) | 1u;
+	pcg32_next(g);
+	g->state += initstate;
+	pcg32_next(g);
+}
+
+int sampled_value(const char* fn, linear_func ufunc, void* udata, const std::vector<double2>& gates,
+                  const std::vector<int>& wires, int nqubits, long nsamples, struct rng_state* rng, numeric* fval)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	TargetHolder th;
+	if (!th.set(ufunc, udata, nqubits)) return fail(fn, E_ARG);
+	int ret = ensure_device(rt->result, sizeof(double2));
+	if (ret) return ret;
+	double2* d_f = static_cast<double2*>(rt->result.ptr);
+	if ((ret = sampled_f_device(*rt, nqubits, (int)(wires.size() / 2), gates.data(), wires.data(), th.spec,
+	                            sample_spec(rng, nsamples), d_f)))
+		return ret;
+	if ((ret = d2h(*rt, fval, d_f, sizeof(double2)))) return ret;
+	if ((ret = sync(*rt))) return ret;
+	advance_rng(rng, nsamples, nqubits);
+	return OK;
+}
+
+}  // namespace
+
+// src/rng.c:13-25: a seeding generator on (seed, stream 6364136223846793005 seed +
+// 1442695040888963407) yields the two seeds and two streams of the pair; equal
+// streams are made distinct (src/pcg_basic.c:112-121)
+extern "C" void seed_rng_state(const uint64_t seed, struct rng_state* state)
+{
+	struct pcg32_random s;
+	pcg32_seed(&s, seed, 6364136223846793005ULL * seed + 1442695040888963407ULL);
+	uint64_t v[4];
+	for (int k = 0; k < 4; k++) {
+		const uint64_t hi = pcg32_next(&s);
+		v[k] = (hi << 32) | pcg32_next(&s);
+	}
+	uint64_t seq2 = v[3];
+	const uint64_t mask = ~0ull >> 1;
+	if ((v[2] & mask) == (seq2 & mask)) seq2 = ~seq2;
+	pcg32_seed(&state->pcgstate.gen[0], v[0], v[2]);
+	pcg32_seed(&state->pcgstate.gen[1], v[1], seq2);
+}
+
+extern "C" void haar_random_statevector(struct statevector* psi, struct rng_state* rng)
+{
+	const char* fn = "haar_random_statevector";
+	Runtime* rt = runtime();
+	if (!rt) return fail_void(fn, E_CUDA);
+	if (!psi || !psi->data || !rng || psi->nqubits < 0 || psi->nqubits > 40) return fail_void(fn, E_ARG);
+	const int L = psi->nqubits;
+	DeviceSpan out;
+	int ret = span_out(*rt, psi->data, sv_bytes(L), 0, out);
+	if (!ret) ret = haar_states_device(*rt, sample_spec(rng, 1), L, 0, 1, static_cast<double2*>(out.dev));
+	if (!ret) ret = span_finish(*rt, out);
+	if (!ret) ret = sync(*rt);
+	if (ret) return fail_void(fn, ret);
+	advance_rng(rng, 1, L);
+}
+
+extern "C" int circuit_unitary_target_sampling(linear_func ufunc, void* udata, const struct mat4x4 gates[],
+                                               const int ngates, const int wires[], const int nqubits,
+                                               const long nsamples, struct rng_state* rng, numeric* fval)
+{
+	const char* fn = "circuit_unitary_target_sampling";
+	if (!gates || !wires || !rng || !fval || ngates < 1 || nsamples < 1 || nqubits < 2 || nqubits > 40)
+		return fail(fn, E_ARG);
+	for (int k = 0; k < ngates; k++)
+		if (!wires_ok(nqubits, wires[2 * k], wires[2 * k + 1])) return fail(fn, E_ARG);
+	std::vector<double2> g(d2(gates[0].data), d2(gates[0].data) + 16 * (size_t)ngates);
+	std::vector<int> w(wires, wires + 2 * (size_t)ngates);
+	return sampled_value(fn, ufunc, udata, g, w, nqubits, nsamples, rng, fval);
+}
+
+extern "C" int brickwall_unitary_target_sampling(linear_func ufunc, void* udata, const struct mat4x4 vlist[],
+                                                 const int nlayers, const int nqubits, const int* perms[],
+                                                 const long nsamples, struct rng_state* rng, numeric* fval)
+{
+	const char* fn = "brickwall_unitary_target_sampling";
+	std::vector<double2> ug;
+	std::vector<int> wires;
+	if (!rng || !fval || nsamples < 1 || !brickwall_of(nqubits, nlayers, vlist, perms, ug, wires)) return fail(fn, E_ARG);
+	const int per = nqubits / 2;
+	std::vector<double2> g(16 * (size_t)nlayers * per);
+	for (int k = 0; k < nlayers * per; k++)
+		memcpy(&g[16 * (size_t)k], &ug[16 * (size_t)(k / per)], 16 * sizeof(double2));
+	return sampled_value(fn, ufunc, udata, g, wires, nqubits, nsamples, rng, fval);
 }

@@ -20,6 +20,7 @@
 #include "manifold.cuh"
 #include "rqc_runtime.h"
 #include "rqcopt_gpu.h"
+#include "sampling.h"
 #include "target_problem.h"
 #include "trust_region.cuh"
 
@@ -445,9 +446,22 @@ struct DeviceOptimizer
 		return OK;
 	}
 
+	// f at the loaded gates from nsamples Haar-random states of rng's stream -> res[0]
+	int eval_f_sampled(struct rng_state* rng, long nsamples)
+	{
+		evals_f++;
+		int ret = sampled_f_device(rt, pb.L, pb.G, pb.gates.data(), pb.wires.data(), th.spec, sample_spec(rng, nsamples), res);
+		if (!ret) advance_rng(rng, nsamples, pb.L);
+		return ret;
+	}
+
 	// Trust region with the dense Riemannian Hessian of a brickwall (src/trust_region.c:230-293,
-	// src/brickwall_opt.c:85-100, 159-186): every evaluation in complex128.
-	int run_hmat(const struct rtr_params* params, int niter, double* f_iter, double2* x_final)
+	// src/brickwall_opt.c:85-100, 159-186): every evaluation in complex128.  With rng, f and
+	// the Hessian are the sampling estimates of src/brickwall_opt.c:189-265, drawing from
+	// rng's stream in the reference's order (f_deriv_hess at x, f at the candidate, ...,
+	// f at the result).
+	int run_hmat(const struct rtr_params* params, int niter, double* f_iter, double2* x_final,
+	             struct rng_state* rng = nullptr, long nsamples = 0)
 	{
 		const int nl = pb.nunits;
 		const size_t nrec = hess_record_count(nl);
@@ -473,7 +487,13 @@ struct DeviceOptimizer
 			// f, gradient vector and Hessian matrix at x (src/trust_region.c:263)
 			if ((ret = load_gates(x))) break;
 			c.ugates = hx.data();
-			if ((ret = hessian_target_device(rt, c, th.spec, rec))) break;
+			if (rng) {
+				const SampleSpec sp = sample_spec(rng, nsamples);
+				if ((ret = hessian_target_device(rt, c, th.spec, rec, &sp))) break;
+				advance_rng(rng, nsamples, pb.L);
+			} else if ((ret = hessian_target_device(rt, c, th.spec, rec))) {
+				break;
+			}
 			if ((ret = project_hessian_device(rt, nl, ug, rec, v.grad, d_hess))) break;
 			if ((ret = RQC_CUDA(cudaMemcpyAsync(fx_slot, rec, sizeof(double), cudaMemcpyDeviceToDevice, rt.stream)))) break;
 			// tCG on the dense Hessian (src/trust_region.c:264)
@@ -487,7 +507,7 @@ struct DeviceOptimizer
 			if ((ret = launched(rt))) break;
 			if ((ret = gemv_device(rt, n, d_hess, v.z, v.heta))) break;
 			if ((ret = load_gates(xn))) break;   // synchronises: boundary is valid after this
-			if ((ret = eval_f(PREC_C128))) break;
+			if ((ret = rng ? eval_f_sampled(rng, nsamples) : eval_f(PREC_C128))) break;
 			k_rtr_rho<<<1, 1, 0, rt.stream>>>(n, v.grad, v.z, v.heta, fx_slot, reinterpret_cast<const double*>(res), v.rtr,
 			                                   boundary);
 			if ((ret = launched(rt))) break;
@@ -498,7 +518,7 @@ struct DeviceOptimizer
 		if (ret) return ret;
 		if ((ret = RQC_CUDA(cudaMemcpyAsync(x_final, x, hx.size() * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
 		if ((ret = load_gates(x))) return ret;
-		if ((ret = eval_f(PREC_C128))) return ret;
+		if ((ret = rng ? eval_f_sampled(rng, nsamples) : eval_f(PREC_C128))) return ret;
 		double2 ff;
 		if ((ret = RQC_CUDA(cudaMemcpyAsync(&ff, res, sizeof(double2), cudaMemcpyDeviceToHost, rt.stream)))) return ret;
 		if ((ret = sync(rt))) return ret;
@@ -512,7 +532,8 @@ struct DeviceOptimizer
 namespace {
 
 void run_optimizer(const char* fn, Problem& pb, linear_func ufunc, void* udata, struct rtr_params* params, int niter,
-                   double* f_iter, const struct mat4x4* start, struct mat4x4* out, bool hmat = false)
+                   double* f_iter, const struct mat4x4* start, struct mat4x4* out, bool hmat = false,
+                   struct rng_state* rng = nullptr, long nsamples = 0)
 {
 	TargetHolder th;
 	if (!th.set(ufunc, udata, pb.L)) {
@@ -528,7 +549,7 @@ void run_optimizer(const char* fn, Problem& pb, linear_func ufunc, void* udata, 
 	DeviceOptimizer opt(*rt, pb, th);
 	int ret = opt.init(reinterpret_cast<const double2*>(start));
 	if (!ret)
-		ret = hmat ? opt.run_hmat(params, niter, f_iter, reinterpret_cast<double2*>(out))
+		ret = hmat ? opt.run_hmat(params, niter, f_iter, reinterpret_cast<double2*>(out), rng, nsamples)
 		           : opt.run(params, niter, f_iter, reinterpret_cast<double2*>(out), rt->precision);
 	if (ret) set_last_error(ret);
 }
@@ -571,4 +592,20 @@ extern "C" void optimize_brickwall_circuit_hmat(linear_func ufunc, void* udata, 
 		return;
 	}
 	run_optimizer("optimize_brickwall_circuit_hmat", pb, ufunc, udata, params, niter, f_iter, vlist_start, vlist_opt, true);
+}
+
+extern "C" void optimize_brickwall_circuit_hmat_sampling(linear_func ufunc, void* udata, const struct mat4x4 vlist_start[],
+                                                         const int nlayers, const int nqubits, const int* perms[],
+                                                         const long nsamples, struct rng_state* rng,
+                                                         struct rtr_params* params, const int niter, double* f_iter,
+                                                         struct mat4x4 vlist_opt[])
+{
+	Problem pb;
+	if (!params || !f_iter || !vlist_opt || !rng || nsamples < 1 ||
+	    !pb.set_brickwall(nqubits, nlayers, vlist_start, nullptr, perms)) {
+		fail_arg("optimize_brickwall_circuit_hmat_sampling", "invalid arguments");
+		return;
+	}
+	run_optimizer("optimize_brickwall_circuit_hmat_sampling", pb, ufunc, udata, params, niter, f_iter, vlist_start,
+	              vlist_opt, true, rng, nsamples);
 }

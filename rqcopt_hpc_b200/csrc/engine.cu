@@ -714,6 +714,47 @@ int target_columns_device(Runtime& rt, const TargetSpec& t, int L, int64_t b0, i
 	return OK;
 }
 
+int target_states_device(Runtime& rt, const TargetSpec& t, int L, const double2* states, int64_t ncols, double2* phi,
+                         double2* p0, double2* p1)
+{
+	const int64_t N = (int64_t)1 << L;
+	const int64_t ngroups = ncols * (N / 4);
+	int ret;
+	if (t.ufunc) {
+		if ((ret = ensure_host_pinned(rt.hpin, (size_t)(2 * ncols) * N * sizeof(double2)))) return ret;
+		double2* hin = reinterpret_cast<double2*>(rt.hpin.ptr);
+		double2* hout = hin + ncols * N;
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(hin, states, ncols * N * sizeof(double2), cudaMemcpyDeviceToHost, rt.stream))))
+			return ret;
+		if ((ret = RQC_CUDA(cudaStreamSynchronize(rt.stream)))) return ret;
+		const linear_func uf = reinterpret_cast<linear_func>(t.ufunc);
+		for (int64_t c = 0; c < ncols; c++) {
+			statevector e = { reinterpret_cast<numeric*>(hin + c * N), L };
+			statevector u = { reinterpret_cast<numeric*>(hout + c * N), L };
+			const int r = uf(&e, t.udata, &u);
+			if (r < 0) {
+				fprintf(stderr, "rqcopt_gpu: call of 'ufunc' failed, return value: %i\n", r);
+				return E_UFUNC;
+			}
+		}
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(p0, hout, ncols * N * sizeof(double2), cudaMemcpyHostToDevice, rt.stream))))
+			return ret;
+		k_conj_neg<double><<<grid_for(rt, ncols * N, 8), TPB, 0, rt.stream>>>(p0, phi, ncols * N);
+		rt.launches++;
+		if ((ret = RQC_CUDA(cudaGetLastError()))) return ret;
+		return RQC_CUDA(cudaStreamSynchronize(rt.stream));
+	}
+	double2* P[2] = { p0, p1 };
+	for (int k = 0; k < t.ngates; k++) {
+		const bool first = k == 0, last = k == t.ngates - 1;
+		if ((ret = launch_apply<double>(rt, 0, last ? 1 : 0, first ? states : P[(k - 1) & 1], last ? phi : P[k & 1],
+		                                nullptr, to_gate<double>(t.gates + 16 * k),
+		                                make_pair_(L, t.wires[2 * k], t.wires[2 * k + 1]), L, ngroups, 0, nullptr, 0)))
+			return ret;
+	}
+	return OK;
+}
+
 int add_device(Runtime& rt, const double2* a, const double2* b, double2* c, long n)
 {
 	RQC_LAUNCH(rt, KC_APPLY, k_add, grid_for(rt, n, 8), a, b, c, (int64_t)n);

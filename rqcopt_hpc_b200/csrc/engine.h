@@ -73,6 +73,9 @@ int column_passes_device(Runtime& rt, int L, int ngates, const double2* gates, c
 // callback; p0 and p1 are two chunk-sized scratch arrays.
 int target_columns_device(Runtime& rt, const TargetSpec& t, int L, int64_t b0, int64_t ncols, double2* phi,
                           double2* p0, double2* p1);
+// The same for given input states: phi[c] = -conj(U states[c]).
+int target_states_device(Runtime& rt, const TargetSpec& t, int L, const double2* states, int64_t ncols, double2* phi,
+                         double2* p0, double2* p1);
 // c = a + b elementwise, n complex entries
 int add_device(Runtime& rt, const double2* a, const double2* b, double2* c, long n);
 

@@ -42,6 +42,7 @@
 #include "manifold.cuh"
 #include "rqc_common.cuh"
 #include "rqcopt_gpu.h"
+#include "sampling.h"
 #include "trust_region.cuh"
 
 namespace rqc {
@@ -443,6 +444,14 @@ __global__ void k_hproject(int nl, const double2* __restrict__ ug, const double2
 	for (int x = 0; x < 16; x++) H[(size_t)(16 * a + x) * m + 16 * b + k] = r[x];
 }
 
+// rec *= scale (the 2^L / nsamples normalisation of the sampling estimator,
+// src/target.c:904-915)
+__global__ void k_scale_rec(double2* __restrict__ rec, int64_t n, double scale)
+{
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		rec[i] = make_double2(rec[i].x * scale, rec[i].y * scale);
+}
+
 // lower triangle from the upper one (src/target.c:981-986)
 __global__ void k_hmirror(int m, double* __restrict__ H)
 {
@@ -705,22 +714,25 @@ struct Sweep
 
 // ------------------------------------------------------------------ engine entry points
 
-int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, double2* d_rec)
+int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, double2* d_rec, const SampleSpec* samp)
 {
 	const int L = c.L, nl = c.nlayers;
 	if (L < 2 || L % 2 || nl < 1) return E_ARG;
+	if (samp && samp->nsamples < 1) return E_ARG;
 	const int per = L / 2, G = nl * per;
 	const int64_t N = (int64_t)1 << L;
+	const int64_t ncols = samp ? samp->nsamples : N;   // basis columns, or sample states
 	// layer kernel (shared-memory tiles) up to L = 12, one kernel per gate beyond
 	const bool layered = L <= 12 && per <= HMAXPER;
 	// states per column: phi_q of every gate, psi_q of every gate (layered) or two psi
-	// buffers, 16 tangents per layer
-	const int64_t nstates = G + (layered ? G : 2) + 16 * (int64_t)nl;
+	// buffers, 16 tangents per layer; sampled: the sample states and two target scratch
+	// states besides
+	const int64_t nstates = G + (layered ? G : 2) + 16 * (int64_t)nl + (samp ? (layered ? 2 : 3) : 0);
 	const size_t col_bytes = (size_t)nstates * N * sizeof(double2);
 	int64_t C = (int64_t)(hess_workspace_limit(rt) / col_bytes);
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, rt.column_chunk);
 	if (t.ufunc) C = std::min<int64_t>(C, std::max<int64_t>(1, ((int64_t)256 << 20) / (N * 16)));
-	C = std::min(C, N);
+	C = std::min(C, ncols);
 	if (C < 1) {
 		fprintf(stderr, "rqcopt_gpu: one basis column of the Hessian sweep needs %zu bytes of workspace, more than the limit\n",
 		        col_bytes);
@@ -733,28 +745,43 @@ int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t
 	double2* P[2] = { phi + (int64_t)G * cs, phi + (int64_t)(G + 1) * cs };
 	double2* psi = phi + (int64_t)G * cs;                              // layered: psi_q at psi + q cs
 	double2* tan = phi + (int64_t)(G + (layered ? G : 2)) * cs;
+	double2* extra = tan + 16 * (int64_t)nl * cs;                       // sampled: scratch (and states)
+	double2* states = samp ? (layered ? psi : extra + 2 * cs) : nullptr;
+	double2* tq[2] = { samp ? extra : P[0], samp ? extra + cs : P[1] };   // target scratch
 	auto phi_at = [&](int q) { return phi + (int64_t)q * cs; };
 	auto psi_at = [&](int q) { return psi + (int64_t)q * cs; };
 
 	Sweep sw(rt, c);
 	if ((ret = sw.init(cs / 4, layered ? (C + (HTILE >> L) - 1) / (HTILE >> L) : 0))) return ret;
-	for (int64_t b0 = 0; b0 < N; b0 += C) {
-		const int64_t Cc = std::min(C, N - b0);
+	for (int64_t b0 = 0; b0 < ncols; b0 += C) {
+		const int64_t Cc = std::min(C, ncols - b0);
 		const int64_t ngroups = Cc * (N / 4);
-		if ((ret = target_columns_device(rt, t, L, b0, Cc, phi_at(G - 1), P[0], P[1]))) return ret;
+		const int64_t basis = samp ? -1 : b0;
+		if (samp) {
+			if ((ret = haar_states_device(rt, *samp, L, b0, Cc, states))) return ret;
+			if ((ret = target_states_device(rt, t, L, states, Cc, phi_at(G - 1), tq[0], tq[1]))) return ret;
+		} else if ((ret = target_columns_device(rt, t, L, b0, Cc, phi_at(G - 1), tq[0], tq[1]))) {
+			return ret;
+		}
 		if ((ret = sw.reverse_chain(phi_at, ngroups, nullptr))) return ret;
 		if (layered) {
-			if ((ret = sw.forward_chain(psi_at, ngroups, b0))) return ret;
+			if ((ret = sw.forward_chain(psi_at, ngroups, basis))) return ret;
 			for (int a = 0; a < nl; a++)
-				if ((ret = sw.layer(a, psi, b0, phi, tan, Cc, cs, true))) return ret;
+				if ((ret = sw.layer(a, psi, basis, phi, tan, Cc, cs, true))) return ret;
 			continue;
 		}
 		for (int q = 0; q < G; q++) {
-			const double2* in = q == 0 ? nullptr : P[(q - 1) & 1];
-			if ((ret = sw.gate(q, in, q == 0 ? b0 : -1, P[q & 1], phi_at(q), tan, ngroups, cs, true))) return ret;
+			const double2* in = q == 0 ? states : P[(q - 1) & 1];
+			if ((ret = sw.gate(q, in, q == 0 ? basis : -1, P[q & 1], phi_at(q), tan, ngroups, cs, true))) return ret;
 		}
 	}
-	return sw.assemble(d_rec);
+	if ((ret = sw.assemble(d_rec))) return ret;
+	if (samp) {
+		const int64_t n = (int64_t)hess_record_count(nl);
+		k_scale_rec<<<grid_of(rt, n, 4), HT, 0, rt.stream>>>(d_rec, n, (double)N / (double)samp->nsamples);
+		ret = checked(rt);
+	}
+	return ret;
 }
 
 int hessian_single_device(Runtime& rt, const HessCircuit& c, const double2* d_cache, const double2* d_dout,

@@ -23,8 +23,12 @@ struct HessCircuit
 // [0] f, [1 + 16 l + e] sum dV_l[e], then the row-major m x m complex Hessian, m = 16 nlayers.
 inline size_t hess_record_count(int nlayers) { return 1 + 16 * (size_t)nlayers + 256 * (size_t)nlayers * nlayers; }
 
-// f, per-layer gradients and the complex Hessian summed over all basis columns.
-int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, double2* d_rec);
+struct SampleSpec;
+
+// f, per-layer gradients and the complex Hessian summed over all basis columns, or,
+// with samp, over samp->nsamples Haar-random states scaled by 2^L / nsamples.
+int hessian_target_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, double2* d_rec,
+                          const SampleSpec* samp = nullptr);
 
 // One state: cache holds the input state of every sequential gate (device, one after
 // another), dout the cotangent of the circuit output; dpsi (device) receives the

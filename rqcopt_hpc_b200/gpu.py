@@ -20,7 +20,8 @@ import os
 import numpy as np
 
 from .abi import (HVP_FUNC, LINEAR_FUNC, RETRACT_FUNC, TARGET_FUNC, TARGET_GRAD_FUNC, TARGET_GRAD_HESS_FUNC,
-                  BrickwallTarget, CircuitTarget, QuantumCircuitCache, RTRParams, Statevector, StatevectorArray,
+                  BrickwallTarget, CircuitTarget, QuantumCircuitCache, RngState, RTRParams, Statevector,
+                  StatevectorArray,
                   TruncatedCGParams, cplx, default_rtr_params, default_tcg_params, ints, perm_pointers, ptr,
                   wrap_ufunc)
 
@@ -91,6 +92,16 @@ _SIGS = {
     "truncated_cg_hmat": (C.c_bool, [VP, VP, I, D, C.POINTER(TruncatedCGParams), VP]),
     "riemannian_trust_region_optimize_hmat": (None, [VP, VP, VP, VP, VP, I, VP, I, C.POINTER(RTRParams), I, VP, VP]),
     "optimize_brickwall_circuit_hmat": (None, [VP, VP, VP, I, I, VP, C.POINTER(RTRParams), I, VP, VP]),
+    "seed_rng_state": (None, [C.c_uint64, C.POINTER(RngState)]),
+    "haar_random_statevector": (None, [PSV, C.POINTER(RngState)]),
+    "circuit_unitary_target_sampling": (I, [VP, VP, VP, I, VP, I, C.c_long, C.POINTER(RngState), VP]),
+    "brickwall_unitary_target_sampling": (I, [VP, VP, VP, I, I, VP, C.c_long, C.POINTER(RngState), VP]),
+    "brickwall_unitary_target_gradient_hessian_sampling": (I, [VP, VP, VP, I, I, VP, C.c_long, C.POINTER(RngState),
+                                                              VP, VP, VP]),
+    "brickwall_unitary_target_gradient_vector_hessian_matrix_sampling": (I, [VP, VP, VP, I, I, VP, C.c_long,
+                                                                            C.POINTER(RngState), VP, VP, VP]),
+    "optimize_brickwall_circuit_hmat_sampling": (None, [VP, VP, VP, I, I, VP, C.c_long, C.POINTER(RngState),
+                                                        C.POINTER(RTRParams), I, VP, VP]),
     "rqcopt_brickwall_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_circuit_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_gpu_set_precision": (I, [I]),
@@ -517,6 +528,84 @@ def brickwall_unitary_target_gradient_vector_hessian_matrix(target, vlist, perms
            lib().brickwall_unitary_target_gradient_vector_hessian_matrix(target.ufunc, target.udata, ptr(vlist), nl,
                                                                          nqubits, C.cast(pp, VP), ptr(f), ptr(g), ptr(H)))
     return f[0], g, H
+
+
+# ------------------------------------------------------------------------ sampling estimator
+# Haar-random states drawn on the GPU from the reference's PCG32x2 stream; every call
+# advances `rng` exactly as the reference's call does.
+
+def seed_rng_state(seed: int) -> RngState:
+    rng = RngState()
+    lib().seed_rng_state(seed, C.byref(rng))
+    return rng
+
+
+def haar_random_statevector(nqubits, rng):
+    out = np.empty(1 << nqubits, np.complex128)
+    lib().haar_random_statevector(C.byref(_sv(out, nqubits)), C.byref(rng))
+    _check_void("haar_random_statevector")
+    return out
+
+
+def circuit_unitary_target_sampling(target, gates, wires, nqubits, nsamples, rng):
+    gates, wires = cplx(gates), ints(wires)
+    f = np.zeros(1, np.complex128)
+    _check("circuit_unitary_target_sampling",
+           lib().circuit_unitary_target_sampling(target.ufunc, target.udata, ptr(gates), gates.shape[0], ptr(wires),
+                                                 nqubits, nsamples, C.byref(rng), ptr(f)))
+    return f[0]
+
+
+def brickwall_unitary_target_sampling(target, vlist, perms, nqubits, nsamples, rng):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    _check("brickwall_unitary_target_sampling",
+           lib().brickwall_unitary_target_sampling(target.ufunc, target.udata, ptr(vlist), vlist.shape[0], nqubits,
+                                                   C.cast(pp, VP), nsamples, C.byref(rng), ptr(f)))
+    return f[0]
+
+
+def brickwall_unitary_target_gradient_hessian_sampling(target, vlist, perms, nqubits, nsamples, rng):
+    vlist = cplx(vlist)
+    nl = vlist.shape[0]
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    dv = np.empty((nl, 4, 4), np.complex128)
+    hess = np.empty((16 * nl, 16 * nl), np.complex128)
+    _check("brickwall_unitary_target_gradient_hessian_sampling",
+           lib().brickwall_unitary_target_gradient_hessian_sampling(target.ufunc, target.udata, ptr(vlist), nl, nqubits,
+                                                                    C.cast(pp, VP), nsamples, C.byref(rng), ptr(f),
+                                                                    ptr(dv), ptr(hess)))
+    return f[0], dv, hess
+
+
+def brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(target, vlist, perms, nqubits, nsamples, rng):
+    vlist = cplx(vlist)
+    nl = vlist.shape[0]
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1, np.complex128)
+    g = np.empty(16 * nl)
+    H = np.empty((16 * nl, 16 * nl))
+    _check("brickwall_unitary_target_gradient_vector_hessian_matrix_sampling",
+           lib().brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(
+               target.ufunc, target.udata, ptr(vlist), nl, nqubits, C.cast(pp, VP), nsamples, C.byref(rng), ptr(f),
+               ptr(g), ptr(H)))
+    return f[0], g, H
+
+
+def optimize_brickwall_circuit_hmat_sampling(target, vlist_start, perms, nqubits, nsamples, rng, niter, params=None):
+    vlist_start = cplx(vlist_start)
+    nl = vlist_start.shape[0]
+    pp, keep = perm_pointers(perms)
+    params = params or default_rtr_params(16 * nl)
+    f_iter = np.empty(niter + 1)
+    vopt = np.empty_like(vlist_start)
+    lib().optimize_brickwall_circuit_hmat_sampling(target.ufunc, target.udata, ptr(vlist_start), nl, nqubits,
+                                                   C.cast(pp, VP), nsamples, C.byref(rng), C.byref(params), niter,
+                                                   ptr(f_iter), ptr(vopt))
+    _check_void("optimize_brickwall_circuit_hmat_sampling")
+    return f_iter, vopt
 
 
 # ------------------------------------------------------------------------ trust region and optimisers

@@ -29,6 +29,9 @@ FIXTURES = [
     # full-Hessian path
     "apply_gate_to_array", "apply_gate_placeholder", "brickwall_unitary_backward_hessian",
     "brickwall_unitary_target_gradient_hessian", "brickwall_unitary_target_gradient_vector_hessian_matrix",
+    # sampling estimator
+    "brickwall_unitary_target_sampling", "brickwall_unitary_target_gradient_hessian_sampling",
+    "brickwall_unitary_target_gradient_vector_hessian_matrix_sampling",
 ]
 
 

@@ -54,3 +54,37 @@ def test_trust_region_iterates_match_reference(oracle, ref):
     assert rel_err(f_o, f_r) <= 1e-12
     assert rel_err(v_o, v_r) <= 1e-10
     assert f_o[-1] < f_o[0]
+
+
+def test_sampling_oracle_matches_reference(oracle, ref):
+    """PCG32x2 seeding and Haar states bit for bit; sampled f, gradient and Hessian and a
+    sampled full-Hessian optimisation to rounding; identical generator state after each call."""
+    ro, rr = oracle.seed_rng_state(677), ref.seed_rng_state(677)
+    assert ro.tuple() == rr.tuple()
+    assert np.array_equal(oracle.haar_random_statevector(6, ro), ref.haar_random_statevector(6, rr))
+    assert ro.tuple() == rr.tuple()
+    vlist, perms, tvlist, tperms = brickwall_instance(6, 3, 0, 3, 1)
+    t = oracle.target("brickwall", (tvlist, tperms))
+    ro, rr = oracle.seed_rng_state(5), ref.seed_rng_state(5)
+    fo = oracle.brickwall_unitary_target_sampling(t, vlist, perms, 6, 100, ro)
+    fr = ref.sampling(0, vlist, perms, 6, (tvlist, tperms), 100, rr)
+    assert abs(fo - fr) <= 1e-14 * abs(fr) and ro.tuple() == rr.tuple()
+    ro, rr = oracle.seed_rng_state(6), ref.seed_rng_state(6)
+    fo, go, Ho = oracle.brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(t, vlist, perms, 6, 40, ro)
+    fr, gr, Hr = ref.sampling(2, vlist, perms, 6, (tvlist, tperms), 40, rr)
+    assert rel_err(go, gr) <= 1e-14 and rel_err(Ho, Hr) <= 1e-14 and ro.tuple() == rr.tuple()
+    ro, rr = oracle.seed_rng_state(7), ref.seed_rng_state(7)
+    fo, vo = oracle.optimize_brickwall_circuit_hmat_sampling(t, vlist, perms, 6, 30, ro, 3)
+    fr, vr = ref.optimize_brickwall_hmat_sampling(vlist, perms, 6, tvlist, tperms, 30, rr, 3)
+    assert rel_err(fo, fr) <= 1e-13 and rel_err(vo, vr) <= 1e-13 and ro.tuple() == rr.tuple()
+
+
+def test_full_hessian_oracle_matches_reference(oracle, ref):
+    vlist, perms, tvlist, tperms = brickwall_instance(8, 3, 0, 3, 1)
+    t = oracle.target("brickwall", (tvlist, tperms))
+    f, g, H = oracle.brickwall_unitary_target_gradient_vector_hessian_matrix(t, vlist, perms, 8)
+    fr, gr, Hr = ref.gradient_vector_hessian_matrix(vlist, perms, 8, tvlist, tperms)
+    assert abs(f - fr) <= 1e-14 * abs(fr) and rel_err(g, gr) <= 1e-14 and rel_err(H, Hr) <= 1e-14
+    fo, vo, acc, bnd = oracle.optimize_brickwall_circuit_hmat(t, vlist, perms, 8, 3)
+    fr2, vr2 = ref.optimize_brickwall_hmat(vlist, perms, 8, tvlist, tperms, 3)
+    assert rel_err(fo, fr2) <= 1e-13 and rel_err(vo, vr2) <= 1e-13

@@ -325,3 +325,45 @@ def test_truncated_cg_hmat(impl):
     z, on_boundary = impl.truncated_cg_hmat(d["grad"], d["hess"], 1.5)
     assert np.max(np.abs(z - d["z"])) <= 1e-14
     assert on_boundary == bool(d["on_boundary"])
+
+
+# ------------------------------------------------------------------ sampling estimator
+# test_target.c:563-624, 1291-1388, 1487-1563: estimates from 10,000 Haar-random states
+# within the reference's statistical bars of the exact values; the Hessian estimate is
+# symmetric.
+
+def test_brickwall_unitary_target_sampling(impl):
+    d = golden("brickwall_unitary_target_sampling")
+    t = impl.target("dense", d["U"])
+    vlist, perms = stack(d, "V", 3), stack(d, "perm", 3)
+    rng = impl.seed_rng_state(677)
+    f = impl.brickwall_unitary_target_sampling(t, vlist, perms, 8, 10000, rng)
+    f_ref = impl.brickwall_unitary_target(t, vlist, perms, 8)
+    assert abs(f - f_ref) / abs(f_ref) <= 0.2
+
+
+def test_brickwall_unitary_target_gradient_hessian_sampling(impl):
+    d = golden("brickwall_unitary_target_gradient_hessian_sampling")
+    t = impl.target("dense", d["U"])
+    vlist, perms = stack(d, "V", 3), stack(d, "perm", 3)
+    rng = impl.seed_rng_state(823)
+    f, dv, hess = impl.brickwall_unitary_target_gradient_hessian_sampling(t, vlist, perms, 6, 10000, rng)
+    assert udist(hess, hess.T) <= 1e-12
+    f_ref, dv_ref, hess_ref = impl.brickwall_unitary_target_gradient_hessian(t, vlist, perms, 6)
+    assert abs(f - f_ref) / abs(f_ref) <= 0.2
+    for j in range(3):
+        assert udist(dv[j], dv_ref[j]) <= 0.2
+    assert udist(hess, hess_ref) <= 0.4
+
+
+def test_brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(impl):
+    d = golden("brickwall_unitary_target_gradient_vector_hessian_matrix_sampling")
+    t = impl.target("fixture")
+    vlist, perms = stack(d, "V", 5), stack(d, "perm", 5)
+    rng = impl.seed_rng_state(401)
+    f, g, H = impl.brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(t, vlist, perms, 6, 10000, rng)
+    assert np.max(np.abs(H - H.T)) <= 1e-14
+    f_ref, g_ref, H_ref = impl.brickwall_unitary_target_gradient_vector_hessian_matrix(t, vlist, perms, 6)
+    assert abs(f - f_ref) / abs(f_ref) <= 0.2
+    assert np.max(np.abs(g - g_ref)) <= 0.3
+    assert np.max(np.abs(H - H_ref)) <= 0.4
