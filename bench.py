@@ -283,6 +283,17 @@ def _ref_hessian_worker(args):
     return time.perf_counter() - t0
 
 
+def _ref_sampling_worker(args):
+    L, depth, tdepth, seed = args
+    from oracle.oracle import Reference
+    r = Reference()
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth)
+    rng = r.seed_rng_state(seed)
+    t0 = time.perf_counter()
+    r.sampling(2, vlist, perms, L, (tvlist, tperms), 1, rng)
+    return time.perf_counter() - t0
+
+
 def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
     """Full-Hessian ("hmat") path.  (1) The reference's own Hessian benchmark
     (examples/benchmark/benchmark_16_qubits.c): brickwall_unitary_forward plus
@@ -390,8 +401,36 @@ def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
           "seconds": tg_s, "seconds_per_iteration": tg_s / niter, "f_first": float(f_iter[0]),
           "f_final": float(f_iter[-1])}
     out["optimize_hmat_L8"] = r3
+
+    # (4) sampling estimator: gradient vector and Hessian matrix from Haar-random states
+    L, depth, tdepth, ns = 14, 8, 4, 64
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth)
+    tg = gpu.Target(brickwall=(tvlist, tperms))
+    rng = gpu.seed_rng_state(2024)
+
+    def sampled():
+        return gpu.brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(tg, vlist, perms, L, ns, rng)
+
+    sampled()
+    _, wall, dev_ms, hs_ms, hs_n, launches = timed(sampled, steps)
+    r4 = {"workload": f"f + gradient vector + Hessian matrix estimated from {ns} Haar-random states, brickwall L={L} "
+                      f"depth {depth} vs brickwall target depth {tdepth} (per-gate sweep)",
+          "samples_per_s_e2e": ns / wall, "ms_per_call": wall * 1e3, "sweep_ms": hs_ms, "gpu_launches": launches,
+          "roofline": roofline(hess_model(L, depth, False), ns, L, hs_ms, hs_n)}
+    out["sampling_L14"] = r4
     if not have_ref:
         return out
+
+    cores = os.cpu_count() or 1
+    with mp.get_context("spawn").Pool(cores) as pool:
+        t0 = time.perf_counter()
+        pool.map(_ref_sampling_worker, [(L, depth, tdepth, 100 + k) for k in range(cores)])
+        tref = time.perf_counter() - t0
+    r4["cpu_baseline"] = {"value": cores / tref, "unit": "samples/s", "cores": cores, "kind": "reference",
+                          "sample": f"{cores} single-sample calls of the reference's "
+                                    f"brickwall_unitary_target_gradient_vector_hessian_matrix_sampling, one per core, "
+                                    f"{tref:.1f} s wall"}
+    r4["speedup_e2e"] = (ns / wall) / (cores / tref)
 
     # reference legs
     vlist, perms, psi, dout, dpsi, dv, hess, wall = single_case
