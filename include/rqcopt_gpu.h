@@ -237,6 +237,29 @@ int brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(linear_func
 	const long nsamples, struct rng_state* rng,
 	numeric* fval, double* grad_vec, double* H);
 
+/* src/target.h:96-98 -- block-encoding target || P^dag W P - H ||_F^2 / 2; hfunc acts on
+ * nqubits / 2 qubits (the even-numbered ones; P puts the odd ones in |0>) */
+int brickwall_blockenc_target(linear_func hfunc, void* hdata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	double* fval);
+/* src/target.h:101-103 */
+int brickwall_blockenc_target_and_gradient(linear_func hfunc, void* hdata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	double* fval, struct mat4x4 dvlist[]);
+/* src/target.h:106-108 */
+int brickwall_blockenc_target_and_gradient_vector(linear_func hfunc, void* hdata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	double* fval, double* grad_vec);
+/* src/target.h:113-121 (COMPLEX_CIRCUIT form: hess1 the second derivative of the residual's
+ * backward pass, hess2 the Gauss-Newton term) */
+int brickwall_blockenc_target_gradient_hessian(linear_func hfunc, void* hdata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	double* fval, struct mat4x4 dvlist[], numeric* hess1, numeric* hess2);
+/* src/target.h:124-126 */
+int brickwall_blockenc_target_gradient_vector_hessian_matrix(linear_func hfunc, void* hdata,
+	const struct mat4x4 vlist[], const int nlayers, const int nqubits, const int* perms[],
+	double* fval, double* grad_vec, double* H);
+
 /* ------------------------------------------------------------------ trust_region.h */
 
 /* src/trust_region.h:10-16 */

@@ -495,6 +495,51 @@ class Oracle:
         return f_iter, vopt
 
 
+    # block-encoding target (hfunc acts on nqubits / 2 qubits)
+    def brickwall_blockenc_target(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1)
+        assert self.lib.orc_blockenc_target(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L, _p(perms), _p(f)) == 0
+        return f[0]
+
+    def brickwall_blockenc_target_and_gradient(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1)
+        dv = np.empty((vlist.shape[0], 4, 4), np.complex128)
+        assert self.lib.orc_blockenc_target_and_gradient(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L, _p(perms),
+                                                         _p(f), _p(dv)) == 0
+        return f[0], dv
+
+    def brickwall_blockenc_target_and_gradient_vector(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        f = np.zeros(1)
+        g = np.empty(16 * vlist.shape[0])
+        assert self.lib.orc_blockenc_target_and_gradient_vector(tgt.ufunc, tgt.udata, _p(vlist), vlist.shape[0], L,
+                                                                _p(perms), _p(f), _p(g)) == 0
+        return f[0], g
+
+    def brickwall_blockenc_target_gradient_hessian(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1)
+        dv = np.empty((nl, 4, 4), np.complex128)
+        h1 = np.empty((16 * nl, 16 * nl), np.complex128)
+        h2 = np.empty_like(h1)
+        assert self.lib.orc_blockenc_target_gradient_hessian(tgt.ufunc, tgt.udata, _p(vlist), nl, L, _p(perms), _p(f),
+                                                             _p(dv), _p(h1), _p(h2)) == 0
+        return f[0], dv, h1, h2
+
+    def brickwall_blockenc_target_gradient_vector_hessian_matrix(self, tgt, vlist, perms, L):
+        vlist, perms = _c(vlist), _i(perms)
+        nl = vlist.shape[0]
+        f = np.zeros(1)
+        g = np.empty(16 * nl)
+        H = np.empty((16 * nl, 16 * nl))
+        assert self.lib.orc_blockenc_target_gradient_vector_hessian_matrix(tgt.ufunc, tgt.udata, _p(vlist), nl, L,
+                                                                           _p(perms), _p(f), _p(g), _p(H)) == 0
+        return f[0], g, H
+
+
 class Reference:
     """The reference's own C sources compiled in _ref/ (built only where the sources exist)."""
 
@@ -650,3 +695,25 @@ class Reference:
                                                          tvlist.shape[0], _p(tperms), L_(nsamples), C.byref(rng),
                                                          niter, _p(f_iter), _p(vopt))
         return f_iter, vopt
+
+    def blockenc(self, mode, vlist, perms, L, hvlist, hperms):
+        """Block-encoding target of the reference with a brickwall H on L / 2 qubits: mode 0 f,
+        1 f and gradient, 2 f, gradient vector, 3 f, gradient and hess1, hess2, 4 f, gradient
+        vector and H."""
+        vlist, perms, hvlist, hperms = _c(vlist), _i(perms), _c(hvlist), _i(hperms)
+        nl = vlist.shape[0]
+        m = 16 * nl
+        f = np.zeros(1)
+        o = [None, None, None]
+        if mode == 1:
+            o[0] = np.empty((nl, 4, 4), np.complex128)
+        elif mode == 2:
+            o[0] = np.empty(m)
+        elif mode == 3:
+            o = [np.empty((nl, 4, 4), np.complex128), np.empty((m, m), np.complex128), np.empty((m, m), np.complex128)]
+        elif mode == 4:
+            o = [np.empty(m), np.empty((m, m)), None]
+        ret = self.lib.refdrv_blockenc(mode, _p(vlist), nl, _p(perms), L, _p(hvlist), hvlist.shape[0], _p(hperms),
+                                       _p(f), *[(_p(x) if x is not None else None) for x in o])
+        assert ret == 0
+        return (f[0],) + tuple(x for x in o if x is not None)

@@ -314,3 +314,24 @@ void refdrv_optimize_brickwall_hmat_sampling(const struct mat4x4* vstart, int nl
 		&params, niter, f_iter, vopt);
 	free(p); free(tp);
 }
+
+/* block-encoding target with a brickwall H on L / 2 qubits (hvlist, hperms_flat [hnlayers][L/2]):
+ * mode 0 f, 1 f + dvlist, 2 f + grad_vec, 3 f + dvlist + hess1 + hess2, 4 f + grad_vec + H */
+int refdrv_blockenc(int mode, const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                    const struct mat4x4* hvlist, int hnlayers, const int* hperms_flat, double* fval,
+                    void* o1, void* o2, void* o3)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** hp = perm_ptrs(hperms_flat, hnlayers, L / 2);
+	struct refdrv_brickwall hop = { hvlist, hnlayers, hp };
+	int ret;
+	switch (mode) {
+	case 0: ret = brickwall_blockenc_target(refdrv_brickwall_ufunc, &hop, vlist, nlayers, L, p, fval); break;
+	case 1: ret = brickwall_blockenc_target_and_gradient(refdrv_brickwall_ufunc, &hop, vlist, nlayers, L, p, fval, o1); break;
+	case 2: ret = brickwall_blockenc_target_and_gradient_vector(refdrv_brickwall_ufunc, &hop, vlist, nlayers, L, p, fval, o1); break;
+	case 3: ret = brickwall_blockenc_target_gradient_hessian(refdrv_brickwall_ufunc, &hop, vlist, nlayers, L, p, fval, o1, o2, o3); break;
+	default: ret = brickwall_blockenc_target_gradient_vector_hessian_matrix(refdrv_brickwall_ufunc, &hop, vlist, nlayers, L, p, fval, o1, o2); break;
+	}
+	free(p); free(hp);
+	return ret;
+}

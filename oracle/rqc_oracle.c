@@ -1386,3 +1386,169 @@ void orc_optimize_brickwall_hmat_sampling(orc_linear_func uf, void* ud, const or
 	                      (const double*)vstart, 32 * nlayers, params, niter, f_iter, (double*)vopt, accepted,
 	                      on_boundary);
 }
+
+/* ------------------------------------------------------------ block-encoding target */
+
+/* index of a half-register basis state b in the full register: bit i of b becomes bit
+ * 2 i + 1 (the even-numbered qubits; the odd ones stay |0>), src/target.c:1148-1157 */
+static long blockenc_index(long b, int half)
+{
+	long c = 0;
+	for (int i = 0; i < half; i++) c |= ((b >> i) & 1L) << (2 * i + 1);
+	return c;
+}
+
+/* src/target.c:1100-1193 (f), 1202-1333 (f and gradient), 1380-1623 (f, gradient and the
+ * two complex Hessians); what: 0 f, 1 f and gradient, 2 everything */
+static int blockenc_sums(int what, orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int L,
+                         const int* perms, double* fval, orc_mat4* dvlist, orc_cplx* hess1, orc_cplx* hess2)
+{
+	const int half = L / 2, per = L / 2, G = nlayers * per, m = 16 * nlayers;
+	const long s = 1L << half, N = 1L << L;
+	orc_sv psi = { sv_alloc(half), half }, hpsi = { sv_alloc(half), half };
+	orc_sv chi = { sv_alloc(L), L }, wchi = { sv_alloc(L), L };
+	orc_sv* cache = (orc_sv*)malloc(G * sizeof(orc_sv));
+	for (int k = 0; k < G; k++) { cache[k].data = sv_alloc(L); cache[k].nqubits = L; }
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* hu = what == 2 ? (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx)) : NULL;
+	orc_cplx* phi = what == 2 ? (orc_cplx*)malloc((size_t)nlayers * s * 16 * sizeof(orc_cplx)) : NULL;
+	orc_cplx* tmp = what == 2 ? (orc_cplx*)malloc((size_t)N * 16 * sizeof(orc_cplx)) : NULL;
+	if (what >= 1) for (int l = 0; l < nlayers; l++) memset(&dvlist[l], 0, sizeof(orc_mat4));
+	if (what == 2) {
+		memset(hess1, 0, (size_t)m * m * sizeof(orc_cplx));
+		memset(hess2, 0, (size_t)m * m * sizeof(orc_cplx));
+	}
+	double f = 0;
+	int ret = 0;
+	for (long b = 0; b < s && !ret; b++) {
+		memset(psi.data, 0, s * sizeof(orc_cplx));
+		psi.data[b] = 1;
+		if (hf(&psi, hd, &hpsi) < 0) { ret = -2; break; }
+		memset(chi.data, 0, N * sizeof(orc_cplx));
+		chi.data[blockenc_index(b, half)] = 1;
+		orc_brickwall_forward(vlist, nlayers, perms, &chi, cache, &wchi);
+		memset(chi.data, 0, N * sizeof(orc_cplx));
+		for (long a = 0; a < s; a++) {
+			const long c = blockenc_index(a, half);
+			const orc_cplx d = wchi.data[c] - hpsi.data[a];
+			f += 0.5 * (creal(d) * creal(d) + cimag(d) * cimag(d));
+			chi.data[c] = conj(d);
+		}
+		if (what == 0) continue;
+		if (what == 1) {
+			orc_brickwall_backward(vlist, nlayers, perms, cache, &chi, &wchi, dv);
+		} else {
+			orc_brickwall_backward_hessian(vlist, nlayers, perms, cache, &chi, &wchi, dv, hu);
+			for (long e = 0; e < (long)m * m; e++) hess1[e] += hu[e];
+			/* Jacobian of P^dag W P e_b in the gate entries of each layer */
+			for (int l = 0; l < nlayers; l++) {
+				orc_apply_brickwall_placeholder(vlist, nlayers, perms, l, cache, tmp);
+				for (long a = 0; a < s; a++)
+					for (int j = 0; j < 16; j++)
+						phi[((size_t)l * s + a) * 16 + j] = tmp[blockenc_index(a, half) * 16 + j];
+			}
+			/* Gauss-Newton part: lower blocks, then the upper ones by conjugate symmetry */
+			memset(hu, 0, (size_t)m * m * sizeof(orc_cplx));
+			for (int l = 0; l < nlayers; l++)
+				for (int k = 0; k <= l; k++)
+					for (long a = 0; a < s; a++)
+						for (int i = 0; i < 16; i++)
+							for (int j = 0; j < 16; j++)
+								hu[hidx(nlayers, l, i, k, j)] += conj(phi[((size_t)l * s + a) * 16 + i])
+								                                * phi[((size_t)k * s + a) * 16 + j];
+			for (int l = 0; l < nlayers; l++)
+				for (int k = l + 1; k < nlayers; k++)
+					for (int i = 0; i < 16; i++)
+						for (int j = 0; j < 16; j++) hu[hidx(nlayers, l, i, k, j)] = conj(hu[hidx(nlayers, k, j, l, i)]);
+			for (long e = 0; e < (long)m * m; e++) hess2[e] += hu[e];
+		}
+		for (int l = 0; l < nlayers; l++)
+			for (int e = 0; e < 16; e++) dvlist[l].data[e] += dv[l].data[e];
+	}
+	*fval = f;
+	for (int k = 0; k < G; k++) free(cache[k].data);
+	free(cache); free(dv); free(hu); free(phi); free(tmp);
+	free(psi.data); free(hpsi.data); free(chi.data); free(wchi.data);
+	return ret;
+}
+
+int orc_blockenc_target(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int L, const int* perms,
+                        double* fval)
+{
+	return blockenc_sums(0, hf, hd, vlist, nlayers, L, perms, fval, NULL, NULL, NULL);
+}
+
+int orc_blockenc_target_and_gradient(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int L,
+                                     const int* perms, double* fval, orc_mat4* dvlist)
+{
+	return blockenc_sums(1, hf, hd, vlist, nlayers, L, perms, fval, dvlist, NULL, NULL);
+}
+
+/* src/target.c:1341-1370 */
+int orc_blockenc_target_and_gradient_vector(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int L,
+                                            const int* perms, double* fval, double* grad_vec)
+{
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	int ret = blockenc_sums(1, hf, hd, vlist, nlayers, L, perms, fval, dv, NULL, NULL);
+	if (!ret)
+		for (int l = 0; l < nlayers; l++) {
+			for (int e = 0; e < 16; e++) dv[l].data[e] = conj(dv[l].data[e]);
+			orc_tangent_to_real(&vlist[l], &dv[l], &grad_vec[16*l]);
+		}
+	free(dv);
+	return ret;
+}
+
+int orc_blockenc_target_gradient_hessian(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int L,
+                                         const int* perms, double* fval, orc_mat4* dvlist, orc_cplx* hess1,
+                                         orc_cplx* hess2)
+{
+	return blockenc_sums(2, hf, hd, vlist, nlayers, L, perms, fval, dvlist, hess1, hess2);
+}
+
+/* src/target.c:1631-1720: H column (j, k) from conj(hess1 Z) + hess2 Z */
+int orc_blockenc_target_gradient_vector_hessian_matrix(orc_linear_func hf, void* hd, const orc_mat4* vlist,
+                                                       int nlayers, int L, const int* perms, double* fval,
+                                                       double* grad_vec, double* H)
+{
+	const int m = 16 * nlayers;
+	orc_mat4* dv = (orc_mat4*)malloc(nlayers * sizeof(orc_mat4));
+	orc_cplx* h1 = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	orc_cplx* h2 = (orc_cplx*)malloc((size_t)m * m * sizeof(orc_cplx));
+	int ret = blockenc_sums(2, hf, hd, vlist, nlayers, L, perms, fval, dv, h1, h2);
+	if (!ret) {
+		for (int l = 0; l < nlayers; l++) {
+			for (int e = 0; e < 16; e++) dv[l].data[e] = conj(dv[l].data[e]);
+			orc_tangent_to_real(&vlist[l], &dv[l], &grad_vec[16*l]);
+		}
+		for (int a = 0; a < nlayers; a++)
+			for (int b = a; b < nlayers; b++)
+				for (int k = 0; k < 16; k++) {
+					double r[16] = { 0 };
+					r[k] = 1;
+					orc_mat4 z, g;
+					orc_real_to_tangent(r, &vlist[b], &z);
+					for (int x = 0; x < 16; x++) {
+						orc_cplx s1 = 0, s2 = 0;
+						for (int y = 0; y < 16; y++) {
+							s1 += h1[hidx(nlayers, a, x, b, y)] * z.data[y];
+							s2 += h2[hidx(nlayers, a, x, b, y)] * z.data[y];
+						}
+						g.data[x] = conj(s1) + s2;
+					}
+					if (a == b) {
+						orc_mat4 p, gh, t;
+						orc_project_tangent(&vlist[a], &g, &p);
+						orc_adjoint(&dv[a], &gh);
+						orc_symmetric_triple_product(&z, &gh, &vlist[a], &t);
+						for (int e = 0; e < 16; e++) g.data[e] = p.data[e] - t.data[e];
+					}
+					orc_tangent_to_real(&vlist[a], &g, r);
+					for (int x = 0; x < 16; x++) H[hidx(nlayers, a, x, b, k)] = r[x];
+				}
+		for (int row = 0; row < m; row++)
+			for (int col = 0; col < row; col++) H[(long)row * m + col] = H[(long)col * m + row];
+	}
+	free(dv); free(h1); free(h2);
+	return ret;
+}

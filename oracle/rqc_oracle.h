@@ -164,6 +164,21 @@ void orc_optimize_brickwall_hmat_sampling(orc_linear_func uf, void* ud, const or
                                           const orc_rtr_params* params, int niter, double* f_iter, orc_mat4* vopt,
                                           int* accepted, int* on_boundary);
 
+/* ---- block-encoding target || P^dag W P - H ||_F^2 / 2 (src/target.c:1100-1720) ----
+ * hfunc applies H to states of nqubits / 2 qubits. */
+int  orc_blockenc_target(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int nqubits,
+                         const int* perms, double* fval);
+int  orc_blockenc_target_and_gradient(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers, int nqubits,
+                                      const int* perms, double* fval, orc_mat4* dvlist);
+int  orc_blockenc_target_and_gradient_vector(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers,
+                                             int nqubits, const int* perms, double* fval, double* grad_vec);
+int  orc_blockenc_target_gradient_hessian(orc_linear_func hf, void* hd, const orc_mat4* vlist, int nlayers,
+                                          int nqubits, const int* perms, double* fval, orc_mat4* dvlist,
+                                          orc_cplx* hess1, orc_cplx* hess2);
+int  orc_blockenc_target_gradient_vector_hessian_matrix(orc_linear_func hf, void* hd, const orc_mat4* vlist,
+                                                        int nlayers, int nqubits, const int* perms, double* fval,
+                                                        double* grad_vec, double* H);
+
 /* ---- targets used by tests and benchmarks ---- */
 /* matrix-free brickwall target U: udata points to orc_brickwall_udata */
 typedef struct { const orc_mat4* vlist; int nlayers; const int* perms; } orc_brickwall_udata;

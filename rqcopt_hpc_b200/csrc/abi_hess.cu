@@ -2,9 +2,9 @@
 // statevector arrays (src/statevector.h:39-49), the array gate kernels
 // (src/gate.h:13-19), the brickwall backward pass with Hessian and the gate
 // placeholder circuit (src/brickwall_circuit.h:17-22), the Hessian targets
-// (src/target.h:70-83) and the random-state sampling estimators with their
+// (src/target.h:70-83), the random-state sampling estimators with their
 // generator (src/target.h:14-17, 46-49, 74-77, 85-88; src/rng.h:21;
-// src/statevector.h:29).  Host buffers are staged through HBM; every call
+// src/statevector.h:29) and the block-encoding target (src/target.h:96-126).  Host buffers are staged through HBM; every call
 // synchronises before returning.
 #include <stdio.h>
 #include <string.h>
@@ -455,4 +455,102 @@ extern "C" int brickwall_unitary_target_sampling(linear_func ufunc, void* udata,
 	for (int k = 0; k < nlayers * per; k++)
 		memcpy(&g[16 * (size_t)k], &ug[16 * (size_t)(k / per)], 16 * sizeof(double2));
 	return sampled_value(fn, ufunc, udata, g, wires, nqubits, nsamples, rng, fval);
+}
+
+// ------------------------------------------------------------------ block-encoding target
+
+namespace {
+
+// mode 0: f; 1: f, dvlist / grad_vec; 2: f, dvlist, hess1, hess2 / grad_vec, H
+int blockenc(const char* fn, linear_func hfunc, void* hdata, const struct mat4x4 vlist[], int nlayers, int nqubits,
+             const int* perms[], int mode, double* fval, struct mat4x4* dvlist, double* grad_vec, numeric* hess1,
+             numeric* hess2, double* H)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	std::vector<double2> ug;
+	std::vector<int> wires;
+	TargetHolder th;
+	if (!fval || !brickwall_of(nqubits, nlayers, vlist, perms, ug, wires) || !th.set(hfunc, hdata, nqubits / 2))
+		return fail(fn, E_ARG);
+	const int m = 16 * nlayers;
+	const size_t nrec = hess_record_count(nlayers);
+	// device: record | hess2 | layer gates | gradient vector | real Hessian
+	int ret = ensure_device(rt->result, (nrec + (size_t)m * m + 16 * (size_t)nlayers) * sizeof(double2) +
+	                                        ((size_t)m + (size_t)m * m) * sizeof(double));
+	if (ret) return ret;
+	double2* rec = static_cast<double2*>(rt->result.ptr);
+	double2* d_h2 = rec + nrec;
+	double2* d_ug = d_h2 + (size_t)m * m;
+	double* d_grad = reinterpret_cast<double*>(d_ug + 16 * nlayers);
+	double* d_H = d_grad + m;
+	HessCircuit c;
+	c.L = nqubits;
+	c.nlayers = nlayers;
+	c.ugates = ug.data();
+	c.wires = wires.data();
+	if ((ret = blockenc_device(*rt, c, th.spec, mode, rec, d_h2))) return ret;
+	if (grad_vec) {
+		if ((ret = RQC_CUDA(cudaMemcpyAsync(d_ug, ug.data(), 16 * (size_t)nlayers * sizeof(double2), cudaMemcpyHostToDevice,
+		                                    rt->stream))))
+			return ret;
+		if ((ret = project_hessian_device(*rt, nlayers, d_ug, rec, d_grad, d_H, mode == 2 ? d_h2 : nullptr))) return ret;
+		if ((ret = d2h(*rt, grad_vec, d_grad, m * sizeof(double)))) return ret;
+		if (H && (ret = d2h(*rt, H, d_H, (size_t)m * m * sizeof(double)))) return ret;
+	}
+	if (dvlist && (ret = d2h(*rt, dvlist, rec + 1, 16 * (size_t)nlayers * sizeof(double2)))) return ret;
+	if (hess1 && (ret = d2h(*rt, hess1, rec + 1 + 16 * nlayers, (size_t)m * m * sizeof(double2)))) return ret;
+	if (hess2 && (ret = d2h(*rt, hess2, d_h2, (size_t)m * m * sizeof(double2)))) return ret;
+	double2 f;
+	if ((ret = d2h(*rt, &f, rec, sizeof(double2)))) return ret;
+	if ((ret = sync(*rt))) return ret;
+	*fval = f.x;
+	return OK;
+}
+
+}  // namespace
+
+extern "C" int brickwall_blockenc_target(linear_func hfunc, void* hdata, const struct mat4x4 vlist[], const int nlayers,
+                                         const int nqubits, const int* perms[], double* fval)
+{
+	return blockenc("brickwall_blockenc_target", hfunc, hdata, vlist, nlayers, nqubits, perms, 0, fval, nullptr, nullptr,
+	                nullptr, nullptr, nullptr);
+}
+
+extern "C" int brickwall_blockenc_target_and_gradient(linear_func hfunc, void* hdata, const struct mat4x4 vlist[],
+                                                      const int nlayers, const int nqubits, const int* perms[],
+                                                      double* fval, struct mat4x4 dvlist[])
+{
+	if (!dvlist) return fail("brickwall_blockenc_target_and_gradient", E_ARG);
+	return blockenc("brickwall_blockenc_target_and_gradient", hfunc, hdata, vlist, nlayers, nqubits, perms, 1, fval,
+	                dvlist, nullptr, nullptr, nullptr, nullptr);
+}
+
+extern "C" int brickwall_blockenc_target_and_gradient_vector(linear_func hfunc, void* hdata, const struct mat4x4 vlist[],
+                                                             const int nlayers, const int nqubits, const int* perms[],
+                                                             double* fval, double* grad_vec)
+{
+	if (!grad_vec) return fail("brickwall_blockenc_target_and_gradient_vector", E_ARG);
+	return blockenc("brickwall_blockenc_target_and_gradient_vector", hfunc, hdata, vlist, nlayers, nqubits, perms, 1,
+	                fval, nullptr, grad_vec, nullptr, nullptr, nullptr);
+}
+
+extern "C" int brickwall_blockenc_target_gradient_hessian(linear_func hfunc, void* hdata, const struct mat4x4 vlist[],
+                                                          const int nlayers, const int nqubits, const int* perms[],
+                                                          double* fval, struct mat4x4 dvlist[], numeric* hess1,
+                                                          numeric* hess2)
+{
+	if (!dvlist || !hess1 || !hess2) return fail("brickwall_blockenc_target_gradient_hessian", E_ARG);
+	return blockenc("brickwall_blockenc_target_gradient_hessian", hfunc, hdata, vlist, nlayers, nqubits, perms, 2, fval,
+	                dvlist, nullptr, hess1, hess2, nullptr);
+}
+
+extern "C" int brickwall_blockenc_target_gradient_vector_hessian_matrix(linear_func hfunc, void* hdata,
+                                                                        const struct mat4x4 vlist[], const int nlayers,
+                                                                        const int nqubits, const int* perms[],
+                                                                        double* fval, double* grad_vec, double* H)
+{
+	if (!grad_vec || !H) return fail("brickwall_blockenc_target_gradient_vector_hessian_matrix", E_ARG);
+	return blockenc("brickwall_blockenc_target_gradient_vector_hessian_matrix", hfunc, hdata, vlist, nlayers, nqubits,
+	                perms, 2, fval, nullptr, grad_vec, nullptr, nullptr, H);
 }

@@ -335,6 +335,117 @@ k_hlayer(const double2* __restrict__ psi, int64_t basis_b0, const double2* __res
 	}
 }
 
+// ------------------------------------------------------------------ block encoding
+
+// full-register index of half-register basis state b: bit i of b at bit 2 i + 1
+// (src/target.c:1148-1157)
+__host__ __device__ __forceinline__ int64_t blockenc_index(int64_t b, int half)
+{
+	int64_t c = 0;
+	for (int i = 0; i < half; i++) c |= ((b >> i) & 1) << (2 * i + 1);
+	return c;
+}
+
+// psi_0 of columns b0 .. b0 + ncols - 1: the basis states P e_b
+__global__ void k_benc_init(double2* __restrict__ states, int L, int64_t b0, int64_t ncols)
+{
+	const int64_t N = (int64_t)1 << L;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncols * N; i += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t c = i >> L, a = i & (N - 1);
+		states[i] = make_double2(a == blockenc_index(b0 + c, L / 2) ? 1.0 : 0.0, 0.0);
+	}
+}
+
+// residual d = P^dag W P e_b - H e_b on the P rows: f += |d|^2 / 2 (per block), chi = P conj(d)
+// (zero elsewhere: chi is cleared before).  hneg[b][a] = -conj((H e_b)[a]).
+__global__ void k_benc_residual(const double2* __restrict__ wout, const double2* __restrict__ hneg, int L, int64_t b0,
+                                int64_t ncols, double2* __restrict__ chi, double2* __restrict__ fpart)
+{
+	__shared__ double red[HT / 32];
+	const int half = L / 2;
+	const int64_t s = (int64_t)1 << half;
+	double acc = 0;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ncols * s; i += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t c = i >> half, a = i & (s - 1);
+		const int64_t idx = (c << L) + blockenc_index(a, half);
+		const double2 hn = hneg[(b0 + c) * s + a];
+		const double2 w = wout[idx];
+		const double dx = w.x + hn.x, dy = w.y - hn.y;   // w - H e_b with H e_b = -conj(hn)
+		acc += 0.5 * (dx * dx + dy * dy);
+		if (chi) chi[idx] = make_double2(dx, -dy);
+	}
+	acc = warp_sum(acc);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0;
+		for (int k = 0; k < HT / 32; k++) t += red[k];
+		fpart[blockIdx.x].x += t;
+	}
+}
+
+// Jacobian rows on the P rows: jac[t][c * s + a] = tan_t[c][P a]
+__global__ void k_benc_gather(const double2* __restrict__ tan, int L, int64_t ncols, int64_t sstride, int m,
+                              double2* __restrict__ jac)
+{
+	const int half = L / 2;
+	const int64_t s = (int64_t)1 << half, K = ncols * s;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)m * K; i += (int64_t)gridDim.x * blockDim.x) {
+		const int64_t t = i / K, r = i % K;
+		jac[i] = tan[t * sstride + ((r >> half) << L) + blockenc_index(r & (s - 1), half)];
+	}
+}
+
+// Gauss-Newton term: part2[(l i), (k j)] += sum_r conj(jac[l i][r]) jac[k j][r] for layer l >= k
+// (src/target.c:1570-1580); one block per entry
+__global__ void k_benc_gram(const double2* __restrict__ jac, int64_t K, int nl, double2* __restrict__ part2)
+{
+	__shared__ double red[2][HT / 32];
+	const int m = 16 * nl;
+	const int e = blockIdx.x;
+	const int row = e / m, col = e % m;
+	if ((row >> 4) < (col >> 4)) return;
+	const double2* __restrict__ x = jac + (int64_t)row * K;
+	const double2* __restrict__ y = jac + (int64_t)col * K;
+	double sx = 0, sy = 0;
+	for (int64_t r = threadIdx.x; r < K; r += HT) {
+		const double2 a = x[r], b = y[r];
+		sx += a.x * b.x + a.y * b.y;     // conj(a) b
+		sy += a.x * b.y - a.y * b.x;
+	}
+	sx = warp_sum(sx);
+	sy = warp_sum(sy);
+	if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = sx; red[1][threadIdx.x >> 5] = sy; }
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double tx = 0, ty = 0;
+		for (int k = 0; k < HT / 32; k++) { tx += red[0][k]; ty += red[1][k]; }
+		part2[e].x += tx;
+		part2[e].y += ty;
+	}
+}
+
+// hess2 from the lower blocks, upper blocks by conjugate symmetry; f from the residual parts
+__global__ void k_benc_finish(const double2* __restrict__ part2, int nl, const double2* __restrict__ fres, int nres,
+                              double2* __restrict__ rec, double2* __restrict__ hess2)
+{
+	const int m = 16 * nl;
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (int64_t)m * m; i += (int64_t)gridDim.x * blockDim.x) {
+		const int row = (int)(i / m), col = (int)(i % m);
+		if (!hess2) break;
+		if ((row >> 4) >= (col >> 4)) hess2[i] = part2[i];
+		else {
+			const double2 v = part2[(int64_t)col * m + row];
+			hess2[i] = make_double2(v.x, -v.y);
+		}
+	}
+	if (blockIdx.x == 0 && threadIdx.x == 0) {
+		double t = 0;
+		for (int k = 0; k < nres; k++) t += fres[k].x;
+		rec[0] = make_double2(t, 0.0);
+	}
+}
+
 // Sum over the blocks of partial slot (slot, entry e)
 __device__ __forceinline__ double2 slot_sum(const double* __restrict__ part, int nbx, size_t slot, int e)
 {
@@ -403,7 +514,7 @@ __global__ void __launch_bounds__(HT) k_happly(const double2* __restrict__ in, d
 // Column (b, k) entries of the real Hessian for layers a <= b (src/target.c:937-987), and
 // the gradient vector (src/target.c:1025-1030).  rec as written by k_hassemble.
 __global__ void k_hproject(int nl, const double2* __restrict__ ug, const double2* __restrict__ rec,
-                           double* __restrict__ grad, double* __restrict__ H)
+                           const double2* __restrict__ hess2, double* __restrict__ grad, double* __restrict__ H)
 {
 	const int m = 16 * nl;
 	const int npairs = nl * (nl + 1) / 2;
@@ -431,6 +542,12 @@ __global__ void k_hproject(int nl, const double2* __restrict__ ug, const double2
 		double2 s = c_(0, 0);
 		for (int y = 0; y < 16; y++) s = c_add(s, c_mul(row[y], z.a[y]));
 		g.a[x] = c_conj(s);
+		if (hess2) {   // block encoding: conj(hess1 Z) + hess2 Z (src/target.c:1673-1683)
+			const double2* row2 = hess2 + (size_t)(16 * a + x) * m + 16 * b;
+			double2 s2 = c_(0, 0);
+			for (int y = 0; y < 16; y++) s2 = c_add(s2, c_mul(row2[y], z.a[y]));
+			g.a[x] = c_add(g.a[x], s2);
+		}
 	}
 	if (a == b) {
 		M4 p, dc, gh, t;
@@ -600,6 +717,9 @@ struct Sweep
 	std::vector<Gate4<double>> gg, gt;
 	std::vector<WirePair> gw;
 
+	bool keep_final = false;   // carry the tangents through the last gate and store them (block encoding)
+	bool psi_only = false;     // gradient only: the psi blocks of the sweep
+
 	Sweep(Runtime& r, const HessCircuit& hc) : rt(r), c(hc), L(hc.L), nl(hc.nlayers), per(hc.L / 2),
 	                                           G(hc.nlayers * (hc.L / 2)), S(1 + 16 * hc.nlayers), nbx(1) {}
 
@@ -649,12 +769,12 @@ struct Sweep
 	{
 		const int a = q / per;
 		const bool last = q == G - 1;
-		const dim3 grid(1 + 16 * (a + 1), nbx);
+		const dim3 grid(psi_only ? 1 : 1 + 16 * (a + 1), nbx);
 		cudaEvent_t ev;
 		launch_begin(rt, KC_HESS, &ev);
 		k_hsweep<<<grid, HT, 0, rt.stream>>>(psi_in, basis_b0, last ? nullptr : psi_out, phi, tan, gg[a], gw[q], L,
-		                                     ngroups, sstride, a, q % per == 0 ? 1 : 0, last ? 0 : 1, part, S,
-		                                     (with_f && last) ? fpart : nullptr);
+		                                     ngroups, sstride, a, q % per == 0 ? 1 : 0, (last && !keep_final) ? 0 : 1, part,
+		                                     S, (with_f && last) ? fpart : nullptr);
 		launch_end(rt, KC_HESS, ev);
 		return RQC_CUDA(cudaGetLastError());
 	}
@@ -690,8 +810,8 @@ struct Sweep
 		lgts.q0 = a * per;
 		lgts.per = per;
 		for (int k = 0; k < per; k++) lgts.w[k] = gw[a * per + k];
-		const bool last = a == nl - 1;
-		const dim3 grid(1 + 16 * (a + 1), nbx);
+		const bool last = a == nl - 1 && !keep_final;
+		const dim3 grid(psi_only ? 1 : 1 + 16 * (a + 1), nbx);
 		cudaEvent_t ev;
 		launch_begin(rt, KC_HESS, &ev);
 		k_hlayer<<<grid, HT, HTILE * sizeof(double2), rt.stream>>>(psi, basis_b0, phi, tan, gg[a], lgts, L, ncols, sstride, a,
@@ -814,12 +934,111 @@ int hessian_single_device(Runtime& rt, const HessCircuit& c, const double2* d_ca
 	return sw.assemble(d_rec);
 }
 
+int blockenc_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, int mode, double2* d_rec, double2* d_hess2)
+{
+	const int L = c.L, nl = c.nlayers;
+	if (L < 2 || L % 2 || nl < 1 || mode < 0 || mode > 2) return E_ARG;
+	const int per = L / 2, G = nl * per, half = L / 2, m = 16 * nl;
+	const int64_t N = (int64_t)1 << L, s = (int64_t)1 << half;
+	const bool hess = mode == 2;
+	const bool layered = L <= 12 && per <= HMAXPER;
+	// states per column: phi_q of every gate; psi_q of every gate (layered) or two psi
+	// buffers and the input states; W P e_b; the tangents (Hessian only)
+	const int64_t nstates = G + (layered ? G : 3) + 1 + (hess ? 16 * (int64_t)nl : 0);
+	const size_t col_bytes = (size_t)nstates * N * sizeof(double2);
+	int64_t C = (int64_t)(hess_workspace_limit(rt) / col_bytes);
+	if (rt.column_chunk > 0) C = std::min<int64_t>(C, rt.column_chunk);
+	C = std::min(C, s);
+	if (C < 1) return E_ALLOC;
+	int ret = ensure_device(rt.work, (size_t)nstates * C * N * sizeof(double2));
+	if (ret) return ret;
+	double2* phi = reinterpret_cast<double2*>(rt.work.ptr);
+	const int64_t cs = C * N;
+	double2* P[2] = { phi + (int64_t)G * cs, phi + (int64_t)(G + 1) * cs };
+	double2* psi = phi + (int64_t)G * cs;
+	double2* states = layered ? psi : phi + (int64_t)(G + 2) * cs;
+	double2* wout = phi + (int64_t)(G + (layered ? G : 3)) * cs;
+	double2* tan = wout + cs;
+	auto phi_at = [&](int q) { return phi + (int64_t)q * cs; };
+	auto psi_at = [&](int q) { return psi + (int64_t)q * cs; };
+	// per evaluation: -conj(H e_b) for all b, target scratch, Jacobian rows, Gauss-Newton parts, f parts
+	const int nres = rt.num_sms * 2;
+	const size_t abytes = (3 * (size_t)s * s + (hess ? (size_t)m * C * s + (size_t)m * m : 0) + nres) * sizeof(double2);
+	if ((ret = ensure_device(rt.arrays, abytes))) return ret;
+	double2* hneg = static_cast<double2*>(rt.arrays.ptr);
+	double2* sc0 = hneg + s * s;
+	double2* sc1 = sc0 + s * s;
+	double2* jac = sc1 + s * s;
+	double2* part2 = hess ? jac + (size_t)m * C * s : jac;
+	double2* fres = hess ? part2 + (size_t)m * m : jac;
+	if ((ret = RQC_CUDA(cudaMemsetAsync(fres, 0, nres * sizeof(double2), rt.stream)))) return ret;
+	if (hess && (ret = RQC_CUDA(cudaMemsetAsync(part2, 0, (size_t)m * m * sizeof(double2), rt.stream)))) return ret;
+	if ((ret = target_columns_device(rt, t, half, 0, s, hneg, sc0, sc1))) return ret;
+
+	Sweep sw(rt, c);
+	sw.keep_final = hess;
+	sw.psi_only = mode == 1;
+	if (mode >= 1 && (ret = sw.init(cs / 4, layered ? (C + (HTILE >> L) - 1) / (HTILE >> L) : 0))) return ret;
+	if (mode == 0) {   // the gates and wires of the forward passes
+		sw.gg.resize(nl);
+		for (int l = 0; l < nl; l++) sw.gg[l] = gate_of(c.ugates + 16 * l, false);
+		sw.gw.resize(G);
+		for (int q = 0; q < G; q++) sw.gw[q] = make_pair_(L, c.wires[2 * q], c.wires[2 * q + 1]);
+	}
+	for (int64_t b0 = 0; b0 < s; b0 += C) {
+		const int64_t Cc = std::min(C, s - b0);
+		const int64_t ngroups = Cc * (N / 4);
+		const int agrid = grid_of(rt, ngroups, 8);
+		k_benc_init<<<grid_of(rt, Cc * N, 8), HT, 0, rt.stream>>>(states, L, b0, Cc);
+		if ((ret = checked(rt))) return ret;
+		// forward pass to W P e_b
+		if (layered && mode >= 1) {
+			if ((ret = sw.forward_chain(psi_at, ngroups, -1))) return ret;
+			k_happly<<<agrid, HT, 0, rt.stream>>>(psi_at(G - 1), wout, sw.gg[(G - 1) / per], sw.gw[G - 1], L, ngroups);
+			if ((ret = checked(rt))) return ret;
+		} else {
+			const double2* in = states;
+			for (int q = 0; q < G; q++) {
+				double2* o = q == G - 1 ? wout : P[q & 1];
+				k_happly<<<agrid, HT, 0, rt.stream>>>(in, o, sw.gg[q / per], sw.gw[q], L, ngroups);
+				if ((ret = checked(rt))) return ret;
+				in = o;
+			}
+		}
+		double2* chi = mode >= 1 ? phi_at(G - 1) : nullptr;
+		if (chi && (ret = RQC_CUDA(cudaMemsetAsync(chi, 0, (size_t)Cc * N * sizeof(double2), rt.stream)))) return ret;
+		k_benc_residual<<<nres, HT, 0, rt.stream>>>(wout, hneg, L, b0, Cc, chi, fres);
+		if ((ret = checked(rt))) return ret;
+		if (mode == 0) continue;
+		if ((ret = sw.reverse_chain(phi_at, ngroups, nullptr))) return ret;
+		if (layered) {
+			for (int a = 0; a < nl; a++)
+				if ((ret = sw.layer(a, psi, -1, phi, tan, Cc, cs, false))) return ret;
+		} else {
+			for (int q = 0; q < G; q++) {
+				const double2* in = q == 0 ? states : P[(q - 1) & 1];
+				if ((ret = sw.gate(q, in, -1, P[q & 1], phi_at(q), tan, ngroups, cs, false))) return ret;
+			}
+		}
+		if (hess) {
+			k_benc_gather<<<grid_of(rt, (int64_t)m * Cc * s, 8), HT, 0, rt.stream>>>(tan, L, Cc, cs, m, jac);
+			if ((ret = checked(rt))) return ret;
+			k_benc_gram<<<m * m, HT, 0, rt.stream>>>(jac, Cc * s, nl, part2);
+			if ((ret = checked(rt))) return ret;
+		}
+	}
+	if (mode >= 1 && (ret = sw.assemble(d_rec))) return ret;
+	k_benc_finish<<<grid_of(rt, (int64_t)m * m, 4), HT, 0, rt.stream>>>(part2, nl, fres, nres, d_rec,
+	                                                                     hess ? d_hess2 : nullptr);
+	return checked(rt);
+}
+
 int project_hessian_device(Runtime& rt, int nlayers, const double2* d_ugates, const double2* d_rec, double* d_grad,
-                           double* d_H)
+                           double* d_H, const double2* d_hess2)
 {
 	const int m = 16 * nlayers;
 	const int n = std::max(nlayers, 16 * nlayers * (nlayers + 1) / 2);
-	k_hproject<<<(n + 63) / 64, 64, 0, rt.stream>>>(nlayers, d_ugates, d_rec, d_grad, d_H);
+	k_hproject<<<(n + 63) / 64, 64, 0, rt.stream>>>(nlayers, d_ugates, d_rec, d_hess2, d_grad, d_H);
 	int ret = checked(rt);
 	if (ret) return ret;
 	k_hmirror<<<grid_of(rt, (int64_t)m * m, 4), HT, 0, rt.stream>>>(m, d_H);

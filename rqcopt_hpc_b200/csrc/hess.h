@@ -38,8 +38,14 @@ int hessian_single_device(Runtime& rt, const HessCircuit& c, const double2* d_ca
 
 // Riemannian gradient vector and real Hessian matrix from a record (src/target.c:937-1035);
 // d_ugates: the layer gates on the device.
+// With d_hess2 (block encoding) the projected matrix is that of conj(hess1 Z) + hess2 Z.
 int project_hessian_device(Runtime& rt, int nlayers, const double2* d_ugates, const double2* d_rec, double* d_grad,
-                           double* d_H);
+                           double* d_H, const double2* d_hess2 = nullptr);
+
+// Block-encoding target || P^dag W P - H ||_F^2 / 2 (src/target.c:1100-1623), H given by t on
+// L/2 qubits.  mode 0: f; 1: f and gradients; 2: f, gradients, hess1 (in the record) and
+// hess2 (m x m, device, may be null otherwise).  The record's f slot holds f (real).
+int blockenc_device(Runtime& rt, const HessCircuit& c, const TargetSpec& t, int mode, double2* d_rec, double2* d_hess2);
 
 // Truncated CG on a dense n x n Hessian in one single-block kernel; d_status[0]
 // receives 1 if the solution stopped on the trust-region boundary.

@@ -92,6 +92,11 @@ _SIGS = {
     "truncated_cg_hmat": (C.c_bool, [VP, VP, I, D, C.POINTER(TruncatedCGParams), VP]),
     "riemannian_trust_region_optimize_hmat": (None, [VP, VP, VP, VP, VP, I, VP, I, C.POINTER(RTRParams), I, VP, VP]),
     "optimize_brickwall_circuit_hmat": (None, [VP, VP, VP, I, I, VP, C.POINTER(RTRParams), I, VP, VP]),
+    "brickwall_blockenc_target": (I, [VP, VP, VP, I, I, VP, VP]),
+    "brickwall_blockenc_target_and_gradient": (I, [VP, VP, VP, I, I, VP, VP, VP]),
+    "brickwall_blockenc_target_and_gradient_vector": (I, [VP, VP, VP, I, I, VP, VP, VP]),
+    "brickwall_blockenc_target_gradient_hessian": (I, [VP, VP, VP, I, I, VP, VP, VP, VP, VP]),
+    "brickwall_blockenc_target_gradient_vector_hessian_matrix": (I, [VP, VP, VP, I, I, VP, VP, VP, VP]),
     "seed_rng_state": (None, [C.c_uint64, C.POINTER(RngState)]),
     "haar_random_statevector": (None, [PSV, C.POINTER(RngState)]),
     "circuit_unitary_target_sampling": (I, [VP, VP, VP, I, VP, I, C.c_long, C.POINTER(RngState), VP]),
@@ -528,6 +533,48 @@ def brickwall_unitary_target_gradient_vector_hessian_matrix(target, vlist, perms
            lib().brickwall_unitary_target_gradient_vector_hessian_matrix(target.ufunc, target.udata, ptr(vlist), nl,
                                                                          nqubits, C.cast(pp, VP), ptr(f), ptr(g), ptr(H)))
     return f[0], g, H
+
+
+# ------------------------------------------------------------------------ block-encoding target
+# || P^dag W P - H ||_F^2 / 2 with H (`target`) acting on nqubits / 2 qubits.
+
+def _blockenc(name, target, vlist, perms, nqubits, outs):
+    vlist = cplx(vlist)
+    pp, keep = perm_pointers(perms)
+    f = np.zeros(1)
+    _check(name, getattr(lib(), name)(target.ufunc, target.udata, ptr(vlist), vlist.shape[0], nqubits, C.cast(pp, VP),
+                                      ptr(f), *[ptr(o) for o in outs]))
+    return (f[0],) + tuple(outs)
+
+
+def brickwall_blockenc_target(target, vlist, perms, nqubits):
+    return _blockenc("brickwall_blockenc_target", target, vlist, perms, nqubits, [])[0]
+
+
+def brickwall_blockenc_target_and_gradient(target, vlist, perms, nqubits):
+    nl = np.shape(vlist)[0]
+    return _blockenc("brickwall_blockenc_target_and_gradient", target, vlist, perms, nqubits,
+                     [np.empty((nl, 4, 4), np.complex128)])
+
+
+def brickwall_blockenc_target_and_gradient_vector(target, vlist, perms, nqubits):
+    nl = np.shape(vlist)[0]
+    return _blockenc("brickwall_blockenc_target_and_gradient_vector", target, vlist, perms, nqubits, [np.empty(16 * nl)])
+
+
+def brickwall_blockenc_target_gradient_hessian(target, vlist, perms, nqubits):
+    nl = np.shape(vlist)[0]
+    m = 16 * nl
+    return _blockenc("brickwall_blockenc_target_gradient_hessian", target, vlist, perms, nqubits,
+                     [np.empty((nl, 4, 4), np.complex128), np.empty((m, m), np.complex128),
+                      np.empty((m, m), np.complex128)])
+
+
+def brickwall_blockenc_target_gradient_vector_hessian_matrix(target, vlist, perms, nqubits):
+    nl = np.shape(vlist)[0]
+    m = 16 * nl
+    return _blockenc("brickwall_blockenc_target_gradient_vector_hessian_matrix", target, vlist, perms, nqubits,
+                     [np.empty(m), np.empty((m, m))])
 
 
 # ------------------------------------------------------------------------ sampling estimator

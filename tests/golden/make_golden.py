@@ -32,6 +32,10 @@ FIXTURES = [
     # sampling estimator
     "brickwall_unitary_target_sampling", "brickwall_unitary_target_gradient_hessian_sampling",
     "brickwall_unitary_target_gradient_vector_hessian_matrix_sampling",
+    # block-encoding target
+    "brickwall_blockenc_target", "brickwall_blockenc_target_and_gradient",
+    "brickwall_blockenc_target_and_gradient_vector", "brickwall_blockenc_target_gradient_hessian",
+    "brickwall_blockenc_target_gradient_vector_hessian_matrix",
 ]
 
 

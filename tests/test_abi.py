@@ -43,12 +43,30 @@ def test_header_compiles(tmp_path, lang):
     subprocess.run([cc, "-fsyntax-only", "-Wall", "-I" + os.path.dirname(HEADER), str(src)], check=True)
 
 
+def _complex_branch(text):
+    """Keep the COMPLEX_CIRCUIT branch of `#ifdef COMPLEX_CIRCUIT ... [#else ...] #endif`
+    blocks (the build this library mirrors); the reference does not nest them."""
+    out, state = [], None
+    for line in text.split("\n"):
+        d = line.strip()
+        if d.startswith("#ifdef COMPLEX_CIRCUIT"):
+            state = "keep"
+        elif state and d.startswith("#else"):
+            state = "skip"
+        elif state and d.startswith("#endif"):
+            state = None
+        elif state != "skip":
+            out.append(line)
+    return "\n".join(out)
+
+
 def _ref_prototypes():
     protos = {}
     for fn in os.listdir(REF_SRC):
         if fn.endswith(".h"):
             text = open(os.path.join(REF_SRC, fn)).read()
             text = re.sub(r"//.*", "", text)
+            text = _complex_branch(text)
             for m in re.finditer(r"^([A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\))\s*;", text, flags=re.M):
                 if not m.group(1).startswith("typedef"):
                     protos[m.group(2)] = m.group(1)

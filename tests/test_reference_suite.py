@@ -367,3 +367,59 @@ def test_brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(impl):
     assert abs(f - f_ref) / abs(f_ref) <= 0.2
     assert np.max(np.abs(g - g_ref)) <= 0.3
     assert np.max(np.abs(H - H_ref)) <= 0.4
+
+
+# ------------------------------------------------------------------ block-encoding target
+# test_target.c:1578-2160: H is the synthetic map on nqubits / 2 qubits
+
+def test_brickwall_blockenc_target(impl):
+    d = golden("brickwall_blockenc_target")
+    t = impl.target("fixture")
+    vlist, perms = stack(d, "V", 5), stack(d, "perm", 5)
+    for k, nl in enumerate([4, 5]):
+        assert abs(impl.brickwall_blockenc_target(t, vlist[:nl], perms[:nl], 8) - d[f"f{k}"]) <= 1e-12
+
+
+def test_brickwall_blockenc_target_and_gradient(impl):
+    d = golden("brickwall_blockenc_target_and_gradient")
+    t = impl.target("fixture")
+    vlist, perms = stack(d, "V", 5), stack(d, "perm", 5)
+    for k, nl in enumerate([4, 5]):
+        f, dv = impl.brickwall_blockenc_target_and_gradient(t, vlist[:nl], perms[:nl], 8)
+        assert abs(f - d[f"f{k}"]) <= 1e-12
+        assert udist(dv, d[f"dVlist{k}"]) <= 1e-12
+        # f is real: the gradient convention is twice the Wirtinger derivative (test_target.c:1724-1729)
+        num = 2 * num_grad_wirtinger(lambda v: impl.brickwall_blockenc_target(t, v, perms[:nl], 8), vlist[:nl])
+        assert udist(dv, num) <= 1e-8
+
+
+def test_brickwall_blockenc_target_and_gradient_vector(impl):
+    d = golden("brickwall_blockenc_target_and_gradient_vector")
+    t = impl.target("fixture")
+    f, g = impl.brickwall_blockenc_target_and_gradient_vector(t, stack(d, "V", 3), stack(d, "perm", 3), 6)
+    assert abs(f - d["f"]) <= 1e-12
+    assert np.max(np.abs(g - d["grad"])) <= 1e-14
+
+
+def test_brickwall_blockenc_target_gradient_hessian(impl):
+    d = golden("brickwall_blockenc_target_gradient_hessian")
+    t = impl.target("fixture")
+    vlist, perms = stack(d, "V", 5), stack(d, "perm", 5)
+    for k, nl in enumerate([4, 5]):
+        f, dv, h1, h2 = impl.brickwall_blockenc_target_gradient_hessian(t, vlist[:nl], perms[:nl], 6)
+        assert udist(h1, h1.T) <= 1e-12
+        assert udist(h2, h2.conj().T) <= 1e-12
+        assert abs(f - d[f"f{k}"]) <= 1e-12
+        assert udist(dv, d[f"dVlist{k}"]) <= 1e-12
+        assert udist(h1, d[f"hess1_{k}"]) <= 1e-12
+        assert udist(h2, d[f"hess2_{k}"]) <= 1e-12
+
+
+def test_brickwall_blockenc_target_gradient_vector_hessian_matrix(impl):
+    d = golden("brickwall_blockenc_target_gradient_vector_hessian_matrix")
+    t = impl.target("fixture")
+    f, g, H = impl.brickwall_blockenc_target_gradient_vector_hessian_matrix(t, stack(d, "V", 5), stack(d, "perm", 5), 6)
+    assert abs(f - d["f"]) <= 1e-12
+    assert np.max(np.abs(g - d["grad"])) <= 1e-14
+    assert np.max(np.abs(H - H.T)) <= 1e-14
+    assert np.max(np.abs(H - d["H"])) <= 1e-13
