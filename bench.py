@@ -294,6 +294,23 @@ def _ref_sampling_worker(args):
     return time.perf_counter() - t0
 
 
+def _benc_case(L, depth, hdepth):
+    """Block-encoding workload: brickwall gates seed 10, H a brickwall of depth hdepth on L/2
+    qubits (seed 11)."""
+    vlist, perms, _, _, _ = workload(L, depth, 1)
+    hv, hp, _, _, _ = workload(L // 2, hdepth, 1, seed=11)
+    return vlist, perms, hv, hp
+
+
+def _ref_blockenc_worker(args):
+    L, depth, hdepth, b0, b1 = args
+    from oracle.oracle import Reference
+    vlist, perms, hv, hp = _benc_case(L, depth, hdepth)
+    t0 = time.perf_counter()
+    Reference().blockenc_hessian_columns(vlist, perms, L, hv, hp, b0, b1)
+    return time.perf_counter() - t0
+
+
 def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
     """Full-Hessian ("hmat") path.  (1) The reference's own Hessian benchmark
     (examples/benchmark/benchmark_16_qubits.c): brickwall_unitary_forward plus
@@ -418,8 +435,36 @@ def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
           "samples_per_s_e2e": ns / wall, "ms_per_call": wall * 1e3, "sweep_ms": hs_ms, "gpu_launches": launches,
           "roofline": roofline(hess_model(L, depth, False), ns, L, hs_ms, hs_n)}
     out["sampling_L14"] = r4
+
+    # (5) block-encoding target: gradient vector and Hessian matrix
+    L, depth, hdepth = 12, 9, 3
+    vlist, perms, hv, hp = _benc_case(L, depth, hdepth)
+    th = gpu.Target(brickwall=(hv, hp))
+
+    def benc():
+        return gpu.brickwall_blockenc_target_gradient_vector_hessian_matrix(th, vlist, perms, L)
+
+    benc()
+    _, wall, dev_ms, hs_ms, hs_n, launches = timed(benc, steps)
+    r5 = {"workload": f"block encoding || P^dag W P - H ||_F^2 / 2: f + gradient vector + Hessian matrix, brickwall "
+                      f"L={L} depth {depth}, H a brickwall of depth {hdepth} on {L // 2} qubits, all {1 << (L // 2)} "
+                      f"columns", "evals_per_s_e2e": 1.0 / wall, "ms_per_call": wall * 1e3, "sweep_ms": hs_ms,
+          "gpu_launches": launches}
+    out["blockenc_L12"] = r5
     if not have_ref:
         return out
+    cores = os.cpu_count() or 1
+    s_cols = 1 << (L // 2)
+    with mp.get_context("spawn").Pool(cores) as pool:
+        t0 = time.perf_counter()
+        pool.map(_ref_blockenc_worker, [(L, depth, hdepth, k, k + 1) for k in range(min(cores, s_cols))])
+        tref = time.perf_counter() - t0
+    v = (min(cores, s_cols) / s_cols) / tref
+    r5["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": min(cores, s_cols), "kind": "reference",
+                          "sample": f"{min(cores, s_cols)} of {s_cols} columns (one per core) through the reference's "
+                                    f"block-encoding Hessian column loop, {tref:.1f} s wall; evals/s = sampled "
+                                    f"fraction / wall time"}
+    r5["speedup_e2e"] = (1.0 / wall) / v
 
     cores = os.cpu_count() or 1
     with mp.get_context("spawn").Pool(cores) as pool:

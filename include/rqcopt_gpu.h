@@ -410,6 +410,16 @@ struct rqcopt_circuit_target
 };
 int rqcopt_circuit_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out);
 
+/* Dense row-major 2^nqubits x 2^nqubits target (the Python module's U, whose `ufunc` is
+ * a zgemv, pymodule/rqcopt_module.c:16-28): psi_out = U psi on the host; a basis
+ * vector (one entry 1, all others 0) costs one column copy instead of the product. */
+struct rqcopt_dense_target
+{
+	const numeric* u;
+	int nqubits;
+};
+int rqcopt_dense_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out);
+
 /* precision of the basis-column passes */
 enum rqcopt_precision
 {

@@ -74,6 +74,19 @@ def ensure_built():
         subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
 
 
+def reference_module():
+    """The reference's Python module (pymodule/rqcopt_module.c) built in _ref, or None."""
+    import glob
+    import importlib.util
+    found = glob.glob(os.path.join(HERE, "_ref", "rqcopt_hpc.*.so"))
+    if not found:
+        return None
+    spec = importlib.util.spec_from_file_location("rqcopt_hpc", found[0])
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def default_rtr(n):
     return RtrParams(TcgParams(2 * n, 1e-8, 1e-6), 0.125, 0.01, 0.1)
 
@@ -717,3 +730,12 @@ class Reference:
                                        _p(f), *[(_p(x) if x is not None else None) for x in o])
         assert ret == 0
         return (f[0],) + tuple(x for x in o if x is not None)
+
+    def blockenc_hessian_columns(self, vlist, perms, L, hvlist, hperms, b0, b1):
+        """f of the block-encoding Hessian column loop over half-register columns [b0, b1)."""
+        vlist, perms, hvlist, hperms = _c(vlist), _i(perms), _c(hvlist), _i(hperms)
+        f = np.zeros(1)
+        ret = self.lib.refdrv_blockenc_hessian_columns(_p(vlist), vlist.shape[0], _p(perms), L, _p(hvlist),
+                                                       hvlist.shape[0], _p(hperms), L_(b0), L_(b1), _p(f))
+        assert ret == 0
+        return f[0]

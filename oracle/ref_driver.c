@@ -335,3 +335,74 @@ int refdrv_blockenc(int mode, const struct mat4x4* vlist, int nlayers, const int
 	free(p); free(hp);
 	return ret;
 }
+
+/*
+ * The column loop of brickwall_blockenc_target_gradient_hessian (src/target.c:1441-1600)
+ * restricted to columns [b0, b1) of the half register, with a brickwall H on L/2 qubits,
+ * through the reference's brickwall_unitary_forward, brickwall_unitary_backward_hessian and
+ * apply_brickwall_unitary_gate_placeholder, so that a bounded sample can be timed.
+ */
+int refdrv_blockenc_hessian_columns(const struct mat4x4* vlist, int nlayers, const int* perms_flat, int L,
+                                    const struct mat4x4* hvlist, int hnlayers, const int* hperms_flat, long b0, long b1,
+                                    double* fval)
+{
+	const int** p = perm_ptrs(perms_flat, nlayers, L);
+	const int** hp = perm_ptrs(hperms_flat, hnlayers, L / 2);
+	struct refdrv_brickwall hop = { hvlist, hnlayers, hp };
+	const int half = L / 2, m = 16 * nlayers;
+	const intqs s = (intqs)1 << half, n = (intqs)1 << L;
+	struct statevector psi, hpsi, chi, wchi;
+	allocate_statevector(half, &psi);
+	allocate_statevector(half, &hpsi);
+	allocate_statevector(L, &chi);
+	allocate_statevector(L, &wchi);
+	struct quantum_circuit_cache cache;
+	int ret = allocate_quantum_circuit_cache(L, nlayers * (L / 2), &cache);
+	struct statevector_array tmp;
+	allocate_statevector_array(L, 16, &tmp);
+	struct mat4x4* dv = malloc(nlayers * sizeof(struct mat4x4));
+	numeric* h1 = malloc((size_t)m * m * sizeof(numeric));
+	numeric* phi = malloc((size_t)nlayers * s * 16 * sizeof(numeric));
+	numeric* h2 = calloc((size_t)m * m, sizeof(numeric));
+	double f = 0;
+	for (long b = b0; b < b1 && !ret; b++) {
+		memset(psi.data, 0, s * sizeof(numeric));
+		psi.data[b] = 1;
+		refdrv_brickwall_ufunc(&psi, &hop, &hpsi);
+		memset(chi.data, 0, n * sizeof(numeric));
+		intqs c = 0;
+		for (int i = 0; i < half; i++) { intqs t = b & ((intqs)1 << i); c += 2 * t * t; }
+		chi.data[c] = 1;
+		if ((ret = brickwall_unitary_forward(vlist, nlayers, p, &chi, &cache, &wchi)) < 0) break;
+		memset(chi.data, 0, n * sizeof(numeric));
+		for (intqs a = 0; a < s; a++) {
+			intqs ca = 0;
+			for (int i = 0; i < half; i++) { intqs t = a & ((intqs)1 << i); ca += 2 * t * t; }
+			const numeric d = wchi.data[ca] - hpsi.data[a];
+			f += 0.5 * (creal(d) * creal(d) + cimag(d) * cimag(d));
+			chi.data[ca] = conj(d);
+		}
+		if ((ret = brickwall_unitary_backward_hessian(vlist, nlayers, p, &cache, &chi, &wchi, dv, h1)) < 0) break;
+		for (int l = 0; l < nlayers; l++) {
+			if ((ret = apply_brickwall_unitary_gate_placeholder(vlist, nlayers, p, l, &cache, &tmp)) < 0) break;
+			for (intqs a = 0; a < s; a++) {
+				intqs ca = 0;
+				for (int i = 0; i < half; i++) { intqs t = a & ((intqs)1 << i); ca += 2 * t * t; }
+				memcpy(&phi[((size_t)l * s + a) * 16], &tmp.data[ca * 16], 16 * sizeof(numeric));
+			}
+		}
+		for (int l = 0; l < nlayers; l++)
+			for (int k = 0; k <= l; k++)
+				for (intqs a = 0; a < s; a++)
+					for (int i = 0; i < 16; i++)
+						for (int j = 0; j < 16; j++)
+							h2[((l*16 + i)*nlayers + k)*16 + j] += conj(phi[((size_t)l * s + a) * 16 + i]) * phi[((size_t)k * s + a) * 16 + j];
+	}
+	*fval = f;
+	free(dv); free(h1); free(phi); free(h2);
+	free_statevector_array(&tmp);
+	free_quantum_circuit_cache(&cache);
+	free_statevector(&psi); free_statevector(&hpsi); free_statevector(&chi); free_statevector(&wchi);
+	free(p); free(hp);
+	return ret;
+}

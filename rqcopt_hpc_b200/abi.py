@@ -83,6 +83,11 @@ class BrickwallTarget(C.Structure):
     _fields_ = [("vlist", C.c_void_p), ("nlayers", C.c_int), ("perms", C.POINTER(C.POINTER(C.c_int)))]
 
 
+class DenseTarget(C.Structure):
+    """struct rqcopt_dense_target: a dense row-major 2^n x 2^n target matrix."""
+    _fields_ = [("u", C.c_void_p), ("nqubits", C.c_int)]
+
+
 class CircuitTarget(C.Structure):
     """struct rqcopt_circuit_target: matrix-free general-circuit target evaluated on the device."""
     _fields_ = [("gates", C.c_void_p), ("ngates", C.c_int), ("wires", C.POINTER(C.c_int))]

@@ -28,6 +28,38 @@ extern "C" int rqcopt_circuit_ufunc(const struct statevector* psi, void* udata, 
 	return apply_quantum_circuit(t->gates, t->ngates, t->wires, psi, psi_out);
 }
 
+extern "C" int rqcopt_dense_ufunc(const struct statevector* psi, void* udata, struct statevector* psi_out)
+{
+	const struct rqcopt_dense_target* t = static_cast<const struct rqcopt_dense_target*>(udata);
+	if (!t || !t->u || !psi || !psi_out || psi->nqubits != t->nqubits || psi_out->nqubits != t->nqubits) return -1;
+	const int64_t n = (int64_t)1 << t->nqubits;
+	const double2* u = reinterpret_cast<const double2*>(t->u);
+	const double2* x = reinterpret_cast<const double2*>(psi->data);
+	double2* y = reinterpret_cast<double2*>(psi_out->data);
+	// a basis vector selects one column of U
+	int64_t one = -1;
+	bool basis = true;
+	for (int64_t j = 0; j < n && basis; j++) {
+		if (x[j].x == 0 && x[j].y == 0) continue;
+		if (x[j].x == 1 && x[j].y == 0 && one < 0) one = j;
+		else basis = false;
+	}
+	if (basis && one >= 0) {
+		for (int64_t r = 0; r < n; r++) y[r] = u[r * n + one];
+		return 0;
+	}
+	for (int64_t r = 0; r < n; r++) {
+		double sx = 0, sy = 0;
+		for (int64_t c = 0; c < n; c++) {
+			const double2 a = u[r * n + c], b = x[c];
+			sx += a.x * b.x - a.y * b.y;
+			sy += a.x * b.y + a.y * b.x;
+		}
+		y[r] = make_double2(sx, sy);
+	}
+	return 0;
+}
+
 namespace rqc {
 
 bool Problem::set_brickwall(int L_, int nlayers, const struct mat4x4* vlist, const struct mat4x4* vdirs,

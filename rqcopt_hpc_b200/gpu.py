@@ -20,7 +20,7 @@ import os
 import numpy as np
 
 from .abi import (HVP_FUNC, LINEAR_FUNC, RETRACT_FUNC, TARGET_FUNC, TARGET_GRAD_FUNC, TARGET_GRAD_HESS_FUNC,
-                  BrickwallTarget, CircuitTarget, QuantumCircuitCache, RngState, RTRParams, Statevector,
+                  BrickwallTarget, CircuitTarget, DenseTarget, QuantumCircuitCache, RngState, RTRParams, Statevector,
                   StatevectorArray,
                   TruncatedCGParams, cplx, default_rtr_params, default_tcg_params, ints, perm_pointers, ptr,
                   wrap_ufunc)
@@ -109,6 +109,7 @@ _SIGS = {
                                                         C.POINTER(RTRParams), I, VP, VP]),
     "rqcopt_brickwall_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_circuit_ufunc": (I, [PSV, VP, PSV]),
+    "rqcopt_dense_ufunc": (I, [PSV, VP, PSV]),
     "rqcopt_gpu_set_precision": (I, [I]),
     "rqcopt_gpu_get_precision": (I, []),
     "rqcopt_gpu_set_refine_threshold": (None, [D]),
@@ -372,11 +373,21 @@ def apply_brickwall_unitary_gate_placeholder(vlist, perms, l, cache):
 
 class Target:
     """A target U for the basis-column sums: a Python callable (host callback, one
-    call per column), or a device-native brickwall / circuit target."""
+    call per column), a device-native brickwall / circuit target, or a dense matrix
+    (library host target: a basis column is a column copy)."""
 
-    def __init__(self, fn=None, brickwall=None, circuit=None):
+    def __init__(self, fn=None, brickwall=None, circuit=None, dense=None):
         self._keep = []
-        if fn is not None:
+        if dense is not None:
+            u = cplx(dense)
+            n = int(u.shape[0]).bit_length() - 1
+            if u.ndim != 2 or u.shape[0] != u.shape[1] or 1 << n != u.shape[0]:
+                raise ValueError("dense target must be a 2^n x 2^n matrix")
+            self.desc = DenseTarget(u.ctypes.data, n)
+            self._keep.append(u)
+            self.ufunc = C.cast(lib().rqcopt_dense_ufunc, VP)
+            self.udata = C.cast(C.pointer(self.desc), VP)
+        elif fn is not None:
             self.cb = wrap_ufunc(fn)
             self.ufunc = C.cast(self.cb, VP)
             self.udata = None
