@@ -88,3 +88,20 @@ def test_full_hessian_oracle_matches_reference(oracle, ref):
     fo, vo, acc, bnd = oracle.optimize_brickwall_circuit_hmat(t, vlist, perms, 8, 3)
     fr2, vr2 = ref.optimize_brickwall_hmat(vlist, perms, 8, tvlist, tperms, 3)
     assert rel_err(fo, fr2) <= 1e-13 and rel_err(vo, vr2) <= 1e-13
+
+
+def test_blockenc_oracle_matches_reference(oracle, ref):
+    """Block-encoding target, H a depth-2 brickwall on 4 of the 8 qubits: f, gradients,
+    both complex Hessians and the projected matrix."""
+    from helpers import periodic_perms
+    vlist, perms, _, _ = brickwall_instance(8, 3, 4, 1, 5)
+    hv, _, _, _ = brickwall_instance(4, 2, 6, 1, 7)
+    hp = periodic_perms(4, 2)
+    t = oracle.target("brickwall", (hv, hp))
+    f, dv, h1, h2 = oracle.brickwall_blockenc_target_gradient_hessian(t, vlist, perms, 8)
+    fr, dvr, h1r, h2r = ref.blockenc(3, vlist, perms, 8, hv, hp)
+    assert abs(f - fr) <= 1e-14 * abs(fr) and rel_err(dv, dvr) <= 1e-14
+    assert rel_err(h1, h1r) <= 1e-14 and rel_err(h2, h2r) <= 1e-14
+    f, g, H = oracle.brickwall_blockenc_target_gradient_vector_hessian_matrix(t, vlist, perms, 8)
+    fr, gr, Hr = ref.blockenc(4, vlist, perms, 8, hv, hp)
+    assert abs(f - fr) <= 1e-14 * abs(fr) and rel_err(g, gr) <= 1e-14 and rel_err(H, Hr) <= 1e-14
