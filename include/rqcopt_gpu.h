@@ -448,6 +448,12 @@ int rqcopt_gpu_set_gates_per_pass(int gates);
 /* last error recorded by a void function (0 if none); reading clears it */
 int rqcopt_gpu_last_error(void);
 
+/* Haar-random sample states with real normal entries, one draw of randn() per
+ * amplitude as in the reference's real build (src/statevector.c:115-121), instead
+ * of complex ones; used by librqcopt_gpu_real.so (rqcopt_gpu_real.h) around its
+ * sampling calls.  The generator state advances by 2 instead of 4 steps per amplitude. */
+void rqcopt_gpu_set_real_samples(int on);
+
 /* number of kernels this library launched since the counter was last reset */
 unsigned long long rqcopt_gpu_launch_count(void);
 void rqcopt_gpu_reset_launch_count(void);

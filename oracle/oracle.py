@@ -739,3 +739,375 @@ class Reference:
                                                        hvlist.shape[0], _p(hperms), L_(b0), L_(b1), _p(f))
         assert ret == 0
         return f[0]
+
+
+# ---------------------------------------------------------------------------- real build
+# The reference compiled without COMPLEX_CIRCUIT (src/config.h:14-22): real states and
+# gates, 6 tangent parameters per gate (src/matrix.c:245-271, 288-300), one real normal
+# per amplitude of a sample state (src/statevector.c:115-121).
+
+REAL_REF_LIB = os.path.join(HERE, "_ref", "librqcopt_ref_real.so")
+_UPPER = (1, 2, 3, 6, 7, 11)
+TARGET_FUNC = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p)
+TARGET_GRAD_FUNC = C.CFUNCTYPE(C.c_double, C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double))
+RETRACT_FUNC = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_void_p, C.POINTER(C.c_double))
+
+
+def real_fixture_map(x):
+    """The reference tests' synthetic target map in the real build (test/test_target.c:26-27)."""
+    n = x.shape[0]
+    i = np.arange(n)
+    return -1.1 * x[((i + 3) * 113) % n] - 0.7 * x[((i + 9) * 173) % n] + 0.5 * x[i] + 0.3 * x[((i + 4) * 199) % n]
+
+
+def real_antisymm(r6):
+    """6 reals -> real antisymmetric 4x4 matrix, isometrically (src/matrix.c:245-271)."""
+    w = np.zeros((4, 4))
+    for k, e in enumerate(_UPPER):
+        w[e // 4, e % 4] = r6[k] / np.sqrt(2.0)
+        w[e % 4, e // 4] = -w[e // 4, e % 4]
+    return w
+
+
+def _to6(r16):
+    """The complex build's 16 parameters of real antisymmetric matrices (their entries) -> the
+    real build's 6 (src/matrix.c:288-300)."""
+    r16 = np.asarray(r16).reshape(-1, 16)
+    return (np.sqrt(2.0) * r16[:, list(_UPPER)]).ravel()
+
+
+def _re(x):
+    if isinstance(x, tuple):
+        return tuple(_re(y) for y in x)
+    if isinstance(x, np.ndarray) and np.iscomplexobj(x):
+        return np.ascontiguousarray(x.real)
+    if isinstance(x, complex):
+        return x.real
+    return x
+
+
+class _FnTarget:
+    def __init__(self, fn):
+        def cb(psi_p, udata, out_p):
+            psi, out = psi_p.contents, out_p.contents
+            n = 1 << psi.nqubits
+            x = np.ctypeslib.as_array(C.cast(psi.data, C.POINTER(C.c_double)), shape=(2 * n,)).view(np.complex128)
+            y = np.ctypeslib.as_array(C.cast(out.data, C.POINTER(C.c_double)), shape=(2 * n,)).view(np.complex128)
+            y[:] = fn(x.copy())
+            return 0
+
+        self.cb = LINEAR_FUNC(cb)
+        self.ufunc = C.cast(self.cb, VP)
+        self.udata = None
+
+
+class RealOracle:
+    """The reference's real build restated as the complex restatement (Oracle) on real
+    inputs: for real gates, states and targets every product and sum the complex build
+    forms has a zero imaginary part and the real build's value as real part, and its
+    conjugations are the identity; the real parts of the results are returned.  What the
+    builds do differently is restated here: the 6-parameter tangents (a real
+    antisymmetric w has the 16 complex-build parameters w.ravel(), and the 6 real-build
+    ones sqrt(2) w[upper]), real sample states, the single block-encoding Hessian
+    hess1 + hess2 (src/target.c:1595-1597), and the optimisers over 6 parameters per
+    gate (src/brickwall_opt.c:22-149, src/circuit_opt.c)."""
+
+    name = "real-oracle"
+
+    def __init__(self):
+        self.o = Oracle()
+
+    def target(self, kind, data=None):
+        if kind == "fixture":
+            return _FnTarget(real_fixture_map)
+        if kind in ("brickwall", "host_brickwall"):
+            return self.o.target("brickwall", (_c(data[0]), data[1]))
+        if kind == "dense":
+            return self.o.target("dense", _c(data))
+        raise ValueError(kind)
+
+    def __getattr__(self, name):
+        fn = getattr(self.o, name)
+
+        def call(*args, **kw):
+            return _re(fn(*[_c(a) if isinstance(a, np.ndarray) and a.dtype == np.float64 and a.ndim >= 2 else a
+                            for a in args], **kw))
+
+        return call
+
+    # states: complex copies of real 1-d inputs (gate-level functions)
+    def _cs(self, fn, *args):
+        return _re(fn(*[_c(a) if isinstance(a, np.ndarray) and a.dtype == np.float64 else a for a in args]))
+
+    def apply_gate(self, V, i, j, psi):
+        return self._cs(self.o.apply_gate, V, i, j, psi)
+
+    def apply_gate_backward(self, V, i, j, psi, dout):
+        return self._cs(self.o.apply_gate_backward, V, i, j, psi, dout)
+
+    def apply_quantum_circuit(self, gates, wires, psi):
+        return _re(self.o.apply_quantum_circuit(_c(gates), wires, _c(psi)))
+
+    def quantum_circuit_forward(self, gates, wires, psi):
+        out, cache = self.o.quantum_circuit_forward(_c(gates), wires, _c(psi))
+        return _re(out), cache
+
+    def quantum_circuit_backward(self, gates, wires, cache, dout):
+        return _re(self.o.quantum_circuit_backward(_c(gates), wires, cache, _c(dout)))
+
+    def quantum_circuit_gates_hessian_vector_product(self, gates, dirs, wires, psi, phi):
+        return _re(self.o.quantum_circuit_gates_hessian_vector_product(_c(gates), _c(dirs), wires, _c(psi), _c(phi)))
+
+    def apply_brickwall_unitary(self, vlist, perms, psi):
+        return _re(self.o.apply_brickwall_unitary(_c(vlist), perms, _c(psi)))
+
+    def brickwall_unitary_forward(self, vlist, perms, psi):
+        out, states = self.o.brickwall_unitary_forward(_c(vlist), perms, _c(psi))
+        return _re(out), states
+
+    def brickwall_unitary_backward_hessian(self, vlist, perms, states, dout):
+        return _re(self.o.brickwall_unitary_backward_hessian(_c(vlist), perms, states, _c(dout)))
+
+    def apply_gate_to_array(self, V, i, j, psi):
+        return _re(self.o.apply_gate_to_array(_c(V), i, j, _c(psi)))
+
+    def apply_gate_backward_array(self, V, i, j, psi, dout):
+        return _re(self.o.apply_gate_backward_array(_c(V), i, j, _c(psi), _c(dout)))
+
+    def apply_gate_placeholder(self, i, j, psi):
+        return _re(self.o.apply_gate_placeholder(i, j, _c(psi)))
+
+    # projected forms: 6 parameters per gate
+    def circuit_unitary_target_and_projected_gradient(self, t, gates, wires, L):
+        f, g = self.o.circuit_unitary_target_and_projected_gradient(t, _c(gates), wires, L)
+        return f.real, _to6(g)
+
+    def circuit_unitary_target_projected_hessian_vector_product(self, t, gates, dirs, wires, L):
+        f, g, h = self.o.circuit_unitary_target_projected_hessian_vector_product(t, _c(gates), _c(dirs), wires, L)
+        return f.real, _to6(g), _to6(h)
+
+    def brickwall_unitary_target_and_projected_gradient(self, t, vlist, perms, L):
+        f, g = self.o.brickwall_unitary_target_and_projected_gradient(t, _c(vlist), perms, L)
+        return f.real, _to6(g)
+
+    def brickwall_unitary_target_projected_hessian_vector_product(self, t, vlist, vdirs, perms, L):
+        f, g, h = self.o.brickwall_unitary_target_projected_hessian_vector_product(t, _c(vlist), _c(vdirs), perms, L)
+        return f.real, _to6(g), _to6(h)
+
+    def brickwall_blockenc_target_gradient_hessian(self, t, vlist, perms, L):
+        f, dv, h1, h2 = self.o.brickwall_blockenc_target_gradient_hessian(t, _c(vlist), perms, L)
+        return f, dv.real.copy(), (h1 + h2).real.copy()
+
+    # sampling: real normal states
+    def _sampled(self, fn, *args):
+        self.o.lib.orc_set_real_samples(1)
+        try:
+            return fn(*args)
+        finally:
+            self.o.lib.orc_set_real_samples(0)
+
+    def haar_random_statevector(self, L, rng):
+        return self._sampled(self.o.haar_random_statevector, L, rng).real.copy()
+
+    def brickwall_unitary_target_sampling(self, t, vlist, perms, L, ns, rng):
+        return self._sampled(self.o.brickwall_unitary_target_sampling, t, _c(vlist), perms, L, ns, rng).real
+
+    def circuit_unitary_target_sampling(self, t, gates, wires, L, ns, rng):
+        return self._sampled(self.o.circuit_unitary_target_sampling, t, _c(gates), wires, L, ns, rng).real
+
+    def brickwall_unitary_target_gradient_hessian_sampling(self, t, vlist, perms, L, ns, rng):
+        return _re(self._sampled(self.o.brickwall_unitary_target_gradient_hessian_sampling, t, _c(vlist), perms, L, ns,
+                                 rng))
+
+    # 4x4 algebra of the real build
+    def real_to_antisymm(self, r6):
+        return real_antisymm(r6)
+
+    def real_to_tangent(self, r6, v):
+        return np.asarray(v).real @ real_antisymm(r6)
+
+    def tangent_to_real(self, v, z):
+        t = np.asarray(v).real.T @ np.asarray(z).real
+        return _to6((0.5 * (t - t.T)).ravel())
+
+    def retract(self, v, r6):
+        return self.o.polar_factor(_c(np.asarray(v).real @ (np.eye(4) + real_antisymm(r6)))).real.copy()
+
+    # optimisers over 6 parameters per gate, on the oracle's trust region
+    def _rtr(self, f, fd, hvp, k, x0, niter):
+        n, m = 6 * k, 16 * k
+        cf = TARGET_FUNC(lambda x, d: f(np.ctypeslib.as_array(x, shape=(m,)).reshape(k, 4, 4).copy()))
+
+        def _fd(x, d, g):
+            fx, gv = fd(np.ctypeslib.as_array(x, shape=(m,)).reshape(k, 4, 4).copy())
+            np.ctypeslib.as_array(g, shape=(n,))[:] = gv
+            return fx
+
+        def _hvp(x, d, vec, out):
+            v = np.ctypeslib.as_array(x, shape=(m,)).reshape(k, 4, 4).copy()
+            r = np.ctypeslib.as_array(vec, shape=(n,)).copy()
+            np.ctypeslib.as_array(out, shape=(n,))[:] = hvp(v, r)
+
+        def _retract(x, eta, rd, xs):
+            v = np.ctypeslib.as_array(x, shape=(m,)).reshape(k, 4, 4)
+            e = np.ctypeslib.as_array(eta, shape=(n,)).reshape(k, 6)
+            np.ctypeslib.as_array(xs, shape=(m,))[:] = np.stack([self.retract(v[i], e[i]) for i in range(k)]).ravel()
+
+        cfd, chvp, cret = TARGET_GRAD_FUNC(_fd), HVP_FUNC(_hvp), RETRACT_FUNC(_retract)
+        x0 = np.ascontiguousarray(x0, np.float64)
+        f_iter, xf = np.empty(niter + 1), np.empty(m)
+        params = default_rtr(n)
+        self.o.lib.orc_rtr_optimize_hvp(C.cast(cf, VP), C.cast(cfd, VP), C.cast(chvp, VP), None, C.cast(cret, VP), None,
+                                        n, _p(x0), m, C.byref(params), niter, _p(f_iter), _p(xf), None, None)
+        return f_iter, xf.reshape(k, 4, 4)
+
+    def optimize_brickwall_circuit_hvp(self, t, vstart, perms, L, niter):
+        k = vstart.shape[0]
+        return self._rtr(
+            lambda v: self.brickwall_unitary_target(t, v, perms, L).real,
+            lambda v: self.brickwall_unitary_target_and_projected_gradient(t, v, perms, L),
+            lambda v, r: self.brickwall_unitary_target_projected_hessian_vector_product(
+                t, v, np.stack([self.real_to_tangent(r[6 * i:6 * i + 6], v[i]) for i in range(k)]), perms, L)[2],
+            k, vstart, niter)
+
+    def optimize_quantum_circuit(self, t, gstart, wires, L, niter):
+        k = gstart.shape[0]
+        return self._rtr(
+            lambda g: self.circuit_unitary_target(t, g, wires, L).real,
+            lambda g: self.circuit_unitary_target_and_projected_gradient(t, g, wires, L),
+            lambda g, r: self.circuit_unitary_target_projected_hessian_vector_product(
+                t, g, np.stack([self.real_to_tangent(r[6 * i:6 * i + 6], g[i]) for i in range(k)]), wires, L)[2],
+            k, gstart, niter)
+
+
+class _RefRtrParams(C.Structure):
+    _fields_ = [("tcg", TcgParams), ("rho_trust", C.c_double), ("radius_init", C.c_double), ("maxradius", C.c_double),
+                ("g_func", C.c_void_p), ("g_data", C.c_void_p), ("g_iter", C.c_void_p)]
+
+
+class _RefBrickwall(C.Structure):
+    _fields_ = [("vlist", C.c_void_p), ("nlayers", C.c_int), ("perms", C.c_void_p)]
+
+
+class RealReference:
+    """The reference's own sources compiled without COMPLEX_CIRCUIT in _ref/, called
+    through their public functions (real arrays; perms as `const int*[]`)."""
+
+    name = "real-reference"
+
+    def __init__(self):
+        if not os.path.exists(REAL_REF_LIB):
+            raise FileNotFoundError(REAL_REF_LIB)
+        self.lib = C.CDLL(REAL_REF_LIB)
+        self.lib.truncated_cg_hvp.restype = C.c_bool
+
+    @staticmethod
+    def available():
+        return os.path.exists(REAL_REF_LIB)
+
+    @staticmethod
+    def _r(a):
+        return np.ascontiguousarray(np.asarray(a).real if np.iscomplexobj(a) else a, dtype=np.float64)
+
+    @staticmethod
+    def _perms(perms):
+        perms = _i(perms)
+        arr = (C.c_void_p * perms.shape[0])(*[perms[k].ctypes.data for k in range(perms.shape[0])])
+        return arr, perms
+
+    def target(self, kind, data=None):
+        if kind == "brickwall":
+            t = _RealRefTarget()
+            t.vlist = self._r(data[0])
+            t.pp, t.pk = self._perms(data[1])
+            t.desc = _RefBrickwall(t.vlist.ctypes.data, t.vlist.shape[0], C.cast(t.pp, VP))
+            t.ufunc = C.cast(self.lib.refdrv_real_brickwall_ufunc, VP)
+            t.udata = C.cast(C.pointer(t.desc), VP)
+            return t
+        fn = real_fixture_map if kind == "fixture" else (lambda x, u=self._r(data): u @ x)
+        return _RealRefTarget(fn)
+
+    def _bw(self, name, t, vlist, perms, L, outs, *extra):
+        vlist = self._r(vlist)
+        pp, keep = self._perms(perms)
+        f = np.zeros(1)
+        ret = getattr(self.lib, name)(t.ufunc, t.udata, _p(vlist), vlist.shape[0], L, C.cast(pp, VP), *extra, _p(f),
+                                      *[_p(o) for o in outs])
+        assert ret == 0, name
+        return f[0]
+
+    def brickwall_unitary_target(self, t, vlist, perms, L):
+        return self._bw("brickwall_unitary_target", t, vlist, perms, L, [])
+
+    def brickwall_unitary_target_and_gradient(self, t, vlist, perms, L):
+        dv = np.empty((len(vlist), 4, 4))
+        return self._bw("brickwall_unitary_target_and_gradient", t, vlist, perms, L, [dv]), dv
+
+    def brickwall_unitary_target_and_projected_gradient(self, t, vlist, perms, L):
+        g = np.empty(6 * len(vlist))
+        return self._bw("brickwall_unitary_target_and_projected_gradient", t, vlist, perms, L, [g]), g
+
+    def brickwall_unitary_target_gradient_hessian(self, t, vlist, perms, L):
+        m = 16 * len(vlist)
+        dv, h = np.empty((len(vlist), 4, 4)), np.empty((m, m))
+        return self._bw("brickwall_unitary_target_gradient_hessian", t, vlist, perms, L, [dv, h]), dv, h
+
+    def brickwall_blockenc_target_gradient_hessian(self, t, vlist, perms, L):
+        m = 16 * len(vlist)
+        dv, h = np.empty((len(vlist), 4, 4)), np.empty((m, m))
+        return self._bw("brickwall_blockenc_target_gradient_hessian", t, vlist, perms, L, [dv, h]), dv, h
+
+    def _hvp(self, name, t, vlist, vdirs, perms, L, outs):
+        vlist, vdirs = self._r(vlist), self._r(vdirs)
+        pp, keep = self._perms(perms)
+        f = np.zeros(1)
+        ret = getattr(self.lib, name)(t.ufunc, t.udata, _p(vlist), _p(vdirs), vlist.shape[0], C.cast(pp, VP), L, _p(f),
+                                      *[_p(o) for o in outs])
+        assert ret == 0, name
+        return f[0]
+
+    def brickwall_unitary_target_hessian_vector_product(self, t, vlist, vdirs, perms, L):
+        dv, hv = np.empty((len(vlist), 4, 4)), np.empty((len(vlist), 4, 4))
+        return self._hvp("brickwall_unitary_target_hessian_vector_product", t, vlist, vdirs, perms, L, [dv, hv]), dv, hv
+
+    def brickwall_unitary_target_projected_hessian_vector_product(self, t, vlist, vdirs, perms, L):
+        g, h = np.empty(6 * len(vlist)), np.empty(6 * len(vlist))
+        return (self._hvp("brickwall_unitary_target_projected_hessian_vector_product", t, vlist, vdirs, perms, L, [g, h]),
+                g, h)
+
+    def seed_rng_state(self, seed):
+        rng = RngState()
+        self.lib.seed_rng_state.argtypes = [C.c_uint64, C.POINTER(RngState)]
+        self.lib.seed_rng_state(seed, C.byref(rng))
+        return rng
+
+    def brickwall_unitary_target_gradient_hessian_sampling(self, t, vlist, perms, L, ns, rng):
+        m = 16 * len(vlist)
+        dv, h = np.empty((len(vlist), 4, 4)), np.empty((m, m))
+        f = self._bw("brickwall_unitary_target_gradient_hessian_sampling", t, vlist, perms, L, [dv, h], C.c_long(ns),
+                     C.byref(rng))
+        return f, dv, h
+
+    def optimize_brickwall_circuit_hvp(self, t, vstart, perms, L, niter):
+        vstart = self._r(vstart)
+        nl = vstart.shape[0]
+        pp, keep = self._perms(perms)
+        params = _RefRtrParams(TcgParams(12 * nl, 1e-8, 1e-6), 0.125, 0.01, 0.1, None, None, None)
+        f_iter, vopt = np.empty(niter + 1), np.empty_like(vstart)
+        self.lib.optimize_brickwall_circuit_hvp(t.ufunc, t.udata, _p(vstart), nl, L, C.cast(pp, VP), C.byref(params),
+                                                niter, _p(f_iter), _p(vopt))
+        return f_iter, vopt
+
+
+class _RealRefTarget:
+    def __init__(self, fn=None):
+        if fn is not None:
+            def cb(psi_p, udata, out_p):
+                psi, out = psi_p.contents, out_p.contents
+                n = 1 << psi.nqubits
+                x = np.ctypeslib.as_array(C.cast(psi.data, C.POINTER(C.c_double)), shape=(n,))
+                np.ctypeslib.as_array(C.cast(out.data, C.POINTER(C.c_double)), shape=(n,))[:] = fn(x.copy())
+                return 0
+
+            self.cb = LINEAR_FUNC(cb)
+            self.ufunc, self.udata = C.cast(self.cb, VP), None

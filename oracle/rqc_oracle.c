@@ -1246,11 +1246,20 @@ static orc_cplx rng_crandn(orc_rng* rng)
 	return x / sqrt(2.0) + I * (y / sqrt(2.0));
 }
 
+/* the reference's real build draws one real normal per amplitude (src/statevector.c:115-121) */
+static int orc_real_samples = 0;
+
+void orc_set_real_samples(int on) { orc_real_samples = on ? 1 : 0; }
+
 /* src/statevector.c:47-66, 102-125 */
 void orc_haar_statevector(orc_sv* psi, orc_rng* rng)
 {
 	const long n = 1L << psi->nqubits;
-	for (long j = 0; j < n; j++) psi->data[j] = rng_crandn(rng);
+	if (orc_real_samples) {
+		for (long j = 0; j < n; j++) psi->data[j] = rng_randn(rng);
+	} else {
+		for (long j = 0; j < n; j++) psi->data[j] = rng_crandn(rng);
+	}
 	double s = 0;
 	for (long j = 0; j < n; j++) s += creal(psi->data[j]) * creal(psi->data[j]) + cimag(psi->data[j]) * cimag(psi->data[j]);
 	const double nrm = sqrt(s);

@@ -148,6 +148,8 @@ typedef struct { uint64_t state, inc; } orc_pcg32;
 typedef struct { orc_pcg32 gen[2]; } orc_rng;
 void orc_seed_rng(uint64_t seed, orc_rng* rng);
 void orc_haar_statevector(orc_sv* psi, orc_rng* rng);
+/* real sample states (one real normal per amplitude), as in the reference's real build */
+void orc_set_real_samples(int on);
 int  orc_circuit_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* gates, int ngates, const int* wires,
                                  int nqubits, long nsamples, orc_rng* rng, orc_cplx* fval);
 int  orc_brickwall_target_sampling(orc_linear_func uf, void* ud, const orc_mat4* vlist, int nlayers, int nqubits,

@@ -2,7 +2,9 @@
 
 Every ``csrc/*.cu`` file is compiled to an object under ``_build/`` (in
 parallel, skipped when up to date) and linked into
-``rqcopt_hpc_b200/librqcopt_gpu.so``.  Usage::
+``rqcopt_hpc_b200/librqcopt_gpu.so``; ``csrc/abi_real.cpp`` (host code) becomes
+``rqcopt_hpc_b200/librqcopt_gpu_real.so``, the real-orthogonal build, which loads
+the first library at run time.  Usage::
 
     python -m rqcopt_hpc_b200.build [--force] [--verbose]
 """
@@ -19,6 +21,9 @@ ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 BUILD = os.path.join(PKG, "_build")
 LIB = os.path.join(PKG, "librqcopt_gpu.so")
+REAL_LIB = os.path.join(PKG, "librqcopt_gpu_real.so")
+REAL_SRC = os.path.join(CSRC, "abi_real.cpp")
+CXX = os.environ.get("CXX", "g++")
 NVCC = os.environ.get("NVCC", "nvcc")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -64,10 +69,22 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         raise RuntimeError("nvcc failed:\n" + "\n".join(errors))
     objs = [o for o, _ in results]
     if force or _stale(LIB, objs):
-        cmd = [NVCC] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart"]
+        # -Bsymbolic: calls between the library's own exports (and its comparisons of
+        # ufunc addresses) bind inside it, also when librqcopt_gpu_real.so, which
+        # exports the same names with real types, is loaded into the process
+        cmd = [NVCC] + ARCH + ["-shared", "-Xlinker", "-Bsymbolic", "-o", LIB] + objs + ["-lcudart"]
         p = subprocess.run(cmd, capture_output=True, text=True)
         if p.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
+    real_deps = [REAL_SRC, os.path.join(ROOT, "include", "rqcopt_gpu_real.h")]
+    if force or _stale(REAL_LIB, real_deps):
+        cmd = [CXX, "-std=c++17", "-O2", "-fPIC", "-Wall", "-fvisibility=hidden", "-shared", "-I" + os.path.join(ROOT, "include"),
+               "-o", REAL_LIB, REAL_SRC, "-ldl", "-Wl,--exclude-libs,ALL"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        p = subprocess.run(cmd, capture_output=True, text=True)
+        if p.returncode != 0:
+            raise RuntimeError(f"real-build library failed: {' '.join(cmd)}\n{p.stdout}\n{p.stderr}")
     return LIB
 
 

@@ -5,7 +5,7 @@
 
 using namespace rqc;
 
-namespace rqc { int take_last_error(); }
+namespace rqc { int take_last_error(); void set_real_samples(int on); }
 
 extern "C" {
 
@@ -49,6 +49,8 @@ int rqcopt_gpu_set_gates_per_pass(int gates)
 }
 
 int rqcopt_gpu_last_error(void) { return take_last_error(); }
+
+void rqcopt_gpu_set_real_samples(int on) { set_real_samples(on); }
 
 unsigned long long rqcopt_gpu_launch_count(void)
 {

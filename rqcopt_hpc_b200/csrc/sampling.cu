@@ -70,20 +70,24 @@ struct Gen2
 	}
 };
 
-// unnormalised complex normal amplitudes of samples s0 .. s0 + total / 2^L - 1
+// unnormalised complex (or, with sp.real, real) normal amplitudes of samples s0 .. s0 + total / 2^L - 1
 __global__ void __launch_bounds__(HTPB) k_haar(SampleSpec sp, int L, int64_t s0, int64_t total, double2* __restrict__ out)
 {
 	const double rs2 = sqrt(2.0);
 	for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r * HRUN < total;
 	     r += (int64_t)gridDim.x * blockDim.x) {
 		const int64_t a0 = r * HRUN;
-		const uint64_t d = 4 * (uint64_t)((s0 << L) + a0);
+		const uint64_t d = (sp.real ? 2 : 4) * (uint64_t)((s0 << L) + a0);
 		Gen2 g{ pcg_jump(sp.state[0], sp.inc[0], d), sp.inc[0], pcg_jump(sp.state[1], sp.inc[1], d), sp.inc[1] };
 		const int n = (int)min((int64_t)HRUN, total - a0);
-		for (int k = 0; k < n; k++) {
-			const double x = g.randn();
-			const double y = g.randn();
-			out[a0 + k] = make_double2(x / rs2, y / rs2);
+		if (sp.real) {
+			for (int k = 0; k < n; k++) out[a0 + k] = make_double2(g.randn(), 0.0);
+		} else {
+			for (int k = 0; k < n; k++) {
+				const double x = g.randn();
+				const double y = g.randn();
+				out[a0 + k] = make_double2(x / rs2, y / rs2);
+			}
 		}
 	}
 }
@@ -151,7 +155,13 @@ size_t sampling_workspace_limit(Runtime& rt)
 	return (size_t)((free_b + rt.work.bytes) * 0.75);
 }
 
+int g_real_samples = 0;
+
 }  // namespace
+
+int real_samples() { return g_real_samples; }
+
+void set_real_samples(int on) { g_real_samples = on ? 1 : 0; }
 
 void pcg_advance_host(uint64_t& state, uint64_t inc, uint64_t delta)
 {

@@ -12,14 +12,20 @@
 namespace rqc {
 
 // The two PCG32 generators of `struct rng_state` at the start of a call.
+// real: states of the reference's real build, one real normal per amplitude
+// (src/statevector.c:115-121) instead of a complex one.
 struct SampleSpec
 {
 	uint64_t state[2], inc[2];
 	int64_t nsamples;
+	int real;
 };
 
 // advance a PCG32 generator (64-bit LCG) by delta steps (jump-ahead)
 void pcg_advance_host(uint64_t& state, uint64_t inc, uint64_t delta);
+
+// process-wide choice of real sample states (rqcopt_gpu_set_real_samples)
+int real_samples();
 
 inline SampleSpec sample_spec(const struct rng_state* rng, long nsamples)
 {
@@ -29,14 +35,15 @@ inline SampleSpec sample_spec(const struct rng_state* rng, long nsamples)
 		sp.inc[k] = rng->pcgstate.gen[k].inc;
 	}
 	sp.nsamples = nsamples;
+	sp.real = real_samples();
 	return sp;
 }
 
 // past nsamples states of 2^L amplitudes: the reference draws 4 outputs of both
-// generators per amplitude (src/rng.c:114-157)
+// generators per complex amplitude, 2 per real one (src/rng.c:114-157)
 inline void advance_rng(struct rng_state* rng, long nsamples, int L)
 {
-	const uint64_t steps = 4 * (uint64_t)nsamples << L;
+	const uint64_t steps = (real_samples() ? 2 : 4) * (uint64_t)nsamples << L;
 	for (int k = 0; k < 2; k++) pcg_advance_host(rng->pcgstate.gen[k].state, rng->pcgstate.gen[k].inc, steps);
 }
 

@@ -7,7 +7,8 @@ Run in a checkout that has the reference project next to it:
 Each ``test_<name>_cplx.hdf5`` (complex-circuit fixtures of the reference's
 ``test/data`` directory, generated there by ``test/test_*.py``) becomes
 ``tests/golden/<name>.npz`` with the same dataset names and the interleaved
-(real, imag) layout unchanged.  The reader is ``hdf5_lite`` in this folder.
+(real, imag) layout unchanged; the real-build fixtures (``test_<name>_real.hdf5``)
+go to ``tests/golden/real/``.  The reader is ``hdf5_lite`` in this folder.
 """
 import os
 import sys
@@ -39,14 +40,33 @@ FIXTURES = [
 ]
 
 
+# the reference's real-orthogonal build (``test_<name>_real.hdf5``) -> ``tests/golden/real/<name>.npz``
+REAL_FIXTURES = [
+    "apply_gate", "apply_gate_backward", "apply_gate_to_array", "apply_gate_placeholder", "apply_quantum_circuit",
+    "quantum_circuit_backward", "quantum_circuit_gates_hessian_vector_product", "apply_brickwall_unitary",
+    "brickwall_unitary_backward", "brickwall_unitary_backward_hessian", "circuit_unitary_target",
+    "circuit_unitary_target_and_gradient", "circuit_unitary_target_hessian_vector_product",
+    "circuit_unitary_target_projected_hessian_vector_product", "brickwall_unitary_target",
+    "brickwall_unitary_target_and_gradient", "brickwall_unitary_target_hessian_vector_product",
+    "brickwall_unitary_target_projected_hessian_vector_product", "brickwall_unitary_target_gradient_hessian",
+    "brickwall_unitary_target_sampling", "brickwall_unitary_target_gradient_hessian_sampling",
+    "brickwall_blockenc_target", "brickwall_blockenc_target_and_gradient", "brickwall_blockenc_target_gradient_hessian",
+    "real_to_tangent", "project_tangent", "polar_factor", "multiply",
+]
+
+
 def main(data_dir):
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for name in FIXTURES:
         arrays = hdf5_lite.read_all(os.path.join(data_dir, f"test_{name}_cplx.hdf5"))
         np.savez(os.path.join(out_dir, f"{name}.npz"), **arrays)
+    os.makedirs(os.path.join(out_dir, "real"), exist_ok=True)
+    for name in REAL_FIXTURES:
+        arrays = hdf5_lite.read_all(os.path.join(data_dir, f"test_{name}_real.hdf5"))
+        np.savez(os.path.join(out_dir, "real", f"{name}.npz"), **arrays)
     arrays = hdf5_lite.read_all(os.path.join(data_dir, "test_truncated_cg.hdf5"))
     np.savez(os.path.join(out_dir, "truncated_cg.npz"), **arrays)
-    print(f"wrote {len(FIXTURES) + 1} fixtures to {out_dir}")
+    print(f"wrote {len(FIXTURES) + 1} + {len(REAL_FIXTURES)} (real build) fixtures to {out_dir}")
 
 
 if __name__ == "__main__":

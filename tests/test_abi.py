@@ -12,6 +12,8 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "rqcopt_gpu.h")
 LIB = os.path.join(ROOT, "rqcopt_hpc_b200", "librqcopt_gpu.so")
+REAL_HEADER = os.path.join(ROOT, "include", "rqcopt_gpu_real.h")
+REAL_LIB = os.path.join(ROOT, "rqcopt_hpc_b200", "librqcopt_gpu_real.so")
 REF_SRC = "/root/reference/src"
 
 
@@ -26,47 +28,57 @@ def _declared_functions(text):
     return names
 
 
-def test_library_exports_every_declared_function():
-    assert os.path.exists(LIB), "build the library first (python -m rqcopt_hpc_b200.build)"
-    lib = ctypes.CDLL(LIB)
-    names = _declared_functions(open(HEADER).read())
+@pytest.mark.parametrize("lib_path,header", [(LIB, HEADER), (REAL_LIB, REAL_HEADER)], ids=["complex", "real"])
+def test_library_exports_every_declared_function(lib_path, header):
+    assert os.path.exists(lib_path), "build the library first (python -m rqcopt_hpc_b200.build)"
+    lib = ctypes.CDLL(lib_path)
+    names = _declared_functions(open(header).read())
     assert len(names) > 60
     missing = [n for n in sorted(names) if not hasattr(lib, n)]
     assert not missing, missing
 
 
+def test_real_library_exports_only_its_interface():
+    """The real-build library hides its internals (C++ runtime instantiations included)."""
+    out = subprocess.run(["nm", "-D", "--defined-only", REAL_LIB], capture_output=True, text=True, check=True).stdout
+    exported = {l.split()[-1] for l in out.splitlines() if " T " in l}
+    assert exported == _declared_functions(open(REAL_HEADER).read())
+
+
 @pytest.mark.parametrize("lang", ["c", "c++"])
-def test_header_compiles(tmp_path, lang):
+@pytest.mark.parametrize("header", ["rqcopt_gpu.h", "rqcopt_gpu_real.h"])
+def test_header_compiles(tmp_path, lang, header):
     src = tmp_path / ("t.c" if lang == "c" else "t.cpp")
-    src.write_text('#include "rqcopt_gpu.h"\nint main(void) { struct rtr_params p; set_rtr_default_params(16, &p); return p.tcg_params.maxiter == 32 ? 0 : 1; }\n')
+    src.write_text(f'#include "{header}"\n' + 'int main(void) { struct rtr_params p; set_rtr_default_params(16, &p); return p.tcg_params.maxiter == 32 ? 0 : 1; }\n')
     cc = "gcc" if lang == "c" else "g++"
     subprocess.run([cc, "-fsyntax-only", "-Wall", "-I" + os.path.dirname(HEADER), str(src)], check=True)
 
 
-def _complex_branch(text):
-    """Keep the COMPLEX_CIRCUIT branch of `#ifdef COMPLEX_CIRCUIT ... [#else ...] #endif`
-    blocks (the build this library mirrors); the reference does not nest them."""
+def _complex_branch(text, complex_build=True):
+    """Keep one branch of `#ifdef COMPLEX_CIRCUIT ... [#else ...] #endif` blocks: the
+    COMPLEX_CIRCUIT one (librqcopt_gpu.so) or the other (librqcopt_gpu_real.so); the
+    reference does not nest them."""
     out, state = [], None
     for line in text.split("\n"):
         d = line.strip()
         if d.startswith("#ifdef COMPLEX_CIRCUIT"):
-            state = "keep"
+            state = "first"
         elif state and d.startswith("#else"):
-            state = "skip"
+            state = "second"
         elif state and d.startswith("#endif"):
             state = None
-        elif state != "skip":
+        elif state is None or (state == "first") == complex_build:
             out.append(line)
     return "\n".join(out)
 
 
-def _ref_prototypes():
+def _ref_prototypes(complex_build=True):
     protos = {}
     for fn in os.listdir(REF_SRC):
         if fn.endswith(".h"):
             text = open(os.path.join(REF_SRC, fn)).read()
             text = re.sub(r"//.*", "", text)
-            text = _complex_branch(text)
+            text = _complex_branch(text, complex_build)
             for m in re.finditer(r"^([A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\))\s*;", text, flags=re.M):
                 if not m.group(1).startswith("typedef"):
                     protos[m.group(2)] = m.group(1)
@@ -83,9 +95,10 @@ def _norm(p):
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_SRC), reason="reference sources not present")
-def test_signatures_match_reference():
-    ref = _ref_prototypes()
-    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+@pytest.mark.parametrize("header,complex_build", [(HEADER, True), (REAL_HEADER, False)], ids=["complex", "real"])
+def test_signatures_match_reference(header, complex_build):
+    ref = _ref_prototypes(complex_build)
+    text = re.sub(r"/\*.*?\*/", "", open(header).read(), flags=re.S)
     ours = {}
     for m in re.finditer(r"^([A-Za-z_][\w\s\*]*?\b([a-z_][a-z0-9_]*)\s*\([^;{]*\))\s*;", text, flags=re.M):
         if not m.group(1).startswith("typedef"):
@@ -96,3 +109,6 @@ def test_signatures_match_reference():
             assert _norm(proto) == _norm(ref[name]), (name, proto, ref[name])
             checked += 1
     assert checked >= 50
+    if not complex_build:
+        # the real build has none of the full-Hessian matrix forms
+        assert not {n for n in ours if "hessian_matrix" in n or "hmat_sampling" in n or n.endswith("_hmat")} - {"truncated_cg_hmat", "riemannian_trust_region_optimize_hmat"}
