@@ -528,6 +528,77 @@ def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
 
 # ----------------------------------------------------------------------------- batched and serving
 
+def _real_workload(L, depth, tdepth, seed=30):
+    """Real orthogonal brickwall (QR of Gaussian matrices, sign-fixed) against a real
+    brickwall target, with a 6-parameter tangent direction per gate."""
+    def orth(rng):
+        q, r = np.linalg.qr(rng.standard_normal((4, 4)))
+        return q * np.sign(np.diagonal(r))
+
+    from rqcopt_hpc_b200 import real
+    rng, trng, drng = (np.random.default_rng(seed + k) for k in range(3))
+    vlist = np.stack([orth(rng) for _ in range(depth)])
+    tvlist = np.stack([orth(trng) for _ in range(tdepth)])
+    vdirs = np.stack([real.real_to_tangent(drng.standard_normal(6), vlist[k]) for k in range(depth)])
+    return vlist, perms_for(L, depth), tvlist, perms_for(L, tdepth), vdirs
+
+
+def _ref_real_columns_worker(args):
+    L, depth, tdepth, b0, b1 = args
+    from oracle.oracle import RealReference
+    vlist, perms, tvlist, tperms, vdirs = _real_workload(L, depth, tdepth)
+    t0 = time.perf_counter()
+    RealReference().brickwall_hvp_columns(vlist, vdirs, perms, L, tvlist, tperms, b0, b1)
+    return time.perf_counter() - t0
+
+
+def real_build_path(gpu, steps=3, L=14, depth=9, tdepth=5, seconds=8.0, with_reference=True):
+    """The reference's real-orthogonal build (librqcopt_gpu_real.so): one f + projected
+    gradient + projected HVP evaluation over all basis columns through the real C ABI
+    (host gates, complex128 engine), against the reference's real build compiled in
+    oracle/_ref on a per-core column sample."""
+    import multiprocessing as mp
+    from rqcopt_hpc_b200 import real
+    vlist, perms, tvlist, tperms, vdirs = _real_workload(L, depth, tdepth)
+    gpu.set_precision(gpu.PRECISION_C128)
+    t = real.Target(brickwall=(tvlist, tperms))
+
+    def ev():
+        return real.brickwall_unitary_target_projected_hessian_vector_product(t, vlist, vdirs, perms, L)
+
+    ev()
+    real.reset_launch_count()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        f, g, h = ev()
+    wall = (time.perf_counter() - t0) / steps
+    launches = real.launch_count() // steps
+    out = {"workload": f"real build: f + projected gradient (6 per gate) + projected HVP, real orthogonal brickwall "
+                       f"L={L} depth {depth} vs real brickwall target depth {tdepth}, all {1 << L} basis columns, "
+                       f"complex128 engine", "evals_per_s_e2e": 1.0 / wall, "ms_per_eval": wall * 1e3,
+           "gpu_launches": launches, "f": float(f)}
+    from oracle.oracle import RealReference
+    if not with_reference or not RealReference.available():
+        return out
+    N = 1 << L
+    t0 = time.perf_counter()
+    RealReference().brickwall_hvp_columns(vlist, vdirs, perms, L, tvlist, tperms, 0, 2)
+    per_col = max((time.perf_counter() - t0) / 2, 1e-6)
+    cores = os.cpu_count() or 1
+    cols = max(1, min(N // cores, int(seconds / per_col)))
+    with mp.get_context("spawn").Pool(cores) as pool:
+        t0 = time.perf_counter()
+        pool.map(_ref_real_columns_worker, [(L, depth, tdepth, k * cols, (k + 1) * cols) for k in range(cores)])
+        tref = time.perf_counter() - t0
+    v = (cores * cols / N) / tref
+    out["cpu_baseline"] = {"value": v, "unit": "evals/s", "cores": cores, "kind": "reference",
+                           "sample": f"{cores * cols} of {N} basis columns ({cols} per core) through the real build's "
+                                     f"quantum_circuit_gates_hessian_vector_product with its brickwall target, "
+                                     f"{tref:.1f} s wall; evals/s = sampled fraction / wall time"}
+    out["speedup_e2e"] = (1.0 / wall) / v
+    return out
+
+
 def batched_c4(gpu, torch, count=512, niter=2):
     """512 independent brickwall instances (even L uniform over 6..12, depth over
     {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), niter trust-region iterations
@@ -675,6 +746,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 512-instance batched measurement")
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-hmat", action="store_true", help="skip the full-Hessian path measurement")
+    ap.add_argument("--no-real", action="store_true", help="skip the real-orthogonal build measurement")
     ap.add_argument("--hmat-case", choices=["target", "single"],
                     help="run one full-Hessian evaluation at --L/--depth/--tdepth and exit (a small case for "
                          "profilers): 'target' sums over all basis columns, 'single' is one state's "
@@ -855,6 +927,9 @@ def main():
             gpu.set_precision(prec)
         if not a.no_hmat and world == 1:
             line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
+            gpu.set_precision(prec)
+        if not a.no_real and world == 1:
+            line["real_build"] = real_build_path(gpu, with_reference=not a.no_cpu_baseline)
             gpu.set_precision(prec)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)

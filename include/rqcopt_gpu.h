@@ -454,6 +454,13 @@ int rqcopt_gpu_last_error(void);
  * sampling calls.  The generator state advances by 2 instead of 4 steps per amplitude. */
 void rqcopt_gpu_set_real_samples(int on);
 
+/* Real problems (real gates and a real target, as in librqcopt_gpu_real.so): the
+ * basis-column sums of the f / gradient / HVP target functions run over the 2^(n-1)
+ * paired columns e_b + i e_{b + 2^(n-1)} and keep the real parts, which are the sums
+ * over all 2^n real columns (half the passes).  Results of complex problems are wrong
+ * in this mode; librqcopt_gpu_real.so sets it around its calls only. */
+void rqcopt_gpu_set_real_pairs(int on);
+
 /* number of kernels this library launched since the counter was last reset */
 unsigned long long rqcopt_gpu_launch_count(void);
 void rqcopt_gpu_reset_launch_count(void);

@@ -1088,6 +1088,18 @@ class RealReference:
                      C.byref(rng))
         return f, dv, h
 
+    def brickwall_hvp_columns(self, vlist, vdirs, perms, L, tvlist, tperms, b0, b1):
+        """Grad+HVP column sum over basis columns [b0, b1) (per-gate sums; brickwall target)."""
+        vlist, vdirs, tvlist = self._r(vlist), self._r(vdirs), self._r(tvlist)
+        perms, tperms = _i(perms), _i(tperms)
+        G = vlist.shape[0] * (L // 2)
+        f, dg, hg = np.zeros(1), np.empty((G, 4, 4)), np.empty((G, 4, 4))
+        ret = self.lib.refdrv_real_brickwall_hvp_columns(_p(vlist), _p(vdirs), vlist.shape[0], _p(perms), L, _p(tvlist),
+                                                         tvlist.shape[0], _p(tperms), L_(b0), L_(b1), _p(f), _p(dg),
+                                                         _p(hg))
+        assert ret == 0
+        return f[0], dg, hg
+
     def optimize_brickwall_circuit_hvp(self, t, vstart, perms, L, niter):
         vstart = self._r(vstart)
         nl = vstart.shape[0]

@@ -52,6 +52,11 @@ int rqcopt_gpu_last_error(void) { return take_last_error(); }
 
 void rqcopt_gpu_set_real_samples(int on) { set_real_samples(on); }
 
+void rqcopt_gpu_set_real_pairs(int on)
+{
+	if (Runtime* rt = runtime()) rt->real_pairs = on ? 1 : 0;
+}
+
 unsigned long long rqcopt_gpu_launch_count(void)
 {
 	Runtime* rt = runtime();

@@ -18,6 +18,11 @@
 //   - Haar-random sample states have one real normal per amplitude
 //     (src/statevector.c:115-121), drawn on the GPU by the complex library in its
 //     real-sample mode;
+//   - the f / gradient / HVP sums run over half the columns: the complex engine takes
+//     the paired basis columns e_b + i e_{b + N/2} (rqcopt_gpu_set_real_pairs); every
+//     sum pairs an adjoint-type state, -conj(U psi) = -(U e_b) + i (U e_{b+N/2}), with a
+//     forward-type state, both propagated by real matrices, so its real part is the
+//     sum of the two real columns' terms;
 //   - the block-encoding Hessian is one matrix, the sum of the two terms
 //     (src/target.c:1595-1597);
 //   - the optimisers run the generic trust region over 6 nlayers (or 6 ngates)
@@ -265,6 +270,16 @@ struct RealSamples
 	void (*set)(int);
 	RealSamples() : set(sym<void (*)(int)>("rqcopt_gpu_set_real_samples")) { if (set) set(1); }
 	~RealSamples() { if (set) set(0); }
+};
+
+// paired basis columns in the complex engine for the duration of a call: the sums of
+// the f / gradient / HVP functions run over 2^(n-1) columns e_b + i e_{b + 2^(n-1)}
+// and keep real parts, which are the sums over the 2^n real columns
+struct RealPairs
+{
+	void (*set)(int);
+	RealPairs() : set(sym<void (*)(int)>("rqcopt_gpu_set_real_pairs")) { if (set) set(1); }
+	~RealPairs() { if (set) set(0); }
 };
 
 typedef const int* const* cperms;
@@ -582,6 +597,7 @@ int circuit_unitary_target(linear_func ufunc, void* udata, const struct mat4x4 g
 {
 	CX(circuit_unitary_target, int, cx::linear_func, void*, const cx::mat4x4*, int, const int*, int, cd*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto g = cmats(gates, ngates);
 	cd f;
 	const int ret = cx_circuit_unitary_target(t.f, t.data, g.data(), ngates, wires, nqubits, &f);
@@ -610,6 +626,7 @@ int circuit_unitary_target_and_gradient(linear_func ufunc, void* udata, const st
 	CX(circuit_unitary_target_and_gradient, int, cx::linear_func, void*, const cx::mat4x4*, int, const int*, int, cd*,
 	   cx::mat4x4*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto g = cmats(gates, ngates);
 	std::vector<cx::mat4x4> dg(ngates);
 	cd f;
@@ -628,6 +645,7 @@ int circuit_unitary_target_and_projected_gradient(linear_func ufunc, void* udata
 	CX(circuit_unitary_target_and_projected_gradient, int, cx::linear_func, void*, const cx::mat4x4*, int, const int*,
 	   int, cd*, double*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto g = cmats(gates, ngates);
 	std::vector<double> g16(16 * (size_t)ngates);
 	cd f;
@@ -648,6 +666,7 @@ int circuit_unitary_target_hessian_vector_product(linear_func ufunc, void* udata
 	CX(circuit_unitary_target_hessian_vector_product, int, cx::linear_func, void*, const cx::mat4x4*, const cx::mat4x4*,
 	   int, const int*, int, cd*, cx::mat4x4*, cx::mat4x4*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto g = cmats(gates, ngates), z = cmats(gatedirs, ngates);
 	std::vector<cx::mat4x4> dg(ngates), hg(ngates);
 	cd f;
@@ -669,6 +688,7 @@ int circuit_unitary_target_projected_hessian_vector_product(linear_func ufunc, v
 	CX(circuit_unitary_target_projected_hessian_vector_product, int, cx::linear_func, void*, const cx::mat4x4*,
 	   const cx::mat4x4*, int, const int*, int, cd*, double*, double*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto g = cmats(gates, ngates), z = cmats(gatedirs, ngates);
 	std::vector<double> g16(16 * (size_t)ngates), h16(16 * (size_t)ngates);
 	cd f;
@@ -687,6 +707,7 @@ int brickwall_unitary_target(linear_func ufunc, void* udata, const struct mat4x4
 {
 	CX(brickwall_unitary_target, int, cx::linear_func, void*, const cx::mat4x4*, int, int, const int**, cd*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto v = cmats(vlist, nlayers);
 	cd f;
 	const int ret = cx_brickwall_unitary_target(t.f, t.data, v.data(), nlayers, nqubits, perms, &f);
@@ -717,6 +738,7 @@ int brickwall_unitary_target_and_gradient(linear_func ufunc, void* udata, const 
 	CX(brickwall_unitary_target_and_gradient, int, cx::linear_func, void*, const cx::mat4x4*, int, int, const int**,
 	   cd*, cx::mat4x4*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto v = cmats(vlist, nlayers);
 	std::vector<cx::mat4x4> dv(nlayers);
 	cd f;
@@ -735,6 +757,7 @@ int brickwall_unitary_target_and_projected_gradient(linear_func ufunc, void* uda
 	CX(brickwall_unitary_target_and_projected_gradient, int, cx::linear_func, void*, const cx::mat4x4*, int, int,
 	   const int**, cd*, double*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto v = cmats(vlist, nlayers);
 	std::vector<double> g16(16 * (size_t)nlayers);
 	cd f;
@@ -755,6 +778,7 @@ int brickwall_unitary_target_hessian_vector_product(linear_func ufunc, void* uda
 	CX(brickwall_unitary_target_hessian_vector_product, int, cx::linear_func, void*, const cx::mat4x4*,
 	   const cx::mat4x4*, int, const int**, int, cd*, cx::mat4x4*, cx::mat4x4*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto v = cmats(vlist, nlayers), z = cmats(vdirs, nlayers);
 	std::vector<cx::mat4x4> dv(nlayers), hv(nlayers);
 	cd f;
@@ -776,6 +800,7 @@ int brickwall_unitary_target_projected_hessian_vector_product(linear_func ufunc,
 	CX(brickwall_unitary_target_projected_hessian_vector_product, int, cx::linear_func, void*, const cx::mat4x4*,
 	   const cx::mat4x4*, int, const int**, int, cd*, double*, double*);
 	Target t(ufunc, udata);
+	RealPairs pairs;
 	const auto v = cmats(vlist, nlayers), z = cmats(vdirs, nlayers);
 	std::vector<double> g16(16 * (size_t)nlayers), h16(16 * (size_t)nlayers);
 	cd f;

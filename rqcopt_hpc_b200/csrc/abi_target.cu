@@ -36,16 +36,29 @@ extern "C" int rqcopt_dense_ufunc(const struct statevector* psi, void* udata, st
 	const double2* u = reinterpret_cast<const double2*>(t->u);
 	const double2* x = reinterpret_cast<const double2*>(psi->data);
 	double2* y = reinterpret_cast<double2*>(psi_out->data);
-	// a basis vector selects one column of U
-	int64_t one = -1;
-	bool basis = true;
-	for (int64_t j = 0; j < n && basis; j++) {
-		if (x[j].x == 0 && x[j].y == 0) continue;
-		if (x[j].x == 1 && x[j].y == 0 && one < 0) one = j;
-		else basis = false;
+	// at most two nonzero entries (a basis vector, or a paired column e_b + i e_b'): only
+	// their columns of U enter, in the same order and arithmetic as the full product
+	int64_t nz[2] = { -1, -1 };
+	int cnt = 0;
+	for (int64_t j = 0; j < n && cnt <= 2; j++)
+		if (x[j].x != 0 || x[j].y != 0) {
+			if (cnt < 2) nz[cnt] = j;
+			cnt++;
+		}
+	if (cnt == 1 && x[nz[0]].x == 1 && x[nz[0]].y == 0) {
+		for (int64_t r = 0; r < n; r++) y[r] = u[r * n + nz[0]];
+		return 0;
 	}
-	if (basis && one >= 0) {
-		for (int64_t r = 0; r < n; r++) y[r] = u[r * n + one];
+	if (cnt <= 2) {
+		for (int64_t r = 0; r < n; r++) {
+			double sx = 0, sy = 0;
+			for (int k = 0; k < cnt; k++) {
+				const double2 a = u[r * n + nz[k]], b = x[nz[k]];
+				sx += a.x * b.x - a.y * b.y;
+				sy += a.x * b.y + a.y * b.x;
+			}
+			y[r] = make_double2(sx, sy);
+		}
 		return 0;
 	}
 	for (int64_t r = 0; r < n; r++) {

@@ -37,10 +37,14 @@ constexpr int NPART = 64;   // doubles of partial sums per block and gate: 16 co
 
 // ---------------------------------------------------------------------------------- helpers
 
+// Paired basis columns (real-orthogonal problems): with c_pair_half = N/2 the column
+// with basis index b (< N/2) is e_b + i e_{b + N/2}; 0 selects plain basis columns.
+__constant__ int64_t c_pair_half = 0;
+
 template <typename T>
 __device__ __forceinline__ cplx<T> basis_amp(int64_t loc, int64_t b)
 {
-	return mk<T>(loc == b ? T(1) : T(0), T(0));
+	return mk<T>(loc == b ? T(1) : T(0), (c_pair_half != 0 && loc == b + c_pair_half) ? T(1) : T(0));
 }
 
 __device__ __forceinline__ void block_add_f(double fx, double fy, double2* __restrict__ fpart)
@@ -442,6 +446,7 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 	using V = cplx<T>;
 	const int L = c.L, G = c.ngates;
 	const int64_t N = (int64_t)1 << L;
+	const int64_t ncols = rt.real_pairs ? N / 2 : N;   // (paired) basis columns
 	const bool tan = mode == EVAL_HVP;
 	const bool host_target = t.ufunc != nullptr;
 
@@ -463,7 +468,7 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 	int64_t C = (int64_t)(workspace_limit(rt) / col_bytes);
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, rt.column_chunk);
 	if (host_target) C = std::min<int64_t>(C, std::max<int64_t>(1, ((int64_t)256 << 20) / (N * 16)));
-	C = std::min(C, N);
+	C = std::min(C, ncols);
 	if (C < 1) {
 		fprintf(stderr, "rqcopt_gpu: one basis column needs %zu bytes of workspace, more than the limit\n", col_bytes);
 		return E_ALLOC;
@@ -494,8 +499,8 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 		hbasis = hcols + C * N;
 	}
 
-	for (int64_t b0 = 0; b0 < N; b0 += C) {
-		const int64_t Cc = std::min(C, N - b0);
+	for (int64_t b0 = 0; b0 < ncols; b0 += C) {
+		const int64_t Cc = std::min(C, ncols - b0);
 		const int64_t ngroups = Cc * (N / 4);
 
 		// target columns phi = -conj(U e_b)
@@ -504,6 +509,7 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 			for (int64_t cidx = 0; cidx < Cc; cidx++) {
 				memset(hbasis, 0, N * sizeof(double2));
 				hbasis[b0 + cidx].x = 1;
+				if (rt.real_pairs) hbasis[b0 + cidx + N / 2].y = 1;
 				statevector e = { reinterpret_cast<numeric*>(hbasis), L };
 				statevector u = { reinterpret_cast<numeric*>(hcols + cidx * N), L };
 				const int r = uf(&e, t.udata, &u);
@@ -578,7 +584,48 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 	return RQC_CUDA(cudaGetLastError());
 }
 
+int set_pair_half_fused(Runtime& rt, int64_t half);
+
+namespace {
+
+__global__ void k_real_part(double2* __restrict__ d, int64_t n)
+{
+	for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+		d[i].y = 0;
+}
+
+int set_pair_half(Runtime& rt, int64_t half)
+{
+	int ret = RQC_CUDA(cudaMemcpyToSymbolAsync(c_pair_half, &half, sizeof(half), 0, cudaMemcpyHostToDevice, rt.stream));
+	return ret ? ret : set_pair_half_fused(rt, half);
+}
+
+}  // namespace
+
+static int evaluate_columns(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision,
+                            double2* d_out);
+
+// With rt.real_pairs (real gates, real target): the 2^(L-1) paired columns
+// e_b + i e_{b + N/2}.  Every sum the engine forms pairs an adjoint-type state (from
+// -conj(U psi)) with a forward-type state, both propagated by real matrices, so its
+// real part is the sum of the two real columns' terms; the imaginary parts (cross
+// terms) are cleared.
 int evaluate(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out)
+{
+	if (!rt.real_pairs) return evaluate_columns(rt, c, t, mode, precision, d_out);
+	if (c.L < 2) return E_ARG;
+	int ret = set_pair_half(rt, (int64_t)1 << (c.L - 1));
+	if (!ret) ret = evaluate_columns(rt, c, t, mode, precision, d_out);
+	const int reset = set_pair_half(rt, 0);
+	if (!ret) ret = reset;
+	if (ret) return ret;
+	k_real_part<<<1, 256, 0, rt.stream>>>(d_out, (int64_t)result_count(c.ngates));
+	rt.launches++;
+	return RQC_CUDA(cudaGetLastError());
+}
+
+static int evaluate_columns(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision,
+                            double2* d_out)
 {
 	if (c.L < 2 || c.ngates < 1) return E_ARG;
 	for (int k = 0; k < 2 * c.ngates; k++)

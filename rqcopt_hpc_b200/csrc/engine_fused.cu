@@ -65,6 +65,16 @@ struct PassGeom
 	uint32_t rest_mask;    // state row bits that are not tile bits
 };
 
+// Paired basis columns (real-orthogonal problems): with c_pair_half = N/2 the column
+// with basis index b (< N/2) is e_b + i e_{b + N/2}; 0 selects plain basis columns.
+__constant__ int64_t c_pair_half = 0;
+
+__device__ __forceinline__ float basis_re(int64_t row, int64_t b) { return row == b ? 1.f : 0.f; }
+__device__ __forceinline__ float basis_im(int64_t row, int64_t b)
+{
+	return (c_pair_half != 0 && row == b + c_pair_half) ? 1.f : 0.f;
+}
+
 template <typename T> struct PassGates { Gate4<T> g[MAXK]; Gate4<T> z[MAXK]; };
 // W_k = G_k^+ Z_k G_k^+ of each gate of a pass (adjoint reconstruction of the tangent state)
 template <typename T> struct PassW { Gate4<T> w[MAXK]; };
@@ -165,7 +175,7 @@ __global__ void __launch_bounds__(TPB2) k2_fwd(const cplx<T>* __restrict__ psi, 
 				S[e] = psi[a];
 				if (TAN) dS[e] = dpsi[a];
 			} else {
-				S[e] = mk<T>(row == pg.b0 + col ? T(1) : T(0), T(0));
+				S[e] = mk<T>(T(basis_re(row, pg.b0 + col)), T(basis_im(row, pg.b0 + col)));
 				if (TAN) dS[e] = czero<V>();
 			}
 		}
@@ -290,7 +300,7 @@ __global__ void __launch_bounds__(TPB2, 1) k2_rev(const cplx<T>* __restrict__ ps
 			const int64_t row = rowbase + rowoff[r], col = colbase + cc;
 			const int64_t a = row * pg.C + col;
 			if (LAST) {
-				Psi[e] = mk<T>(row == pg.b0 + col ? T(1) : T(0), T(0));
+				Psi[e] = mk<T>(T(basis_re(row, pg.b0 + col)), T(basis_im(row, pg.b0 + col)));
 				if (TAN) dPsi[e] = czero<V>();
 			} else {
 				Psi[e] = psi[a];
@@ -594,7 +604,7 @@ __global__ void __launch_bounds__(NTF) k3_fwd(const double2* __restrict__ psi, c
 				if (TAN) dS[pe] = rb[i];
 			} else {
 				const int64_t row = rowbase + rowoff[r], col = colbase + cc;
-				S[pe] = make_double2(row == pg.b0 + col ? 1.0 : 0.0, 0.0);
+				S[pe] = make_double2(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col));
 				if (TAN) dS[pe] = make_double2(0, 0);
 			}
 		}
@@ -705,7 +715,7 @@ __global__ void __launch_bounds__(NTR, 1) k3_rev(const double2* __restrict__ psi
 			const int pe = sidx(r, cc);
 			if (LAST) {
 				const int64_t row = rowbase + rowoff[r], col = colbase + cc;
-				Psi[pe] = make_double2(row == pg.b0 + col ? 1.0 : 0.0, 0.0);
+				Psi[pe] = make_double2(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col));
 				if (TAN) dPsi[pe] = make_double2(0, 0);
 			} else {
 				Psi[pe] = ra[i];
@@ -1100,7 +1110,8 @@ __global__ void __launch_bounds__(NT4F, 3) k4_fwd(const float2* __restrict__ psi
 			} else {
 				const int64_t row = rowbase + ro[i], col = colbase + c2i;
 				*reinterpret_cast<float4*>(stage(buf, 0) + pe) =
-				    make_float4(row == pg.b0 + col ? 1.f : 0.f, 0.f, row == pg.b0 + col + 1 ? 1.f : 0.f, 0.f);
+				    make_float4(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col), basis_re(row, pg.b0 + col + 1),
+				                basis_im(row, pg.b0 + col + 1));
 				if (TAN) *reinterpret_cast<float4*>(stage(buf, 1) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
 			}
 			if (FSUM) cp_async16(stage(buf, NS - 1) + pe, phi + a);
@@ -1270,7 +1281,8 @@ __global__ void __launch_bounds__(NT4R, 1) k4_rev(const float2* __restrict__ psi
 			if (LAST) {
 				const int64_t row = rowbase + ro[i], col = colbase + c2i;
 				*reinterpret_cast<float4*>(stage(buf, 0) + pe) =
-				    make_float4(row == pg.b0 + col ? 1.f : 0.f, 0.f, row == pg.b0 + col + 1 ? 1.f : 0.f, 0.f);
+				    make_float4(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col), basis_re(row, pg.b0 + col + 1),
+				                basis_im(row, pg.b0 + col + 1));
 				if (TAN) *reinterpret_cast<float4*>(stage(buf, 2) + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
 			} else {
 				cp_async16(stage(buf, 0) + pe, psi + a);
@@ -2009,6 +2021,7 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	constexpr int CW = ColsPer<T>::v;
 	const int L = c.L, G = c.ngates;
 	const int64_t N = (int64_t)1 << L;
+	const int64_t ncols = rt.real_pairs ? N / 2 : N;   // (paired) basis columns
 	const bool tan = mode == EVAL_HVP;
 	const bool host_target = t.ufunc != nullptr;
 	std::vector<Pass> passes = schedule(L, G, c.wires, maxk);
@@ -2033,7 +2046,7 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	int64_t C = C_mem;
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, ((rt.column_chunk + CW - 1) / CW) * CW);
 	if (host_target) C = std::min<int64_t>(C, std::max<int64_t>(CW, ((int64_t)256 << 20) / (N * 16)));
-	C = std::min<int64_t>(C, ((N + CW - 1) / CW) * CW);
+	C = std::min<int64_t>(C, ((ncols + CW - 1) / CW) * CW);
 	C = (C / CW) * CW;
 	if (C < CW || C > C_mem) {
 		fprintf(stderr, "rqcopt_gpu: %d columns need %zu bytes of workspace, more than the limit\n", CW, CW * col_bytes);
@@ -2075,8 +2088,8 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 		dstage = reinterpret_cast<double2*>(rt.stage[2].ptr);
 	}
 
-	for (int64_t b0 = 0; b0 < N; b0 += C) {
-		const int64_t Cc = std::min(C, N - b0);
+	for (int64_t b0 = 0; b0 < ncols; b0 += C) {
+		const int64_t Cc = std::min(C, ncols - b0);
 		const int64_t ncg = (Cc + CW - 1) / CW;
 		auto geom = [&](const Pass& p) {
 			PassGeom g = p.geom;
@@ -2093,6 +2106,7 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 			for (int64_t j = 0; j < Cc; j++) {
 				memset(hbasis, 0, N * sizeof(double2));
 				hbasis[b0 + j].x = 1;
+				if (rt.real_pairs) hbasis[b0 + j + N / 2].y = 1;
 				statevector e = { reinterpret_cast<numeric*>(hbasis), L };
 				statevector u = { reinterpret_cast<numeric*>(hcols + j * N), L };
 				const int r = uf(&e, t.udata, &u);
@@ -2205,6 +2219,11 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 }
 
 }  // namespace
+
+int set_pair_half_fused(Runtime& rt, int64_t half)
+{
+	return RQC_CUDA(cudaMemcpyToSymbolAsync(c_pair_half, &half, sizeof(half), 0, cudaMemcpyHostToDevice, rt.stream));
+}
 
 int evaluate_fused(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, int maxk, double2* d_out)
 {

@@ -43,6 +43,7 @@ struct Runtime
 	double refine_threshold = 1e-5;
 	size_t workspace_limit = 0;
 	long column_chunk = 0;
+	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
 
 	// instrumentation
