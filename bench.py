@@ -747,10 +747,12 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving measurement")
     ap.add_argument("--no-hmat", action="store_true", help="skip the full-Hessian path measurement")
     ap.add_argument("--no-real", action="store_true", help="skip the real-orthogonal build measurement")
-    ap.add_argument("--hmat-case", choices=["target", "single"],
-                    help="run one full-Hessian evaluation at --L/--depth/--tdepth and exit (a small case for "
-                         "profilers): 'target' sums over all basis columns, 'single' is one state's "
-                         "forward + backward_hessian")
+    ap.add_argument("--hmat-case", choices=["target", "single", "sampling", "blockenc", "real"],
+                    help="run one evaluation at --L/--depth/--tdepth and exit (a small case for profilers): "
+                         "'target' the full Hessian over all basis columns, 'single' one state's forward + "
+                         "backward_hessian, 'sampling' the full Hessian from 64 Haar states, 'blockenc' the "
+                         "block-encoding Hessian with H of depth --tdepth on L/2 qubits, 'real' the real build's "
+                         "f + projected gradient + projected HVP")
     ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
     ap.add_argument("--serving-wall", type=float, default=45.0)
     a = ap.parse_args()
@@ -795,6 +797,20 @@ def main():
             f, g, H = gpu.brickwall_unitary_target_gradient_vector_hessian_matrix(
                 gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L)
             print(json.dumps({"hmat_case": "target", "L": L, "depth": depth, "f": f.real, "H_norm": float(np.abs(H).max())}))
+        elif a.hmat_case == "sampling":
+            f, g, H = gpu.brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(
+                gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L, 64, gpu.seed_rng_state(42))
+            print(json.dumps({"hmat_case": "sampling", "L": L, "depth": depth, "f": f.real}))
+        elif a.hmat_case == "blockenc":
+            vl, pm, hv, hp = _benc_case(L, depth, tdepth)
+            f, g, H = gpu.brickwall_blockenc_target_gradient_vector_hessian_matrix(gpu.Target(brickwall=(hv, hp)), vl, pm, L)
+            print(json.dumps({"hmat_case": "blockenc", "L": L, "depth": depth, "f": float(f)}))
+        elif a.hmat_case == "real":
+            from rqcopt_hpc_b200 import real
+            vl, pm, tv, tp, vd = _real_workload(L, depth, tdepth)
+            f, g, h = real.brickwall_unitary_target_projected_hessian_vector_product(real.Target(brickwall=(tv, tp)), vl,
+                                                                                     vd, pm, L)
+            print(json.dumps({"hmat_case": "real", "L": L, "depth": depth, "f": float(f)}))
         else:
             rng = np.random.default_rng(16)
             psi = (rng.standard_normal(1 << L) + 1j * rng.standard_normal(1 << L)) / np.sqrt(2 << L)
