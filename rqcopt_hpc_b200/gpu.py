@@ -117,6 +117,8 @@ _SIGS = {
     "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
+    "rqcopt_gpu_set_real_pairs": (None, [I]),
+    "rqcopt_gpu_set_real_samples": (None, [I]),
     "rqcopt_gpu_launch_count": (C.c_ulonglong, []),
     "rqcopt_gpu_reset_launch_count": (None, []),
     "rqcopt_gpu_enable_kernel_timing": (None, [I]),

@@ -400,3 +400,43 @@ def test_gpu_real_build_matches_real_oracle_at_l12(gpu):
     fo, gvo, hvo = o.brickwall_unitary_target_projected_hessian_vector_product(o.target("brickwall", (tv, tp)), vlist,
                                                                                vdirs, perms, L)
     assert abs(f - fo) <= 1e-12 * abs(fo) and rel_err(gv, gvo) <= 1e-12 and rel_err(hv, hvo) <= 1e-12
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("L,precision,gpp,chunk", [(14, "c128", 4, 0), (12, "mixed", 4, 0), (12, "c64", 4, 40),
+                                                   (10, "c128", 1, 24), (10, "c64", 1, 0)])
+def test_paired_columns_equal_plain_columns(gpu, L, precision, gpp, chunk):
+    """Size-independent check of the paired basis columns: the complex library on real
+    gates and a real target, with and without rqcopt_gpu_set_real_pairs, gives the same
+    f, gradient and HVP (real parts; complex128 1e-12, complex64 passes 1e-5 as the
+    mixed engine's own bar), on the fused engine (4 gates per pass) and the per-gate
+    engine (1), with ragged column chunks."""
+    vlist, perms, tv, tp = _real_instance(L, 6, 40 + L, 3, 41 + L)
+    rng = np.random.default_rng(L)
+    vdirs = np.stack([vlist[k] @ real_antisymm(rng.standard_normal(6)) for k in range(6)])
+    t = gpu.Target(brickwall=(tv.astype(complex), tp))
+    prec = {"c128": gpu.PRECISION_C128, "mixed": gpu.PRECISION_MIXED, "c64": gpu.PRECISION_C64}[precision]
+    tol = 1e-12 if precision == "c128" else 1e-5
+    gpu.set_precision(prec)
+    gpu.set_gates_per_pass(gpp)
+    gpu.set_column_chunk(chunk)
+    try:
+        plain = gpu.brickwall_unitary_target_hessian_vector_product(t, vlist.astype(complex), vdirs.astype(complex),
+                                                                     perms, L)
+        gpu.lib().rqcopt_gpu_set_real_pairs(1)
+        try:
+            paired = gpu.brickwall_unitary_target_hessian_vector_product(t, vlist.astype(complex),
+                                                                          vdirs.astype(complex), perms, L)
+        finally:
+            gpu.lib().rqcopt_gpu_set_real_pairs(0)
+    finally:
+        gpu.set_precision(gpu.PRECISION_C128)
+        gpu.set_gates_per_pass(4)
+        gpu.set_column_chunk(0)
+    f0, dv0, hv0 = plain
+    f1, dv1, hv1 = paired
+    assert abs(f1.imag) == 0 and np.all(dv1.imag == 0) and np.all(hv1.imag == 0)
+    assert abs(f1.real - f0.real) <= tol * abs(f0.real)
+    assert rel_err(dv1.real, dv0.real) <= tol and rel_err(hv1.real, hv0.real) <= tol
+    # the plain evaluation of a real problem has zero imaginary parts up to rounding
+    assert np.max(np.abs(dv0.imag)) <= 10 * tol * np.max(np.abs(dv0.real))
