@@ -599,6 +599,40 @@ def real_build_path(gpu, steps=3, L=14, depth=9, tdepth=5, seconds=8.0, with_ref
     return out
 
 
+def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50):
+    """The reference's Python module API (pymodule/rqcopt_module.c): optimize_brickwall_circuit
+    with a dense Haar-random 2^L x 2^L target U, through rqcopt_hpc_b200.rqcopt_hpc (the GPU
+    library) and through the reference module compiled in oracle/_ref (single-threaded C);
+    seconds per trust-region iteration."""
+    from rqcopt_hpc_b200 import rqcopt_hpc
+    rng = np.random.default_rng(seed)
+    z = (rng.standard_normal((1 << L, 1 << L)) + 1j * rng.standard_normal((1 << L, 1 << L))) / np.sqrt(2)
+    q, r = np.linalg.qr(z)
+    U = np.ascontiguousarray(q * (np.diagonal(r) / np.abs(np.diagonal(r))))
+    vlist, perms, _, _, _ = workload(L, depth, 1)
+    vl, pm = list(vlist), [list(map(int, p)) for p in perms]
+    rqcopt_hpc.optimize_brickwall_circuit(L, U, vl, pm, 1)
+    t0 = time.perf_counter()
+    _, f_iter = rqcopt_hpc.optimize_brickwall_circuit(L, U, vl, pm, niter)
+    wall = (time.perf_counter() - t0) / niter
+    out = {"workload": f"rqcopt_hpc.optimize_brickwall_circuit (the reference's Python module API), L={L} depth {depth}, "
+                       f"dense Haar-random target U, {niter} iterations", "seconds_per_iteration": wall,
+           "f_first": float(f_iter[0]), "f_final": float(f_iter[-1])}
+    from oracle.oracle import reference_module
+    ref = reference_module()
+    if ref is None:
+        return out
+    t0 = time.perf_counter()
+    _, fr = ref.optimize_brickwall_circuit(L, U, vl, pm, ref_niter)
+    tref = (time.perf_counter() - t0) / ref_niter
+    out["cpu_baseline"] = {"value": tref, "unit": "s per iteration", "cores": 1, "kind": "reference",
+                           "sample": f"{ref_niter} iterations of the reference module's optimize_brickwall_circuit "
+                                     f"(single-threaded C)"}
+    out["speedup_per_iteration"] = tref / wall
+    out["f_iter_max_rel_diff_vs_reference"] = float(np.max(np.abs(f_iter[:ref_niter + 1] - fr)) / np.max(np.abs(fr)))
+    return out
+
+
 def batched_c4(gpu, torch, count=512, niter=2):
     """512 independent brickwall instances (even L uniform over 6..12, depth over
     {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), niter trust-region iterations
@@ -943,6 +977,9 @@ def main():
             gpu.set_precision(prec)
         if not a.no_hmat and world == 1:
             line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
+            gpu.set_precision(prec)
+        if not a.no_hmat and world == 1:
+            line["front_end"] = front_end_path()
             gpu.set_precision(prec)
         if not a.no_real and world == 1:
             line["real_build"] = real_build_path(gpu, with_reference=not a.no_cpu_baseline)
