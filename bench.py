@@ -449,7 +449,10 @@ def hmat_path(gpu, torch, stream, hbm_peak, with_reference=True, steps=3):
     r5 = {"workload": f"block encoding || P^dag W P - H ||_F^2 / 2: f + gradient vector + Hessian matrix, brickwall "
                       f"L={L} depth {depth}, H a brickwall of depth {hdepth} on {L // 2} qubits, all {1 << (L // 2)} "
                       f"columns", "evals_per_s_e2e": 1.0 / wall, "ms_per_call": wall * 1e3, "sweep_ms": hs_ms,
-          "gpu_launches": launches}
+          "gpu_launches": launches,
+          "roofline": roofline(hess_model(L, depth, False), 1 << (L // 2), L, hs_ms, hs_n)}
+    r5["roofline"]["bytes_model"] += (" (the 2^(L/2) block-encoding columns; the tangents the sweep also carries "
+                                      "through the last gate are not counted)")
     out["blockenc_L12"] = r5
     if not have_ref:
         return out
@@ -573,10 +576,32 @@ def real_build_path(gpu, steps=3, L=14, depth=9, tdepth=5, seconds=8.0, with_ref
         f, g, h = ev()
     wall = (time.perf_counter() - t0) / steps
     launches = real.launch_count() // steps
+    # reverse-pass kernel time of one more evaluation (CUDA events around each launch)
+    gpu.enable_kernel_timing(True)
+    gpu.kernel_time(gpu.KC_REVERSE)
+    ev()
+    rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
+    gpu.enable_kernel_timing(False)
+    N = 1 << L
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    rbytes = float(6 * rev_n - 5) * N * (N // 2) * 16   # rev_n passes over N/2 paired columns
+    achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
     out = {"workload": f"real build: f + projected gradient (6 per gate) + projected HVP, real orthogonal brickwall "
-                       f"L={L} depth {depth} vs real brickwall target depth {tdepth}, all {1 << L} basis columns, "
-                       f"complex128 engine", "evals_per_s_e2e": 1.0 / wall, "ms_per_eval": wall * 1e3,
-           "gpu_launches": launches, "f": float(f)}
+                       f"L={L} depth {depth} vs real brickwall target depth {tdepth}, all {N} basis columns as "
+                       f"{N // 2} paired columns, complex128 engine", "evals_per_s_e2e": 1.0 / wall,
+           "ms_per_eval": wall * 1e3, "gpu_launches": launches, "f": float(f),
+           "roofline": {"kernel": "k3_rev (complex128 FP64-MMA gradient/HVP pass)", "bound": "hbm",
+                        "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak if achieved else None,
+                        "bytes_model": "(6P-5) x 2^L x 2^(L-1) x 16 B per evaluation (P reverse passes over the "
+                                       "paired columns)", "passes": rev_n, "reverse_ms": rev_ms,
+                        "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks
+                        else "fallback 6650 GB/s"}}
     from oracle.oracle import RealReference
     if not with_reference or not RealReference.available():
         return out

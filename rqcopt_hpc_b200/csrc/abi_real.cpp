@@ -199,14 +199,22 @@ struct HostCallback
 {
 	linear_func f;
 	void* data;
+	std::vector<double> re, im, ore, oim;   // column buffers, reused across calls
 };
 
 // a real linear_func applied to the complex column psi: its real and imaginary parts
 int host_callback(const cx::statevector* psi, void* udata, cx::statevector* out)
 {
-	const HostCallback* cb = static_cast<const HostCallback*>(udata);
+	HostCallback* cb = static_cast<HostCallback*>(udata);
 	const size_t n = dim(psi->nqubits);
-	std::vector<double> re(n), im(n), ore(n), oim(n, 0.0);
+	std::vector<double>& re = cb->re;
+	std::vector<double>& im = cb->im;
+	std::vector<double>& ore = cb->ore;
+	std::vector<double>& oim = cb->oim;
+	re.resize(n);
+	im.resize(n);
+	ore.resize(n);
+	oim.assign(n, 0.0);
 	bool has_im = false;
 	for (size_t k = 0; k < n; k++) {
 		re[k] = psi->data[k].real();
@@ -257,7 +265,8 @@ struct Target
 			f = sym<cx::linear_func>("rqcopt_dense_ufunc");
 			data = &dt;
 		} else {
-			cb = { ufunc, udata };
+			cb.f = ufunc;
+			cb.data = udata;
 			f = host_callback;
 			data = &cb;
 		}
