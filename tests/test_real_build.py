@@ -440,3 +440,19 @@ def test_paired_columns_equal_plain_columns(gpu, L, precision, gpp, chunk):
     assert rel_err(dv1.real, dv0.real) <= tol and rel_err(hv1.real, hv0.real) <= tol
     # the plain evaluation of a real problem has zero imaginary parts up to rounding
     assert np.max(np.abs(dv0.imag)) <= 10 * tol * np.max(np.abs(dv0.real))
+
+
+def test_real_library_rejects_invalid_arguments():
+    """Invalid sizes, permutations and wires are refused with the library's argument error
+    (-6) before any device work, as in the complex library (no GPU needed)."""
+    from rqcopt_hpc_b200 import real
+    vlist, perms, tv, tp = _real_instance(6, 3, 1, 2, 2)
+    t = real.Target(brickwall=(tv, tp))
+    calls = [lambda: real.brickwall_unitary_target(t, vlist, perms, 5),
+             lambda: real.brickwall_unitary_target_and_projected_gradient(t, vlist, np.zeros((3, 6), np.int32), 6),
+             lambda: real.circuit_unitary_target(t, vlist, [[0, 0], [1, 2], [2, 3]], 6),
+             lambda: real.brickwall_blockenc_target(t, vlist, perms, 5)]
+    for call in calls:
+        with pytest.raises(real.RqcError) as e:
+            call()
+        assert e.value.code == -6
