@@ -104,11 +104,11 @@ extern "C" void apply_gate_to_array(const struct mat4x4* gate, const int i, cons
                                     const struct statevector_array* psi, struct statevector_array* psi_out)
 {
 	const char* fn = "apply_gate_to_array";
-	Runtime* rt = runtime();
-	if (!rt) return fail_void(fn, E_CUDA);
 	if (!gate || !psi || !psi_out || !psi->data || !psi_out->data || psi->nqubits != psi_out->nqubits ||
 	    psi->nstates != psi_out->nstates || psi->nstates < 1 || !wires_ok(psi->nqubits, i, j))
 		return fail_void(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return fail_void(fn, E_CUDA);
 	const size_t bytes = sv_bytes(psi->nqubits) * psi->nstates;
 	DeviceSpan in, out;
 	int ret = span_in(*rt, psi->data, bytes, 0, in);
@@ -125,12 +125,12 @@ extern "C" void apply_gate_backward_array(const struct mat4x4* gate, const int i
                                           struct mat4x4* dgates)
 {
 	const char* fn = "apply_gate_backward_array";
-	Runtime* rt = runtime();
-	if (!rt) return fail_void(fn, E_CUDA);
 	// the gate itself does not enter the gate gradients (src/gate.c:269-377)
 	if (!gate || !psi || !dpsi_out || !dgates || !psi->data || !dpsi_out->data || psi->nqubits != dpsi_out->nqubits ||
 	    psi->nstates < 1 || !wires_ok(psi->nqubits, i, j))
 		return fail_void(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return fail_void(fn, E_CUDA);
 	const int L = psi->nqubits, ns = psi->nstates;
 	DeviceSpan in, dout;
 	int ret = span_in(*rt, psi->data, sv_bytes(L) * ns, 0, in);
@@ -148,11 +148,11 @@ extern "C" void apply_gate_placeholder(const int i, const int j, const struct st
                                        struct statevector_array* psi_out)
 {
 	const char* fn = "apply_gate_placeholder";
-	Runtime* rt = runtime();
-	if (!rt) return fail_void(fn, E_CUDA);
 	if (!psi || !psi_out || !psi->data || !psi_out->data || psi->nqubits != psi_out->nqubits || psi_out->nstates != 16 ||
 	    !wires_ok(psi->nqubits, i, j))
 		return fail_void(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return fail_void(fn, E_CUDA);
 	const int L = psi->nqubits;
 	DeviceSpan in, out;
 	int ret = span_in(*rt, psi->data, sv_bytes(L), 0, in);
@@ -171,14 +171,14 @@ extern "C" int brickwall_unitary_backward_hessian(const struct mat4x4 vlist[], i
                                                   struct mat4x4 dvlist[], numeric* hess)
 {
 	const char* fn = "brickwall_unitary_backward_hessian";
-	Runtime* rt = runtime();
-	if (!rt) return E_CUDA;
 	std::vector<double2> ug;
 	std::vector<int> wires;
 	if (!dpsi || !dpsi_out || !cache || !dvlist || !hess || !dpsi->data || !dpsi_out->data ||
 	    dpsi_out->nqubits != dpsi->nqubits || !brickwall_of(dpsi->nqubits, nlayers, vlist, perms, ug, wires) ||
 	    cache->nqubits != dpsi->nqubits || cache->ngates != nlayers * (dpsi->nqubits / 2) || !cache->psi_list)
 		return fail(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
 	const int L = dpsi->nqubits, G = cache->ngates, m = 16 * nlayers;
 	const size_t N = (size_t)1 << L;
 	for (int k = 0; k < G; k++)
@@ -213,14 +213,14 @@ extern "C" int apply_brickwall_unitary_gate_placeholder(const struct mat4x4 vlis
                                                         struct statevector_array* psi_out)
 {
 	const char* fn = "apply_brickwall_unitary_gate_placeholder";
-	Runtime* rt = runtime();
-	if (!rt) return E_CUDA;
 	std::vector<double2> ug;
 	std::vector<int> wires;
 	if (!cache || !psi_out || !psi_out->data || psi_out->nstates != 16 || cache->nqubits != psi_out->nqubits ||
 	    !brickwall_of(cache->nqubits, nlayers, vlist, perms, ug, wires) || cache->ngates != nlayers * (cache->nqubits / 2) ||
 	    l < 0 || l >= nlayers || !cache->psi_list)
 		return fail(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
 	const int L = cache->nqubits, per = L / 2, G = cache->ngates;
 	const size_t N = (size_t)1 << L;
 	for (int p = 0; p < per; p++)
@@ -260,13 +260,13 @@ int hessian_target(const char* fn, linear_func ufunc, void* udata, const struct 
                    int nqubits, const int* perms[], numeric* fval, struct mat4x4* dvlist, numeric* hess,
                    double* grad_vec, double* H, const SampleSpec* samp = nullptr)
 {
-	Runtime* rt = runtime();
-	if (!rt) return E_CUDA;
 	std::vector<double2> ug;
 	std::vector<int> wires;
 	TargetHolder th;
 	if (!brickwall_of(nqubits, nlayers, vlist, perms, ug, wires) || !th.set(ufunc, udata, nqubits))
 		return fail(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
 	const int m = 16 * nlayers;
 	const size_t nrec = hess_record_count(nlayers);
 	// device: record | layer gates | gradient vector | real Hessian
@@ -375,10 +375,10 @@ void pcg32_seed(struct pcg32_random* g, uint64_t initstate, uint64_t initseq)
 int sampled_value(const char* fn, linear_func ufunc, void* udata, const std::vector<double2>& gates,
                   const std::vector<int>& wires, int nqubits, long nsamples, struct rng_state* rng, numeric* fval)
 {
-	Runtime* rt = runtime();
-	if (!rt) return E_CUDA;
 	TargetHolder th;
 	if (!th.set(ufunc, udata, nqubits)) return fail(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
 	int ret = ensure_device(rt->result, sizeof(double2));
 	if (ret) return ret;
 	double2* d_f = static_cast<double2*>(rt->result.ptr);
@@ -415,9 +415,9 @@ extern "C" void seed_rng_state(const uint64_t seed, struct rng_state* state)
 extern "C" void haar_random_statevector(struct statevector* psi, struct rng_state* rng)
 {
 	const char* fn = "haar_random_statevector";
+	if (!psi || !psi->data || !rng || psi->nqubits < 0 || psi->nqubits > 40) return fail_void(fn, E_ARG);
 	Runtime* rt = runtime();
 	if (!rt) return fail_void(fn, E_CUDA);
-	if (!psi || !psi->data || !rng || psi->nqubits < 0 || psi->nqubits > 40) return fail_void(fn, E_ARG);
 	const int L = psi->nqubits;
 	DeviceSpan out;
 	int ret = span_out(*rt, psi->data, sv_bytes(L), 0, out);
@@ -466,13 +466,13 @@ int blockenc(const char* fn, linear_func hfunc, void* hdata, const struct mat4x4
              const int* perms[], int mode, double* fval, struct mat4x4* dvlist, double* grad_vec, numeric* hess1,
              numeric* hess2, double* H)
 {
-	Runtime* rt = runtime();
-	if (!rt) return E_CUDA;
 	std::vector<double2> ug;
 	std::vector<int> wires;
 	TargetHolder th;
 	if (!fval || !brickwall_of(nqubits, nlayers, vlist, perms, ug, wires) || !th.set(hfunc, hdata, nqubits / 2))
 		return fail(fn, E_ARG);
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
 	const int m = 16 * nlayers;
 	const size_t nrec = hess_record_count(nlayers);
 	// device: record | hess2 | layer gates | gradient vector | real Hessian
