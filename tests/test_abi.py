@@ -112,3 +112,24 @@ def test_signatures_match_reference(header, complex_build):
     if not complex_build:
         # the real build has none of the full-Hessian matrix forms
         assert not {n for n in ours if "hessian_matrix" in n or "hmat_sampling" in n or n.endswith("_hmat")} - {"truncated_cg_hmat", "riemannian_trust_region_optimize_hmat"}
+
+
+def test_invalid_arguments_refused_before_device_work():
+    """The full-Hessian, sampling and block-encoding entry points refuse invalid sizes
+    and permutations with the argument error (-6) before touching the device (no GPU needed)."""
+    import numpy as np
+    from rqcopt_hpc_b200 import gpu
+    from helpers import brickwall_instance
+    vlist, perms, tv, tp = brickwall_instance(6, 3, 1, 2, 2)
+    t = gpu.Target(brickwall=(tv, tp))
+    bad_perms = np.zeros((3, 6), np.int32)
+    calls = [lambda: gpu.brickwall_unitary_target_gradient_hessian(t, vlist, perms, 5),
+             lambda: gpu.brickwall_unitary_target_gradient_vector_hessian_matrix(t, vlist, bad_perms, 6),
+             lambda: gpu.brickwall_unitary_target_gradient_hessian_sampling(t, vlist, perms, 7, 10,
+                                                                            gpu.seed_rng_state(1)),
+             lambda: gpu.brickwall_blockenc_target_and_gradient(t, vlist, perms, 5),
+             lambda: gpu.brickwall_blockenc_target_gradient_vector_hessian_matrix(t, vlist, bad_perms, 6)]
+    for call in calls:
+        with pytest.raises(gpu.RqcError) as e:
+            call()
+        assert e.value.code == -6
