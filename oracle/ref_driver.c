@@ -126,7 +126,7 @@ int refdrv_brickwall_projected_hvp(const struct mat4x4* vlist, const struct mat4
 	return ret;
 }
 
-/* the north-star driver with a brickwall target and default RTR parameters */
+/* optimize_brickwall_circuit_hvp with a brickwall target and default RTR parameters */
 void refdrv_optimize_brickwall(const struct mat4x4* vstart, int nlayers, int L, const int* perms_flat,
                                const struct mat4x4* tvlist, int tnlayers, const int* tperms_flat,
                                int niter, double* f_iter, struct mat4x4* vopt)
