@@ -1,12 +1,15 @@
-"""Minimal read-only HDF5 reader for the reference's test fixtures.
+"""Minimal read-only HDF5 reader for the files of the rqcopt_hpc project: the test
+fixtures (test/data/*.hdf5) and the example inputs and outputs (examples/*/*.hdf5).
 
-The fixtures under the reference's ``test/data/`` directory are small HDF5
-files written by h5py with the "earliest" file format: superblock version 0,
-a root group stored as a symbol table (version-1 B-tree plus local heap),
-version-1 object headers, and contiguous or compact datasets of little-endian
-IEEE doubles or integers.  Only that subset is implemented; anything else
-raises ``ValueError``.  h5py and libhdf5 are not available in this
-environment, which is why this reader exists.
+Those files are small HDF5 files written by h5py or libhdf5 with the "earliest" file
+format: superblock version 0, a root group stored as a symbol table (version-1 B-tree
+plus local heap), version-1 object headers, and contiguous or compact datasets of
+little-endian IEEE doubles or integers.  Only that subset is implemented; anything
+else raises ``ValueError``.  It exists because h5py and libhdf5 are not available
+everywhere this library runs.
+
+    from rqcopt_hpc_b200 import h5read
+    arrays = h5read.read_all("ising1d_dynamics_opt_n3_init.hdf5")   # {name: numpy array}
 """
 from __future__ import annotations
 

@@ -8,15 +8,17 @@ Each ``test_<name>_cplx.hdf5`` (complex-circuit fixtures of the reference's
 ``test/data`` directory, generated there by ``test/test_*.py``) becomes
 ``tests/golden/<name>.npz`` with the same dataset names and the interleaved
 (real, imag) layout unchanged; the real-build fixtures (``test_<name>_real.hdf5``)
-go to ``tests/golden/real/``.  The reader is ``hdf5_lite`` in this folder.
+go to ``tests/golden/real/``, and the ising1d example's input and the outputs the
+reference stored for it (``examples/ising1d/*.hdf5``) to ``tests/golden/examples/``.
+The reader is ``rqcopt_hpc_b200.h5read``.
 """
 import os
 import sys
 
 import numpy as np
 
-sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
-import hdf5_lite  # noqa: E402
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+from rqcopt_hpc_b200 import h5read  # noqa: E402
 
 FIXTURES = [
     "apply_gate", "apply_gate_backward", "apply_quantum_circuit", "quantum_circuit_backward",
@@ -55,18 +57,33 @@ REAL_FIXTURES = [
 ]
 
 
+# the ising1d example of the reference (examples/ising1d): input, and the outputs of
+# ising1d_dynamics_opt.c (full-Hessian trust region, 10 iterations) and
+# ising1d_dynamics_opt_sampling.c (16 samples, seed 42)
+EXAMPLES = {
+    "ising1d_n3_init": "ising1d/ising1d_dynamics_opt_n3_init.hdf5",
+    "ising1d_n3": "ising1d/ising1d_dynamics_opt_n3.hdf5",
+    "ising1d_sampling_n3": "ising1d/ising1d_dynamics_opt_sampling_n3.hdf5",
+}
+
+
 def main(data_dir):
     out_dir = os.path.dirname(os.path.abspath(__file__))
     for name in FIXTURES:
-        arrays = hdf5_lite.read_all(os.path.join(data_dir, f"test_{name}_cplx.hdf5"))
+        arrays = h5read.read_all(os.path.join(data_dir, f"test_{name}_cplx.hdf5"))
         np.savez(os.path.join(out_dir, f"{name}.npz"), **arrays)
     os.makedirs(os.path.join(out_dir, "real"), exist_ok=True)
     for name in REAL_FIXTURES:
-        arrays = hdf5_lite.read_all(os.path.join(data_dir, f"test_{name}_real.hdf5"))
+        arrays = h5read.read_all(os.path.join(data_dir, f"test_{name}_real.hdf5"))
         np.savez(os.path.join(out_dir, "real", f"{name}.npz"), **arrays)
-    arrays = hdf5_lite.read_all(os.path.join(data_dir, "test_truncated_cg.hdf5"))
+    arrays = h5read.read_all(os.path.join(data_dir, "test_truncated_cg.hdf5"))
     np.savez(os.path.join(out_dir, "truncated_cg.npz"), **arrays)
-    print(f"wrote {len(FIXTURES) + 1} + {len(REAL_FIXTURES)} (real build) fixtures to {out_dir}")
+    examples_dir = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(data_dir))), "examples")
+    os.makedirs(os.path.join(out_dir, "examples"), exist_ok=True)
+    for name, rel in EXAMPLES.items():
+        arrays = h5read.read_all(os.path.join(examples_dir, rel))
+        np.savez(os.path.join(out_dir, "examples", f"{name}.npz"), **arrays)
+    print(f"wrote {len(FIXTURES) + 1} + {len(REAL_FIXTURES)} (real build) + {len(EXAMPLES)} (example) fixtures to {out_dir}")
 
 
 if __name__ == "__main__":
