@@ -9,7 +9,8 @@ Each ``test_<name>_cplx.hdf5`` (complex-circuit fixtures of the reference's
 ``tests/golden/<name>.npz`` with the same dataset names and the interleaved
 (real, imag) layout unchanged; the real-build fixtures (``test_<name>_real.hdf5``)
 go to ``tests/golden/real/``, and the ising1d example's input and the outputs the
-reference stored for it (``examples/ising1d/*.hdf5``) to ``tests/golden/examples/``.
+reference stored for it (``examples/ising1d/*.hdf5``), and the same for the
+molecular example, to ``tests/golden/examples/``.
 The reader is ``rqcopt_hpc_b200.h5read``.
 """
 import os
@@ -57,13 +58,16 @@ REAL_FIXTURES = [
 ]
 
 
-# the ising1d example of the reference (examples/ising1d): input, and the outputs of
+# the example inputs and the outputs the reference stored for them: ising1d (examples/ising1d),
 # ising1d_dynamics_opt.c (full-Hessian trust region, 10 iterations) and
 # ising1d_dynamics_opt_sampling.c (16 samples, seed 42)
 EXAMPLES = {
     "ising1d_n3_init": "ising1d/ising1d_dynamics_opt_n3_init.hdf5",
     "ising1d_n3": "ising1d/ising1d_dynamics_opt_n3.hdf5",
     "ising1d_sampling_n3": "ising1d/ising1d_dynamics_opt_sampling_n3.hdf5",
+    # examples/molecular/molecular_dynamics_opt.c: general circuit, HVP trust region
+    "molecular_init": "molecular/molecular_dynamics_opt_init.hdf5",
+    "molecular": "molecular/molecular_dynamics_opt.hdf5",
 }
 
 

@@ -1,11 +1,12 @@
-"""The reference's ising1d example (examples/ising1d): its input and the outputs the
-reference stored for it (full-Hessian trust region, and its sampling form with 16
-samples and seed 42; 10 iterations each) as golden vectors.
+"""The reference's examples as golden vectors: their inputs and the outputs the
+reference stored for them.  ising1d (examples/ising1d): full-Hessian trust region, and
+its sampling form with 16 samples and seed 42.  molecular (examples/molecular): HVP
+trust region on a general circuit.  10 iterations each.
 
 CPU: the HDF5 reader reads the example files (where the reference is present); the
-compiled reference module reproduces the stored full-Hessian run exactly, and the
-oracle restatement to 1e-12 (f iterates) and 1e-9 (gates).  GPU: the library through
-the Python module to 1e-10 and 1e-9.
+compiled reference module reproduces the stored full-Hessian and molecular runs
+exactly, and the oracle restatement to 1e-12 (f iterates) and 1e-9 (gates).  GPU: the
+library through the Python module to 1e-10 and 1e-9.
 
 The sampling run is pinned through its first 8 iterates (f_iter[0..7]).  Its Haar
 states come from libm's log and sin, whose last bits differ between machines.  The
@@ -21,7 +22,7 @@ from helpers import GOLDEN
 from oracle.oracle import reference_module
 
 EX = os.path.join(GOLDEN, "examples")
-REF_EXAMPLES = "/root/reference/examples/ising1d"
+REF_EXAMPLES = "/root/reference/examples"
 
 
 def _load(name):
@@ -30,20 +31,26 @@ def _load(name):
 
 
 def _init():
-    from rqcopt_hpc_b200.ising1d import load_init
-    return load_init(_load("ising1d_n3_init"))
+    from rqcopt_hpc_b200.examples import load_ising1d
+    return load_ising1d(_load("ising1d_n3_init"))
 
 
-def _expected(name):
+def _expected(name, key="Vlist"):
     d = _load(name)
-    return d["Vlist"][..., 0] + 1j * d["Vlist"][..., 1], d["f_iter"]
+    return d[key][..., 0] + 1j * d[key][..., 1], d["f_iter"]
+
+
+def _molecular():
+    from rqcopt_hpc_b200.examples import load_molecular
+    return load_molecular(_load("molecular_init"))
 
 
 @pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
 def test_reader_reads_the_example_files():
     from rqcopt_hpc_b200 import h5read
-    for f, name in [("ising1d_dynamics_opt_n3_init.hdf5", "ising1d_n3_init"),
-                    ("ising1d_dynamics_opt_n3.hdf5", "ising1d_n3")]:
+    for f, name in [("ising1d/ising1d_dynamics_opt_n3_init.hdf5", "ising1d_n3_init"),
+                    ("ising1d/ising1d_dynamics_opt_n3.hdf5", "ising1d_n3"),
+                    ("molecular/molecular_dynamics_opt_init.hdf5", "molecular_init")]:
         a, b = h5read.read_all(os.path.join(REF_EXAMPLES, f)), _load(name)
         assert sorted(a) == sorted(b) and all(np.array_equal(a[k], b[k]) for k in a)
 
@@ -80,12 +87,37 @@ def test_oracle_reproduces_stored_outputs(oracle, sampling):
         assert np.max(np.abs(vo - ve)) <= 1e-9
 
 
+@pytest.mark.skipif(reference_module() is None, reason="reference module build not present")
+def test_reference_module_reproduces_stored_molecular_run():
+    u, g, w = _molecular()
+    go, fi = reference_module().optimize_quantum_circuit(5, u, list(g), w, 10)
+    ge, fe = _expected("molecular", "gates")
+    assert np.array_equal(fi, fe) and np.array_equal(go, ge)
+
+
+def test_oracle_reproduces_stored_molecular_run(oracle):
+    u, g, w = _molecular()
+    fi, go = oracle.optimize_quantum_circuit(oracle.target("dense", u), g, np.asarray(w, np.int32), 5, 10)[:2]
+    ge, fe = _expected("molecular", "gates")
+    assert np.max(np.abs(fi - fe)) <= 1e-12 * np.max(np.abs(fe))
+    assert np.max(np.abs(go - ge)) <= 1e-9
+
+
+@pytest.mark.gpu
+def test_gpu_reproduces_stored_molecular_run(gpu):
+    from rqcopt_hpc_b200.examples import run_molecular
+    go, fi, _ = run_molecular(*_molecular(), 10)
+    ge, fe = _expected("molecular", "gates")
+    assert np.max(np.abs(fi - fe)) <= 1e-10 * np.max(np.abs(fe))
+    assert np.max(np.abs(go - ge)) <= 1e-9
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("sampling", [False, True])
 def test_gpu_reproduces_stored_outputs(gpu, sampling):
-    from rqcopt_hpc_b200.ising1d import run
+    from rqcopt_hpc_b200.examples import run_ising1d
     u, v, perms = _init()
-    vo, fi, _ = run(u, v, perms, 10, sampling)
+    vo, fi, _ = run_ising1d(u, v, perms, 10, sampling)
     ve, fe = _expected("ising1d_sampling_n3" if sampling else "ising1d_n3")
     n = 8 if sampling else len(fe)
     assert np.max(np.abs(fi[:n] - fe[:n])) <= 1e-10 * np.max(np.abs(fe))
