@@ -2,7 +2,7 @@
  * CPU oracle for the rqcopt_hpc matrix-free circuit-optimisation path.
  *
  * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
- * algorithm (cmendl/rqcopt_hpc, src/*.c) used as the checker for the GPU
+ * algorithm (the C sources of cmendl/rqcopt_hpc, src/) used as the checker for the GPU
  * library.  Only the tests, the smoke check and the CPU-baseline leg of the
  * benchmark load it; the product library never links or calls it.
  *
