@@ -130,3 +130,38 @@ def test_gpu_reproduces_stored_outputs(gpu, sampling):
     assert np.max(np.abs(fi[:n] - fe[:n])) <= 1e-10 * np.max(np.abs(fe))
     if not sampling:
         assert np.max(np.abs(vo - ve)) <= 1e-9
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_EXAMPLES), reason="reference examples not present")
+def test_driver_command_line(tmp_path, monkeypatch, capsys):
+    """The driver reads the example's HDF5 input, passes the reference driver's arguments
+    to the Python module, prints the iterates and writes the reference's output layout
+    (the optimisation itself is stubbed here; the GPU tests above run it)."""
+    from rqcopt_hpc_b200 import examples, rqcopt_hpc
+    calls = {}
+
+    def fake_brickwall(L, U, vlist, perms, niter, **kw):
+        calls["brickwall"] = (L, U.shape, len(vlist), perms, niter, kw)
+        return np.stack(vlist), np.arange(niter + 1, dtype=float)
+
+    def fake_circuit(n, U, gates, wires, niter):
+        calls["circuit"] = (n, U.shape, len(gates), wires, niter)
+        return np.stack(gates), np.arange(niter + 1, dtype=float)
+
+    monkeypatch.setattr(rqcopt_hpc, "optimize_brickwall_circuit", fake_brickwall)
+    monkeypatch.setattr(rqcopt_hpc, "optimize_quantum_circuit", fake_circuit)
+    out = tmp_path / "r.npz"
+    examples.main(["ising1d", os.path.join(REF_EXAMPLES, "ising1d/ising1d_dynamics_opt_n3_init.hdf5"), "--sampling",
+                   "--out", str(out)])
+    L, ushape, nl, perms, niter, kw = calls["brickwall"]
+    assert (L, ushape, nl, niter, kw) == (6, (64, 64), 3, 10, {"nsamples": 16, "seed": 42})
+    assert perms == [p.tolist() for p in _load("ising1d_n3_init").values() if p.dtype == np.int32]
+    with np.load(out) as z:
+        assert z["Vlist"].shape == (3, 4, 4, 2) and z["f_iter"].shape == (11,)
+    assert "f_iter[10] = 10.000000000000" in capsys.readouterr().out
+    examples.main(["molecular", os.path.join(REF_EXAMPLES, "molecular/molecular_dynamics_opt_init.hdf5"),
+                   "--out", str(out)])
+    n, ushape, ng, wires, niter = calls["circuit"]
+    assert (n, ushape, ng, len(wires), niter) == (5, (32, 32), 18, 18, 10)
+    with np.load(out) as z:
+        assert z["gates"].shape == (18, 4, 4, 2)
