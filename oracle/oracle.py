@@ -380,6 +380,18 @@ class Oracle:
                                        C.byref(SV(out.ctypes.data, L)))
         return out, states
 
+    def brickwall_unitary_backward(self, vlist, perms, states, dpsi_out):
+        """src/brickwall_circuit.c:85-124: the backward pass of the brickwall as a sequential
+        circuit (layer l's gate on pairs (perms[l][2p], perms[l][2p + 1])), the gate
+        gradients of each layer's L/2 pairs summed into the layer gradient."""
+        vlist, perms, dpsi_out = _c(vlist), _i(perms), _c(dpsi_out)
+        L, nl = _nq(dpsi_out), vlist.shape[0]
+        per = L // 2
+        gates = np.repeat(vlist, per, axis=0)
+        wires = np.stack([perms[l, 2 * p:2 * p + 2] for l in range(nl) for p in range(per)])
+        dpsi, dg = self.quantum_circuit_backward(gates, wires, [_c(s) for s in states], dpsi_out)
+        return dpsi, dg.reshape(nl, per, 4, 4).sum(axis=1)
+
     def brickwall_unitary_backward_hessian(self, vlist, perms, states, dpsi_out):
         vlist, perms, dpsi_out = _c(vlist), _i(perms), _c(dpsi_out)
         L, nl = _nq(dpsi_out), vlist.shape[0]

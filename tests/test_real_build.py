@@ -138,6 +138,17 @@ def test_apply_brickwall_unitary(impl):
         assert udist(impl.apply_brickwall_unitary(vlist[:nl], perms[:nl], d["psi"]), d[f"chi{k}"]) <= 1e-12
 
 
+def test_brickwall_unitary_backward(impl):
+    d = golden_real("brickwall_unitary_backward")
+    vlist, perms, psi, dout = stack(d, "V", 4), stack(d, "perm", 4), d["psi"], d["dpsi_out"]
+    for nl in (3, 4):
+        out, cache = impl.brickwall_unitary_forward(vlist[:nl], perms[:nl], psi)
+        assert udist(out, d[f"psi_out{nl - 3}"]) <= 1e-12
+        dpsi, dv = impl.brickwall_unitary_backward(vlist[:nl], perms[:nl], cache, dout)
+        assert udist(dpsi, _ngrad(lambda x: impl.apply_brickwall_unitary(vlist[:nl], perms[:nl], x), psi, dout)) <= 1e-8
+        assert udist(dv, _ngrad(lambda v: impl.apply_brickwall_unitary(v, perms[:nl], psi), vlist[:nl], dout)) <= 1e-8
+
+
 def test_brickwall_unitary_backward_hessian(impl):
     d = golden_real("brickwall_unitary_backward_hessian")
     V, Z, P, psi, dout = stack(d, "V", 4), stack(d, "Z", 4), stack(d, "perm", 4), d["psi"], d["dpsi_out"]

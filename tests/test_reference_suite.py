@@ -95,8 +95,6 @@ def test_apply_brickwall_unitary(impl):
 
 
 def test_brickwall_unitary_backward(impl):
-    if impl.name == "oracle":
-        pytest.skip("the oracle restates the brickwall backward through the circuit backward (checked above)")
     d = golden("brickwall_unitary_backward")
     vlist, perms, psi, dout = stack(d, "V", 4), stack(d, "perm", 4), d["psi"], d["dpsi_out"]
     for nl in [3, 4]:
