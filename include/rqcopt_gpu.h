@@ -102,6 +102,8 @@ int allocate_statevector(int nqubits, struct statevector* psi);
 void free_statevector(struct statevector* psi);
 /* src/statevector.h:32 */
 void add_statevectors(const struct statevector* psi1, const struct statevector* psi2, struct statevector* psi_sum);
+/* src/statevector.h:26 -- permutes qubit wires on the host (device statevectors through host copies) */
+void transpose_statevector(const struct statevector* psi, const int* perm, struct statevector* psi_trans);
 /* src/rng.h:21 */
 void seed_rng_state(const uint64_t seed, struct rng_state* state);
 /* src/statevector.h:29 -- generated on the GPU; advances rng exactly as the reference does */

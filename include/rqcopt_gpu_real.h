@@ -94,6 +94,8 @@ int allocate_statevector(int nqubits, struct statevector* psi);                 
 void free_statevector(struct statevector* psi);                                       /* src/statevector.h:20 */
 void add_statevectors(const struct statevector* psi1, const struct statevector* psi2,
 	struct statevector* psi_sum);                                                     /* src/statevector.h:32 */
+void transpose_statevector(const struct statevector* psi, const int* perm,
+	struct statevector* psi_trans);                                                   /* src/statevector.h:26 */
 void seed_rng_state(const uint64_t seed, struct rng_state* state);                    /* src/rng.h:21 */
 /* src/statevector.h:29 -- real normal entries (src/statevector.c:115-121), drawn on the GPU */
 void haar_random_statevector(struct statevector* psi, struct rng_state* rng);

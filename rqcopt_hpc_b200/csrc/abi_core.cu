@@ -102,6 +102,54 @@ extern "C" void add_statevectors(const struct statevector* psi1, const struct st
 	if (ret) set_last_error(ret);
 }
 
+// psi_trans[j] = psi[k], k the index j with qubit i moved to qubit perm[i]
+// (src/statevector.c:72-98).  A wire permutation, not on the optimisation path: it
+// runs on the host, with device-memory statevectors copied through host memory.
+extern "C" void transpose_statevector(const struct statevector* psi, const int* perm, struct statevector* psi_trans)
+{
+	if (!psi || !psi_trans || !perm || !psi->data || !psi_trans->data || psi->nqubits != psi_trans->nqubits ||
+	    psi->nqubits < 0 || psi->nqubits > 40) {
+		fail_arg("transpose_statevector", "invalid statevectors");
+		return;
+	}
+	const int L = psi->nqubits;
+	std::vector<int64_t> strides(L > 0 ? L : 1);
+	std::vector<char> seen(L > 0 ? L : 1, 0);
+	for (int i = 0; i < L; i++) {
+		if (perm[i] < 0 || perm[i] >= L || seen[perm[i]]) {
+			fail_arg("transpose_statevector", "'perm' is not a permutation of the qubits");
+			return;
+		}
+		seen[perm[i]] = 1;
+		strides[L - 1 - i] = (int64_t)1 << (L - 1 - perm[i]);
+	}
+	// device statevectors are permuted in host copies (host and managed memory in place)
+	auto on_device = [](const void* p) {
+		cudaPointerAttributes a;
+		if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+			cudaGetLastError();
+			return false;
+		}
+		return a.type == cudaMemoryTypeDevice;
+	};
+	const int64_t n = (int64_t)1 << L;
+	const bool din = on_device(psi->data), dout = on_device(psi_trans->data);
+	std::vector<double2> hin(din ? n : 0), hout(dout ? n : 0);
+	if (din && RQC_CUDA(cudaMemcpy(hin.data(), psi->data, n * sizeof(double2), cudaMemcpyDeviceToHost))) {
+		set_last_error(E_CUDA);
+		return;
+	}
+	const double2* src = din ? hin.data() : reinterpret_cast<const double2*>(psi->data);
+	double2* dst = dout ? hout.data() : reinterpret_cast<double2*>(psi_trans->data);
+	for (int64_t j = 0; j < n; j++) {
+		int64_t k = 0;
+		for (int i = 0; i < L; i++) k += ((j >> i) & 1) * strides[i];
+		dst[j] = src[k];
+	}
+	if (dout && RQC_CUDA(cudaMemcpy(psi_trans->data, hout.data(), n * sizeof(double2), cudaMemcpyHostToDevice)))
+		set_last_error(E_CUDA);
+}
+
 // ------------------------------------------------------------------------- gates
 
 extern "C" void apply_gate(const struct mat4x4* gate, const int i, const int j, const struct statevector* psi,

@@ -334,6 +334,32 @@ void add_statevectors(const struct statevector* psi1, const struct statevector* 
 	for (size_t k = 0; k < dim(psi1->nqubits); k++) psi_sum->data[k] = psi1->data[k] + psi2->data[k];
 }
 
+// psi_trans[j] = psi[k], k the index j with qubit i moved to qubit perm[i] (src/statevector.c:72-98)
+void transpose_statevector(const struct statevector* psi, const int* perm, struct statevector* psi_trans)
+{
+	g_error = 0;
+	if (!psi || !psi_trans || !perm || psi->nqubits != psi_trans->nqubits || psi->nqubits < 0 || psi->nqubits > 40) {
+		g_error = E_ARG;
+		return;
+	}
+	const int L = psi->nqubits;
+	std::vector<long> strides(L > 0 ? L : 1);
+	std::vector<char> seen(L > 0 ? L : 1, 0);
+	for (int i = 0; i < L; i++) {
+		if (perm[i] < 0 || perm[i] >= L || seen[perm[i]]) {
+			g_error = E_ARG;
+			return;
+		}
+		seen[perm[i]] = 1;
+		strides[L - 1 - i] = 1L << (L - 1 - perm[i]);
+	}
+	for (long j = 0; j < (1L << L); j++) {
+		long k = 0;
+		for (int i = 0; i < L; i++) k += ((j >> i) & 1) * strides[i];
+		psi_trans->data[j] = psi->data[k];
+	}
+}
+
 void seed_rng_state(const uint64_t seed, struct rng_state* state)
 {
 	g_error = 0;

@@ -46,6 +46,7 @@ _SIGS = {
     "allocate_statevector": (I, [I, PSV]),
     "free_statevector": (None, [PSV]),
     "add_statevectors": (None, [PSV, PSV, PSV]),
+    "transpose_statevector": (None, [PSV, VP, PSV]),
     "apply_gate": (None, [VP, I, I, PSV, PSV]),
     "apply_gate_backward": (None, [VP, I, I, PSV, PSV, PSV, VP]),
     "apply_quantum_circuit": (I, [VP, I, VP, PSV, PSV]),
@@ -185,6 +186,16 @@ def _nq(psi):
 
 
 # ------------------------------------------------------------------------ gates and circuits
+
+def transpose_statevector(psi, perm):
+    """Qubit i of psi moved to qubit perm[i] (src/statevector.c:72-98)."""
+    psi, perm = cplx(psi), ints(perm)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    lib().transpose_statevector(C.byref(_sv(psi, L)), ptr(perm), C.byref(_sv(out, L)))
+    _check_void("transpose_statevector")
+    return out
+
 
 def apply_gate(V, i, j, psi):
     psi = cplx(psi)

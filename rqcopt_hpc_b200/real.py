@@ -32,7 +32,7 @@ class RqcError(RuntimeError):
         self.code = code
 
 
-_VOID = {"free_statevector", "add_statevectors", "apply_gate", "apply_gate_backward", "apply_gate_to_array",
+_VOID = {"free_statevector", "add_statevectors", "transpose_statevector", "apply_gate", "apply_gate_backward", "apply_gate_to_array",
          "apply_gate_backward_array", "apply_gate_placeholder", "free_quantum_circuit_cache", "seed_rng_state",
          "haar_random_statevector", "free_statevector_array", "optimize_brickwall_circuit_hvp",
          "optimize_quantum_circuit", "riemannian_trust_region_optimize_hvp", "riemannian_trust_region_optimize_hmat",
@@ -94,6 +94,14 @@ def _sva(a, L):
 
 
 # ------------------------------------------------------------------------ gates and circuits
+
+def transpose_statevector(psi, perm):
+    psi, perm = real(psi), ints(perm)
+    L = _nq(psi)
+    out = np.empty_like(psi)
+    _void("transpose_statevector", _sv(psi, L), ptr(perm), _sv(out, L))
+    return out
+
 
 def apply_gate(V, i, j, psi):
     V, psi = real(V), real(psi)

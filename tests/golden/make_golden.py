@@ -29,7 +29,7 @@ FIXTURES = [
     "brickwall_unitary_target", "brickwall_unitary_target_and_gradient",
     "brickwall_unitary_target_and_projected_gradient", "brickwall_unitary_target_hessian_vector_product",
     "brickwall_unitary_target_projected_hessian_vector_product",
-    "real_to_tangent", "project_tangent", "polar_factor", "multiply",
+    "real_to_tangent", "project_tangent", "polar_factor", "multiply", "transpose_statevector",
     # full-Hessian path
     "apply_gate_to_array", "apply_gate_placeholder", "brickwall_unitary_backward_hessian",
     "brickwall_unitary_target_gradient_hessian", "brickwall_unitary_target_gradient_vector_hessian_matrix",
@@ -54,7 +54,7 @@ REAL_FIXTURES = [
     "brickwall_unitary_target_projected_hessian_vector_product", "brickwall_unitary_target_gradient_hessian",
     "brickwall_unitary_target_sampling", "brickwall_unitary_target_gradient_hessian_sampling",
     "brickwall_blockenc_target", "brickwall_blockenc_target_and_gradient", "brickwall_blockenc_target_gradient_hessian",
-    "real_to_tangent", "project_tangent", "polar_factor", "multiply",
+    "real_to_tangent", "project_tangent", "polar_factor", "multiply", "transpose_statevector",
 ]
 
 
