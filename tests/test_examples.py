@@ -165,3 +165,15 @@ def test_driver_command_line(tmp_path, monkeypatch, capsys):
     assert (n, ushape, ng, len(wires), niter) == (5, (32, 32), 18, 18, 10)
     with np.load(out) as z:
         assert z["gates"].shape == (18, 4, 4, 2)
+
+
+def test_reader_refuses_files_outside_its_subset(tmp_path):
+    from rqcopt_hpc_b200 import h5read
+    junk = tmp_path / "junk.hdf5"
+    junk.write_bytes(b"not an hdf5 file at all")
+    with pytest.raises(ValueError):
+        h5read.read_all(str(junk))
+    newer = tmp_path / "v2.hdf5"
+    newer.write_bytes(b"\x89HDF\r\n\x1a\n" + bytes([2]) + bytes(64))   # superblock version 2
+    with pytest.raises(ValueError):
+        h5read.read_all(str(newer))
