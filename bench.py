@@ -624,7 +624,7 @@ def real_build_path(gpu, steps=3, L=14, depth=9, tdepth=5, seconds=8.0, with_ref
     return out
 
 
-def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50):
+def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50, with_reference=True):
     """The reference's Python module API (pymodule/rqcopt_module.c): optimize_brickwall_circuit
     with a dense Haar-random 2^L x 2^L target U, through rqcopt_hpc_b200.rqcopt_hpc (the GPU
     library) and through the reference module compiled in oracle/_ref (single-threaded C);
@@ -643,6 +643,8 @@ def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50):
     out = {"workload": f"rqcopt_hpc.optimize_brickwall_circuit (the reference's Python module API), L={L} depth {depth}, "
                        f"dense Haar-random target U, {niter} iterations", "seconds_per_iteration": wall,
            "f_first": float(f_iter[0]), "f_final": float(f_iter[-1])}
+    if not with_reference:
+        return out
     from oracle.oracle import reference_module
     ref = reference_module()
     if ref is None:
@@ -1004,7 +1006,7 @@ def main():
             line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
             gpu.set_precision(prec)
         if not a.no_hmat and world == 1:
-            line["front_end"] = front_end_path()
+            line["front_end"] = front_end_path(with_reference=not a.no_cpu_baseline)
             gpu.set_precision(prec)
         if not a.no_real and world == 1:
             line["real_build"] = real_build_path(gpu, with_reference=not a.no_cpu_baseline)
