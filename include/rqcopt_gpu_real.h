@@ -97,6 +97,22 @@ void add_statevectors(const struct statevector* psi1, const struct statevector* 
 void transpose_statevector(const struct statevector* psi, const int* perm,
 	struct statevector* psi_trans);                                                   /* src/statevector.h:26 */
 void seed_rng_state(const uint64_t seed, struct rng_state* state);                    /* src/rng.h:21 */
+/* src/pcg_basic.h:38-60 and src/rng.h:29-61 -- host random numbers, the reference's stream */
+void pcg32_srandom_r(const uint64_t initstate, const uint64_t initseq, struct pcg32_random* rng);
+uint32_t pcg32_random_r(struct pcg32_random* rng);
+uint32_t pcg32_boundedrand_r(const uint32_t bound, struct pcg32_random* rng);
+void pcg32x2_srandom_r(uint64_t seed1, uint64_t seed2, uint64_t seq1, uint64_t seq2, struct pcg32x2_random* rng);
+uint64_t pcg32x2_random_r(struct pcg32x2_random* rng);
+uint64_t pcg32x2_boundedrand_r(const uint64_t bound, struct pcg32x2_random* rng);
+uint32_t rand_uint32(struct rng_state* state);
+uint64_t rand_uint64(struct rng_state* state);
+uint64_t rand_interval(const uint64_t bound, struct rng_state* state);
+void rand_choice(const uint64_t bound, const uint64_t num_samples, struct rng_state* state, uint64_t* ret);
+double randu(struct rng_state* state);
+float randuf(struct rng_state* state);
+double randn(struct rng_state* state);
+float randnf(struct rng_state* state);
+void normalize_statevector(struct statevector* psi);                                  /* src/statevector.h:23 */
 /* src/statevector.h:29 -- real normal entries (src/statevector.c:115-121), drawn on the GPU */
 void haar_random_statevector(struct statevector* psi, struct rng_state* rng);
 int allocate_statevector_array(int nqubits, int nstates, struct statevector_array* psi_list);  /* src/statevector.h:47 */

@@ -360,6 +360,117 @@ void transpose_statevector(const struct statevector* psi, const int* perm, struc
 	}
 }
 
+// the host random numbers need no real form: forwarded (src/pcg_basic.c, src/rng.c)
+void pcg32_srandom_r(const uint64_t initstate, const uint64_t initseq, struct pcg32_random* rng)
+{
+	CX(pcg32_srandom_r, void, uint64_t, uint64_t, struct pcg32_random*);
+	cx_pcg32_srandom_r(initstate, initseq, rng);
+}
+
+uint32_t pcg32_random_r(struct pcg32_random* rng)
+{
+	CX(pcg32_random_r, uint32_t, struct pcg32_random*);
+	return cx_pcg32_random_r(rng);
+}
+
+uint32_t pcg32_boundedrand_r(const uint32_t bound, struct pcg32_random* rng)
+{
+	CX(pcg32_boundedrand_r, uint32_t, uint32_t, struct pcg32_random*);
+	return cx_pcg32_boundedrand_r(bound, rng);
+}
+
+void pcg32x2_srandom_r(uint64_t seed1, uint64_t seed2, uint64_t seq1, uint64_t seq2, struct pcg32x2_random* rng)
+{
+	CX(pcg32x2_srandom_r, void, uint64_t, uint64_t, uint64_t, uint64_t, struct pcg32x2_random*);
+	cx_pcg32x2_srandom_r(seed1, seed2, seq1, seq2, rng);
+}
+
+uint64_t pcg32x2_random_r(struct pcg32x2_random* rng)
+{
+	CX(pcg32x2_random_r, uint64_t, struct pcg32x2_random*);
+	return cx_pcg32x2_random_r(rng);
+}
+
+uint64_t pcg32x2_boundedrand_r(const uint64_t bound, struct pcg32x2_random* rng)
+{
+	CX(pcg32x2_boundedrand_r, uint64_t, uint64_t, struct pcg32x2_random*);
+	return cx_pcg32x2_boundedrand_r(bound, rng);
+}
+
+uint32_t rand_uint32(struct rng_state* state)
+{
+	CX(rand_uint32, uint32_t, struct rng_state*);
+	return cx_rand_uint32(state);
+}
+
+uint64_t rand_uint64(struct rng_state* state)
+{
+	CX(rand_uint64, uint64_t, struct rng_state*);
+	return cx_rand_uint64(state);
+}
+
+uint64_t rand_interval(const uint64_t bound, struct rng_state* state)
+{
+	CX(rand_interval, uint64_t, uint64_t, struct rng_state*);
+	return cx_rand_interval(bound, state);
+}
+
+void rand_choice(const uint64_t bound, const uint64_t num_samples, struct rng_state* state, uint64_t* ret)
+{
+	g_error = 0;
+	CX(rand_choice, void, uint64_t, uint64_t, struct rng_state*, uint64_t*);
+	cx_rand_choice(bound, num_samples, state, ret);
+}
+
+double randu(struct rng_state* state)
+{
+	CX(randu, double, struct rng_state*);
+	return cx_randu(state);
+}
+
+float randuf(struct rng_state* state)
+{
+	CX(randuf, float, struct rng_state*);
+	return cx_randuf(state);
+}
+
+double randn(struct rng_state* state)
+{
+	CX(randn, double, struct rng_state*);
+	return cx_randn(state);
+}
+
+float randnf(struct rng_state* state)
+{
+	CX(randnf, float, struct rng_state*);
+	return cx_randnf(state);
+}
+
+// src/statevector.c:47-66 (real build): divide by the 2-norm unless it is zero
+void normalize_statevector(struct statevector* psi)
+{
+	g_error = 0;
+	if (!psi || !psi->data || psi->nqubits < 0 || psi->nqubits > 40) {
+		g_error = E_ARG;
+		return;
+	}
+	const size_t n = dim(psi->nqubits);
+	double scale = 0, ssq = 1;   // scaled sum of squares
+	for (size_t k = 0; k < n; k++) {
+		const double av = std::fabs(psi->data[k]);
+		if (av == 0) continue;
+		if (scale < av) {
+			ssq = 1 + ssq * (scale / av) * (scale / av);
+			scale = av;
+		} else {
+			ssq += (av / scale) * (av / scale);
+		}
+	}
+	const double nrm = scale * std::sqrt(ssq);
+	if (nrm > 0)
+		for (size_t k = 0; k < n; k++) psi->data[k] *= 1. / nrm;
+}
+
 void seed_rng_state(const uint64_t seed, struct rng_state* state)
 {
 	g_error = 0;
