@@ -1112,6 +1112,23 @@ class RealReference:
         assert ret == 0
         return f[0], dg, hg
 
+    def circuit_unitary_target_projected_hessian_vector_product(self, t, gates, dirs, wires, L):
+        gates, dirs, wires = self._r(gates), self._r(dirs), _i(wires)
+        f, g, h = np.zeros(1), np.empty(6 * gates.shape[0]), np.empty(6 * gates.shape[0])
+        ret = self.lib.circuit_unitary_target_projected_hessian_vector_product(
+            t.ufunc, t.udata, _p(gates), _p(dirs), gates.shape[0], _p(wires), L, _p(f), _p(g), _p(h))
+        assert ret == 0
+        return f[0], g, h
+
+    def optimize_quantum_circuit(self, t, gstart, wires, L, niter):
+        gstart, wires = self._r(gstart), _i(wires)
+        ng = gstart.shape[0]
+        params = _RefRtrParams(TcgParams(12 * ng, 1e-8, 1e-6), 0.125, 0.01, 0.1, None, None, None)
+        f_iter, gopt = np.empty(niter + 1), np.empty_like(gstart)
+        self.lib.optimize_quantum_circuit(t.ufunc, t.udata, _p(gstart), ng, L, _p(wires), C.byref(params), niter,
+                                          _p(f_iter), _p(gopt))
+        return f_iter, gopt
+
     def optimize_brickwall_circuit_hvp(self, t, vstart, perms, L, niter):
         vstart = self._r(vstart)
         nl = vstart.shape[0]

@@ -391,6 +391,29 @@ def test_real_oracle_matches_compiled_real_build():
     _compare_with_reference(RealOracle(), RealReference(), 1e-13)
 
 
+def _circuit_case(L=7, ng=9, seed=21):
+    rng = np.random.default_rng(seed)
+    gates = np.stack([_real_orthogonal(rng) for _ in range(ng)])
+    wires = np.stack([rng.choice(L, 2, replace=False) for _ in range(ng)]).astype(np.int32)
+    dirs = np.stack([gates[k] @ real_antisymm(rng.standard_normal(6)) for k in range(ng)])
+    return gates, wires, dirs
+
+
+@ref_needed
+def test_real_oracle_circuit_paths_match_compiled_real_build():
+    """General circuits against the dense real target of the reference tests' map:
+    projected HVP to 1e-13 and a 4-iteration optimize_quantum_circuit to 1e-10."""
+    o, r = RealOracle(), RealReference()
+    gates, wires, dirs = _circuit_case()
+    to, tr = o.target("fixture"), r.target("fixture")
+    f, g, h = o.circuit_unitary_target_projected_hessian_vector_product(to, gates, dirs, wires, 7)
+    fr, gr, hr = r.circuit_unitary_target_projected_hessian_vector_product(tr, gates, dirs, wires, 7)
+    assert abs(f - fr) <= 1e-13 * abs(fr) and rel_err(g, gr) <= 1e-13 and rel_err(h, hr) <= 1e-13
+    fi, go = o.optimize_quantum_circuit(to, gates, wires, 7, 4)
+    fir, gor = r.optimize_quantum_circuit(tr, gates, wires, 7, 4)
+    assert rel_err(fi, fir) <= 1e-10 and rel_err(go, gor) <= 1e-9
+
+
 @ref_needed
 @pytest.mark.gpu
 def test_gpu_real_build_matches_compiled_real_build(gpu):
