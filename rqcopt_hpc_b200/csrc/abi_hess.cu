@@ -353,25 +353,6 @@ extern "C" int brickwall_unitary_target_gradient_vector_hessian_matrix_sampling(
 
 namespace {
 
-uint32_t pcg32_next(struct pcg32_random* g)
-{
-	const uint64_t old = g->state;
-	g->state = old * 6364136223846793005ULL + g->inc;
-	const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
-	const uint32_t rot = (uint32_t)(old >> 59u);
-	return (xs >> rot) | (xs << ((32u - rot) & 31u));
-}
-
-// PCG32 seeding with a state and a stream (src/pcg_basic.c:31-38)
-void pcg32_seed(struct pcg32_random* g, uint64_t initstate, uint64_t initseq)
-{
-	g->state = 0;
-	g->inc = (initseq << 1u) | 1u;
-	pcg32_next(g);
-	g->state += initstate;
-	pcg32_next(g);
-}
-
 int sampled_value(const char* fn, linear_func ufunc, void* udata, const std::vector<double2>& gates,
                   const std::vector<int>& wires, int nqubits, long nsamples, struct rng_state* rng, numeric* fval)
 {
@@ -392,25 +373,6 @@ int sampled_value(const char* fn, linear_func ufunc, void* udata, const std::vec
 }
 
 }  // namespace
-
-// src/rng.c:13-25: a seeding generator on (seed, stream 6364136223846793005 seed +
-// 1442695040888963407) yields the two seeds and two streams of the pair; equal
-// streams are made distinct (src/pcg_basic.c:112-121)
-extern "C" void seed_rng_state(const uint64_t seed, struct rng_state* state)
-{
-	struct pcg32_random s;
-	pcg32_seed(&s, seed, 6364136223846793005ULL * seed + 1442695040888963407ULL);
-	uint64_t v[4];
-	for (int k = 0; k < 4; k++) {
-		const uint64_t hi = pcg32_next(&s);
-		v[k] = (hi << 32) | pcg32_next(&s);
-	}
-	uint64_t seq2 = v[3];
-	const uint64_t mask = ~0ull >> 1;
-	if ((v[2] & mask) == (seq2 & mask)) seq2 = ~seq2;
-	pcg32_seed(&state->pcgstate.gen[0], v[0], v[2]);
-	pcg32_seed(&state->pcgstate.gen[1], v[1], seq2);
-}
 
 extern "C" void haar_random_statevector(struct statevector* psi, struct rng_state* rng)
 {

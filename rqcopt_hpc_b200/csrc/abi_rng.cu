@@ -83,6 +83,20 @@ uint64_t pcg32x2_boundedrand_r(const uint64_t bound, struct pcg32x2_random* rng)
 	}
 }
 
+// src/rng.c:13-25: a seeding generator on (seed, stream 6364136223846793005 seed +
+// 1442695040888963407) yields the two seeds and two streams of the pair
+void seed_rng_state(const uint64_t seed, struct rng_state* state)
+{
+	struct pcg32_random s;
+	pcg32_srandom_r(seed, PCG_MULT * seed + 1442695040888963407ULL, &s);
+	uint64_t v[4];
+	for (int k = 0; k < 4; k++) {
+		const uint64_t hi = pcg32_random_r(&s);
+		v[k] = (hi << 32) | pcg32_random_r(&s);
+	}
+	pcg32x2_srandom_r(v[0], v[1], v[2], v[3], &state->pcgstate);
+}
+
 // src/rng.c:32-36: the first generator alone
 uint32_t rand_uint32(struct rng_state* state) { return pcg32_random_r(&state->pcgstate.gen[0]); }
 
