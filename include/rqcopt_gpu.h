@@ -468,6 +468,15 @@ void rqcopt_gpu_set_workspace_limit(size_t bytes);
 /* number of basis columns per chunk; 0 selects it from the workspace limit */
 void rqcopt_gpu_set_column_chunk(long columns);
 
+/* Restrict the basis-column sums of the target functions (circuit_unitary_target*,
+ * brickwall_unitary_target* and the optimisers that call them) to the columns
+ * [begin, end); end = 0 means up to the last column, and (0, 0), the default, restores
+ * the full sums.  It is the column loop of src/target.c:335-369 run over a contiguous
+ * sample, so that a large evaluation can be checked column by column against a CPU
+ * implementation of the same range.  Returns 0, or -6 if begin < 0, end < 0 or
+ * 0 < end <= begin. */
+int rqcopt_gpu_set_column_range(long begin, long end);
+
 /* gates fused per HBM round trip in the basis-column passes: 1 runs one kernel
  * per gate, 2..4 (default 4) group consecutive gates into passes over
  * eight-qubit tiles of column-interleaved chunks */
@@ -475,6 +484,13 @@ int rqcopt_gpu_set_gates_per_pass(int gates);
 
 /* last error recorded by a void function (0 if none); reading clears it */
 int rqcopt_gpu_last_error(void);
+
+/* Per-iteration record of the last optimize_brickwall_circuit_hvp / optimize_quantum_circuit
+ * call on this device (the decisions of src/trust_region.c:330-352): step accepted (rho >
+ * rho_trust), tCG ended on the trust-region boundary, tCG inner iterations (Hessian-vector
+ * products), and whether those products ran in complex128 (1) or complex64 (0).  Fills up to
+ * `capacity` entries of each non-null array and returns the number of iterations recorded. */
+int rqcopt_gpu_optimizer_trace(int* accepted, int* on_boundary, int* inner_iterations, int* refined, int capacity);
 
 /* Haar-random sample states with real normal entries, one draw of randn() per
  * amplitude as in the reference's real build (src/statevector.c:115-121), instead
@@ -521,12 +537,17 @@ int rqcopt_apply_quantum_circuit_c64(const struct mat4x4 gates[], int ngates, co
  * device allocation, for callers that cannot call cudaMalloc at that point (a
  * process whose device memory belongs to its own pool, a latency-critical
  * thread that must not take the device-wide synchronisation an allocation or
- * free can imply, a host callback running inside other GPU work).
+ * free can imply, a host callback such as a target's linear_func that another
+ * library's column loop calls on an ordinary host thread while it holds the
+ * device memory).  It makes CUDA calls and waits for its stream, so it must not
+ * be called from a stream host function (cudaLaunchHostFunc,
+ * cudaStreamAddCallback), where CUDA calls are not allowed.
  *
  * Its only scratch (per-tile partial sums of dgate) is a static device array
  * of 2 MiB + 256 B that every GPU loading the library keeps until exit.
- *   - psi, dpsi_out and dpsi must hold device or managed memory (host buffers
- *     would need staging, i.e. allocation); dgate may be host or device memory;
+ *   - psi, dpsi_out and dpsi must hold managed memory or device memory of the
+ *     current device (host buffers would need staging, i.e. allocation; memory
+ *     of another GPU is refused); dgate may be host or device memory;
  *   - at most RQCOPT_NOALLOC_MAX_QUBITS qubits; larger states are rejected
  *     with -6 and a message on stderr;
  *   - work is issued on `stream` (a cudaStream_t, NULL for the legacy default

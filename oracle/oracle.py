@@ -123,6 +123,14 @@ class Oracle:
     def target(self, kind, data=None):
         return _Target(self.lib, kind, data)
 
+    def add_statevectors(self, psi1, psi2):
+        psi1, psi2 = _c(psi1), _c(psi2)
+        L = _nq(psi1)
+        out = np.empty_like(psi1)
+        self.lib.orc_add_statevectors(C.byref(SV(psi1.ctypes.data, L)), C.byref(SV(psi2.ctypes.data, L)),
+                                      C.byref(SV(out.ctypes.data, L)))
+        return out
+
     # gates and circuits
     def apply_gate(self, V, i, j, psi):
         psi, V = _c(psi), _c(V)
@@ -206,13 +214,13 @@ class Oracle:
                                                  L_(0), L_(1 << L), _p(f), _p(dg))
         return f[0], dg
 
-    def circuit_unitary_target_hessian_vector_product(self, tgt, gates, dirs, wires, L):
+    def circuit_unitary_target_hessian_vector_product(self, tgt, gates, dirs, wires, L, b0=0, b1=None):
         gates, dirs, wires = _c(gates), _c(dirs), _i(wires)
         f = np.zeros(1, np.complex128)
         dg = np.empty((gates.shape[0], 4, 4), np.complex128)
         hg = np.empty_like(dg)
-        self.lib.orc_circuit_target_hvp(tgt.ufunc, tgt.udata, _p(gates), _p(dirs), gates.shape[0], _p(wires), L, L_(0),
-                                        L_(1 << L), _p(f), _p(dg), _p(hg))
+        self.lib.orc_circuit_target_hvp(tgt.ufunc, tgt.udata, _p(gates), _p(dirs), gates.shape[0], _p(wires), L, L_(b0),
+                                        L_(b1 if b1 is not None else 1 << L), _p(f), _p(dg), _p(hg))
         return f[0], dg, hg
 
     def circuit_unitary_target_and_projected_gradient(self, tgt, gates, wires, L):

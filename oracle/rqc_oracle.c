@@ -225,6 +225,15 @@ void orc_retract(const orc_mat4* u, const double* eta, orc_mat4* v)
 	orc_polar_factor(&w, v);
 }
 
+/* ------------------------------------------------------------------- statevectors */
+
+/* src/statevector.c:132-142: psi_sum = psi1 + psi2, element by element */
+void orc_add_statevectors(const orc_sv* psi1, const orc_sv* psi2, orc_sv* psi_sum)
+{
+	const long n = 1L << psi1->nqubits;
+	for (long k = 0; k < n; k++) psi_sum->data[k] = psi1->data[k] + psi2->data[k];
+}
+
 /* ------------------------------------------------------------------- gates */
 
 /* src/gate.c:10-76: psi_out = (gate on wires i, j) psi; row index of the gate is 2*b_i + b_j */

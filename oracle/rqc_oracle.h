@@ -53,6 +53,7 @@ void orc_polar_factor(const orc_mat4* a, orc_mat4* u);
 void orc_retract(const orc_mat4* u, const double* eta, orc_mat4* v);
 
 /* ---- gates and circuits (src/gate.c, src/quantum_circuit.c, src/brickwall_circuit.c) ---- */
+void orc_add_statevectors(const orc_sv* psi1, const orc_sv* psi2, orc_sv* psi_sum);
 void orc_apply_gate(const orc_mat4* g, int i, int j, const orc_sv* psi, orc_sv* out);
 void orc_apply_gate_backward(const orc_mat4* g, int i, int j, const orc_sv* psi,
                              const orc_sv* dpsi_out, orc_sv* dpsi, orc_mat4* dg);

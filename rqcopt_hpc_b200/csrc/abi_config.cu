@@ -39,6 +39,16 @@ void rqcopt_gpu_set_column_chunk(long columns)
 	if (Runtime* rt = runtime()) rt->column_chunk = columns > 0 ? columns : 0;
 }
 
+int rqcopt_gpu_set_column_range(long begin, long end)
+{
+	if (begin < 0 || end < 0 || (end != 0 && end <= begin)) return E_ARG;
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	rt->col_begin = begin;
+	rt->col_end = end;
+	return 0;
+}
+
 int rqcopt_gpu_set_gates_per_pass(int gates)
 {
 	if (gates < 1 || gates > 4) return E_ARG;
@@ -46,6 +56,21 @@ int rqcopt_gpu_set_gates_per_pass(int gates)
 	if (!rt) return E_CUDA;
 	rt->gates_per_pass = gates;
 	return 0;
+}
+
+int rqcopt_gpu_optimizer_trace(int* accepted, int* on_boundary, int* inner_iterations, int* refined, int capacity)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	const int n = (int)rt->opt_trace.size();
+	for (int k = 0; k < n && k < capacity; k++) {
+		const Runtime::IterTrace& t = rt->opt_trace[k];
+		if (accepted) accepted[k] = t.accepted;
+		if (on_boundary) on_boundary[k] = t.on_boundary;
+		if (inner_iterations) inner_iterations[k] = t.inner;
+		if (refined) refined[k] = t.refined;
+	}
+	return n;
 }
 
 int rqcopt_gpu_last_error(void) { return take_last_error(); }

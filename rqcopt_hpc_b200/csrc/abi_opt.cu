@@ -398,6 +398,7 @@ struct DeviceOptimizer
 		hvp_prec = precision == PREC_C128 ? PREC_C128 : PREC_C64;
 		double* fx_slot = scratch + n;
 		const int threads = 64, blocks = (pb.nunits + threads - 1) / threads;
+		rt.opt_trace.clear();
 		for (int k = 0; k < niter && !ret; k++) {
 			// f and gradient at x (src/trust_region.c:328)
 			if ((ret = load_gates(x))) break;
@@ -413,11 +414,13 @@ struct DeviceOptimizer
 			if ((ret = read_state(rt, v.tcg, &st))) break;
 			if (precision == PREC_MIXED && hvp_prec != PREC_C128 && sqrt(st.rsq) < rt.refine_threshold) hvp_prec = PREC_C128;
 			bool boundary = false;
+			int inner = 0;
 			for (int it = 0; it < params->tcg_params.maxiter; it++) {
 				if ((ret = eval_hvp(v.d, v.hd, hvp_prec))) break;
 				k_tcg_step<<<1, 1, 0, rt.stream>>>(n, v.d, v.hd, v.z, v.r, v.tcg);
 				if ((ret = launched(rt))) break;
 				if ((ret = read_state(rt, v.tcg, &st))) break;
+				inner = it + 1;
 				if (st.status == TCG_BOUNDARY) { boundary = true; break; }
 				if (st.status == TCG_CONVERGED) break;
 			}
@@ -433,6 +436,7 @@ struct DeviceOptimizer
 			if ((ret = launched(rt))) break;
 			if ((ret = read_state(rt, v.rtr, &rs))) break;
 			f_iter[k] = rs.fx;
+			rt.opt_trace.push_back({rs.accept, boundary ? 1 : 0, inner, hvp_prec == PREC_C128 ? 1 : 0});
 			if (rs.accept) std::swap(x, xn);
 		}
 		if (ret) return ret;

@@ -465,10 +465,12 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 	// states per column: PHI, P0, P1 (+ D0, D1) and the cached forward states
 	const int64_t nstates = mode == EVAL_F ? 3 : (mode == EVAL_GRAD ? 3 + (G - 1) : 5 + 2 * (int64_t)(G - 1));
 	const size_t col_bytes = (size_t)nstates * N * sizeof(V);
+	const int64_t cbeg = std::min<int64_t>(rt.col_begin, ncols);
+	const int64_t cend = rt.col_end > 0 ? std::min<int64_t>(rt.col_end, ncols) : ncols;
 	int64_t C = (int64_t)(workspace_limit(rt) / col_bytes);
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, rt.column_chunk);
 	if (host_target) C = std::min<int64_t>(C, std::max<int64_t>(1, ((int64_t)256 << 20) / (N * 16)));
-	C = std::min(C, ncols);
+	C = std::min(C, std::max<int64_t>(1, cend - cbeg));
 	if (C < 1) {
 		fprintf(stderr, "rqcopt_gpu: one basis column needs %zu bytes of workspace, more than the limit\n", col_bytes);
 		return E_ALLOC;
@@ -499,8 +501,8 @@ static int evaluate_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, in
 		hbasis = hcols + C * N;
 	}
 
-	for (int64_t b0 = 0; b0 < ncols; b0 += C) {
-		const int64_t Cc = std::min(C, ncols - b0);
+	for (int64_t b0 = cbeg; b0 < cend; b0 += C) {
+		const int64_t Cc = std::min(C, cend - b0);
 		const int64_t ngroups = Cc * (N / 4);
 
 		// target columns phi = -conj(U e_b)

@@ -68,11 +68,14 @@ struct PassGeom
 // Paired basis columns (real-orthogonal problems): with c_pair_half = N/2 the column
 // with basis index b (< N/2) is e_b + i e_{b + N/2}; 0 selects plain basis columns.
 __constant__ int64_t c_pair_half = 0;
+// End of the column range of the current evaluation: the columns of a chunk's last
+// column group at or beyond it are zero (they add nothing to any sum).
+__constant__ int64_t c_col_end = INT64_MAX;
 
-__device__ __forceinline__ float basis_re(int64_t row, int64_t b) { return row == b ? 1.f : 0.f; }
+__device__ __forceinline__ float basis_re(int64_t row, int64_t b) { return (row == b && b < c_col_end) ? 1.f : 0.f; }
 __device__ __forceinline__ float basis_im(int64_t row, int64_t b)
 {
-	return (c_pair_half != 0 && row == b + c_pair_half) ? 1.f : 0.f;
+	return (c_pair_half != 0 && b < c_col_end && row == b + c_pair_half) ? 1.f : 0.f;
 }
 
 template <typename T> struct PassGates { Gate4<T> g[MAXK]; Gate4<T> z[MAXK]; };
@@ -2042,11 +2045,13 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	// states per column: PHI, P0, P1 (+ D0, D1) and the pass checkpoints
 	const int64_t nstates = mode == EVAL_F ? 3 : (mode == EVAL_GRAD ? 3 + nck : 5 + 2 * nck);
 	const size_t col_bytes = (size_t)nstates * N * sizeof(V);
+	const int64_t cbeg = std::min<int64_t>(rt.col_begin, ncols);
+	const int64_t cend = rt.col_end > 0 ? std::min<int64_t>(rt.col_end, ncols) : ncols;
 	const int64_t C_mem = (int64_t)(workspace_limit2(rt) / col_bytes);
 	int64_t C = C_mem;
 	if (rt.column_chunk > 0) C = std::min<int64_t>(C, ((rt.column_chunk + CW - 1) / CW) * CW);
 	if (host_target) C = std::min<int64_t>(C, std::max<int64_t>(CW, ((int64_t)256 << 20) / (N * 16)));
-	C = std::min<int64_t>(C, ((ncols + CW - 1) / CW) * CW);
+	C = std::min<int64_t>(C, ((std::max<int64_t>(1, cend - cbeg) + CW - 1) / CW) * CW);
 	C = (C / CW) * CW;
 	if (C < CW || C > C_mem) {
 		fprintf(stderr, "rqcopt_gpu: %d columns need %zu bytes of workspace, more than the limit\n", CW, CW * col_bytes);
@@ -2088,8 +2093,10 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 		dstage = reinterpret_cast<double2*>(rt.stage[2].ptr);
 	}
 
-	for (int64_t b0 = 0; b0 < ncols; b0 += C) {
-		const int64_t Cc = std::min(C, ncols - b0);
+	if ((ret = RQC_CUDA(cudaMemcpyToSymbolAsync(c_col_end, &cend, sizeof(cend), 0, cudaMemcpyHostToDevice, rt.stream))))
+		return ret;
+	for (int64_t b0 = cbeg; b0 < cend; b0 += C) {
+		const int64_t Cc = std::min(C, cend - b0);
 		const int64_t ncg = (Cc + CW - 1) / CW;
 		auto geom = [&](const Pass& p) {
 			PassGeom g = p.geom;

@@ -5,15 +5,18 @@
 // pass: code that runs while its process has handed all device memory to its
 // own pool, code on a latency-critical thread that must not take the
 // device-wide synchronisation a cudaMalloc/cudaFree can imply, or host
-// callbacks invoked from inside another library's work.  This entry point
-// therefore uses no allocator at all: the only memory it needs beyond the
+// callbacks such as a target's linear_func, which another library's column
+// loop calls on an ordinary host thread while that library holds the device
+// memory.  This entry point therefore uses no allocator at all: the only
+// memory it needs beyond the
 // caller's inputs and outputs -- the per-tile partial sums of dG and the reduced
 // dG -- lives in the file-scope array below, which every GPU that loads the
 // library holds until the process exits (2 MiB + 256 B).
 //
 // Limits and sharing:
 //   - states of at most 2^25 amplitudes (25 qubits); larger states are rejected;
-//   - statevector data must be device or managed memory (nothing is staged);
+//   - statevector data must be managed memory or device memory of the current
+//     device (nothing is staged);
 //   - every call shares the array, and each call overwrites what it uses before
 //     reading it; calls whose work overlaps on the GPU (different streams or
 //     host threads) race on it.
@@ -100,14 +103,18 @@ __global__ void k_noalloc_reduce(const double* __restrict__ partials, int ntiles
 	out[t] = sum;
 }
 
-bool device_accessible(const void* p)
+// Managed memory, or device memory of device `dev` (the device the kernels run
+// on).  Device memory of another GPU is refused: the kernels would read it over
+// a peer mapping that may not exist, and the scratch they use belongs to `dev`.
+bool device_accessible(const void* p, int dev)
 {
 	cudaPointerAttributes a;
 	if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
 		cudaGetLastError();
 		return false;
 	}
-	return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+	if (a.type == cudaMemoryTypeManaged) return true;
+	return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 int report(cudaError_t e, const char* what)
@@ -138,12 +145,6 @@ extern "C" int rqcopt_apply_gate_backward_noalloc(const struct mat4x4* gate, con
 		        "2^%d amplitudes)\n", fn, L, RQCOPT_NOALLOC_MAX_QUBITS, RQCOPT_NOALLOC_MAX_QUBITS);
 		return -6;
 	}
-	if (!device_accessible(psi->data) || !device_accessible(dpsi_out->data) || !device_accessible(dpsi->data)) {
-		fprintf(stderr, "%s: statevector data must be device or managed memory (no staging without allocation)\n", fn);
-		return -6;
-	}
-
-	// one-time set-up per device: the device address of the static scratch
 	int dev = -1;
 	int ret = report(cudaGetDevice(&dev), "cudaGetDevice");
 	if (ret) return ret;
@@ -151,6 +152,14 @@ extern "C" int rqcopt_apply_gate_backward_noalloc(const struct mat4x4* gate, con
 		fprintf(stderr, "%s: device ordinal %d out of range\n", fn, dev);
 		return -6;
 	}
+	if (!device_accessible(psi->data, dev) || !device_accessible(dpsi_out->data, dev) ||
+	    !device_accessible(dpsi->data, dev)) {
+		fprintf(stderr, "%s: statevector data must be managed memory or device memory of the current device %d "
+		        "(no staging without allocation)\n", fn, dev);
+		return -6;
+	}
+
+	// one-time set-up per device: the device address of the static scratch
 	if (!g_scratch_addr[dev]) {
 		void* p = nullptr;
 		if ((ret = report(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress"))) return ret;

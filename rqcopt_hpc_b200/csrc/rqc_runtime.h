@@ -43,11 +43,19 @@ struct Runtime
 	double refine_threshold = 1e-5;
 	size_t workspace_limit = 0;
 	long column_chunk = 0;
+	// basis columns the target sums run over: [col_begin, col_end), col_end 0 = to the last
+	// column (rqcopt_gpu_set_column_range)
+	int64_t col_begin = 0, col_end = 0;
 	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
 
 	// instrumentation
 	unsigned long long launches = 0;
+	// per-iteration record of the last optimize_* call with Hessian-vector products:
+	// step accepted, tCG ended on the trust-region boundary, tCG inner iterations,
+	// Hessian-vector products in complex128 (1) or complex64 (0)
+	struct IterTrace { int accepted, on_boundary, inner, refined; };
+	std::vector<IterTrace> opt_trace;
 	bool timing = false;
 	double time_ms[KC_COUNT] = {0, 0, 0, 0, 0};
 	long time_count[KC_COUNT] = {0, 0, 0, 0, 0};

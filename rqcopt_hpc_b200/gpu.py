@@ -116,7 +116,9 @@ _SIGS = {
     "rqcopt_gpu_set_refine_threshold": (None, [D]),
     "rqcopt_gpu_set_workspace_limit": (None, [C.c_size_t]),
     "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
+    "rqcopt_gpu_set_column_range": (I, [C.c_long, C.c_long]),
     "rqcopt_gpu_last_error": (I, []),
+    "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
     "rqcopt_gpu_set_real_pairs": (None, [I]),
     "rqcopt_gpu_set_real_samples": (None, [I]),
@@ -194,6 +196,20 @@ def transpose_statevector(psi, perm):
     out = np.empty_like(psi)
     lib().transpose_statevector(C.byref(_sv(psi, L)), ptr(perm), C.byref(_sv(out, L)))
     _check_void("transpose_statevector")
+    return out
+
+
+def add_statevectors(psi1, psi2):
+    """psi1 + psi2 (src/statevector.c:132-142); numpy arrays or CUDA tensors."""
+    if hasattr(psi1, "data_ptr"):
+        import torch
+        out = torch.empty_like(psi1)
+    else:
+        psi1, psi2 = cplx(psi1), cplx(psi2)
+        out = np.empty_like(psi1)
+    L = _nq(psi1)
+    lib().add_statevectors(C.byref(_sv(psi1, L)), C.byref(_sv(psi2, L)), C.byref(_sv(out, L)))
+    _check_void("add_statevectors")
     return out
 
 
@@ -842,6 +858,22 @@ def set_gates_per_pass(k: int):
 
 def set_column_chunk(cols: int):
     lib().rqcopt_gpu_set_column_chunk(cols)
+
+
+def optimizer_trace():
+    """Per-iteration (accepted, on_boundary, tcg_inner_iterations, refined) arrays of the
+    last Hessian-vector-product optimisation on this device."""
+    n = lib().rqcopt_gpu_optimizer_trace(None, None, None, None, 0)
+    if n < 0:
+        raise RqcError("rqcopt_gpu_optimizer_trace", n)
+    a, b, c, d = (np.zeros(n, np.int32) for _ in range(4))
+    lib().rqcopt_gpu_optimizer_trace(a.ctypes.data, b.ctypes.data, c.ctypes.data, d.ctypes.data, n)
+    return {"accepted": a, "on_boundary": b, "inner": c, "refined": d}
+
+
+def set_column_range(begin: int = 0, end: int = 0):
+    """Restrict the target functions' basis-column sums to [begin, end) (end 0: to the last column)."""
+    _check("rqcopt_gpu_set_column_range", lib().rqcopt_gpu_set_column_range(begin, end))
 
 
 def set_workspace_limit(nbytes: int):

@@ -94,17 +94,25 @@ def test_batch_optimize_retraces_single_optimizer(gpu):
 
 
 def test_batch_mixed_precision_optimize(gpu):
+    """Batched mixed precision (complex64 HVPs, complex128 once the gradient norm falls
+    below 1e-5) on problems the trust region drives to convergence within 80 iterations
+    (the tCG takes many inner steps once the steps leave the trust-region boundary): the
+    final f of every problem equals the single-problem complex128 optimiser's to 1e-10
+    relative, and the batched complex128 run retraces it."""
     from rqcopt_hpc_b200 import batch
-    probs = [_problem(8, 3, 3, 51), _problem(10, 3, 3, 52)]
-    niter = 8
+    from rqcopt_hpc_b200.workloads import brickwall_problem
+    probs = [brickwall_problem(6, 3, 3, 0, 1), brickwall_problem(8, 3, 3, 0, 1), brickwall_problem(6, 5, 3, 5, 6)]
+    niter = 80
     f128, _ = batch.optimize(probs, niter, gpu.PRECISION_C128)
     fmix, _ = batch.optimize(probs, niter, gpu.PRECISION_MIXED)
-    f64, _ = batch.optimize(probs, niter, gpu.PRECISION_C64)
-    for k in range(len(probs)):
-        # monotone trust-region decrease and the same first value (complex128 f in mixed mode)
+    f64, _ = batch.optimize(probs, 4, gpu.PRECISION_C64)
+    for k, (L, vlist, perms, tvlist, tperms) in enumerate(probs):
+        fs, _ = gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L, niter)
+        # the same first value (complex128 f in mixed mode) and a monotone trust-region decrease
         assert fmix[k][0] == f128[k][0]
         assert np.all(np.diff(fmix[k]) <= 1e-9 * abs(fmix[k][0]))
-        assert abs(fmix[k][-1] - f128[k][-1]) <= 1e-3 * abs(f128[k][-1])
+        assert abs(f128[k][-1] - fs[-1]) <= 1e-10 * abs(fs[-1])
+        assert abs(fmix[k][-1] - fs[-1]) <= 1e-10 * abs(fs[-1]), (k, fmix[k][-1], fs[-1])
         assert abs(f64[k][0] - f128[k][0]) <= 1e-5 * abs(f128[k][0])
 
 

@@ -104,13 +104,97 @@ def test_complex64_passes_within_single_precision(gpu, oracle):
 
 
 def test_trust_region_retraces_oracle(gpu, oracle):
+    """f iterates, final gates and the accept / reject and on-boundary decision of every
+    iteration equal the oracle's (src/trust_region.c:330-352)."""
     L = 8
     vlist, perms, tvlist, tperms = brickwall_instance(L, 5, 0, 3, 1)
+    gpu.set_precision(gpu.PRECISION_C128)
     f_g, v_g = gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tvlist, tperms)), vlist, perms, L, 10)
+    tr = gpu.optimizer_trace()
     f_o, v_o, acc, bnd = oracle.optimize_brickwall_circuit_hvp(oracle.target("brickwall", (tvlist, tperms)),
                                                                 vlist, perms, L, 10)
     assert rel_err(f_g, f_o) <= 1e-12
     assert rel_err(v_g, v_o) <= 1e-10
+    assert np.array_equal(tr["accepted"], acc)
+    assert np.array_equal(tr["on_boundary"], bnd)
+    assert not tr["refined"].any() or np.all(tr["refined"] == 1)   # complex128 throughout
+
+
+def test_general_circuit_trust_region_decisions_match_oracle(gpu, oracle):
+    L = 6
+    rng = np.random.default_rng(77)
+    gates = np.stack([haar_unitary(rng) for _ in range(7)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(7)], np.int32)
+    _, _, tvlist, tperms = brickwall_instance(L, 1, 0, 3, 78)
+    gpu.set_precision(gpu.PRECISION_C128)
+    f_g, g_g = gpu.optimize_quantum_circuit(gpu.Target(brickwall=(tvlist, tperms)), gates, wires, L, 12)
+    tr = gpu.optimizer_trace()
+    f_o, g_o, acc, bnd = oracle.optimize_quantum_circuit(oracle.target("brickwall", (tvlist, tperms)), gates, wires,
+                                                         L, 12)
+    assert rel_err(f_g, f_o) <= 1e-12
+    assert np.array_equal(tr["accepted"], acc)
+    assert np.array_equal(tr["on_boundary"], bnd)
+
+
+@pytest.mark.parametrize("L,depth,seed,niter", [(8, 3, 0, 60), (6, 5, 5, 80)])
+def test_mixed_precision_reaches_the_complex128_optimum(gpu, oracle, L, depth, seed, niter):
+    """Mixed precision (complex64 HVPs until the gradient norm falls below 1e-5, then
+    complex128) on problems the trust region drives to convergence within niter
+    iterations (the oracle's gradient norm ends below 1e-8): the refinement engages,
+    tCG takes several inner steps, and the final f agrees with the complex128 run and
+    with the oracle's FP64 run to 1e-10 relative."""
+    vlist, perms, tvlist, tperms = brickwall_instance(L, depth, seed, 3, seed + 1)
+    tgt = gpu.Target(brickwall=(tvlist, tperms))
+    try:
+        gpu.set_precision(gpu.PRECISION_C128)
+        f128, v128 = gpu.optimize_brickwall_circuit_hvp(tgt, vlist, perms, L, niter)
+        gpu.set_precision(gpu.PRECISION_MIXED)
+        fmix, vmix = gpu.optimize_brickwall_circuit_hvp(tgt, vlist, perms, L, niter)
+        tr = gpu.optimizer_trace()
+    finally:
+        gpu.set_precision(gpu.PRECISION_C128)
+    f_o, v_o, _, _ = oracle.optimize_brickwall_circuit_hvp(oracle.target("brickwall", (tvlist, tperms)), vlist, perms,
+                                                           L, niter)
+    assert tr["refined"][0] == 0 and tr["refined"][-1] == 1, tr["refined"]
+    assert tr["inner"].max() >= 3
+    assert abs(fmix[-1] - f128[-1]) <= 1e-10 * abs(f128[-1]), (fmix[-1], f128[-1])
+    assert abs(fmix[-1] - f_o[-1]) <= 1e-10 * abs(f_o[-1])
+    # the mixed run's reported f values are complex128 evaluations: each equals the oracle's f at its iterate
+    _, g_final = oracle.brickwall_unitary_target_and_projected_gradient(oracle.target("brickwall", (tvlist, tperms)),
+                                                                        vmix, perms, L)
+    assert np.linalg.norm(g_final) <= 1e-6
+
+
+def test_add_statevectors_matches_oracle(gpu, oracle):
+    """src/statevector.c:132-142 on host arrays (staged), device tensors and managed
+    statevectors from allocate_statevector."""
+    import ctypes as C
+    import torch
+    from rqcopt_hpc_b200.abi import Statevector
+    rng = np.random.default_rng(91)
+    for L in (1, 3, 20):
+        a, b = crandn(1 << L, rng), crandn(1 << L, rng)
+        want = oracle.add_statevectors(a, b)
+        assert np.array_equal(gpu.add_statevectors(a, b), want)
+        ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+        assert np.array_equal(gpu.add_statevectors(ta, tb).cpu().numpy(), want)
+    lib = gpu.lib()
+    L = 10
+    sv = [Statevector() for _ in range(3)]
+    for s in sv:
+        assert lib.allocate_statevector(L, C.byref(s)) == 0
+    try:
+        a, b = crandn(1 << L, rng), crandn(1 << L, rng)
+        for s, v in zip(sv[:2], (a, b)):
+            C.memmove(s.data, v.ctypes.data, v.nbytes)
+        lib.add_statevectors(C.byref(sv[0]), C.byref(sv[1]), C.byref(sv[2]))
+        assert lib.rqcopt_gpu_last_error() == 0
+        out = np.empty(1 << L, np.complex128)
+        C.memmove(out.ctypes.data, sv[2].data, out.nbytes)
+        assert np.array_equal(out, oracle.add_statevectors(a, b))
+    finally:
+        for s in sv:
+            lib.free_statevector(C.byref(s))
 
 
 def test_forward_adjoint_round_trip(gpu):

@@ -46,6 +46,22 @@ def test_column_range_matches_reference(oracle, ref):
     assert rel_err(hv, hvr) <= 1e-12
 
 
+def test_headline_size_column_sample_matches_reference(oracle, ref):
+    """L=16, depth 9 against a depth-5 target (seeds 10 / 11 / 12): per-gate sums of two
+    basis columns, the pin of the oracle at the headline size."""
+    vlist, perms, tvlist, tperms = brickwall_instance(16, 9, 10, 5, 11)
+    r = random_tangent_dirs(vlist, 12)
+    vdirs = np.stack([vlist[k] @ real_to_antisymm(r[k]) for k in range(9)])
+    gates, dirs = np.repeat(vlist, 8, axis=0), np.repeat(vdirs, 8, axis=0)
+    wires = np.concatenate([perms[l].reshape(8, 2) for l in range(9)]).astype(np.int32)
+    t = oracle.target("brickwall", (tvlist, tperms))
+    f, dg, hg = oracle.circuit_unitary_target_hessian_vector_product(t, gates, dirs, wires, 16, 40000, 40002)
+    fr, dgr, hgr = ref.brickwall_hvp_columns(vlist, vdirs, perms, 16, tvlist, tperms, 40000, 40002)
+    assert abs(f - fr) <= 1e-12 * abs(fr)
+    assert rel_err(dg, dgr) <= 1e-12
+    assert rel_err(hg, hgr) <= 1e-12
+
+
 def test_trust_region_iterates_match_reference(oracle, ref):
     vlist, perms, tvlist, tperms, _ = _c1()
     t = oracle.target("brickwall", (tvlist, tperms))

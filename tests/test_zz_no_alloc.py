@@ -34,7 +34,12 @@ def _on_device(a):
     return torch.from_numpy(np.ascontiguousarray(a)).to("cuda")
 
 
-def test_noalloc_matches_apply_gate_backward_on_two_calls(gpu):
+def _call(f, SV, V, i, j, psi_d, dout_d, dpsi_d, L, dgate_ptr, stream=None):
+    return f(V.ctypes.data, i, j, C.byref(SV(psi_d.data_ptr(), L)), C.byref(SV(dout_d.data_ptr(), L)),
+             C.byref(SV(dpsi_d.data_ptr(), L)), dgate_ptr, stream)
+
+
+def test_noalloc_matches_apply_gate_backward_on_two_calls(gpu, oracle):
     import torch
     f, SV = _entry(gpu)
     rng = np.random.default_rng(7)
@@ -43,20 +48,63 @@ def test_noalloc_matches_apply_gate_backward_on_two_calls(gpu):
         V = np.ascontiguousarray(crandn((4, 4), rng))
         psi, dout = crandn(1 << L, rng), crandn(1 << L, rng)
         dpsi_ref, dV_ref = gpu.apply_gate_backward(V, i, j, psi, dout)
+        dpsi_orc, dV_orc = oracle.apply_gate_backward(V, i, j, psi, dout)
 
         psi_d, dout_d = _on_device(psi), _on_device(dout)
         dpsi_d = torch.empty_like(psi_d)
         dV = np.zeros((4, 4), np.complex128)
         torch.cuda.synchronize()
         free_before = torch.cuda.mem_get_info()[0]
-        rc = f(V.ctypes.data, i, j, C.byref(SV(psi_d.data_ptr(), L)), C.byref(SV(dout_d.data_ptr(), L)),
-               C.byref(SV(dpsi_d.data_ptr(), L)), dV.ctypes.data, None)
+        rc = _call(f, SV, V, i, j, psi_d, dout_d, dpsi_d, L, dV.ctypes.data)
         free_after = torch.cuda.mem_get_info()[0]
         assert rc == 0
         assert rel_err(dpsi_d.cpu().numpy(), dpsi_ref) <= 1e-12
         assert rel_err(dV, dV_ref) <= 1e-12
+        # and directly against the CPU oracle of the reference's apply_gate_backward
+        assert rel_err(dpsi_d.cpu().numpy(), dpsi_orc) <= 1e-12
+        assert rel_err(dV, dV_orc) <= 1e-12
         if L == 9:   # the scratch was set up by the first call; no device memory is taken now
             assert free_after == free_before
+
+
+def test_noalloc_at_the_size_limit_and_the_smallest_state(gpu, oracle):
+    """25 qubits fill every tile slot of the static scratch; 2 qubits use one group."""
+    import torch
+    f, SV = _entry(gpu)
+    rng = np.random.default_rng(11)
+    for L, i, j in [(MAX_QUBITS, 24, 0), (2, 1, 0)]:
+        V = np.ascontiguousarray(crandn((4, 4), rng))
+        psi, dout = crandn(1 << L, rng), crandn(1 << L, rng)
+        dpsi_orc, dV_orc = oracle.apply_gate_backward(V, i, j, psi, dout)
+        psi_d, dout_d = _on_device(psi), _on_device(dout)
+        del psi, dout
+        dpsi_d = torch.empty_like(psi_d)
+        dV = np.zeros((4, 4), np.complex128)
+        assert _call(f, SV, V, i, j, psi_d, dout_d, dpsi_d, L, dV.ctypes.data) == 0
+        assert rel_err(dpsi_d.cpu().numpy(), dpsi_orc) <= 1e-12
+        assert rel_err(dV, dV_orc) <= 1e-12
+        del psi_d, dout_d, dpsi_d
+        torch.cuda.empty_cache()
+
+
+def test_noalloc_on_a_caller_stream_with_device_dgate(gpu, oracle):
+    """Work issued on the caller's own stream; dgate in device memory."""
+    import torch
+    f, SV = _entry(gpu)
+    rng = np.random.default_rng(13)
+    L, i, j = 14, 5, 9
+    V = np.ascontiguousarray(crandn((4, 4), rng))
+    psi, dout = crandn(1 << L, rng), crandn(1 << L, rng)
+    dpsi_orc, dV_orc = oracle.apply_gate_backward(V, i, j, psi, dout)
+    psi_d, dout_d = _on_device(psi), _on_device(dout)
+    dpsi_d = torch.empty_like(psi_d)
+    dV_d = torch.zeros((4, 4), dtype=torch.complex128, device="cuda")
+    s = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    for _ in range(2):
+        assert _call(f, SV, V, i, j, psi_d, dout_d, dpsi_d, L, dV_d.data_ptr(), C.c_void_p(s.cuda_stream)) == 0
+        assert rel_err(dpsi_d.cpu().numpy(), dpsi_orc) <= 1e-12
+        assert rel_err(dV_d.cpu().numpy(), dV_orc) <= 1e-12
 
 
 def test_noalloc_rejects_states_beyond_the_scratch(gpu):
