@@ -76,6 +76,17 @@ def flops_per_eval(L, G, Gt):
     return float(N) * N * (32 * Gt + 292 * G - 124)
 
 
+def reverse_flops_per_eval(L, G):
+    """Algorithmic flops of the reverse (gradient/HVP) passes of one evaluation as the
+    reference executes them: per gate and amplitude of each of the N = 2^L columns, the
+    outer sums dG += phi (x) psi and HZ += phi (x) dpsi + dphi (x) psi and the adjoint
+    updates phi' = G^T phi, dphi' = G^T dphi + Z^T phi: six 4x4 complex products of an
+    amplitude group, 6 x 32 = 192 flop per amplitude (states rebuilt inside a fused pass
+    are not counted)."""
+    N = 1 << L
+    return 192.0 * G * N * N
+
+
 def reverse_bytes_per_eval(L, P, itemsize):
     """Algorithmic HBM bytes of the reverse (gradient/HVP) passes of one evaluation with P
     passes (one per gate, or one per group of fused gates): per column 6P - 5 statevector
@@ -133,6 +144,39 @@ class ClockSampler:
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+# ----------------------------------------------------------------------------- arithmetic peaks
+
+def measure_fp_peaks(torch, n=8192, reps=5):
+    """Dense FP64 and FP32 throughput of this GPU, measured here the way the bf16 figure of
+    MEASURED_PEAKS.json is measured: cuBLAS GEMMs (torch.matmul) of n x n x n, float64 and
+    float32 with TF32 off, best of `reps` (2 n^3 flop each), CUDA events."""
+    out = {}
+    prev = torch.backends.cuda.matmul.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    try:
+        for name, dt in (("fp64_tflops", torch.float64), ("fp32_tflops", torch.float32)):
+            a = torch.randn(n, n, dtype=dt, device="cuda")
+            b = torch.randn(n, n, dtype=dt, device="cuda")
+            c = torch.matmul(a, b)
+            best = None
+            for _ in range(reps):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                torch.matmul(a, b, out=c)
+                e1.record()
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                best = ms if best is None else min(best, ms)
+            out[name] = 2.0 * n ** 3 / (best * 1e-3) / 1e12
+            del a, b, c
+        torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32 = prev
+    out["how"] = (f"torch.matmul {n}^3 (cuBLAS DGEMM / SGEMM with TF32 off), best of {reps}, 2 n^3 flop, CUDA events, "
+                  "measured in this run")
+    return out
 
 
 # ----------------------------------------------------------------------------- CPU baseline
@@ -660,133 +704,228 @@ def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50, with_reference=
     return out
 
 
-def batched_c4(gpu, torch, count=512, niter=2):
-    """512 independent brickwall instances (even L uniform over 6..12, depth over
-    {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), niter trust-region iterations
-    each: the batched complex64 path (one persistent kernel per round, CUDA-graph
-    rounds) against the plain per-instance complex128 optimiser loop."""
+def batched_c4(gpu, torch, count=512, niter=30, sample_every=8):
+    """C4: 512 independent brickwall instances (even L uniform over 6..12, depth over
+    {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), 30 trust-region iterations each.
+    The batched mixed-precision path (complex64 passes with FP64 sums, complex128 f,
+    gradient and refinement; one persistent kernel per round on a device work queue,
+    CUDA-graph rounds) runs all instances.  The plain per-instance complex128 loop
+    (optimize_brickwall_circuit_hvp one instance after another) runs on every
+    `sample_every`-th instance, and so does the batched path once more, so the speed-up
+    compares the two on identical work; the full loop's time is that sample's time scaled
+    by count / sample size."""
     from rqcopt_hpc_b200 import batch
     from rqcopt_hpc_b200.workloads import batched_instances
     probs = batched_instances(count)
-    out = {"workload": f"{count} brickwall instances, L in {{6,8,10,12}}, depth in {{3,5,7,9}}, {niter} RTR iterations"}
-    warm = batch.Batch(16, niter)   # kernel set-up outside the timed run
+    sample = probs[::sample_every]
+    out = {"workload": f"{count} brickwall instances, L in {{6,8,10,12}}, depth in {{3,5,7,9}}, target depth 3, "
+                       f"{niter} RTR iterations each"}
+    warm = batch.Batch(16, 2)   # kernel and graph set-up outside the timed runs
     for p in probs[:16]:
-        warm.add(p, niter, gpu.PRECISION_C64)
+        warm.add(p, 2, gpu.PRECISION_MIXED)
     while warm.run(32) > 0:
         pass
     warm.close()
-    b = batch.Batch(count, niter)
-    for p in probs:
-        b.add(p, niter, gpu.PRECISION_C64)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    while b.run(32) > 0:
-        pass
-    torch.cuda.synchronize()
-    tb = time.perf_counter() - t0
-    ev, hv = b.evaluations()
-    fb = np.array([b.result(s)[0][-1] for s in range(count)])
-    b.close()
+
+    def run_batched(ps):
+        b = batch.Batch(len(ps), niter)
+        for p in ps:
+            b.add(p, niter, gpu.PRECISION_MIXED)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        while b.run(32) > 0:
+            pass
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        ev, hv = b.evaluations()
+        f = np.array([b.result(k)[0][-1] for k in range(len(ps))])
+        b.close()
+        return sec, ev, hv, f
+
+    tb, ev, hv, fb = run_batched(probs)
+    tbs, evs, _, fbs = run_batched(sample)
     gpu.set_precision(gpu.PRECISION_C128)
-    # warm-up: one instance of every (L, depth) class, so that workspace growth and
-    # kernel set-up fall outside the timed loop
     seen = set()
-    for (L, vl, pm, tv, tp) in probs:
+    for (L, vl, pm, tv, tp) in sample:
         if (L, len(vl)) not in seen:
             seen.add((L, len(vl)))
-            gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, niter)
+            gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, 2)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     fp = []
-    for (L, vl, pm, tv, tp) in probs:
+    for (L, vl, pm, tv, tp) in sample:
         f, _ = gpu.optimize_brickwall_circuit_hvp(gpu.Target(brickwall=(tv, tp)), vl, pm, L, niter)
         fp.append(f[-1])
     torch.cuda.synchronize()
-    tp_ = time.perf_counter() - t0
+    tps = time.perf_counter() - t0
     fp = np.array(fp)
-    out["batched_c64"] = {"seconds": tb, "evaluations": ev, "hvp_evaluations": hv, "evals_per_s": ev / tb,
-                          "instance_iterations_per_s": count * niter / tb}
-    out["per_instance_c128"] = {"seconds": tp_, "instance_iterations_per_s": count * niter / tp_}
-    out["speedup"] = tp_ / tb
-    out["f_final_max_rel_diff"] = float(np.max(np.abs(fb - fp) / np.abs(fp)))
+    out["batched_mixed"] = {"instances": count, "seconds": tb, "evaluations": ev, "hvp_evaluations": hv,
+                            "evals_per_s": ev / tb, "instance_iterations_per_s": count * niter / tb}
+    out["sample"] = {"instances": len(sample), "every": sample_every, "batched_mixed_seconds": tbs,
+                     "per_instance_c128_seconds": tps,
+                     "f_final_max_rel_diff_mixed_vs_c128": float(np.max(np.abs(fbs - fp) / np.abs(fp)))}
+    out["per_instance_c128_full_seconds_scaled"] = tps * count / len(sample)
+    out["speedup"] = tps / tbs
     return out
 
 
-def serving_c5(gpu, rate=200.0, duration=1.0, wall=45.0, niter=100, grad_tol=1e-8, sizes=(8, 10, 12, 14)):
-    """Poisson arrivals (seed 40) of brickwall optimisation requests (even L in 8..14,
+def serving_c5(gpu, rate=200.0, duration=60.0, wall=60.0, niter=100, grad_tol=1e-8, sizes=(8, 10, 12, 14),
+               precisions=("mixed", "plain_c128")):
+    """C5: Poisson arrivals (seed 40) of brickwall optimisation requests (even L in 8..14,
     P(L) ~ 2^(-(L-8)/2), depth in {3,5,7,9}, target depth 3), each stopping at gradient
     norm grad_tol or after niter iterations, admitted into a running batch within a
-    150 GB device budget; p50 / p99 time from arrival to completion of the requests
-    completed within `wall` seconds (the offered load far exceeds one GPU, so the
-    latencies are queue-dominated and the rest is reported as still running)."""
+    150 GB device budget, for the mixed-precision and the plain complex128 path in turn.
+    Each run offers `duration` seconds of arrivals and is measured for `wall` seconds:
+    p50 / p99 time from arrival to completion of the requests completed in that window,
+    completions per second, and the requests still running or queued at its end (at 200
+    req/s the offered load exceeds one GPU, so latencies are queue-dominated)."""
     from rqcopt_hpc_b200 import batch, serving
-    reqs = serving.c5_requests(rate=rate, duration=duration, niter=niter, grad_tol=grad_tol,
-                               precision=gpu.PRECISION_MIXED, sizes=sizes)
-    b = batch.Batch(capacity=4096, max_iterations=niter, sharing=True)
-    srv = serving.Server(b, capacity=4096, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=4)
-    t0 = time.perf_counter()
-    done, left = serving.run_arrivals(srv, reqs, wall_limit=wall)
-    el = time.perf_counter() - t0
-    ev, hv = b.evaluations()
-    b.close()
-    out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s ({len(reqs)} requests, L in {set(sizes)}), "
-                       f"measured for {wall:g} s",
-           "precision": "mixed", "wall_s": el, "completed": len(done), "still_running_or_queued": len(left),
-           "completed_per_s": len(done) / el, "evaluations": ev, "rounds": srv.rounds}
-    out.update(serving.latency_stats(done))
-    if done:
-        out["mean_iterations"] = float(np.mean([r.iterations for r in done]))
+    code = {"mixed": gpu.PRECISION_MIXED, "plain_c128": gpu.PRECISION_C128}
+    out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s (seed 40), L in {set(sizes)}, stop at gradient "
+                       f"norm {grad_tol:g} or {niter} iterations, 150 GB admission budget, measured for {wall:g} s"}
+    for name in precisions:
+        reqs = serving.c5_requests(rate=rate, duration=duration, niter=niter, grad_tol=grad_tol,
+                                   precision=code[name], sizes=sizes)
+        b = batch.Batch(capacity=4096, max_iterations=niter, sharing=True)
+        srv = serving.Server(b, capacity=4096, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=4)
+        t0 = time.perf_counter()
+        done, left = serving.run_arrivals(srv, reqs, wall_limit=wall)
+        el = time.perf_counter() - t0
+        ev, hv = b.evaluations()
+        b.close()
+        r = {"offered": len(reqs), "wall_s": el, "completed": len(done), "still_running_or_queued": len(left),
+             "completed_per_s": len(done) / el, "evaluations": ev, "rounds": srv.rounds}
+        r.update(serving.latency_stats(done))
+        if done:
+            r["mean_iterations"] = float(np.mean([q.iterations for q in done]))
+            r["converged"] = int(sum(q.iterations < niter for q in done))
+        out[name] = r
+    if "mixed" in out and "plain_c128" in out:
+        out["completed_ratio_mixed_over_plain"] = out["mixed"]["completed"] / max(out["plain_c128"]["completed"], 1)
     return out
 
-
-# ----------------------------------------------------------------------------- mixed vs plain
 
 def _relerr(a, b):
     a, b = np.asarray(a), np.asarray(b)
     return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
 
 
-def compare_plain(gpu, torch, stream, step, res_mixed, steps):
-    """The same evaluation with plain complex128 passes (one warm-up, `steps` timed), and
-    the error of the complex64-pass result against it."""
-    gpu.set_precision(gpu.PRECISION_C128)
-    ref = step()
+def compare_mixed(gpu, torch, stream, step, res_c128, steps, L, G, Gt, P, hbm_peak, fp32_peak):
+    """The same evaluation with complex64 passes and FP64 sums (MIXED mode: direct target
+    calls run the complex64 passes), one warm-up and `steps` timed (CUDA events on the
+    library stream), its error against the complex128 result of the headline, and the
+    roofline of its dominant kernel (k5_rev, HBM) and of the whole evaluation against the
+    measured FP32 peak."""
+    gpu.set_precision(gpu.PRECISION_MIXED)
+    step()
     torch.cuda.synchronize()
+    gpu.enable_kernel_timing(True)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(steps):
-        step()
+        res = step()
     e1.record(stream)
     torch.cuda.synchronize()
+    rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
+    gpu.enable_kernel_timing(False)
+    gpu.set_precision(gpu.PRECISION_C128)
     ms = e0.elapsed_time(e1) / steps
-    return {"evals_per_s": 1e3 / ms, "ms_per_step": ms,
-            "mixed_rel_err": {"f": _relerr(res_mixed[0], ref[0]), "grad": _relerr(res_mixed[1], ref[1]),
-                              "hvp": _relerr(res_mixed[2], ref[2])}}
+    rbytes = reverse_bytes_per_eval(L, P, 8) * steps
+    achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
+    flops = flops_per_eval(L, G, Gt)
+    out = {"precision": "complex64 passes (3xTF32 MMA), FP64 sums", "evals_per_s": 1e3 / ms, "ms_per_step": ms,
+           "rel_err_vs_c128": {"f": _relerr(res[0], res_c128[0]), "grad": _relerr(res[1], res_c128[1]),
+                               "hvp": _relerr(res[2], res_c128[2])},
+           "roofline": {"kernel": "k5_rev (complex64 reverse pass, adjoint reconstruction, 4 fused gates)",
+                        "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
+                        "frac": achieved / hbm_peak if achieved else None, "launches": rev_n,
+                        "avg_launch_ms": rev_ms / max(rev_n, 1),
+                        "traffic": rbytes / max(rev_n, 1) * TRAFFIC_RATIO[8]},
+           "eval_flops": {"per_eval": flops, "achieved_tflops": flops / (ms * 1e-3) / 1e12, "peak_tflops": fp32_peak,
+                          "frac": flops / (ms * 1e-3) / 1e12 / fp32_peak if fp32_peak else None,
+                          "peak_source": "FP32 peak measured in this run (cuBLAS SGEMM, TF32 off)"}}
+    return out
 
 
-def rtr_equal_error(gpu, L=12, depth=5, tdepth=3, niter=12):
-    """Riemannian trust region (reference defaults) from the same start in plain complex128 and
-    in mixed precision (complex64 HVPs until the gradient norm falls below the refinement
-    threshold, complex128 f, gradient and refinement): wall time and the final f of each
-    (each mode runs once untimed first, so that its workspace and kernels are set up)."""
-    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, seed=0, tseed=1, dseed=2)
+def mixed_equal_error(gpu, L=10, depth=3, tdepth=3, niter=60, seed=0, tseed=1):
+    """Time to the same optimum: optimize_brickwall_circuit_hvp (reference defaults) from the
+    same start, plain complex128 and mixed precision (complex64 HVPs until the gradient norm
+    falls below the refinement threshold 1e-5, then complex128; f and gradient always
+    complex128), on a workload the trust region drives to convergence within niter
+    iterations.  Reports each run's wall time, its final f, the relative difference of the
+    final f values, the iteration from which f stays within 1e-10 of its final value, and
+    the Hessian-vector products each run made in each precision."""
+    vlist, perms, tvlist, tperms, _ = workload(L, depth, tdepth, seed=seed, tseed=tseed, dseed=2)
     target = gpu.Target(brickwall=(tvlist, tperms))
-    out = {"workload": f"brickwall L={L} depth={depth} vs brickwall target depth={tdepth}, {niter} RTR iterations"}
+    out = {"workload": f"optimize_brickwall_circuit_hvp, brickwall L={L} depth={depth} vs brickwall target "
+                       f"depth={tdepth} (seeds {seed}/{tseed}), {niter} RTR iterations, run to convergence"}
     runs = {}
     for name, p in (("plain_c128", gpu.PRECISION_C128), ("mixed", gpu.PRECISION_MIXED)):
         gpu.set_precision(p)
-        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)   # warm-up
+        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, 2)   # workspace and kernels set up
         t0 = time.perf_counter()
         f_iter, vopt = gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)
-        runs[name] = (time.perf_counter() - t0, f_iter)
-        out[name] = {"seconds": runs[name][0], "f_final": float(f_iter[-1])}
+        sec = time.perf_counter() - t0
+        tr = gpu.optimizer_trace()
+        gpu.set_precision(gpu.PRECISION_C128)
+        _, g = gpu.brickwall_unitary_target_and_projected_gradient(target, vopt, perms, L)
+        near = np.abs(f_iter - f_iter[-1]) <= 1e-10 * abs(f_iter[-1])
+        conv = int(np.argmax([np.all(near[k:]) for k in range(len(near))]))
+        hv = int(tr["inner"].sum() + len(tr["inner"]))   # tCG products + the model product per iteration
+        hv128 = int(((tr["inner"] + 1) * tr["refined"]).sum())
+        refine_at = int(np.argmax(tr["refined"])) if tr["refined"].any() else None
+        runs[name] = (sec, f_iter)
+        out[name] = {"seconds": sec, "f_final": float(f_iter[-1]), "grad_norm_final": float(np.linalg.norm(g)),
+                     "converged_at_iteration": conv, "hvp_evaluations": hv, "hvp_complex128": hv128,
+                     "hvp_complex64": hv - hv128, "refined_from_iteration": refine_at,
+                     "max_tcg_inner_iterations": int(tr["inner"].max())}
     fp, fm = runs["plain_c128"][1][-1], runs["mixed"][1][-1]
     out["f_final_rel_diff"] = abs(fm - fp) / max(abs(fp), 1e-300)
+    out["equal_error"] = bool(out["f_final_rel_diff"] <= 1e-10)
     out["speedup"] = runs["plain_c128"][0] / runs["mixed"][0]
     return out
 
 
-# ----------------------------------------------------------------------------- main
+def summary(line):
+    """Compact figures of every leg, the last key of the JSON line (so that they stay in
+    view where only the end of a long line is kept)."""
+    def g(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    def r(x, n=3):
+        return None if x is None else float(f"{x:.{n}g}")
+
+    out = {"c128_evals_per_s": r(line.get("value")), "c128_e2e_evals_per_s": r(g(line, "e2e", "value")),
+           "roofline_frac": r(g(line, "roofline", "frac")), "cpu_ref_evals_per_s": r(g(line, "cpu_baseline", "value"))}
+    if "mixed" in line:
+        out["mixed_evals_per_s"] = r(g(line, "mixed", "evals_per_s"))
+        out["mixed_over_plain"] = r(line.get("mixed_over_plain"))
+        out["mixed_rel_err_f_grad_hvp"] = [r(g(line, "mixed", "rel_err_vs_c128", k), 2) for k in ("f", "grad", "hvp")]
+        out["k5_rev_hbm_frac"] = r(g(line, "mixed", "roofline", "frac"))
+    me = line.get("mixed_equal_error")
+    if me:
+        out["equal_error"] = {"rel_diff": r(me.get("f_final_rel_diff"), 2), "speedup": r(me.get("speedup")),
+                              "s_plain": r(g(me, "plain_c128", "seconds")), "s_mixed": r(g(me, "mixed", "seconds"))}
+    gt = line.get("gate_throughput")
+    if gt:
+        out["c3_dram_gbs"] = {f"{p}_{k}": r(g(gt, p, f"gates_per_round_trip_{k}", "dram_gbs"))
+                              for p in ("c128", "c64") for k in (1, 4)}
+        out["c3_gate_equiv_gbs"] = {f"{p}_{k}": r(g(gt, p, f"gates_per_round_trip_{k}", "gate_equivalent_gbs"))
+                                    for p in ("c128", "c64") for k in (1, 4)}
+    bt = line.get("batched")
+    if bt:
+        out["c4"] = {"s_batched_512x30": r(g(bt, "batched_mixed", "seconds")), "speedup": r(bt.get("speedup")),
+                     "s_c128_scaled": r(bt.get("per_instance_c128_full_seconds_scaled"))}
+    sv = line.get("serving")
+    if sv:
+        out["c5"] = {k: {"done": g(sv, k, "completed"), "p50_s": r((g(sv, k, "p50_ms") or 0) / 1e3),
+                         "p99_s": r((g(sv, k, "p99_ms") or 0) / 1e3)} for k in ("mixed", "plain_c128") if k in sv}
+    return out
+
 
 def main():
     ap = argparse.ArgumentParser()
@@ -794,8 +933,9 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "c64", "c128"],
-                    help="mixed / c64: complex64 passes with FP64 sums; c128: plain complex128")
+    ap.add_argument("--precision", default="c128", choices=["mixed", "c64", "c128"],
+                    help="c128 (default): plain complex128, the reference's arithmetic; mixed / c64: complex64 "
+                         "passes with FP64 sums")
     ap.add_argument("--L", type=int, default=16)
     ap.add_argument("--depth", type=int, default=9)
     ap.add_argument("--tdepth", type=int, default=5)
@@ -815,7 +955,7 @@ def main():
                          "block-encoding Hessian with H of depth --tdepth on L/2 qubits, 'real' the real build's "
                          "f + projected gradient + projected HVP")
     ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
-    ap.add_argument("--serving-wall", type=float, default=45.0)
+    ap.add_argument("--serving-wall", type=float, default=60.0)
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -916,11 +1056,16 @@ def main():
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clk:
+        # every step goes through the C ABI with host buffers (gates in; f, gradient and
+        # HVP out): the events on the library stream give the device time, the host
+        # clock around the same steps the end-to-end time
+        t0 = time.perf_counter()
         ev0.record(stream)
         for _ in range(a.steps):
             res = step()
         ev1.record(stream)
         barrier()
+        e2e_ms = (time.perf_counter() - t0) * 1e3
     launches = gpu.launch_count()
     dev_ms = ev0.elapsed_time(ev1)
     rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
@@ -929,39 +1074,55 @@ def main():
     fus_ms, fus_n = gpu.kernel_time(gpu.KC_FUSED)
     gpu.enable_kernel_timing(False)
 
-    # end-to-end through the C ABI with host buffers
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        step()
-    barrier()
-    e2e_ms = (time.perf_counter() - t0) * 1e3
-
     from rqcopt_hpc_b200.replicas import max_over_ranks, whole_job_rate
     dev_ms, e2e_ms = max_over_ranks([dev_ms, e2e_ms], device="cuda")
 
     if rank == 0:
         itemsize = 16 if prec == gpu.PRECISION_C128 else 8
-        rev_kernel = ("k3_rev (complex128 FP64-MMA gradient/HVP pass" if itemsize == 16
-                      else "k5_rev (complex64 3xTF32-MMA gradient/HVP pass rebuilding states with adjoint gates")
         peaks = {}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         except (OSError, ValueError):
             pass
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
+        hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+        fp = measure_fp_peaks(torch) if world == 1 else {}
         npass = G if a.gates_per_pass == 1 else -(-G // a.gates_per_pass)
-        rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
-        achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
         value = whole_job_rate(world, a.steps, dev_ms)
-        # DRAM bytes per launch: the algorithmic bytes per launch times the traffic /
-        # algorithmic ratio measured by ncu on a smaller case of the same kernel
-        # (dram__bytes_read + dram__bytes_write of one middle pass at L=12)
-        ratio = TRAFFIC_RATIO.get(itemsize) if a.gates_per_pass > 1 else None
-        traffic = rbytes / max(rev_n, 1) * ratio if ratio else None
-        traffic_src = (f"ncu capture of one middle pass at L=12 (traffic / algorithmic = {ratio}), "
-                       "scaled to the bytes of an average launch here") if ratio else None
         flops = flops_per_eval(L, G, Gt)
+        rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
+        gbs = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
+        if itemsize == 16:
+            # complex128: the reverse pass does ~11 flop per byte it moves, above the FP64
+            # ridge (~6 flop/B), so its roofline is the FP64 tensor pipe (DMMA) that runs it
+            rflops = reverse_flops_per_eval(L, G) * a.steps
+            achieved = rflops / (rev_ms * 1e-3) / 1e12 if rev_ms > 0 else None
+            fp64 = fp.get("fp64_tflops")
+            roof = {"kernel": ("k3_rev (complex128 reverse pass on the FP64 tensor pipe, DMMA m8n8k4, "
+                               f"{a.gates_per_pass} fused gates over a column chunk)"),
+                    "bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
+                    "frac": achieved / fp64 if (achieved and fp64) else None,
+                    "flops_model": "192 flop per amplitude, gate and basis column (six 4x4 complex products of an "
+                                   "amplitude group: the outer sums dG, HZ and the adjoint updates phi, dphi); states "
+                                   "rebuilt inside a pass not counted",
+                    "peak_source": "FP64 peak measured in this run (cuBLAS DGEMM 8192^3)",
+                    "traffic": rbytes / max(rev_n, 1) * 0.99,
+                    "traffic_source": "ncu capture of one middle k3_rev pass at L=12 (DRAM bytes / algorithmic = "
+                                      "0.99), scaled to the bytes of an average launch here",
+                    "hbm_view": {"achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak if gbs else None,
+                                 "peak_source": hbm_src},
+                    "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)}
+        else:
+            ratio = TRAFFIC_RATIO.get(itemsize) if a.gates_per_pass > 1 else None
+            roof = {"kernel": "k5_rev (complex64 reverse pass, adjoint reconstruction, 3xTF32 MMA, "
+                              f"{a.gates_per_pass} fused gates over a column chunk)",
+                    "bytes_model": "(6P-5) * 2^L * 2^L * itemsize per evaluation (P passes): reads of phi, dphi, psi, "
+                                   "dpsi and writes of phi', dphi' per pass",
+                    "bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": gbs / hbm_peak if gbs else None, "peak_source": hbm_src,
+                    "traffic": rbytes / max(rev_n, 1) * ratio if ratio else None,
+                    "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)}
+        peak_eval = fp.get("fp64_tflops") if itemsize == 16 else fp.get("fp32_tflops")
         line = {
             "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": dev_ms / a.steps, "higher_is_better": True, "scaling": "weak",
@@ -972,25 +1133,22 @@ def main():
             "e2e": {"value": whole_job_rate(world, a.steps, e2e_ms), "unit": "evals/s",
                     "h2d_bytes_per_step": int(vlist.nbytes + vdirs.nbytes + tvlist.nbytes + perms.nbytes + tperms.nbytes),
                     "d2h_bytes_per_step": int(16 + 2 * 16 * depth * 8)},
-            "roofline": {"kernel": ("k_reverse (gradient/HVP pass of one gate over a column chunk)" if a.gates_per_pass == 1
-                                    else f"{rev_kernel} of {a.gates_per_pass} fused gates over a column chunk)"),
-                         "bytes_model": "(6P-5) * 2^L * 2^L * itemsize per evaluation (P passes): reads of "
-                                        "phi, dphi, psi, dpsi and writes of phi', dphi' per pass",
-                         "bound": "hbm",
-                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
-                         "frac": achieved / hbm_peak if achieved else None,
-                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if peaks else "fallback 6650",
-                         "traffic": traffic, "traffic_source": traffic_src,
-                         "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)},
+            "roofline": roof,
             "kernel_share": {"reverse_ms": rev_ms, "forward_ms": fwd_ms, "apply_ms": app_ms,
                              "fused_forward_ms": fus_ms, "device_ms": dev_ms},
-            "fp64_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12},
+            "eval_flops": {"per_eval": flops, "achieved_tflops": flops * a.steps / (dev_ms * 1e-3) / 1e12,
+                           "peak_tflops": peak_eval,
+                           "frac": (flops * a.steps / (dev_ms * 1e-3) / 1e12 / peak_eval) if peak_eval else None,
+                           "model": "N^2 (32 G_t + 292 G - 124): the reference's flops of one evaluation",
+                           "peak_source": ("FP64" if itemsize == 16 else "FP32") + " peak measured in this run"},
+            "measured_peaks": fp,
             "clocks": clk.summary(), "gpu_launches": int(launches),
         }
-        if not a.no_compare and world == 1 and prec != gpu.PRECISION_C128:
-            line["plain_c128"] = compare_plain(gpu, torch, stream, step, res, a.steps)
-            line["mixed_over_plain"] = line["plain_c128"]["ms_per_step"] / line["ms_per_step"]
-            line["rtr_equal_error"] = rtr_equal_error(gpu)
+        if world == 1 and prec == gpu.PRECISION_C128 and not a.no_compare:
+            line["mixed"] = compare_mixed(gpu, torch, stream, step, res, min(a.steps, 3), L, G, Gt, npass, hbm_peak,
+                                          fp.get("fp32_tflops"))
+            line["mixed_over_plain"] = line["ms_per_step"] / line["mixed"]["ms_per_step"]
+            line["mixed_equal_error"] = mixed_equal_error(gpu)
             gpu.set_precision(prec)
         if not a.no_gate_throughput:
             line["gate_throughput"] = gate_throughput(gpu, torch)
@@ -999,8 +1157,6 @@ def main():
             gpu.set_precision(prec)
         if not a.no_serving and world == 1:
             line["serving"] = serving_c5(gpu, wall=a.serving_wall)
-            # a load one GPU sustains: 2 req/s of the two smallest size classes
-            line["serving_sustainable"] = serving_c5(gpu, rate=2.0, duration=10.0, wall=40.0, sizes=(8, 10))
             gpu.set_precision(prec)
         if not a.no_hmat and world == 1:
             line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
@@ -1013,6 +1169,7 @@ def main():
             gpu.set_precision(prec)
         if not a.no_cpu_baseline and world == 1:
             line["cpu_baseline"] = cpu_baseline(L, depth, tdepth, seconds=a.cpu_seconds)
+        line["summary"] = summary(line)
         print(json.dumps(line))
     if world > 1:
         torch.distributed.destroy_process_group()

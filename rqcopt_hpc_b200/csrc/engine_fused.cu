@@ -471,7 +471,7 @@ __global__ void __launch_bounds__(TPB2, 1) k2_rev(const cplx<T>* __restrict__ ps
 
 __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 {
-	asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+	asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
 	             : "+d"(d0), "+d"(d1)
 	             : "d"(a), "d"(b));
 }
@@ -558,7 +558,7 @@ __device__ __forceinline__ void apply_unit(const double* in, const double* din, 
 
 // Forward pass (complex128).  Same contract as k2_fwd.
 template <bool TAN, int IN, int OUT>
-__global__ void __launch_bounds__(NTF) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+__global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
                                               double2* __restrict__ psi_o, double2* __restrict__ dpsi_o,
                                               const double2* __restrict__ phi, PassGeom pg, PassGates<double> gates,
                                               double2* __restrict__ fpart)
