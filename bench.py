@@ -847,7 +847,7 @@ def compare_mixed(gpu, torch, stream, step, res_c128, steps, L, G, Gt, P, hbm_pe
     return out
 
 
-def mixed_equal_error(gpu, L=10, depth=3, tdepth=3, niter=60, seed=0, tseed=1):
+def mixed_equal_error(gpu, L=12, depth=3, tdepth=3, niter=80, seed=0, tseed=1):
     """Time to the same optimum: optimize_brickwall_circuit_hvp (reference defaults) from the
     same start, plain complex128 and mixed precision (complex64 HVPs until the gradient norm
     falls below the refinement threshold 1e-5, then complex128; f and gradient always
@@ -955,6 +955,8 @@ def main():
                          "block-encoding Hessian with H of depth --tdepth on L/2 qubits, 'real' the real build's "
                          "f + projected gradient + projected HVP")
     ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
+    ap.add_argument("--reconstruct", type=int, default=1, choices=[0, 1],
+                    help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0)")
     ap.add_argument("--serving-wall", type=float, default=60.0)
     a = ap.parse_args()
 
@@ -1033,7 +1035,8 @@ def main():
     prec = {"c128": gpu.PRECISION_C128, "c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED}[a.precision]
     gpu.set_precision(prec)
     gpu.set_gates_per_pass(a.gates_per_pass)
-    config["gates_per_pass"] = a.gates_per_pass
+    gpu.set_reconstruct(bool(a.reconstruct))
+    gpu.set_column_chunk(a.column_chunk)
     vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
     target = gpu.Target(brickwall=(tvlist, tperms))
 
@@ -1098,8 +1101,10 @@ def main():
             rflops = reverse_flops_per_eval(L, G) * a.steps
             achieved = rflops / (rev_ms * 1e-3) / 1e12 if rev_ms > 0 else None
             fp64 = fp.get("fp64_tflops")
-            roof = {"kernel": ("k3_rev (complex128 reverse pass on the FP64 tensor pipe, DMMA m8n8k4, "
-                               f"{a.gates_per_pass} fused gates over a column chunk)"),
+            roof = {"kernel": (("k6_rev (complex128 reverse pass rebuilding states with adjoint gates" if a.reconstruct
+                                else "k3_rev (complex128 reverse pass recomputing states")
+                               + f" on the FP64 tensor pipe, DMMA m8n8k4, {a.gates_per_pass} fused gates over a column "
+                                 "chunk)"),
                     "bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                     "frac": achieved / fp64 if (achieved and fp64) else None,
                     "flops_model": "192 flop per amplitude, gate and basis column (six 4x4 complex products of an "

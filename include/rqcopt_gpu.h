@@ -482,6 +482,12 @@ int rqcopt_gpu_set_column_range(long begin, long end);
  * eight-qubit tiles of column-interleaved chunks */
 int rqcopt_gpu_set_gates_per_pass(int gates);
 
+/* complex128 reverse passes over fused gates: 1 (default) rebuilds the state entering
+ * each gate from the pass output with the adjoint gate when every gate is unitary to
+ * 1e-14 (four tiles in shared memory, two blocks per SM); 0 recomputes those states
+ * from the pass input.  Both give the same sums to rounding. */
+void rqcopt_gpu_set_reconstruct(int on);
+
 /* last error recorded by a void function (0 if none); reading clears it */
 int rqcopt_gpu_last_error(void);
 

@@ -49,6 +49,11 @@ int rqcopt_gpu_set_column_range(long begin, long end)
 	return 0;
 }
 
+void rqcopt_gpu_set_reconstruct(int on)
+{
+	if (Runtime* rt = runtime()) rt->recon_c128 = on ? 1 : 0;
+}
+
 int rqcopt_gpu_set_gates_per_pass(int gates)
 {
 	if (gates < 1 || gates > 4) return E_ARG;

@@ -662,7 +662,7 @@ int gate_apply_device(Runtime& rt, int L, const double2* gate, int i, int j, con
 int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const double2* d_in,
                          double2* d_out, long ncols)
 {
-	if (ncols == 1 && rt.gates_per_pass > 1 && L >= 10)
+	if (ncols == 1 && rt.gates_per_pass > 1 && L >= 10 && L <= 31)
 		return apply_circuit_fused_device(rt, L, ngates, gates, wires, d_in, d_out, rt.gates_per_pass);
 	// ping-pong between d_out and one scratch buffer so that the last gate writes d_out
 	const size_t bytes = (size_t)ncols * ((size_t)1 << L) * sizeof(double2);
@@ -681,7 +681,7 @@ int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, c
 int apply_circuit_device_c64(Runtime& rt, int L, int ngates, const double2* gates, const int* wires, const float2* d_in,
                              float2* d_out)
 {
-	if (rt.gates_per_pass > 1 && L >= 10)
+	if (rt.gates_per_pass > 1 && L >= 10 && L <= 31)
 		return apply_circuit_fused_device_c64(rt, L, ngates, gates, wires, d_in, d_out, rt.gates_per_pass);
 	const size_t bytes = ((size_t)1 << L) * sizeof(float2);
 	int ret;

@@ -556,7 +556,8 @@ __device__ __forceinline__ void apply_unit(const double* in, const double* din, 
 	if (TAN) dout[st] = make_double2(z0, z1);
 }
 
-// Forward pass (complex128).  Same contract as k2_fwd.
+// Forward pass (complex128).  Same contract as k2_fwd; OUT 3 writes the pass output
+// and adds f, as the last pass does when the reverse pass rebuilds states from it.
 template <bool TAN, int IN, int OUT>
 __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
                                               double2* __restrict__ psi_o, double2* __restrict__ dpsi_o,
@@ -632,20 +633,21 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 			const int r = e >> 2, cc = e & 3;
 			const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
 			const int pe = sidx(r, cc);
-			if (OUT == 2) {
+			if (OUT == 2 || OUT == 3) {
 				const double2 p = phi[a], v = S[pe];
 				fx += p.x * v.x - p.y * v.y;
 				fy += p.x * v.y + p.y * v.x;
-			} else if (OUT == 1) {
+			}
+			if (OUT == 1) {
 				psi_o[a] = cneg_conj(S[pe]);
-			} else {
+			} else if (OUT != 2) {
 				psi_o[a] = S[pe];
 				if (TAN) dpsi_o[a] = dS[pe];
 			}
 		}
 		__syncthreads();
 	}
-	if (OUT == 2) {
+	if (OUT == 2 || OUT == 3) {
 		__shared__ double red[2][NTF / 32];
 		fx = warp_sum(fx);
 		fy = warp_sum(fy);
@@ -1624,6 +1626,167 @@ __global__ void __launch_bounds__(NT5, 2) k5_rev(const float2* __restrict__ psi,
 	}
 }
 
+// ------------------------------------------------------------------------------ complex128 reverse pass, adjoint reconstruction
+
+// Per-gate operands of the reconstructing complex128 reverse pass, formed on the host in
+// FP64: gc = conj(G) (as a row-vector operand it applies G^+) and wn = -W, W = G^+ Z G^+.
+struct PassAdj { Gate4<double> gc[MAXK]; Gate4<double> wn[MAXK]; };
+
+constexpr int NT6 = 256;   // threads of the reconstructing complex128 reverse kernel (two blocks per SM)
+constexpr int EPT6 = (1 << MAXNB) * 4 / NT6;   // tile elements per thread and state
+
+inline size_t k6_rev_smem(bool tan)
+{
+	const size_t A = (size_t)(1 << MAXNB) * 4;
+	const size_t tiles = (tan ? 4 : 2) * A * sizeof(double2);
+	const size_t red = (size_t)(NT6 / 32) * MAXK * NPART3 * sizeof(double);
+	return 64 * MAXK * sizeof(double2) + (1 << MAXNB) * sizeof(int) + std::max(tiles, red);
+}
+
+// Reverse pass (complex128) for unitary gates.  It starts from the state at the OUTPUT
+// of the pass (psi, dpsi: the next pass's checkpoint, or the circuit's final state) and
+// walks back through the pass, rebuilding the state entering each gate with the adjoint
+// gate on the FP64 tensor pipe,
+//   psi_k = G^+ psi_{k+1},  dpsi_k = G^+ dpsi_{k+1} - W psi_{k+1},  W = G^+ Z G^+,
+// so that no state inside the pass is recomputed or kept: four tiles (psi, dpsi, phi,
+// dphi), updated in place, and two blocks per SM whose load, compute and store phases
+// overlap.  For each gate, per unit of eight amplitude groups: rebuild psi_k, dpsi_k;
+// add the outer sums dG_k += phi (x) psi_k, HZ_k += phi (x) dpsi_k + dphi (x) psi_k; move
+// phi, dphi through gate k.  Partials and contract as in k3_rev.
+template <bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+                                                 const double2* __restrict__ phi, const double2* __restrict__ dphi,
+                                                 double2* __restrict__ phi_o, double2* __restrict__ dphi_o, PassGeom pg,
+                                                 PassGates<double> gates, PassAdj adj, double* __restrict__ part, int nblk)
+{
+	constexpr int CW = 4;
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
+	double2* sg = reinterpret_cast<double2*>(smem_raw);           // [MAXK][64]: G, Z, conj(G), -W
+	int* rowoff = reinterpret_cast<int*>(sg + 64 * MAXK);
+	double2* tiles = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));
+	double2* Psi = tiles;
+	double2* Phi = tiles + A;
+	double2* dPsi = TAN ? tiles + 2 * A : nullptr;
+	double2* dPhi = TAN ? tiles + 3 * A : nullptr;
+	for (int e = threadIdx.x; e < 64 * MAXK; e += blockDim.x) {
+		const int k = e / 64, w = e % 64;
+		if (k >= K) continue;
+		double2 v = make_double2(0, 0);
+		if (w < 16) v = gates.g[k].m[w];
+		else if (w < 32) v = TAN ? gates.z[k].m[w - 16] : make_double2(0, 0);
+		else if (w < 48) v = adj.gc[k].m[w - 32];
+		else v = TAN ? adj.wn[k].m[w - 48] : make_double2(0, 0);
+		sg[e] = v;
+	}
+	row_offsets(pg, rowoff);
+	__syncthreads();
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	double cg0[MAXK], cg1[MAXK], ch0[MAXK], ch1[MAXK];
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) { cg0[k] = cg1[k] = ch0[k] = ch1[k] = 0; }
+	const int units = R / 8;
+	double* fPsi = reinterpret_cast<double*>(Psi);
+	double* fPhi = reinterpret_cast<double*>(Phi);
+	double* fdPsi = reinterpret_cast<double*>(dPsi);
+	double* fdPhi = reinterpret_cast<double*>(dPhi);
+
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cgp * CW;
+#pragma unroll
+		for (int i = 0; i < EPT6; i++) {
+			const int e = threadIdx.x + i * NT6;
+			if (e >= A) continue;
+			const int r = e >> 2, cc = e & 3;
+			const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+			const int pe = sidx(r, cc);
+			cp_async16(Psi + pe, psi + a);
+			cp_async16(Phi + pe, phi + a);
+			if (TAN) {
+				cp_async16(dPsi + pe, dpsi + a);
+				if (FIRST) dPhi[pe] = make_double2(0, 0);
+				else cp_async16(dPhi + pe, dphi + a);
+			}
+		}
+		cp_async_commit();
+		cp_async_wait_all();
+		__syncthreads();
+#pragma unroll
+		for (int k = MAXK - 1; k >= 0; k--) {
+			if (k >= K) continue;
+			const StepLane sl(pg.gi[k], pg.gj[k], lane);
+			const bool first_gate = FIRST && k == K - 1;
+			const bool last_gate = LAST && k == 0;
+			double bc[2], bw[2] = {0, 0}, bg[2], bz[2] = {0, 0};
+			bfrag(sg + 64 * k + 32, false, lane, bc);             // G^+ (row-vector operand conj(G))
+			if (TAN) bfrag(sg + 64 * k + 48, true, lane, bw);     // -W
+			bfrag(sg + 64 * k, false, lane, bg);                  // G^T (row-vector operand G)
+			if (TAN) bfrag(sg + 64 * k + 16, false, lane, bz);    // Z^T
+			for (int u = warp; u < units; u += nwarps) {
+				// 1. the state (and tangent) entering gate k, in place
+				if (TAN && !last_gate)
+					apply_unit<true>(fPsi, fdPsi, Psi, dPsi, u, sl, bc, bw, false, lane, true);
+				else
+					apply_unit<false>(fPsi, nullptr, Psi, nullptr, u, sl, bc, bw, false, lane, true);
+				__syncwarp();
+				// 2. outer sums over the two sets of four groups
+				const int base0 = insert2(2 * u, sl.lo, sl.hi), base1 = insert2(2 * u + 1, sl.lo, sl.hi);
+				const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+				const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+				const double p0 = fPhi[i0], x0 = fPsi[i0], p1 = fPhi[i1], x1 = fPsi[i1];
+				dmma(cg0[k], cg1[k], p0, x0);
+				dmma(cg0[k], cg1[k], p1, x1);
+				if (TAN && !last_gate) {
+					dmma(ch0[k], ch1[k], p0, fdPsi[i0]);
+					dmma(ch0[k], ch1[k], p1, fdPsi[i1]);
+				}
+				if (TAN && !first_gate) {
+					dmma(ch0[k], ch1[k], fdPhi[i0], x0);
+					dmma(ch0[k], ch1[k], fdPhi[i1], x1);
+				}
+				if (last_gate) continue;
+				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place)
+				apply_unit<TAN>(fPhi, fdPhi, Phi, dPhi, u, sl, bg, bz, first_gate, lane, true);
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+#pragma unroll
+			for (int i = 0; i < EPT6; i++) {
+				const int e = threadIdx.x + i * NT6;
+				if (e >= A) continue;
+				const int r = e >> 2, cc = e & 3;
+				const int64_t a = (rowbase + rowoff[r]) * pg.C + colbase + cc;
+				const int pe = sidx(r, cc);
+				phi_o[a] = Phi[pe];
+				if (TAN) dphi_o[a] = dPhi[pe];
+			}
+		}
+		__syncthreads();
+	}
+
+	// sum the warps' raw 8x8 accumulators; lane l holds entries 2l, 2l+1
+	double* red = reinterpret_cast<double*>(tiles);   // [warps][MAXK][128]
+#pragma unroll
+	for (int k = 0; k < MAXK; k++) {
+		if (k >= K) break;
+		double* w = red + ((size_t)warp * MAXK + k) * NPART3;
+		w[2 * lane] = cg0[k];
+		w[2 * lane + 1] = cg1[k];
+		w[64 + 2 * lane] = TAN ? ch0[k] : 0.0;
+		w[64 + 2 * lane + 1] = TAN ? ch1[k] : 0.0;
+	}
+	__syncthreads();
+	for (int idx = threadIdx.x; idx < K * NPART3; idx += blockDim.x) {
+		const int k = idx / NPART3, v = idx % NPART3;
+		double s = 0;
+		for (int w = 0; w < nwarps; w++) s += red[((size_t)w * MAXK + k) * NPART3 + v];
+		part[(size_t)k * nblk * NPART3 + (size_t)blockIdx.x * NPART3 + v] += s;
+	}
+}
+
 // Sum the complex64 engine's raw partials over blocks and fold them into complex dG, HZ.
 // Lane (g, t) of an outer-sum MMA holds C[g][2t..2t+1] (v 0,1) and C[g+8][2t..2t+1]
 // (v 2,3): dG raw R[g][2t+i] = v_i, HZ raw R[g][2t+i] = v_{2+i}.
@@ -1841,7 +2004,7 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 			int ret = prepare(k3_fwd<TAN, IN, OUT>, fwd_smem<T>(MAXNB), &per_sm, NTF);
 			if (ret) return ret;
 		}
-		const int grid = OUT == 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
+		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
 		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
 	} else {
 		if (!per_sm) {
@@ -1929,6 +2092,46 @@ int launch_rev5_any(Runtime& rt, bool first, bool last, const float2* psi, const
 	return launch_rev5<TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk, scratch);
 }
 
+template <bool TAN, bool FIRST, bool LAST>
+int launch_rev6(Runtime& rt, const double2* psi, const double2* dpsi, const double2* phi, const double2* dphi,
+                double2* phi_o, double2* dphi_o, const PassGeom& pg, const PassGates<double>& gates, const PassAdj& adj,
+                double* part, int nblk)
+{
+	static bool ready = false;
+	if (!ready) {
+		int per_sm;
+		int ret = prepare(k6_rev<TAN, FIRST, LAST>, k6_rev_smem(TAN), &per_sm, NT6);
+		if (ret) return ret;
+		ready = true;
+	}
+	RQC_LAUNCH3(rt, KC_REVERSE, (k6_rev<TAN, FIRST, LAST>), nblk, NT6, k6_rev_smem(TAN), psi, dpsi, phi, dphi, phi_o,
+	            dphi_o, pg, gates, adj, part, nblk);
+	return OK;
+}
+
+template <bool TAN>
+int launch_rev6_any(Runtime& rt, bool first, bool last, const double2* psi, const double2* dpsi, const double2* phi,
+                    const double2* dphi, double2* phi_o, double2* dphi_o, const PassGeom& pg,
+                    const PassGates<double>& gates, const PassAdj& adj, double* part, int nblk)
+{
+	if (first && last)
+		return launch_rev6<TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, adj, part, nblk);
+	if (first)
+		return launch_rev6<TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, adj, part, nblk);
+	if (last)
+		return launch_rev6<TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, adj, part, nblk);
+	return launch_rev6<TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, adj, part, nblk);
+}
+
+int rev_grid6(Runtime& rt, bool tan)
+{
+	int per_sm = 1;
+	const int ret = tan ? prepare(k6_rev<true, false, false>, k6_rev_smem(true), &per_sm, NT6)
+	                    : prepare(k6_rev<false, false, false>, k6_rev_smem(false), &per_sm, NT6);
+	if (ret) per_sm = 1;
+	return rt.num_sms * per_sm;
+}
+
 int rev_grid5(Runtime& rt, bool tan)
 {
 	int per_sm = 1;
@@ -1938,9 +2141,10 @@ int rev_grid5(Runtime& rt, bool tan)
 	return rt.num_sms * per_sm;
 }
 
-// every gate unitary to 1e-10 (max |G^+ G - I|): the reverse pass may then rebuild
-// states with adjoint gates
-bool gates_unitary(const double2* gates, int G)
+// every gate unitary to `tol` (max |G^+ G - I|): the reverse pass may then rebuild
+// states with adjoint gates (1e-10 for complex64 passes; complex128 passes, which must
+// agree with the reference to 1e-12, ask for 1e-14)
+bool gates_unitary(const double2* gates, int G, double tol = 1e-10)
 {
 	for (int k = 0; k < G; k++) {
 		const double2* g = gates + 16 * (size_t)k;
@@ -1952,10 +2156,42 @@ bool gates_unitary(const double2* gates, int G)
 					re += a.x * b.x + a.y * b.y;
 					im += a.x * b.y - a.y * b.x;
 				}
-				if (fabs(re - (r == c ? 1.0 : 0.0)) > 1e-10 || fabs(im) > 1e-10) return false;
+				if (fabs(re - (r == c ? 1.0 : 0.0)) > tol || fabs(im) > tol) return false;
 			}
 	}
 	return true;
+}
+
+// conj(G) and -W = -G^+ Z G^+ of every gate of a pass, in FP64 (complex128 reconstruction)
+PassAdj pass_adj(const Pass& p, const double2* gates, const double2* dirs)
+{
+	PassAdj pa;
+	memset(&pa, 0, sizeof(pa));
+	for (int k = 0; k < p.K; k++) {
+		const double2* g = gates + 16 * (size_t)(p.first + k);
+		for (int e = 0; e < 16; e++) pa.gc[k].m[e] = make_double2(g[e].x, -g[e].y);
+		if (!dirs) continue;
+		const double2* z = dirs + 16 * (size_t)(p.first + k);
+		double2 gh[16], t[16], w[16];
+		for (int r = 0; r < 4; r++)
+			for (int c = 0; c < 4; c++) gh[4 * r + c] = make_double2(g[4 * c + r].x, -g[4 * c + r].y);
+		auto mul = [](const double2* a, const double2* b, double2* o) {
+			for (int r = 0; r < 4; r++)
+				for (int c = 0; c < 4; c++) {
+					double re = 0, im = 0;
+					for (int q = 0; q < 4; q++) {
+						const double2 x = a[4 * r + q], y = b[4 * q + c];
+						re += x.x * y.x - x.y * y.y;
+						im += x.x * y.y + x.y * y.x;
+					}
+					o[4 * r + c] = make_double2(re, im);
+				}
+		};
+		mul(gh, z, t);
+		mul(t, gh, w);
+		for (int e = 0; e < 16; e++) pa.wn[k].m[e] = make_double2(-w[e].x, -w[e].y);
+	}
+	return pa;
 }
 
 // W = G^+ Z G^+ of every gate of a pass
@@ -2038,8 +2274,11 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	// (the next checkpoint, or the final state) and rebuild states with adjoint gates
 	bool recon = false;
 	if constexpr (!std::is_same<T, double>::value) recon = mode != EVAL_F && gates_unitary(c.gates, G);
-	std::vector<PassW<float>> pw(recon && tan ? P : 0);
+	else recon = mode != EVAL_F && rt.recon_c128 && gates_unitary(c.gates, G, 1e-14);
+	std::vector<PassW<float>> pw(recon && tan && !std::is_same<T, double>::value ? P : 0);
 	for (int p = 0; p < (int)pw.size(); p++) pw[p] = pass_w(passes[p], c.gates, c.dirs);
+	std::vector<PassAdj> padj(recon && std::is_same<T, double>::value ? P : 0);
+	for (int p = 0; p < (int)padj.size(); p++) padj[p] = pass_adj(passes[p], c.gates, tan ? c.dirs : nullptr);
 	const int64_t nck = recon ? P : P - 1;   // checkpoints (recon: also the final state)
 
 	// states per column: PHI, P0, P1 (+ D0, D1) and the pass checkpoints
@@ -2067,7 +2306,8 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	auto ck_at = [&](int p) { return ck + (int64_t)(p - 1) * C * N; };
 	auto dck_at = [&](int p) { return dck + (int64_t)(p - 1) * C * N; };
 
-	const int nblk = recon ? rev_grid5(rt, tan) : rev_grid<T>(rt, tan);
+	const int nblk = recon ? (std::is_same<T, double>::value ? rev_grid6(rt, tan) : rev_grid5(rt, tan))
+	                       : rev_grid<T>(rt, tan);
 	// blocks of the forward launches that sum f (one FP64 partial each)
 	const int nfb = std::is_same<T, double>::value ? nblk : 2 * rt.num_sms;
 	const int nps = std::is_same<T, double>::value ? NPART3 : NRAW4;   // partial doubles per gate and block
@@ -2157,10 +2397,8 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 				const V* in = first ? nullptr : ck_at(p);
 				V* out = (last && !recon) ? nullptr : ck_at(p + 1);
 				if (recon && last) {
-					if constexpr (!std::is_same<T, double>::value) {
-						if (first) ret = launch_fwd<T, false, 1, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
-						else ret = launch_fwd<T, false, 0, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
-					}
+					if (first) ret = launch_fwd<T, false, 1, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
+					else ret = launch_fwd<T, false, 0, 3>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				} else if (first && last) ret = launch_fwd<T, false, 1, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				else if (first) ret = launch_fwd<T, false, 1, 0>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
 				else if (last) ret = launch_fwd<T, false, 0, 2>(rt, in, nullptr, out, nullptr, PHI, g, pgates[p], fpart, nfb);
@@ -2171,10 +2409,8 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 				V* out = (last && !recon) ? nullptr : ck_at(p + 1);
 				V* dout = (last && !recon) ? nullptr : dck_at(p + 1);
 				if (recon && last) {
-					if constexpr (!std::is_same<T, double>::value) {
-						if (first) ret = launch_fwd<T, true, 1, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
-						else ret = launch_fwd<T, true, 0, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
-					}
+					if (first) ret = launch_fwd<T, true, 1, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
+					else ret = launch_fwd<T, true, 0, 3>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				} else if (first && last) ret = launch_fwd<T, true, 1, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				else if (first) ret = launch_fwd<T, true, 1, 0>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
 				else if (last) ret = launch_fwd<T, true, 0, 2>(rt, in, din, out, dout, PHI, g, pgates[p], fpart, nfb);
@@ -2192,6 +2428,19 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 			const V* ph = first ? PHI : Pb[cur];
 			const V* dph = (first || !tan) ? nullptr : Db[cur];
 			double* pp = part + (size_t)passes[p].first * nblk * nps;
+			if constexpr (std::is_same<T, double>::value) {
+				if (recon) {
+					if (tan)
+						ret = launch_rev6_any<true>(rt, first, last, ck_at(p + 1), dck_at(p + 1), ph, dph,
+						                            last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], padj[p],
+						                            pp, nblk);
+					else
+						ret = launch_rev6_any<false>(rt, first, last, ck_at(p + 1), nullptr, ph, nullptr,
+						                             last ? nullptr : Pb[nxt], nullptr, g, pgates[p], padj[p], pp, nblk);
+					if (ret) return ret;
+					continue;
+				}
+			}
 			if constexpr (!std::is_same<T, double>::value) {
 				if (recon) {
 					if (tan)

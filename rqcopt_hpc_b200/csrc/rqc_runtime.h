@@ -37,6 +37,7 @@ struct Runtime
 	Buffer stage[4];      // staging of host statevectors
 	Buffer arrays;        // statevector arrays and gate-input caches of the full-Hessian calls
 	Buffer hpin;          // pinned host scratch
+	Buffer status;        // device status word of kernels with bounded waits (non-zero: a wait gave up)
 
 	// configuration
 	int precision = 0;
@@ -48,6 +49,7 @@ struct Runtime
 	int64_t col_begin = 0, col_end = 0;
 	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
+	int recon_c128 = 1;       // complex128 reverse passes rebuild states with adjoint gates (unitary gates)
 
 	// instrumentation
 	unsigned long long launches = 0;

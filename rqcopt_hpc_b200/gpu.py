@@ -117,6 +117,7 @@ _SIGS = {
     "rqcopt_gpu_set_workspace_limit": (None, [C.c_size_t]),
     "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
     "rqcopt_gpu_set_column_range": (I, [C.c_long, C.c_long]),
+    "rqcopt_gpu_set_reconstruct": (None, [I]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
@@ -854,6 +855,11 @@ def set_precision(mode: int):
 
 def set_gates_per_pass(k: int):
     _check("rqcopt_gpu_set_gates_per_pass", lib().rqcopt_gpu_set_gates_per_pass(k))
+
+
+def set_reconstruct(on: bool):
+    """complex128 reverse passes rebuild states with adjoint gates (True) or recompute them (False)."""
+    lib().rqcopt_gpu_set_reconstruct(1 if on else 0)
 
 
 def set_column_chunk(cols: int):

@@ -197,6 +197,35 @@ def test_add_statevectors_matches_oracle(gpu, oracle):
             lib.free_statevector(C.byref(s))
 
 
+@pytest.mark.parametrize("L,depth,chunk", [(8, 5, 0), (10, 7, 24), (12, 3, 0)])
+def test_reconstructing_reverse_pass_matches_recomputing(gpu, oracle, L, depth, chunk):
+    """complex128 reverse passes: rebuilding the states inside a pass with adjoint gates
+    (the default for unitary gates) and recomputing them from the pass input give the
+    same f, gradient and HVP, both within 1e-12 of the oracle (L <= 10); ragged chunks."""
+    vlist, perms, tvlist, tperms = brickwall_instance(L, depth, 40 + L, 3, 41 + L)
+    vdirs = _dirs(vlist, 42 + L)
+    tgt = gpu.Target(brickwall=(tvlist, tperms))
+    gpu.set_column_chunk(chunk)
+    try:
+        res = {}
+        for on in (True, False):
+            gpu.set_reconstruct(on)
+            res[on] = (gpu.brickwall_unitary_target_projected_hessian_vector_product(tgt, vlist, vdirs, perms, L),
+                       gpu.brickwall_unitary_target_and_projected_gradient(tgt, vlist, perms, L))
+    finally:
+        gpu.set_reconstruct(True)
+    (f1, g1, h1), (fg1, gg1) = res[True]
+    (f0, g0, h0), (fg0, gg0) = res[False]
+    assert abs(f1 - f0) <= 1e-13 * abs(f0)
+    assert rel_err(g1, g0) <= 1e-13 and rel_err(h1, h0) <= 1e-13
+    assert abs(fg1 - fg0) <= 1e-13 * abs(fg0) and rel_err(gg1, gg0) <= 1e-13
+    if L <= 10:
+        fo, go, ho = oracle.brickwall_unitary_target_projected_hessian_vector_product(
+            oracle.target("brickwall", (tvlist, tperms)), vlist, vdirs, perms, L)
+        assert abs(f1 - fo) <= 1e-12 * abs(fo)
+        assert rel_err(g1, go) <= 1e-12 and rel_err(h1, ho) <= 1e-12
+
+
 def test_forward_adjoint_round_trip(gpu):
     """Forward through 64 random Haar gates on random distinct pairs, then the adjoint
     gates in reverse order, recovers the input state (L = 20, complex128)."""
