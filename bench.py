@@ -270,7 +270,7 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
         res[name] = r
         del psi, out, back
         torch.cuda.empty_cache()
-    gpu.set_gates_per_pass(4)
+    gpu.set_autotune(True)
     return res
 
 
@@ -940,7 +940,8 @@ def main():
     ap.add_argument("--depth", type=int, default=9)
     ap.add_argument("--tdepth", type=int, default=5)
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
-    ap.add_argument("--gates-per-pass", type=int, default=4, help="gates fused per HBM round trip (1-4)")
+    ap.add_argument("--gates-per-pass", type=int, default=0,
+                    help="gates fused per HBM round trip (1-4); 0 (default): chosen by the library's autotuner")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-gate-throughput", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the complex128 comparison and the RTR runs")
@@ -955,8 +956,9 @@ def main():
                          "block-encoding Hessian with H of depth --tdepth on L/2 qubits, 'real' the real build's "
                          "f + projected gradient + projected HVP")
     ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
-    ap.add_argument("--reconstruct", type=int, default=1, choices=[0, 1],
-                    help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0)")
+    ap.add_argument("--reconstruct", type=int, default=-1, choices=[-1, 0, 1],
+                    help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0); "
+                         "-1 (default): chosen by the autotuner")
     ap.add_argument("--serving-wall", type=float, default=60.0)
     a = ap.parse_args()
 
@@ -1034,9 +1036,13 @@ def main():
     lib = gpu.lib()
     prec = {"c128": gpu.PRECISION_C128, "c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED}[a.precision]
     gpu.set_precision(prec)
-    gpu.set_gates_per_pass(a.gates_per_pass)
-    gpu.set_reconstruct(bool(a.reconstruct))
-    gpu.set_column_chunk(a.column_chunk)
+    gpu.set_autotune(True)
+    if a.gates_per_pass:
+        gpu.set_gates_per_pass(a.gates_per_pass)
+    if a.reconstruct >= 0:
+        gpu.set_reconstruct(bool(a.reconstruct))
+    if a.column_chunk:
+        gpu.set_column_chunk(a.column_chunk)
     vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
     target = gpu.Target(brickwall=(tvlist, tperms))
 
@@ -1070,6 +1076,7 @@ def main():
         barrier()
         e2e_ms = (time.perf_counter() - t0) * 1e3
     launches = gpu.launch_count()
+    tuned = gpu.last_config()
     dev_ms = ev0.elapsed_time(ev1)
     rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
     fwd_ms, fwd_n = gpu.kernel_time(gpu.KC_FORWARD)
@@ -1090,7 +1097,8 @@ def main():
         hbm_peak = peaks.get("hbm_gbs", 6650.0)
         hbm_src = "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
         fp = measure_fp_peaks(torch) if world == 1 else {}
-        npass = G if a.gates_per_pass == 1 else -(-G // a.gates_per_pass)
+        gpp = tuned["gates_per_pass"]
+        npass = G if gpp == 1 else -(-G // gpp)
         value = whole_job_rate(world, a.steps, dev_ms)
         flops = flops_per_eval(L, G, Gt)
         rbytes = reverse_bytes_per_eval(L, npass, itemsize) * a.steps
@@ -1101,10 +1109,10 @@ def main():
             rflops = reverse_flops_per_eval(L, G) * a.steps
             achieved = rflops / (rev_ms * 1e-3) / 1e12 if rev_ms > 0 else None
             fp64 = fp.get("fp64_tflops")
-            roof = {"kernel": (("k6_rev (complex128 reverse pass rebuilding states with adjoint gates" if a.reconstruct
-                                else "k3_rev (complex128 reverse pass recomputing states")
-                               + f" on the FP64 tensor pipe, DMMA m8n8k4, {a.gates_per_pass} fused gates over a column "
-                                 "chunk)"),
+            roof = {"kernel": (("k6_rev (complex128 reverse pass rebuilding states with adjoint gates"
+                                if tuned["reconstruct"] else "k3_rev (complex128 reverse pass recomputing states")
+                               + f" on the FP64 tensor pipe, DMMA m8n8k4, {gpp} fused gates over a column chunk)"
+                               if gpp > 1 else "k_reverse (complex128 gradient/HVP pass of one gate, FP64)"),
                     "bound": "tensor", "achieved": achieved, "peak": fp64, "unit": "TFLOP/s",
                     "frac": achieved / fp64 if (achieved and fp64) else None,
                     "flops_model": "192 flop per amplitude, gate and basis column (six 4x4 complex products of an "
@@ -1118,9 +1126,9 @@ def main():
                                  "peak_source": hbm_src},
                     "launches": rev_n, "avg_launch_ms": rev_ms / max(rev_n, 1)}
         else:
-            ratio = TRAFFIC_RATIO.get(itemsize) if a.gates_per_pass > 1 else None
+            ratio = TRAFFIC_RATIO.get(itemsize) if gpp > 1 else None
             roof = {"kernel": "k5_rev (complex64 reverse pass, adjoint reconstruction, 3xTF32 MMA, "
-                              f"{a.gates_per_pass} fused gates over a column chunk)",
+                              f"{gpp} fused gates over a column chunk)",
                     "bytes_model": "(6P-5) * 2^L * 2^L * itemsize per evaluation (P passes): reads of phi, dphi, psi, "
                                    "dpsi and writes of phi', dphi' per pass",
                     "bound": "hbm", "achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
@@ -1147,6 +1155,9 @@ def main():
                            "model": "N^2 (32 G_t + 292 G - 124): the reference's flops of one evaluation",
                            "peak_source": ("FP64" if itemsize == 16 else "FP32") + " peak measured in this run"},
             "measured_peaks": fp,
+            "tuned": {"gates_per_pass": gpp, "column_chunk": tuned["column_chunk"] or "from workspace",
+                      "reconstruct": tuned["reconstruct"], "chosen_by_autotuner": tuned["tuned"],
+                      "sample_ms_per_column": tuned["ms_per_column"]},
             "clocks": clk.summary(), "gpu_launches": int(launches),
         }
         if world == 1 and prec == gpu.PRECISION_C128 and not a.no_compare:

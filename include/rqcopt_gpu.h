@@ -479,8 +479,25 @@ int rqcopt_gpu_set_column_range(long begin, long end);
 
 /* gates fused per HBM round trip in the basis-column passes: 1 runs one kernel
  * per gate, 2..4 (default 4) group consecutive gates into passes over
- * eight-qubit tiles of column-interleaved chunks */
+ * eight-qubit tiles of column-interleaved chunks.  Setting it fixes it for the
+ * autotuner too (as do rqcopt_gpu_set_column_chunk with a positive count and
+ * rqcopt_gpu_set_reconstruct). */
 int rqcopt_gpu_set_gates_per_pass(int gates);
+
+/* Autotuning of the basis-column sums (on by default): on the first evaluation of a
+ * problem shape (qubits, gates, target gates, precision, mode, paired columns) with at
+ * least 2^26 amplitude x gate updates and a device-native target, the library times the
+ * candidate gates-per-pass (1-4), column chunks and complex128 reverse variants on a
+ * sample of up to 4096 basis columns with CUDA events and keeps the fastest for the rest
+ * of the process; choices fixed by the setters above are kept.  Results are the same to
+ * rounding whichever configuration runs.  rqcopt_gpu_set_autotune(1) also releases the
+ * fixed choices and restores the defaults; 0 turns tuning off.  Returns 0 or -5. */
+int rqcopt_gpu_set_autotune(int on);
+/* configuration of the last target evaluation on this device: gates per pass, column
+ * chunk (0: from the workspace), complex128 reconstruction, and the tuned sample's time
+ * per basis column in ms; returns 1 if the autotuner chose it, 0 if the defaults / fixed
+ * settings ran, -5 without a device */
+int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, double* ms_per_column);
 
 /* complex128 reverse passes over fused gates: 1 (default) rebuilds the state entering
  * each gate from the pass output with the adjoint gate when every gate is unitary to

@@ -36,7 +36,36 @@ void rqcopt_gpu_set_workspace_limit(size_t bytes)
 
 void rqcopt_gpu_set_column_chunk(long columns)
 {
-	if (Runtime* rt = runtime()) rt->column_chunk = columns > 0 ? columns : 0;
+	if (Runtime* rt = runtime()) {
+		rt->column_chunk = columns > 0 ? columns : 0;
+		rt->pin_chunk = columns > 0;
+	}
+}
+
+int rqcopt_gpu_set_autotune(int on)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	rt->autotune = on ? 1 : 0;
+	if (on) {
+		rt->pin_gpp = rt->pin_chunk = rt->pin_recon = false;
+		rt->gates_per_pass = 4;
+		rt->column_chunk = 0;
+		rt->recon_c128 = 1;
+	}
+	return 0;
+}
+
+int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, double* ms_per_column)
+{
+	Runtime* rt = runtime();
+	if (!rt) return E_CUDA;
+	const Runtime::TuneChoice& c = rt->last_choice;
+	if (gates_per_pass) *gates_per_pass = c.gates_per_pass;
+	if (column_chunk) *column_chunk = c.column_chunk;
+	if (reconstruct) *reconstruct = c.recon;
+	if (ms_per_column) *ms_per_column = c.ms_per_column;
+	return c.tuned;
 }
 
 int rqcopt_gpu_set_column_range(long begin, long end)
@@ -51,7 +80,10 @@ int rqcopt_gpu_set_column_range(long begin, long end)
 
 void rqcopt_gpu_set_reconstruct(int on)
 {
-	if (Runtime* rt = runtime()) rt->recon_c128 = on ? 1 : 0;
+	if (Runtime* rt = runtime()) {
+		rt->recon_c128 = on ? 1 : 0;
+		rt->pin_recon = true;
+	}
 }
 
 int rqcopt_gpu_set_gates_per_pass(int gates)
@@ -60,6 +92,7 @@ int rqcopt_gpu_set_gates_per_pass(int gates)
 	Runtime* rt = runtime();
 	if (!rt) return E_CUDA;
 	rt->gates_per_pass = gates;
+	rt->pin_gpp = true;
 	return 0;
 }
 

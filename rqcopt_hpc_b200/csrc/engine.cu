@@ -607,6 +607,12 @@ int set_pair_half(Runtime& rt, int64_t half)
 static int evaluate_columns(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision,
                             double2* d_out);
 
+// the configured evaluation (gates per pass, column chunk, reverse variant as set in rt)
+int evaluate_configured(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out)
+{
+	return evaluate_columns(rt, c, t, mode, precision, d_out);
+}
+
 // With rt.real_pairs (real gates, real target): the 2^(L-1) paired columns
 // e_b + i e_{b + N/2}.  Every sum the engine forms pairs an adjoint-type state (from
 // -conj(U psi)) with a forward-type state, both propagated by real matrices, so its
@@ -614,10 +620,10 @@ static int evaluate_columns(Runtime& rt, const CircuitSpec& c, const TargetSpec&
 // terms) are cleared.
 int evaluate(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out)
 {
-	if (!rt.real_pairs) return evaluate_columns(rt, c, t, mode, precision, d_out);
+	if (!rt.real_pairs) return evaluate_autotuned(rt, c, t, mode, precision, d_out);
 	if (c.L < 2) return E_ARG;
 	int ret = set_pair_half(rt, (int64_t)1 << (c.L - 1));
-	if (!ret) ret = evaluate_columns(rt, c, t, mode, precision, d_out);
+	if (!ret) ret = evaluate_autotuned(rt, c, t, mode, precision, d_out);
 	const int reset = set_pair_half(rt, 0);
 	if (!ret) ret = reset;
 	if (ret) return ret;

@@ -39,6 +39,14 @@ inline size_t result_count(int ngates) { return 1 + 32 * (size_t)ngates; }
 // Returns 0, E_UFUNC if the host callback fails, E_ALLOC or E_CUDA.
 int evaluate(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out);
 
+// evaluate() with the configuration in rt as it stands (no autotuning)
+int evaluate_configured(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out);
+
+// evaluate_configured() under the configuration the autotuner picked for this problem
+// shape (autotune.cu), tuning on first use when rt.autotune is set and the problem is
+// large enough for the choice to matter
+int evaluate_autotuned(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int mode, int precision, double2* d_out);
+
 // Apply a circuit to a batch of states: out = C in, for `ncols` states of 2^L
 // amplitudes stored one after another (device pointers; in and out distinct).
 int apply_circuit_device(Runtime& rt, int L, int ngates, const double2* gates, const int* wires,

@@ -118,6 +118,8 @@ _SIGS = {
     "rqcopt_gpu_set_column_chunk": (None, [C.c_long]),
     "rqcopt_gpu_set_column_range": (I, [C.c_long, C.c_long]),
     "rqcopt_gpu_set_reconstruct": (None, [I]),
+    "rqcopt_gpu_set_autotune": (I, [I]),
+    "rqcopt_gpu_last_config": (I, [VP, VP, VP, VP]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
@@ -855,6 +857,24 @@ def set_precision(mode: int):
 
 def set_gates_per_pass(k: int):
     _check("rqcopt_gpu_set_gates_per_pass", lib().rqcopt_gpu_set_gates_per_pass(k))
+
+
+def set_autotune(on: bool):
+    """Autotuning of the basis-column sums (on by default); turning it on also releases the
+    settings fixed by set_gates_per_pass / set_column_chunk / set_reconstruct."""
+    _check("rqcopt_gpu_set_autotune", lib().rqcopt_gpu_set_autotune(1 if on else 0))
+
+
+def last_config():
+    """Configuration of the last target evaluation: gates per pass, column chunk (0: from
+    the workspace), reconstruction, sample ms per column and whether the autotuner chose it."""
+    g, r = C.c_int(), C.c_int()
+    ch, ms = C.c_long(), C.c_double()
+    tuned = lib().rqcopt_gpu_last_config(C.byref(g), C.byref(ch), C.byref(r), C.byref(ms))
+    if tuned < 0:
+        raise RqcError("rqcopt_gpu_last_config", tuned)
+    return {"gates_per_pass": g.value, "column_chunk": ch.value, "reconstruct": bool(r.value),
+            "ms_per_column": ms.value, "tuned": bool(tuned)}
 
 
 def set_reconstruct(on: bool):

@@ -59,7 +59,7 @@ def _restore(gpu):
     yield
     gpu.set_column_range(0, 0)
     gpu.set_precision(gpu.PRECISION_C128)
-    gpu.set_gates_per_pass(4)
+    gpu.set_autotune(True)
 
 
 def _check(f, dg, hg, ref, tol):
