@@ -556,6 +556,56 @@ __device__ __forceinline__ void apply_unit(const double* in, const double* din, 
 	if (TAN) dout[st] = make_double2(z0, z1);
 }
 
+// apply_unit for two units of a warp at once (u0 and, if has1, u1; has1 is the same for
+// all lanes): both units' operands are loaded before either is stored, so the two
+// independent MMA chains overlap; in place like apply_unit(..., inplace = true).
+template <bool TAN>
+__device__ __forceinline__ void apply_unit2(const double* in, const double* din, double2* out, double2* dout, int u0,
+                                           int u1, bool has1, const StepLane& sl, const double bg[2], const double bz[2],
+                                           bool dzero, int lane)
+{
+	const int cc = (lane >> 2) & 3;
+	const int bs0 = insert2(2 * u0 + (lane >> 4), sl.lo, sl.hi);
+	const int bs1 = insert2(2 * (has1 ? u1 : u0) + (lane >> 4), sl.lo, sl.hi);
+	const int j00 = sidx(bs0 | sl.m_k0, cc) * 2 + sl.part_out, j01 = sidx(bs0 | sl.m_k1, cc) * 2 + sl.part_out;
+	const int j10 = sidx(bs1 | sl.m_k0, cc) * 2 + sl.part_out, j11 = sidx(bs1 | sl.m_k1, cc) * 2 + sl.part_out;
+	const double a00 = in[j00], a01 = in[j01], a10 = in[j10], a11 = in[j11];
+	double d00 = 0, d01 = 0, d10 = 0, d11 = 0;
+	if (TAN && !dzero) {
+		d00 = din[j00];
+		d01 = din[j01];
+		d10 = din[j10];
+		d11 = din[j11];
+	}
+	double y0a = 0, y1a = 0, y0b = 0, y1b = 0, z0a = 0, z1a = 0, z0b = 0, z1b = 0;
+	dmma(y0a, y1a, a00, bg[0]);
+	dmma(y0b, y1b, a10, bg[0]);
+	if (TAN) {
+		dmma(z0a, z1a, a00, bz[0]);
+		dmma(z0b, z1b, a10, bz[0]);
+	}
+	dmma(y0a, y1a, a01, bg[1]);
+	dmma(y0b, y1b, a11, bg[1]);
+	if (TAN) {
+		dmma(z0a, z1a, a01, bz[1]);
+		dmma(z0b, z1b, a11, bz[1]);
+		if (!dzero) {
+			dmma(z0a, z1a, d00, bg[0]);
+			dmma(z0b, z1b, d10, bg[0]);
+			dmma(z0a, z1a, d01, bg[1]);
+			dmma(z0b, z1b, d11, bg[1]);
+		}
+	}
+	__syncwarp();
+	const int st0 = sidx(bs0 | sl.m_st, cc), st1 = sidx(bs1 | sl.m_st, cc);
+	out[st0] = make_double2(y0a, y1a);
+	if (TAN) dout[st0] = make_double2(z0a, z1a);
+	if (has1) {
+		out[st1] = make_double2(y0b, y1b);
+		if (TAN) dout[st1] = make_double2(z0b, z1b);
+	}
+}
+
 // Forward pass (complex128).  Same contract as k2_fwd; OUT 3 writes the pass output
 // and adds f, as the last pass does when the reverse pass rebuilds states from it.
 template <bool TAN, int IN, int OUT>
@@ -622,9 +672,9 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 			bfrag(sg + 32 * k, true, lane, bg);
 			if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
 			const bool dzero = IN == 1 && k == 0;
-			for (int u = warp; u < units; u += nwarps)
-				apply_unit<TAN>(reinterpret_cast<const double*>(S), reinterpret_cast<const double*>(dS), S, dS, u, sl, bg,
-				                bz, dzero, lane, true);
+			for (int u = warp; u < units; u += 2 * nwarps)
+				apply_unit2<TAN>(reinterpret_cast<const double*>(S), reinterpret_cast<const double*>(dS), S, dS, u,
+				                 u + nwarps, u + nwarps < units, sl, bg, bz, dzero, lane);
 			__syncthreads();
 		}
 		for (int i = 0; i < EPTF; i++) {
@@ -1724,31 +1774,39 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 			if (TAN) bfrag(sg + 64 * k + 48, true, lane, bw);     // -W
 			bfrag(sg + 64 * k, false, lane, bg);                  // G^T (row-vector operand G)
 			if (TAN) bfrag(sg + 64 * k + 16, false, lane, bz);    // Z^T
-			for (int u = warp; u < units; u += nwarps) {
-				// 1. the state (and tangent) entering gate k, in place
+			for (int u = warp; u < units; u += 2 * nwarps) {
+				const int u1 = u + nwarps;
+				const bool has1 = u1 < units;   // the same for the whole warp
+				// 1. the state (and tangent) entering gate k, in place, for both units
 				if (TAN && !last_gate)
-					apply_unit<true>(fPsi, fdPsi, Psi, dPsi, u, sl, bc, bw, false, lane, true);
+					apply_unit2<true>(fPsi, fdPsi, Psi, dPsi, u, u1, has1, sl, bc, bw, false, lane);
 				else
-					apply_unit<false>(fPsi, nullptr, Psi, nullptr, u, sl, bc, bw, false, lane, true);
+					apply_unit2<false>(fPsi, nullptr, Psi, nullptr, u, u1, has1, sl, bc, bw, false, lane);
 				__syncwarp();
-				// 2. outer sums over the two sets of four groups
-				const int base0 = insert2(2 * u, sl.lo, sl.hi), base1 = insert2(2 * u + 1, sl.lo, sl.hi);
-				const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
-				const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
-				const double p0 = fPhi[i0], x0 = fPsi[i0], p1 = fPhi[i1], x1 = fPsi[i1];
-				dmma(cg0[k], cg1[k], p0, x0);
-				dmma(cg0[k], cg1[k], p1, x1);
-				if (TAN && !last_gate) {
-					dmma(ch0[k], ch1[k], p0, fdPsi[i0]);
-					dmma(ch0[k], ch1[k], p1, fdPsi[i1]);
-				}
-				if (TAN && !first_gate) {
-					dmma(ch0[k], ch1[k], fdPhi[i0], x0);
-					dmma(ch0[k], ch1[k], fdPhi[i1], x1);
+				// 2. outer sums over the two sets of four groups of each unit
+#pragma unroll
+				for (int q = 0; q < 2; q++) {
+					if (q == 1 && !has1) break;
+					const int uq = q ? u1 : u;
+					const int base0 = insert2(2 * uq, sl.lo, sl.hi), base1 = insert2(2 * uq + 1, sl.lo, sl.hi);
+					const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+					const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+					const double p0 = fPhi[i0], x0 = fPsi[i0], p1 = fPhi[i1], x1 = fPsi[i1];
+					double dx0 = 0, dx1 = 0, dp0 = 0, dp1 = 0;
+					if (TAN && !last_gate) { dx0 = fdPsi[i0]; dx1 = fdPsi[i1]; }
+					if (TAN && !first_gate) { dp0 = fdPhi[i0]; dp1 = fdPhi[i1]; }
+					dmma(cg0[k], cg1[k], p0, x0);
+					if (TAN && !last_gate) dmma(ch0[k], ch1[k], p0, dx0);
+					dmma(cg0[k], cg1[k], p1, x1);
+					if (TAN && !last_gate) dmma(ch0[k], ch1[k], p1, dx1);
+					if (TAN && !first_gate) {
+						dmma(ch0[k], ch1[k], dp0, x0);
+						dmma(ch0[k], ch1[k], dp1, x1);
+					}
 				}
 				if (last_gate) continue;
-				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place)
-				apply_unit<TAN>(fPhi, fdPhi, Phi, dPhi, u, sl, bg, bz, first_gate, lane, true);
+				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place), both units
+				apply_unit2<TAN>(fPhi, fdPhi, Phi, dPhi, u, u1, has1, sl, bg, bz, first_gate, lane);
 			}
 			__syncthreads();
 		}
