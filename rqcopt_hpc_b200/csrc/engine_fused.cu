@@ -1783,7 +1783,9 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 				else
 					apply_unit2<false>(fPsi, nullptr, Psi, nullptr, u, u1, has1, sl, bc, bw, false, lane);
 				__syncwarp();
-				// 2. outer sums over the two sets of four groups of each unit
+				// 2. outer sums over the two sets of four groups of each unit, into fresh
+				//    partial sums per unit (short MMA chains), then added to the gate's sums
+				double tg[2][2] = {{0, 0}, {0, 0}}, th[2][2] = {{0, 0}, {0, 0}};
 #pragma unroll
 				for (int q = 0; q < 2; q++) {
 					if (q == 1 && !has1) break;
@@ -1795,14 +1797,20 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 					double dx0 = 0, dx1 = 0, dp0 = 0, dp1 = 0;
 					if (TAN && !last_gate) { dx0 = fdPsi[i0]; dx1 = fdPsi[i1]; }
 					if (TAN && !first_gate) { dp0 = fdPhi[i0]; dp1 = fdPhi[i1]; }
-					dmma(cg0[k], cg1[k], p0, x0);
-					if (TAN && !last_gate) dmma(ch0[k], ch1[k], p0, dx0);
-					dmma(cg0[k], cg1[k], p1, x1);
-					if (TAN && !last_gate) dmma(ch0[k], ch1[k], p1, dx1);
+					dmma(tg[q][0], tg[q][1], p0, x0);
+					if (TAN && !last_gate) dmma(th[q][0], th[q][1], p0, dx0);
+					dmma(tg[q][0], tg[q][1], p1, x1);
+					if (TAN && !last_gate) dmma(th[q][0], th[q][1], p1, dx1);
 					if (TAN && !first_gate) {
-						dmma(ch0[k], ch1[k], dp0, x0);
-						dmma(ch0[k], ch1[k], dp1, x1);
+						dmma(th[q][0], th[q][1], dp0, x0);
+						dmma(th[q][0], th[q][1], dp1, x1);
 					}
+				}
+				cg0[k] += tg[0][0] + tg[1][0];
+				cg1[k] += tg[0][1] + tg[1][1];
+				if (TAN) {
+					ch0[k] += th[0][0] + th[1][0];
+					ch1[k] += th[0][1] + th[1][1];
 				}
 				if (last_gate) continue;
 				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place), both units

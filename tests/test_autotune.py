@@ -1,7 +1,9 @@
 """The autotuner of the basis-column sums (rqcopt_gpu_set_autotune): it picks gates
 per pass, column chunk and the complex128 reverse variant by timing candidates on a
 column sample, so every candidate must give the same f, projected gradient and
-projected HVP (to 1e-12 relative), and settings the caller fixes must be kept."""
+projected HVP (to 1e-12 relative in complex128; within the 1e-5 bar of complex64
+passes, whose rounding depends on how gates are grouped into passes), and settings
+the caller fixes must be kept."""
 import itertools
 
 import numpy as np
@@ -42,16 +44,17 @@ def test_every_candidate_gives_the_tuned_result(gpu, oracle, precision, tol):
     assert gpu.last_config() == cfg
     assert abs(again[0] - tuned[0]) <= 1e-14 * abs(tuned[0])
     recon = (True, False) if precision == "C128" else (True,)
-    for gpp, chunk, rc in itertools.product((1, 2, 3, 4), (0, 2048, 512), recon):
+    for gpp, chunk, rc in itertools.product((1, 2, 3, 4), (4096, 2048, 512), recon):
         gpu.set_gates_per_pass(gpp)
         gpu.set_column_chunk(chunk)
         gpu.set_reconstruct(rc)
         f, g, h = gpu.brickwall_unitary_target_projected_hessian_vector_product(tgt, vlist, vdirs, perms, L)
         used = gpu.last_config()
         assert not used["tuned"] and used["gates_per_pass"] == gpp and used["column_chunk"] == chunk
-        assert abs(f - tuned[0]) <= 1e-12 * abs(tuned[0]), (gpp, chunk, rc)
-        assert rel_err(g, tuned[1]) <= 1e-12, (gpp, chunk, rc)
-        assert rel_err(h, tuned[2]) <= 1e-12, (gpp, chunk, rc)
+        # complex128: the same sums to rounding; complex64: within the single-precision bar
+        assert abs(f - tuned[0]) <= tol * abs(tuned[0]), (gpp, chunk, rc)
+        assert rel_err(g, tuned[1]) <= tol, (gpp, chunk, rc)
+        assert rel_err(h, tuned[2]) <= tol, (gpp, chunk, rc)
     if precision == "C128":
         fo, go, ho = oracle.brickwall_unitary_target_projected_hessian_vector_product(
             oracle.target("brickwall", (tvlist, tperms)), vlist, vdirs, perms, L)
