@@ -494,10 +494,17 @@ int rqcopt_gpu_set_gates_per_pass(int gates);
  * fixed choices and restores the defaults; 0 turns tuning off.  Returns 0 or -5. */
 int rqcopt_gpu_set_autotune(int on);
 /* configuration of the last target evaluation on this device: gates per pass, column
- * chunk (0: from the workspace), complex128 reconstruction, and the tuned sample's time
- * per basis column in ms; returns 1 if the autotuner chose it, 0 if the defaults / fixed
- * settings ran, -5 without a device */
-int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, double* ms_per_column);
+ * chunk (0: from the workspace), complex128 reconstruction, complex64 passes on the FP32
+ * pipe (1) or the TF32 MMA (0), and the tuned sample's time per basis column in ms;
+ * returns 1 if the autotuner chose it, 0 if the defaults / fixed settings ran, -5 without
+ * a device */
+int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, int* c64_fp32_pipe,
+                           double* ms_per_column);
+/* complex64 fused passes: 1 (default) in FP32 FMAs, four threads per amplitude group and
+ * the gate coefficients in registers; 0 on the TF32 tensor-core MMA with the three-term
+ * split (FP32 accuracy).  Both meet the complex64 bar; fixing it keeps it for the
+ * autotuner. */
+void rqcopt_gpu_set_c64_fp32_pipe(int on);
 
 /* complex128 reverse passes over fused gates: 1 (default) rebuilds the state entering
  * each gate from the pass output with the adjoint gate when every gate is unitary to

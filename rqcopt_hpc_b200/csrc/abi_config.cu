@@ -48,15 +48,17 @@ int rqcopt_gpu_set_autotune(int on)
 	if (!rt) return E_CUDA;
 	rt->autotune = on ? 1 : 0;
 	if (on) {
-		rt->pin_gpp = rt->pin_chunk = rt->pin_recon = false;
+		rt->pin_gpp = rt->pin_chunk = rt->pin_recon = rt->pin_ffma = false;
 		rt->gates_per_pass = 4;
 		rt->column_chunk = 0;
 		rt->recon_c128 = 1;
+		rt->c64_ffma = 1;
 	}
 	return 0;
 }
 
-int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, double* ms_per_column)
+int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, int* c64_fp32_pipe,
+                           double* ms_per_column)
 {
 	Runtime* rt = runtime();
 	if (!rt) return E_CUDA;
@@ -64,6 +66,7 @@ int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconst
 	if (gates_per_pass) *gates_per_pass = c.gates_per_pass;
 	if (column_chunk) *column_chunk = c.column_chunk;
 	if (reconstruct) *reconstruct = c.recon;
+	if (c64_fp32_pipe) *c64_fp32_pipe = c.ffma;
 	if (ms_per_column) *ms_per_column = c.ms_per_column;
 	return c.tuned;
 }
@@ -76,6 +79,14 @@ int rqcopt_gpu_set_column_range(long begin, long end)
 	rt->col_begin = begin;
 	rt->col_end = end;
 	return 0;
+}
+
+void rqcopt_gpu_set_c64_fp32_pipe(int on)
+{
+	if (Runtime* rt = runtime()) {
+		rt->c64_ffma = on ? 1 : 0;
+		rt->pin_ffma = true;
+	}
 }
 
 void rqcopt_gpu_set_reconstruct(int on)

@@ -4,9 +4,10 @@
 // column chunks; how fast depends on three choices that interact with the problem
 // shape and the GPU: gates fused per HBM round trip (1 = one kernel per gate, 2..4 =
 // fused passes over eight-qubit tiles), columns per chunk (larger chunks amortise the
-// per-launch cost, smaller ones keep more of the working set in L2), and for
-// complex128 whether the reverse passes rebuild the states inside a pass with adjoint
-// gates or recompute them from the pass input.
+// per-launch cost, smaller ones keep more of the working set in L2), for complex128
+// whether the reverse passes rebuild the states inside a pass with adjoint gates or
+// recompute them from the pass input, and for complex64 whether the passes run on the
+// FP32 FMA pipe or on the TF32 tensor-core MMA.
 //
 // On the first evaluation of a problem shape (qubits, gates, target gates, precision,
 // mode, target kind, paired columns) large enough for the choice to matter, every
@@ -33,19 +34,21 @@ namespace {
 // configured defaults (their evaluations take well under a millisecond)
 constexpr double TUNE_MIN_WORK = 1 << 26;
 
-struct Config { int gpp; long chunk; int recon; };
+struct Config { int gpp; long chunk; int recon; int ffma; };
 
 struct Saved
 {
-	int gpp, recon;
+	int gpp, recon, ffma;
 	long chunk;
 	int64_t b, e;
 	explicit Saved(const Runtime& rt)
-		: gpp(rt.gates_per_pass), recon(rt.recon_c128), chunk(rt.column_chunk), b(rt.col_begin), e(rt.col_end) {}
+		: gpp(rt.gates_per_pass), recon(rt.recon_c128), ffma(rt.c64_ffma), chunk(rt.column_chunk), b(rt.col_begin),
+		  e(rt.col_end) {}
 	void restore(Runtime& rt) const
 	{
 		rt.gates_per_pass = gpp;
 		rt.recon_c128 = recon;
+		rt.c64_ffma = ffma;
 		rt.column_chunk = chunk;
 		rt.col_begin = b;
 		rt.col_end = e;
@@ -57,6 +60,7 @@ void apply(Runtime& rt, const Config& k)
 	rt.gates_per_pass = k.gpp;
 	rt.column_chunk = k.chunk;
 	rt.recon_c128 = k.recon;
+	rt.c64_ffma = k.ffma;
 }
 
 // milliseconds of one evaluation under configuration k over the sample [b, e) (the
@@ -92,13 +96,13 @@ int evaluate_autotuned(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, i
 	const double work = (double)ncols * (double)N * (double)(c.ngates + t.ngates);
 	// host-callback targets are not tuned: the sample runs would call the caller's ufunc
 	if (!rt.autotune || rt.tuning || c.L < 4 || work < TUNE_MIN_WORK || t.ufunc ||
-	    (rt.pin_gpp && rt.pin_chunk && rt.pin_recon)) {
-		rt.last_choice = {rt.gates_per_pass, rt.column_chunk, rt.recon_c128, 0.0, 0};
+	    (rt.pin_gpp && rt.pin_chunk && rt.pin_recon && rt.pin_ffma)) {
+		rt.last_choice = {rt.gates_per_pass, rt.column_chunk, rt.recon_c128, rt.c64_ffma, 0.0, 0};
 		return evaluate_configured(rt, c, t, mode, precision, d_out);
 	}
-	const std::array<long, 10> key = {c.L, c.ngates, t.ngates, precision, mode, t.ufunc ? 1 : 0, rt.real_pairs,
+	const std::array<long, 11> key = {c.L, c.ngates, t.ngates, precision, mode, t.ufunc ? 1 : 0, rt.real_pairs,
 	                                  rt.pin_gpp ? rt.gates_per_pass : 0, rt.pin_chunk ? rt.column_chunk : -1,
-	                                  rt.pin_recon ? rt.recon_c128 : -1};
+	                                  rt.pin_recon ? rt.recon_c128 : -1, rt.pin_ffma ? rt.c64_ffma : -1};
 	const Saved saved(rt);
 	auto it = rt.tune_cache.find(key);
 	if (it == rt.tune_cache.end()) {
@@ -109,7 +113,7 @@ int evaluate_autotuned(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, i
 		const int64_t ns = std::max<int64_t>(1, e - b);
 		rt.tuning = true;
 		int err = 0;
-		Config best = {saved.gpp, saved.chunk, saved.recon};
+		Config best = {saved.gpp, saved.chunk, saved.recon, saved.ffma};
 		double best_ms = time_config(rt, best, c, t, mode, precision, d_out, b, e, &err);
 		auto consider = [&](const Config& k) {
 			if (err) return;
@@ -120,22 +124,27 @@ int evaluate_autotuned(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, i
 		const Config base = best;
 		if (!rt.pin_gpp)
 			for (int g = 1; g <= 4; g++)
-				if (g != base.gpp) consider({g, base.chunk, base.recon});
+				if (g != base.gpp) consider({g, base.chunk, base.recon, base.ffma});
 		// columns per chunk (0: as many as the workspace holds)
 		const Config after_gpp = best;
 		if (!rt.pin_chunk)
 			for (long ch : {0L, 2048L, 512L})
-				if (ch != after_gpp.chunk && (ch == 0 || ch < ns)) consider({after_gpp.gpp, ch, after_gpp.recon});
+				if (ch != after_gpp.chunk && (ch == 0 || ch < ns))
+					consider({after_gpp.gpp, ch, after_gpp.recon, after_gpp.ffma});
 		// reverse variant (complex128 fused passes of HVP / gradient evaluations)
 		if (!rt.pin_recon && precision == PREC_C128 && best.gpp > 1 && mode != EVAL_F)
-			consider({best.gpp, best.chunk, 1 - best.recon});
+			consider({best.gpp, best.chunk, 1 - best.recon, best.ffma});
+		// complex64 passes on the FP32 pipe or the TF32 MMA
+		if (!rt.pin_ffma && precision != PREC_C128 && best.gpp > 1)
+			consider({best.gpp, best.chunk, best.recon, 1 - best.ffma});
 		rt.tuning = false;
 		saved.restore(rt);
 		if (err) return err;
-		it = rt.tune_cache.emplace(key, Runtime::TuneChoice{best.gpp, best.chunk, best.recon, best_ms / (double)ns, 1}).first;
+		it = rt.tune_cache.emplace(key, Runtime::TuneChoice{best.gpp, best.chunk, best.recon, best.ffma, best_ms / (double)ns, 1})
+		         .first;
 	}
 	const Runtime::TuneChoice& ch = it->second;
-	apply(rt, {ch.gates_per_pass, ch.column_chunk, ch.recon});
+	apply(rt, {ch.gates_per_pass, ch.column_chunk, ch.recon, ch.ffma});
 	rt.last_choice = ch;
 	const int ret = evaluate_configured(rt, c, t, mode, precision, d_out);
 	saved.restore(rt);

@@ -1853,6 +1853,348 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 	}
 }
 
+// ------------------------------------------------------------------------------ complex64 passes on the FP32 pipe
+
+// The complex64 passes in FP32 FMAs.  Four threads share an amplitude group: thread
+// q = lane & 3 computes component q of every product and owns row q of the outer sums,
+// column cc = (lane >> 2) & 7 of the tile; a warp handles one group base (eight columns)
+// per step, so every operand load is one 64-byte row read by four threads at once and
+// every gate coefficient a thread needs (row or column q of G, Z, W: 12 complex numbers)
+// stays in registers for the whole gate.  No operand splitting, no fragment exchange:
+// 4 x 4 complex products at the FP32 FMA rate (about 2x the FP64 rate on B200).
+// Tiles are the k5 tiles (256 rows x 8 columns, rows swizzled by prow so the four rows a
+// warp stores land in both halves of the bank window).
+constexpr int NT7 = 256;
+constexpr int CPT7 = (1 << MAXNB) * 4 / NT7;   // 16-byte chunks per thread and state (two columns each)
+
+__device__ __forceinline__ float2 c7fma(float2 a, float2 b, float2 c)   // a * b + c
+{
+	return make_float2(fmaf(a.x, b.x, fmaf(-a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(a.y, b.x, c.y)));
+}
+__device__ __forceinline__ float2 c7fma_conj(float2 a, float2 b, float2 c)   // conj(a) * b + c
+{
+	return make_float2(fmaf(a.x, b.x, fmaf(a.y, b.y, c.x)), fmaf(a.x, b.y, fmaf(-a.y, b.x, c.y)));
+}
+
+inline size_t k7_fwd_smem() { return 32 * MAXK * sizeof(float2) + 2 * (size_t)AMAX4 * sizeof(float2); }
+inline size_t k7_rev_smem()
+{
+	return 48 * MAXK * sizeof(float2) + 4 * (size_t)AMAX4 * sizeof(float2) + (size_t)(NT7 / 32) * MAXK * 4 * 16 * sizeof(double);
+}
+
+// Forward pass (complex64, FP32 FMAs).  Same contract as k4_fwd: IN 0 reads psi/dpsi, 1
+// starts from basis columns; OUT 0 stores psi/dpsi, 1 stores -conj(psi), 2 adds f = <phi, psi>
+// without storing, 3 stores and adds f.
+template <bool TAN, int IN, int OUT>
+__global__ void __launch_bounds__(NT7, 3) k7_fwd(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+                                                 float2* __restrict__ psi_o, float2* __restrict__ dpsi_o,
+                                                 const float2* __restrict__ phi, PassGeom pg, PassGates<float> gates,
+                                                 double2* __restrict__ fpart)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, K = pg.K;
+	float2* sg = reinterpret_cast<float2*>(smem_raw);   // [MAXK][32]: G, Z
+	float2* S = sg + 32 * MAXK;
+	float2* dS = S + AMAX4;
+	for (int e = threadIdx.x; e < 32 * MAXK; e += blockDim.x) {
+		const int k = e / 32, w = e % 32;
+		sg[e] = k >= K ? make_float2(0.f, 0.f) : (w < 16 ? gates.g[k].m[w] : (TAN ? gates.z[k].m[w - 16] : make_float2(0.f, 0.f)));
+	}
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	const int q = lane & 3, cc = (lane >> 2) & 7;
+	int ro[CPT7];
+#pragma unroll
+	for (int i = 0; i < CPT7; i++) {
+		const int r = (threadIdx.x + i * NT7) >> 2;
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		ro[i] = o;
+	}
+	double fx = 0, fy = 0;
+	__syncthreads();
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cgp * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT7; i++) {
+			const int e = threadIdx.x + i * NT7;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int pe = prow(r) * CW4 + c2i;
+			if (IN == 0) {
+				const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+				cp_async16(S + pe, psi + a);
+				if (TAN) cp_async16(dS + pe, dpsi + a);
+			} else {
+				const int64_t row = rowbase + ro[i], col = colbase + c2i;
+				*reinterpret_cast<float4*>(S + pe) =
+				    make_float4(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col), basis_re(row, pg.b0 + col + 1),
+				                basis_im(row, pg.b0 + col + 1));
+				if (TAN) *reinterpret_cast<float4*>(dS + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+			}
+		}
+		if (IN == 0) {
+			cp_async_commit();
+			cp_async_wait_all();
+		}
+		__syncthreads();
+#pragma unroll 1
+		for (int k = 0; k < K; k++) {
+			float2 g[4], z[4];
+#pragma unroll
+			for (int m = 0; m < 4; m++) {
+				g[m] = sg[32 * k + 4 * q + m];              // row q of G
+				z[m] = TAN ? sg[32 * k + 16 + 4 * q + m] : make_float2(0.f, 0.f);   // row q of Z
+			}
+			const bool dzero = IN == 1 && k == 0;
+			const int bi = pg.gi[k], bj = pg.gj[k];
+			for (int b6 = warp; b6 < R / 4; b6 += nwarps) {
+				int rows[4];
+				group_rows(b6, bi, bj, rows);
+				float2 x[4], dx[4];
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					x[m] = S[prow(rows[m]) * CW4 + cc];
+					dx[m] = (TAN && !dzero) ? dS[prow(rows[m]) * CW4 + cc] : make_float2(0.f, 0.f);
+				}
+				float2 y = make_float2(0.f, 0.f), dy = make_float2(0.f, 0.f);
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					y = c7fma(g[m], x[m], y);
+					if (TAN) {
+						dy = c7fma(z[m], x[m], dy);
+						if (!dzero) dy = c7fma(g[m], dx[m], dy);
+					}
+				}
+				__syncwarp();
+				const int st = prow(sel4_int(rows, q)) * CW4 + cc;
+				S[st] = y;
+				if (TAN) dS[st] = dy;
+			}
+			__syncthreads();
+		}
+#pragma unroll
+		for (int i = 0; i < CPT7; i++) {
+			const int e = threadIdx.x + i * NT7;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			const float4 v = *reinterpret_cast<const float4*>(S + pe);
+			if (OUT == 2 || OUT == 3) {
+				const float4 p = *reinterpret_cast<const float4*>(phi + a);
+				fx += (double)p.x * v.x - (double)p.y * v.y + (double)p.z * v.z - (double)p.w * v.w;
+				fy += (double)p.x * v.y + (double)p.y * v.x + (double)p.z * v.w + (double)p.w * v.z;
+			}
+			if (OUT == 1) {
+				*reinterpret_cast<float4*>(psi_o + a) = make_float4(-v.x, v.y, -v.z, v.w);
+			} else if (OUT != 2) {
+				*reinterpret_cast<float4*>(psi_o + a) = v;
+				if (TAN) *reinterpret_cast<float4*>(dpsi_o + a) = *reinterpret_cast<const float4*>(dS + pe);
+			}
+		}
+		__syncthreads();
+	}
+	if (OUT == 2 || OUT == 3) {
+		__shared__ double red[2][NT7 / 32];
+		fx = warp_sum(fx);
+		fy = warp_sum(fy);
+		if (lane == 0) { red[0][warp] = fx; red[1][warp] = fy; }
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			double sx = 0, sy = 0;
+			for (int w = 0; w < nwarps; w++) { sx += red[0][w]; sy += red[1][w]; }
+			fpart[blockIdx.x].x += sx;
+			fpart[blockIdx.x].y += sy;
+		}
+	}
+}
+
+// Reverse pass (complex64, FP32 FMAs) for unitary gates: from the state at the pass
+// OUTPUT it rebuilds the state entering each gate with the adjoint gate (as k5_rev),
+//   psi_k = G^+ psi_{k+1},  dpsi_k = G^+ dpsi_{k+1} - W psi_{k+1},  W = G^+ Z G^+,
+// adds the outer sums dG_k += phi (x) psi_k, HZ_k += phi (x) dpsi_k + dphi (x) psi_k and
+// moves phi, dphi through gate k, all in place in four tiles.  Per gate and tile the
+// FP32 sums of a thread (eight group-columns) are reduced over the warp and added to
+// FP64 per-warp sums in shared memory; partials leave in the k2 layout
+// (part + k * nblk * 64 + blockIdx.x * 64: [0, 32) dG, [32, 64) HZ, re/im interleaved).
+template <bool TAN, bool FIRST, bool LAST>
+__global__ void __launch_bounds__(NT7, 2) k7_rev(const float2* __restrict__ psi, const float2* __restrict__ dpsi,
+                                                 const float2* __restrict__ phi, const float2* __restrict__ dphi,
+                                                 float2* __restrict__ phi_o, float2* __restrict__ dphi_o, PassGeom pg,
+                                                 PassGates<float> gates, PassW<float> wg, double* __restrict__ part,
+                                                 int nblk)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const int R = 1 << pg.NB, K = pg.K;
+	float2* sg = reinterpret_cast<float2*>(smem_raw);   // [MAXK][48]: G, Z, W
+	float2* Psi = sg + 48 * MAXK;
+	float2* Phi = Psi + AMAX4;
+	float2* dPsi = Phi + AMAX4;
+	float2* dPhi = dPsi + AMAX4;
+	double* accw = reinterpret_cast<double*>(dPhi + AMAX4);   // [warp][MAXK][4 rows][16]
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+	for (int e = threadIdx.x; e < 48 * MAXK; e += blockDim.x) {
+		const int k = e / 48, w = e % 48;
+		float2 v = make_float2(0.f, 0.f);
+		if (k < K) {
+			if (w < 16) v = gates.g[k].m[w];
+			else if (TAN && w < 32) v = gates.z[k].m[w - 16];
+			else if (TAN && w >= 32) v = wg.w[k].m[w - 32];
+		}
+		sg[e] = v;
+	}
+	for (int e = threadIdx.x; e < nwarps * MAXK * 64; e += blockDim.x) accw[e] = 0;
+	const int q = lane & 3, cc = (lane >> 2) & 7;
+	int ro[CPT7];
+#pragma unroll
+	for (int i = 0; i < CPT7; i++) {
+		const int r = (threadIdx.x + i * NT7) >> 2;
+		int o = 0;
+		for (int b = 0; b < pg.NB; b++)
+			if ((r >> b) & 1) o |= 1 << pg.tbit[b];
+		ro[i] = o;
+	}
+	__syncthreads();
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
+		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cgp * CW4;
+#pragma unroll
+		for (int i = 0; i < CPT7; i++) {
+			const int e = threadIdx.x + i * NT7;
+			if (e >= 4 * R) continue;
+			const int r = e >> 2, c2i = 2 * (e & 3);
+			const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+			const int pe = prow(r) * CW4 + c2i;
+			cp_async16(Psi + pe, psi + a);
+			cp_async16(Phi + pe, phi + a);
+			if (TAN) {
+				cp_async16(dPsi + pe, dpsi + a);
+				if (FIRST) *reinterpret_cast<float4*>(dPhi + pe) = make_float4(0.f, 0.f, 0.f, 0.f);
+				else cp_async16(dPhi + pe, dphi + a);
+			}
+		}
+		cp_async_commit();
+		cp_async_wait_all();
+		__syncthreads();
+#pragma unroll 1
+		for (int k = K - 1; k >= 0; k--) {
+			const bool first_gate = FIRST && k == K - 1;
+			const bool last_gate = LAST && k == 0;
+			float2 gcol[4], zcol[4], wrow[4];
+#pragma unroll
+			for (int m = 0; m < 4; m++) {
+				gcol[m] = sg[48 * k + 4 * m + q];                                        // G[m][q]
+				zcol[m] = TAN ? sg[48 * k + 16 + 4 * m + q] : make_float2(0.f, 0.f);     // Z[m][q]
+				wrow[m] = TAN ? sg[48 * k + 32 + 4 * q + m] : make_float2(0.f, 0.f);     // W[q][m]
+			}
+			float2 ag[4], ah[4];   // row q of this gate's sums: dG[q][c], HZ[q][c]
+#pragma unroll
+			for (int c = 0; c < 4; c++) { ag[c] = make_float2(0.f, 0.f); ah[c] = make_float2(0.f, 0.f); }
+			const int bi = pg.gi[k], bj = pg.gj[k];
+			for (int b6 = warp; b6 < R / 4; b6 += nwarps) {
+				int rows[4], pr[4];
+				group_rows(b6, bi, bj, rows);
+#pragma unroll
+				for (int m = 0; m < 4; m++) pr[m] = prow(rows[m]) * CW4 + cc;
+				float2 x[4], dx[4], p[4], dp[4];
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					x[m] = Psi[pr[m]];
+					dx[m] = (TAN && !last_gate) ? dPsi[pr[m]] : make_float2(0.f, 0.f);
+					p[m] = Phi[pr[m]];
+					dp[m] = (TAN && !first_gate) ? dPhi[pr[m]] : make_float2(0.f, 0.f);
+				}
+				// 1. psi_k (and dpsi_k), component q, in place
+				float2 y = make_float2(0.f, 0.f), dy = make_float2(0.f, 0.f);
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					y = c7fma_conj(gcol[m], x[m], y);
+					if (TAN && !last_gate) {
+						dy = c7fma_conj(gcol[m], dx[m], dy);
+						dy = c7fma(make_float2(-wrow[m].x, -wrow[m].y), x[m], dy);
+					}
+				}
+				__syncwarp();
+				Psi[pr[q]] = y;
+				if (TAN && !last_gate) dPsi[pr[q]] = dy;
+				__syncwarp();
+				// 2. row q of the outer sums with the rebuilt psi_k, dpsi_k
+				const float2 pq = p[q], dpq = dp[q];
+#pragma unroll
+				for (int c = 0; c < 4; c++) {
+					const float2 xc = Psi[pr[c]];
+					ag[c] = c7fma(pq, xc, ag[c]);
+					if (TAN) {
+						if (!last_gate) ah[c] = c7fma(pq, dPsi[pr[c]], ah[c]);
+						if (!first_gate) ah[c] = c7fma(dpq, xc, ah[c]);
+					}
+				}
+				if (last_gate) continue;
+				// 3. phi' = G^T phi, dphi' = G^T dphi + Z^T phi (component q, in place; every lane
+				//    read phi before the __syncwarp above)
+				float2 u = make_float2(0.f, 0.f), du = make_float2(0.f, 0.f);
+#pragma unroll
+				for (int m = 0; m < 4; m++) {
+					u = c7fma(gcol[m], p[m], u);
+					if (TAN) {
+						du = c7fma(zcol[m], p[m], du);
+						if (!first_gate) du = c7fma(gcol[m], dp[m], du);
+					}
+				}
+				Phi[pr[q]] = u;
+				if (TAN) dPhi[pr[q]] = du;
+			}
+			// sums over the eight columns of the warp (lanes with the same q), then into FP64
+			float v[16];
+#pragma unroll
+			for (int c = 0; c < 4; c++) {
+				v[2 * c] = ag[c].x;
+				v[2 * c + 1] = ag[c].y;
+				v[8 + 2 * c] = ah[c].x;
+				v[8 + 2 * c + 1] = ah[c].y;
+			}
+#pragma unroll
+			for (int t = 0; t < 16; t++) {
+				if (!TAN && t >= 8) break;
+				float x = v[t];
+				x += __shfl_xor_sync(0xffffffffu, x, 4);
+				x += __shfl_xor_sync(0xffffffffu, x, 8);
+				x += __shfl_xor_sync(0xffffffffu, x, 16);
+				v[t] = x;
+			}
+			if (lane < 4) {
+				double* a = accw + ((size_t)(warp * MAXK + k) * 4 + q) * 16;
+#pragma unroll
+				for (int t = 0; t < 16; t++) a[t] += (double)v[t];
+			}
+			__syncthreads();
+		}
+		if (!LAST) {
+#pragma unroll
+			for (int i = 0; i < CPT7; i++) {
+				const int e = threadIdx.x + i * NT7;
+				if (e >= 4 * R) continue;
+				const int r = e >> 2, c2i = 2 * (e & 3);
+				const int64_t a = (rowbase + ro[i]) * pg.C + colbase + c2i;
+				const int pe = prow(r) * CW4 + c2i;
+				*reinterpret_cast<float4*>(phi_o + a) = *reinterpret_cast<const float4*>(Phi + pe);
+				if (TAN) *reinterpret_cast<float4*>(dphi_o + a) = *reinterpret_cast<const float4*>(dPhi + pe);
+			}
+		}
+		__syncthreads();
+	}
+	// block sums in the k2 layout: t < 32 dG (row t / 8, entry (t % 8) / 2, re/im t % 2), t >= 32 HZ
+	for (int idx = threadIdx.x; idx < K * NPART2; idx += blockDim.x) {
+		const int k = idx / NPART2, t = idx % NPART2;
+		const int qq = (t & 31) >> 3, slot = (t >= 32 ? 8 : 0) + (t & 7);
+		double sum = 0;
+		for (int w = 0; w < nwarps; w++) sum += accw[((size_t)(w * MAXK + k) * 4 + qq) * 16 + slot];
+		part[(size_t)k * nblk * NPART2 + (size_t)blockIdx.x * NPART2 + t] += sum;
+	}
+}
+
 // Sum the complex64 engine's raw partials over blocks and fold them into complex dG, HZ.
 // Lane (g, t) of an outer-sum MMA holds C[g][2t..2t+1] (v 0,1) and C[g+8][2t..2t+1]
 // (v 2,3): dG raw R[g][2t+i] = v_i, HZ raw R[g][2t+i] = v_{2+i}.
@@ -2072,6 +2414,15 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 		}
 		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
 		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
+	} else if (rt.c64_ffma) {
+		static int per_sm7 = 0;
+		if (!per_sm7) {
+			int ret = prepare(k7_fwd<TAN, IN, OUT>, k7_fwd_smem(), &per_sm7, NT7);
+			if (ret) return ret;
+		}
+		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm7));
+		RQC_LAUNCH3(rt, KC_FUSED, (k7_fwd<TAN, IN, OUT>), grid, NT7, k7_fwd_smem(), psi, dpsi, psi_o, dpsi_o, phi, pg, gates,
+		            fpart);
 	} else {
 		if (!per_sm) {
 			int ret = prepare(k4_fwd<TAN, IN, OUT>, k4_fwd_smem(MAXNB, TAN, OUT >= 2), &per_sm, NT4F);
@@ -2194,6 +2545,46 @@ int rev_grid6(Runtime& rt, bool tan)
 	int per_sm = 1;
 	const int ret = tan ? prepare(k6_rev<true, false, false>, k6_rev_smem(true), &per_sm, NT6)
 	                    : prepare(k6_rev<false, false, false>, k6_rev_smem(false), &per_sm, NT6);
+	if (ret) per_sm = 1;
+	return rt.num_sms * per_sm;
+}
+
+template <bool TAN, bool FIRST, bool LAST>
+int launch_rev7(Runtime& rt, const float2* psi, const float2* dpsi, const float2* phi, const float2* dphi, float2* phi_o,
+                float2* dphi_o, const PassGeom& pg, const PassGates<float>& gates, const PassW<float>& wg, double* part,
+                int nblk)
+{
+	static bool ready = false;
+	if (!ready) {
+		int per_sm;
+		int ret = prepare(k7_rev<TAN, FIRST, LAST>, k7_rev_smem(), &per_sm, NT7);
+		if (ret) return ret;
+		ready = true;
+	}
+	RQC_LAUNCH3(rt, KC_REVERSE, (k7_rev<TAN, FIRST, LAST>), nblk, NT7, k7_rev_smem(), psi, dpsi, phi, dphi, phi_o, dphi_o,
+	            pg, gates, wg, part, nblk);
+	return OK;
+}
+
+template <bool TAN>
+int launch_rev7_any(Runtime& rt, bool first, bool last, const float2* psi, const float2* dpsi, const float2* phi,
+                    const float2* dphi, float2* phi_o, float2* dphi_o, const PassGeom& pg, const PassGates<float>& gates,
+                    const PassW<float>& wg, double* part, int nblk)
+{
+	if (first && last)
+		return launch_rev7<TAN, true, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk);
+	if (first)
+		return launch_rev7<TAN, true, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk);
+	if (last)
+		return launch_rev7<TAN, false, true>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk);
+	return launch_rev7<TAN, false, false>(rt, psi, dpsi, phi, dphi, phi_o, dphi_o, pg, gates, wg, part, nblk);
+}
+
+int rev_grid7(Runtime& rt, bool tan)
+{
+	int per_sm = 1;
+	const int ret = tan ? prepare(k7_rev<true, false, false>, k7_rev_smem(), &per_sm, NT7)
+	                    : prepare(k7_rev<false, false, false>, k7_rev_smem(), &per_sm, NT7);
 	if (ret) per_sm = 1;
 	return rt.num_sms * per_sm;
 }
@@ -2372,11 +2763,13 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 	auto ck_at = [&](int p) { return ck + (int64_t)(p - 1) * C * N; };
 	auto dck_at = [&](int p) { return dck + (int64_t)(p - 1) * C * N; };
 
-	const int nblk = recon ? (std::is_same<T, double>::value ? rev_grid6(rt, tan) : rev_grid5(rt, tan))
+	// complex64 reverse passes on the FP32 pipe (k7_rev) or on the TF32 MMA (k5_rev)
+	const bool ffma = !std::is_same<T, double>::value && recon && rt.c64_ffma;
+	const int nblk = recon ? (std::is_same<T, double>::value ? rev_grid6(rt, tan) : (ffma ? rev_grid7(rt, tan) : rev_grid5(rt, tan)))
 	                       : rev_grid<T>(rt, tan);
 	// blocks of the forward launches that sum f (one FP64 partial each)
 	const int nfb = std::is_same<T, double>::value ? nblk : 2 * rt.num_sms;
-	const int nps = std::is_same<T, double>::value ? NPART3 : NRAW4;   // partial doubles per gate and block
+	const int nps = std::is_same<T, double>::value ? NPART3 : (ffma ? NPART2 : NRAW4);   // partial doubles per gate and block
 	const size_t part_doubles = (size_t)G * nblk * nps + 2 * (size_t)nfb;
 	if ((ret = ensure_device(rt.partials, part_doubles * sizeof(double)))) return ret;
 	double* part = reinterpret_cast<double*>(rt.partials.ptr);
@@ -2508,6 +2901,17 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 				}
 			}
 			if constexpr (!std::is_same<T, double>::value) {
+				if (ffma) {
+					if (tan)
+						ret = launch_rev7_any<true>(rt, first, last, ck_at(p + 1), dck_at(p + 1), ph, dph,
+						                            last ? nullptr : Pb[nxt], last ? nullptr : Db[nxt], g, pgates[p], pw[p],
+						                            pp, nblk);
+					else
+						ret = launch_rev7_any<false>(rt, first, last, ck_at(p + 1), nullptr, ph, nullptr,
+						                             last ? nullptr : Pb[nxt], nullptr, g, pgates[p], PassW<float>{}, pp, nblk);
+					if (ret) return ret;
+					continue;
+				}
 				if (recon) {
 					if (tan)
 						ret = launch_rev5_any<true>(rt, first, last, ck_at(p + 1), dck_at(p + 1), ph, dph,
@@ -2534,6 +2938,8 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 
 	if (std::is_same<T, double>::value)
 		k3_reduce<<<G + 1, NPART3, 0, rt.stream>>>(part, G, nblk, fpart, nfb, tan ? 1 : 0, d_out);
+	else if (ffma)
+		k2_reduce<<<G + 1, NPART2, 0, rt.stream>>>(part, G, nblk, fpart, nfb, tan ? 1 : 0, d_out);
 	else
 		k4_reduce<<<G + 1, NRAW4, 0, rt.stream>>>(part, G, nblk, fpart, nfb, tan ? 1 : 0, d_out);
 	rt.launches++;

@@ -52,15 +52,16 @@ struct Runtime
 	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
 	int recon_c128 = 1;       // complex128 reverse passes rebuild states with adjoint gates (unitary gates)
+	int c64_ffma = 1;         // complex64 fused passes on the FP32 pipe (k7) rather than the TF32 MMA (k4 / k5)
 
 	// autotuning of the basis-column engine (autotune.cu): the configuration chosen per
 	// problem shape, and the one the last evaluation ran with
-	struct TuneChoice { int gates_per_pass; long column_chunk; int recon; double ms_per_column; int tuned; };
+	struct TuneChoice { int gates_per_pass; long column_chunk; int recon; int ffma; double ms_per_column; int tuned; };
 	int autotune = 1;
 	bool tuning = false;
-	bool pin_gpp = false, pin_chunk = false, pin_recon = false;   // set explicitly by the caller
-	std::map<std::array<long, 10>, TuneChoice> tune_cache;
-	TuneChoice last_choice = {0, 0, 0, 0.0, 0};
+	bool pin_gpp = false, pin_chunk = false, pin_recon = false, pin_ffma = false;   // set explicitly by the caller
+	std::map<std::array<long, 11>, TuneChoice> tune_cache;
+	TuneChoice last_choice = {0, 0, 0, 0, 0.0, 0};
 
 	// instrumentation
 	unsigned long long launches = 0;

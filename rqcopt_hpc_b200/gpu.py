@@ -119,7 +119,8 @@ _SIGS = {
     "rqcopt_gpu_set_column_range": (I, [C.c_long, C.c_long]),
     "rqcopt_gpu_set_reconstruct": (None, [I]),
     "rqcopt_gpu_set_autotune": (I, [I]),
-    "rqcopt_gpu_last_config": (I, [VP, VP, VP, VP]),
+    "rqcopt_gpu_last_config": (I, [VP, VP, VP, VP, VP]),
+    "rqcopt_gpu_set_c64_fp32_pipe": (None, [I]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
@@ -868,13 +869,18 @@ def set_autotune(on: bool):
 def last_config():
     """Configuration of the last target evaluation: gates per pass, column chunk (0: from
     the workspace), reconstruction, sample ms per column and whether the autotuner chose it."""
-    g, r = C.c_int(), C.c_int()
+    g, r, f = C.c_int(), C.c_int(), C.c_int()
     ch, ms = C.c_long(), C.c_double()
-    tuned = lib().rqcopt_gpu_last_config(C.byref(g), C.byref(ch), C.byref(r), C.byref(ms))
+    tuned = lib().rqcopt_gpu_last_config(C.byref(g), C.byref(ch), C.byref(r), C.byref(f), C.byref(ms))
     if tuned < 0:
         raise RqcError("rqcopt_gpu_last_config", tuned)
     return {"gates_per_pass": g.value, "column_chunk": ch.value, "reconstruct": bool(r.value),
-            "ms_per_column": ms.value, "tuned": bool(tuned)}
+            "c64_fp32_pipe": bool(f.value), "ms_per_column": ms.value, "tuned": bool(tuned)}
+
+
+def set_c64_fp32_pipe(on: bool):
+    """complex64 fused passes in FP32 FMAs (True) or on the TF32 MMA (False)."""
+    lib().rqcopt_gpu_set_c64_fp32_pipe(1 if on else 0)
 
 
 def set_reconstruct(on: bool):

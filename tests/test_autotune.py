@@ -48,6 +48,7 @@ def test_every_candidate_gives_the_tuned_result(gpu, oracle, precision, tol):
         gpu.set_gates_per_pass(gpp)
         gpu.set_column_chunk(chunk)
         gpu.set_reconstruct(rc)
+        gpu.set_c64_fp32_pipe(True)
         f, g, h = gpu.brickwall_unitary_target_projected_hessian_vector_product(tgt, vlist, vdirs, perms, L)
         used = gpu.last_config()
         assert not used["tuned"] and used["gates_per_pass"] == gpp and used["column_chunk"] == chunk

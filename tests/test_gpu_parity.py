@@ -226,6 +226,34 @@ def test_reconstructing_reverse_pass_matches_recomputing(gpu, oracle, L, depth, 
         assert rel_err(g1, go) <= 1e-12 and rel_err(h1, ho) <= 1e-12
 
 
+@pytest.mark.parametrize("L,depth,chunk", [(8, 5, 0), (10, 7, 40), (12, 3, 0)])
+def test_complex64_fp32_pipe_matches_tf32_mma(gpu, oracle, L, depth, chunk):
+    """complex64 fused passes on the FP32 pipe (four threads per amplitude group) and on
+    the TF32 MMA (three-term split): f, gradient and HVP (and f / gradient evaluations)
+    agree with each other and with the oracle within the complex64 bar 1e-5; ragged chunks."""
+    vlist, perms, tvlist, tperms = brickwall_instance(L, depth, 50 + L, 3, 51 + L)
+    vdirs = _dirs(vlist, 52 + L)
+    tgt = gpu.Target(brickwall=(tvlist, tperms))
+    gpu.set_precision(gpu.PRECISION_C64)
+    gpu.set_column_chunk(chunk)
+    try:
+        res = {}
+        for on in (True, False):
+            gpu.set_c64_fp32_pipe(on)
+            res[on] = (gpu.brickwall_unitary_target_projected_hessian_vector_product(tgt, vlist, vdirs, perms, L),
+                       gpu.brickwall_unitary_target_and_projected_gradient(tgt, vlist, perms, L),
+                       gpu.brickwall_unitary_target(tgt, vlist, perms, L))
+            assert gpu.last_config()["c64_fp32_pipe"] == on
+    finally:
+        gpu.set_autotune(True)
+    fo, go, ho = oracle.brickwall_unitary_target_projected_hessian_vector_product(
+        oracle.target("brickwall", (tvlist, tperms)), vlist, vdirs, perms, L)
+    for on in (True, False):
+        (f, g, h), (fg, gg), ff = res[on]
+        assert abs(f - fo) <= 1e-5 * abs(fo) and abs(fg - fo) <= 1e-5 * abs(fo) and abs(ff - fo) <= 1e-5 * abs(fo)
+        assert rel_err(g, go) <= 1e-5 and rel_err(h, ho) <= 1e-5 and rel_err(gg, go) <= 1e-5
+
+
 def test_forward_adjoint_round_trip(gpu):
     """Forward through 64 random Haar gates on random distinct pairs, then the adjoint
     gates in reverse order, recovers the input state (L = 20, complex128)."""
