@@ -633,17 +633,22 @@ def real_build_path(gpu, steps=3, L=14, depth=9, tdepth=5, seconds=8.0, with_ref
     except (OSError, ValueError):
         pass
     hbm_peak = peaks.get("hbm_gbs", 6650.0)
-    rbytes = float(6 * rev_n - 5) * N * (N // 2) * 16   # rev_n passes over N/2 paired columns
+    cfg = gpu.last_config()
+    G = depth * (L // 2)
+    npass = G if cfg["gates_per_pass"] == 1 else -(-G // cfg["gates_per_pass"])
+    rbytes = float(6 * npass - 5) * N * (N // 2) * 16   # npass reverse passes per column over N/2 paired columns
     achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
     out = {"workload": f"real build: f + projected gradient (6 per gate) + projected HVP, real orthogonal brickwall "
                        f"L={L} depth {depth} vs real brickwall target depth {tdepth}, all {N} basis columns as "
                        f"{N // 2} paired columns, complex128 engine", "evals_per_s_e2e": 1.0 / wall,
            "ms_per_eval": wall * 1e3, "gpu_launches": launches, "f": float(f),
-           "roofline": {"kernel": "k3_rev (complex128 FP64-MMA gradient/HVP pass)", "bound": "hbm",
+           "roofline": {"kernel": ("k6_rev" if cfg["reconstruct"] else "k3_rev") + " (complex128 FP64-MMA "
+                                  "gradient/HVP pass)", "bound": "hbm",
                         "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                         "frac": achieved / hbm_peak if achieved else None,
                         "bytes_model": "(6P-5) x 2^L x 2^(L-1) x 16 B per evaluation (P reverse passes over the "
-                                       "paired columns)", "passes": rev_n, "reverse_ms": rev_ms,
+                                       "paired columns)", "passes_per_column": npass, "launches": rev_n,
+                        "reverse_ms": rev_ms,
                         "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks
                         else "fallback 6650 GB/s"}}
     from oracle.oracle import RealReference
@@ -704,7 +709,7 @@ def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50, with_reference=
     return out
 
 
-def batched_c4(gpu, torch, count=512, niter=30, sample_every=8):
+def batched_c4(gpu, torch, count=512, niter=30, sample_every=16):
     """C4: 512 independent brickwall instances (even L uniform over 6..12, depth over
     {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), 30 trust-region iterations each.
     The batched mixed-precision path (complex64 passes with FP64 sums, complex128 f,
@@ -769,25 +774,28 @@ def batched_c4(gpu, torch, count=512, niter=30, sample_every=8):
     return out
 
 
-def serving_c5(gpu, rate=200.0, duration=60.0, wall=60.0, niter=100, grad_tol=1e-8, sizes=(8, 10, 12, 14),
-               precisions=("mixed", "plain_c128")):
+def serving_c5(gpu, rate=200.0, duration=60.0, wall=70.0, niter=100, grad_tol=1e-8, sizes=(8, 10, 12, 14),
+               capacity=128, precisions=("mixed", "plain_c128")):
     """C5: Poisson arrivals (seed 40) of brickwall optimisation requests (even L in 8..14,
     P(L) ~ 2^(-(L-8)/2), depth in {3,5,7,9}, target depth 3), each stopping at gradient
-    norm grad_tol or after niter iterations, admitted into a running batch within a
-    150 GB device budget, for the mixed-precision and the plain complex128 path in turn.
-    Each run offers `duration` seconds of arrivals and is measured for `wall` seconds:
-    p50 / p99 time from arrival to completion of the requests completed in that window,
-    completions per second, and the requests still running or queued at its end (at 200
-    req/s the offered load exceeds one GPU, so latencies are queue-dominated)."""
+    norm grad_tol or after niter iterations, admitted first come first served into a
+    running batch of at most `capacity` requests within a 150 GB device budget, for the
+    mixed-precision and the plain complex128 path in turn.  Each run offers `duration`
+    seconds of arrivals and is measured for `wall` seconds: p50 / p99 time from arrival to
+    completion of the requests completed in that window, completions per second, and the
+    requests still running or queued at its end (at 200 req/s the offered load exceeds one
+    GPU, so these latencies are queue-dominated)."""
     from rqcopt_hpc_b200 import batch, serving
     code = {"mixed": gpu.PRECISION_MIXED, "plain_c128": gpu.PRECISION_C128}
     out = {"workload": f"Poisson {rate:g} req/s for {duration:g} s (seed 40), L in {set(sizes)}, stop at gradient "
-                       f"norm {grad_tol:g} or {niter} iterations, 150 GB admission budget, measured for {wall:g} s"}
+                       f"norm {grad_tol:g} or {niter} iterations, at most {capacity} requests in the running batch, "
+                       f"150 GB admission budget, measured for {wall:g} s"}
     for name in precisions:
         reqs = serving.c5_requests(rate=rate, duration=duration, niter=niter, grad_tol=grad_tol,
                                    precision=code[name], sizes=sizes)
-        b = batch.Batch(capacity=4096, max_iterations=niter, sharing=True)
-        srv = serving.Server(b, capacity=4096, hbm_budget_bytes=150e9, footprint=batch.footprint, rounds_per_step=4)
+        b = batch.Batch(capacity=capacity, max_iterations=niter, sharing=True)
+        srv = serving.Server(b, capacity=capacity, hbm_budget_bytes=150e9, footprint=batch.footprint,
+                             rounds_per_step=4)
         t0 = time.perf_counter()
         done, left = serving.run_arrivals(srv, reqs, wall_limit=wall)
         el = time.perf_counter() - t0
@@ -827,20 +835,25 @@ def compare_mixed(gpu, torch, stream, step, res_c128, steps, L, G, Gt, P, hbm_pe
     e1.record(stream)
     torch.cuda.synchronize()
     rev_ms, rev_n = gpu.kernel_time(gpu.KC_REVERSE)
+    cfg = gpu.last_config()
     gpu.enable_kernel_timing(False)
     gpu.set_precision(gpu.PRECISION_C128)
     ms = e0.elapsed_time(e1) / steps
+    P = G if cfg["gates_per_pass"] == 1 else -(-G // cfg["gates_per_pass"])
     rbytes = reverse_bytes_per_eval(L, P, 8) * steps
     achieved = rbytes / (rev_ms * 1e-3) / 1e9 if rev_ms > 0 else None
     flops = flops_per_eval(L, G, Gt)
-    out = {"precision": "complex64 passes (3xTF32 MMA), FP64 sums", "evals_per_s": 1e3 / ms, "ms_per_step": ms,
+    pipe = "FP32 FMA pipe" if cfg["c64_fp32_pipe"] else "3xTF32 MMA"
+    out = {"precision": f"complex64 passes ({pipe}), FP64 sums", "evals_per_s": 1e3 / ms, "ms_per_step": ms,
+           "tuned": cfg,
            "rel_err_vs_c128": {"f": _relerr(res[0], res_c128[0]), "grad": _relerr(res[1], res_c128[1]),
                                "hvp": _relerr(res[2], res_c128[2])},
-           "roofline": {"kernel": "k5_rev (complex64 reverse pass, adjoint reconstruction, 4 fused gates)",
+           "roofline": {"kernel": ("k7_rev (complex64 reverse pass on the FP32 pipe" if cfg["c64_fp32_pipe"]
+                                   else "k5_rev (complex64 reverse pass on the 3xTF32 MMA")
+                                  + f", adjoint reconstruction, {cfg['gates_per_pass']} fused gates)",
                         "bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s",
                         "frac": achieved / hbm_peak if achieved else None, "launches": rev_n,
-                        "avg_launch_ms": rev_ms / max(rev_n, 1),
-                        "traffic": rbytes / max(rev_n, 1) * TRAFFIC_RATIO[8]},
+                        "avg_launch_ms": rev_ms / max(rev_n, 1)},
            "eval_flops": {"per_eval": flops, "achieved_tflops": flops / (ms * 1e-3) / 1e12, "peak_tflops": fp32_peak,
                           "frac": flops / (ms * 1e-3) / 1e12 / fp32_peak if fp32_peak else None,
                           "peak_source": "FP32 peak measured in this run (cuBLAS SGEMM, TF32 off)"}}
@@ -862,7 +875,9 @@ def mixed_equal_error(gpu, L=12, depth=3, tdepth=3, niter=80, seed=0, tseed=1):
     runs = {}
     for name, p in (("plain_c128", gpu.PRECISION_C128), ("mixed", gpu.PRECISION_MIXED)):
         gpu.set_precision(p)
-        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, 2)   # workspace and kernels set up
+        # one untimed run of the same length: workspace, kernels and the autotuner's choice
+        # for every evaluation kind the run meets (the mixed run's complex128 refinement too)
+        gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)
         t0 = time.perf_counter()
         f_iter, vopt = gpu.optimize_brickwall_circuit_hvp(target, vlist, perms, L, niter)
         sec = time.perf_counter() - t0
@@ -905,7 +920,7 @@ def summary(line):
         out["mixed_evals_per_s"] = r(g(line, "mixed", "evals_per_s"))
         out["mixed_over_plain"] = r(line.get("mixed_over_plain"))
         out["mixed_rel_err_f_grad_hvp"] = [r(g(line, "mixed", "rel_err_vs_c128", k), 2) for k in ("f", "grad", "hvp")]
-        out["k5_rev_hbm_frac"] = r(g(line, "mixed", "roofline", "frac"))
+        out["c64_reverse_hbm_frac"] = r(g(line, "mixed", "roofline", "frac"))
     me = line.get("mixed_equal_error")
     if me:
         out["equal_error"] = {"rel_diff": r(me.get("f_final_rel_diff"), 2), "speedup": r(me.get("speedup")),
@@ -920,10 +935,11 @@ def summary(line):
     if bt:
         out["c4"] = {"s_batched_512x30": r(g(bt, "batched_mixed", "seconds")), "speedup": r(bt.get("speedup")),
                      "s_c128_scaled": r(bt.get("per_instance_c128_full_seconds_scaled"))}
-    sv = line.get("serving")
-    if sv:
-        out["c5"] = {k: {"done": g(sv, k, "completed"), "p50_s": r((g(sv, k, "p50_ms") or 0) / 1e3),
-                         "p99_s": r((g(sv, k, "p99_ms") or 0) / 1e3)} for k in ("mixed", "plain_c128") if k in sv}
+    for key, nm in (("serving", "c5"), ("serving_sustainable", "c5_2req_s")):
+        sv = line.get(key)
+        if sv:
+            out[nm] = {k: {"done": g(sv, k, "completed"), "p50_s": r((g(sv, k, "p50_ms") or 0) / 1e3),
+                           "p99_s": r((g(sv, k, "p99_ms") or 0) / 1e3)} for k in ("mixed", "plain_c128") if k in sv}
     return out
 
 
@@ -959,7 +975,7 @@ def main():
     ap.add_argument("--reconstruct", type=int, default=-1, choices=[-1, 0, 1],
                     help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0); "
                          "-1 (default): chosen by the autotuner")
-    ap.add_argument("--serving-wall", type=float, default=60.0)
+    ap.add_argument("--serving-wall", type=float, default=70.0)
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1173,6 +1189,8 @@ def main():
             gpu.set_precision(prec)
         if not a.no_serving and world == 1:
             line["serving"] = serving_c5(gpu, wall=a.serving_wall)
+            line["serving_sustainable"] = serving_c5(gpu, rate=2.0, duration=10.0, wall=15.0, sizes=(8, 10),
+                                                     capacity=32)
             gpu.set_precision(prec)
         if not a.no_hmat and world == 1:
             line["hmat"] = hmat_path(gpu, torch, stream, hbm_peak, with_reference=not a.no_cpu_baseline)
