@@ -972,6 +972,8 @@ def main():
                          "block-encoding Hessian with H of depth --tdepth on L/2 qubits, 'real' the real build's "
                          "f + projected gradient + projected HVP")
     ap.add_argument("--column-chunk", type=int, default=0, help="basis columns per chunk (0: from the workspace)")
+    ap.add_argument("--c64-pipe", default="auto", choices=["auto", "fp32", "mma"],
+                    help="complex64 passes on the FP32 FMA pipe or the 3xTF32 MMA (auto: the autotuner's choice)")
     ap.add_argument("--reconstruct", type=int, default=-1, choices=[-1, 0, 1],
                     help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0); "
                          "-1 (default): chosen by the autotuner")
@@ -1059,6 +1061,8 @@ def main():
         gpu.set_reconstruct(bool(a.reconstruct))
     if a.column_chunk:
         gpu.set_column_chunk(a.column_chunk)
+    if a.c64_pipe != "auto":
+        gpu.set_c64_fp32_pipe(a.c64_pipe == "fp32")
     vlist, perms, tvlist, tperms, vdirs = workload(L, depth, tdepth)
     target = gpu.Target(brickwall=(tvlist, tperms))
 

@@ -2792,8 +2792,11 @@ int evaluate_fused_t(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, int
 		dstage = reinterpret_cast<double2*>(rt.stage[2].ptr);
 	}
 
-	if ((ret = RQC_CUDA(cudaMemcpyToSymbolAsync(c_col_end, &cend, sizeof(cend), 0, cudaMemcpyHostToDevice, rt.stream))))
-		return ret;
+	if (cend != rt.col_end_dev) {   // a copy from host memory waits for the stream: only when it changes
+		if ((ret = RQC_CUDA(cudaMemcpyToSymbolAsync(c_col_end, &cend, sizeof(cend), 0, cudaMemcpyHostToDevice, rt.stream))))
+			return ret;
+		rt.col_end_dev = cend;
+	}
 	for (int64_t b0 = cbeg; b0 < cend; b0 += C) {
 		const int64_t Cc = std::min(C, cend - b0);
 		const int64_t ncg = (Cc + CW - 1) / CW;

@@ -49,6 +49,7 @@ struct Runtime
 	// basis columns the target sums run over: [col_begin, col_end), col_end 0 = to the last
 	// column (rqcopt_gpu_set_column_range)
 	int64_t col_begin = 0, col_end = 0;
+	int64_t col_end_dev = -1;    // the column end the fused kernels hold (__constant__), -1 unset
 	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
 	int recon_c128 = 1;       // complex128 reverse passes rebuild states with adjoint gates (unitary gates)
