@@ -52,7 +52,7 @@ int rqcopt_gpu_set_autotune(int on)
 		rt->gates_per_pass = 4;
 		rt->column_chunk = 0;
 		rt->recon_c128 = 1;
-		rt->c64_ffma = 1;
+		rt->c64_ffma = 0;
 	}
 	return 0;
 }
