@@ -978,6 +978,9 @@ def main():
                     help="complex128 reverse passes rebuild states with adjoint gates (1) or recompute them (0); "
                          "-1 (default): chosen by the autotuner")
     ap.add_argument("--serving-wall", type=float, default=70.0)
+    ap.add_argument("--c3-qubits", type=int, default=28, help="qubits of the gate-throughput state (C3: 28)")
+    ap.add_argument("--gate-throughput-only", action="store_true",
+                    help="run only the gate-throughput leg and print it (a small case for profilers)")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -1052,6 +1055,9 @@ def main():
 
     from rqcopt_hpc_b200 import gpu
     lib = gpu.lib()
+    if a.gate_throughput_only:
+        print(json.dumps({"gate_throughput": gate_throughput(gpu, torch, L=a.c3_qubits)}))
+        return
     prec = {"c128": gpu.PRECISION_C128, "c64": gpu.PRECISION_C64, "mixed": gpu.PRECISION_MIXED}[a.precision]
     gpu.set_precision(prec)
     gpu.set_autotune(True)
@@ -1187,7 +1193,7 @@ def main():
             line["mixed_equal_error"] = mixed_equal_error(gpu)
             gpu.set_precision(prec)
         if not a.no_gate_throughput:
-            line["gate_throughput"] = gate_throughput(gpu, torch)
+            line["gate_throughput"] = gate_throughput(gpu, torch, L=a.c3_qubits)
         if not a.no_batched and world == 1:
             line["batched"] = batched_c4(gpu, torch)
             gpu.set_precision(prec)
