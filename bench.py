@@ -248,10 +248,8 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
             run = lambda g, w, a, b: lib.rqcopt_apply_quantum_circuit_c64(g.ctypes.data, G, w.ctypes.data, a.data_ptr(),
                                                                           b.data_ptr(), L)
         r = {"state_gib": state_bytes / 2 ** 30, "recovery_tolerance": tol}
-        for gpp in (1, 4, "4_single_buffered"):
-            gpu.set_sv_double_buffer(gpp != "4_single_buffered")
-            gpp_n = 4 if gpp == "4_single_buffered" else gpp
-            gpu.set_gates_per_pass(gpp_n)
+        for gpp in (1, 4):
+            gpu.set_gates_per_pass(gpp)
             run(gates, wires, psi, out)   # warm-up
             torch.cuda.synchronize()
             e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
@@ -262,7 +260,7 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
             e[2].record(stream)
             torch.cuda.synchronize()
             t_f, t_b = e[0].elapsed_time(e[1]), e[1].elapsed_time(e[2])
-            trips = G if gpp_n == 1 else -(-G // gpp_n)
+            trips = G if gpp == 1 else -(-G // gpp)
             err = float(torch.max(torch.abs(back - psi)))
             r[f"gates_per_round_trip_{gpp}"] = {
                 "forward_ms": t_f, "backward_ms": t_b, "round_trips": trips,
@@ -272,7 +270,6 @@ def gate_throughput(gpu, torch, L=28, G=256, seed=20):
         res[name] = r
         del psi, out, back
         torch.cuda.empty_cache()
-    gpu.set_sv_double_buffer(True)
     gpu.set_autotune(True)
     return res
 

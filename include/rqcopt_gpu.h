@@ -500,13 +500,6 @@ int rqcopt_gpu_set_autotune(int on);
  * a device */
 int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, int* c64_fp32_pipe,
                            double* ms_per_column);
-/* single-state passes of several gates (apply_quantum_circuit, apply_brickwall_unitary and
- * rqcopt_apply_quantum_circuit_c64 on states of 12-31 qubits): 1 (default) double-buffers
- * the 64 KiB tiles in one block per SM, one warp issuing the TMA bulk copies of the next
- * tile while eight warps apply the gates to the current one; 0 runs three single-buffered
- * blocks per SM.  Same results. */
-void rqcopt_gpu_set_sv_double_buffer(int on);
-
 /* complex64 fused passes: 1 in FP32 FMAs, four threads per amplitude group and the gate
  * coefficients in registers; 0 (default) on the TF32 tensor-core MMA with the three-term
  * split (FP32 accuracy), which issues about half the instructions and measured faster on

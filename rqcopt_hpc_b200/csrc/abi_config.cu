@@ -81,11 +81,6 @@ int rqcopt_gpu_set_column_range(long begin, long end)
 	return 0;
 }
 
-void rqcopt_gpu_set_sv_double_buffer(int on)
-{
-	if (Runtime* rt = runtime()) rt->sv_double_buffer = on ? 1 : 0;
-}
-
 void rqcopt_gpu_set_c64_fp32_pipe(int on)
 {
 	if (Runtime* rt = runtime()) {

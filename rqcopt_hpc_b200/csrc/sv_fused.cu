@@ -183,8 +183,7 @@ __global__ void __launch_bounds__(SVT_TPB, 3) k_sv_tile(const cplx<T>* __restric
 				             ::"r"(smem_u32(S + ((size_t)r << ps.m))), "l"(in + base + roff[r]), "r"(run_bytes),
 				             "r"(smem_u32(bar)) : "memory");
 		}
-		// the block decides together, so that no thread leaves while others wait at a barrier
-		if (!__syncthreads_and(mbar_wait(bar, parity) ? 1 : 0)) {
+		if (!mbar_wait(bar, parity)) {
 			ok = false;
 			if (threadIdx.x == 0) atomicExch(err, 1);
 			break;
@@ -226,142 +225,6 @@ __global__ void __launch_bounds__(SVT_TPB, 3) k_sv_tile(const cplx<T>* __restric
 	if (!ok && warp == 0) {
 		// the loads of the tile that timed out may still land: wait (bounded) before the block exits
 		mbar_wait(bar, parity);
-	}
-}
-
-// Double-buffered form of k_sv_tile, one block per SM: warp 8 (the producer) moves the
-// tiles with TMA bulk copies, warps 0-7 (the consumers) apply the gates.  Tile i of the
-// block uses buffer i & 1; the producer stores tile i-2 and loads tile i into that
-// buffer while the consumers work on tile i-1, so HBM traffic overlaps the gate work.
-//   loaded[b]   : completes when the bulk loads of the tile in buffer b have landed
-//                 (one arrival with the expected bytes, by the producer);
-//   computed[b] : completes when the eight consumer warps are done with buffer b.
-// Every wait is bounded (~2 s); a wait that gives up sets *err and its warp leaves.
-constexpr int SVD_CONSUMERS = 256;
-constexpr int SVD_TPB = SVD_CONSUMERS + 32;
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar)
-{
-	asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-template <typename T>
-__global__ void __launch_bounds__(SVD_TPB, 1) k_sv_tile2(const cplx<T>* __restrict__ in, cplx<T>* __restrict__ out,
-                                                          SvTile ps, SvGates<T> gates, int* __restrict__ err)
-{
-	using V = cplx<T>;
-	extern __shared__ __align__(128) unsigned char sm_raw[];
-	V* S0 = reinterpret_cast<V*>(sm_raw);
-	int64_t* roff = reinterpret_cast<int64_t*>(sm_raw + 2 * SVT_TILE_BYTES);
-	uint64_t* bars = reinterpret_cast<uint64_t*>(roff + SVT_MAXRUNS);   // loaded[2], computed[2]
-	Gate4<T>* sgate = reinterpret_cast<Gate4<T>*>(bars + 4);
-	const int A = 1 << ps.NB, nruns = 1 << (ps.NB - ps.m);
-	const uint32_t run_bytes = (uint32_t)(sizeof(V) << ps.m);
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	const int64_t ntl = ps.ntiles > blockIdx.x ? (ps.ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;   // tiles of this block
-	for (int r = threadIdx.x; r < nruns; r += blockDim.x) {
-		int64_t o = 0;
-		for (int b = 0; b < ps.NB - ps.m; b++)
-			if ((r >> b) & 1) o |= (int64_t)1 << ps.hbit[b];
-		roff[r] = o;
-	}
-	for (int e = threadIdx.x; e < SV_MAXK * 16; e += blockDim.x) sgate[e / 16].m[e % 16] = gates.g[e / 16].m[e % 16];
-	if (threadIdx.x == 0) {
-		for (int b = 0; b < 2; b++) {
-			asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bars + b)) : "memory");
-			asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + 2 + b)), "r"(SVD_CONSUMERS / 32)
-			             : "memory");
-		}
-		asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-	}
-	__syncthreads();
-	auto tile_base = [&](int64_t i) { return sv_deposit((int64_t)blockIdx.x + i * gridDim.x, ps.rest_mask); };
-	auto buf = [&](int64_t i) { return S0 + ((size_t)(i & 1) << SvtBits<T>::v); };
-
-	if (warp == SVD_CONSUMERS / 32) {
-		// producer
-		auto store = [&](int64_t i) {
-			const int64_t base = tile_base(i);
-			V* S = buf(i);
-			for (int r = lane; r < nruns; r += 32)
-				asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;"
-				             ::"l"(out + base + roff[r]), "r"(smem_u32(S + ((size_t)r << ps.m))), "r"(run_bytes) : "memory");
-			asm volatile("cp.async.bulk.commit_group;" ::: "memory");
-		};
-		for (int64_t i = 0; i < ntl; i++) {
-			const int b = (int)(i & 1);
-			if (i >= 2) {
-				// buffer b held tile i-2: wait for the consumers, write it back, and let the
-				// copies read it out before the next load overwrites it
-				if (!mbar_wait(bars + 2 + b, (uint32_t)(((i - 2) >> 1) & 1))) {
-					if (lane == 0) atomicExch(err, 1);
-					break;
-				}
-				store(i - 2);
-				asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
-			}
-			asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-			if (lane == 0)
-				asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bars + b)),
-				             "r"((uint32_t)(A * sizeof(V))) : "memory");
-			__syncwarp();
-			const int64_t base = tile_base(i);
-			V* S = buf(i);
-			for (int r = lane; r < nruns; r += 32)
-				asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-				             ::"r"(smem_u32(S + ((size_t)r << ps.m))), "l"(in + base + roff[r]), "r"(run_bytes),
-				             "r"(smem_u32(bars + b)) : "memory");
-		}
-		// the last two tiles
-		for (int64_t i = ntl >= 2 ? ntl - 2 : 0; i < ntl; i++) {
-			if (!mbar_wait(bars + 2 + (i & 1), (uint32_t)((i >> 1) & 1))) {
-				if (lane == 0) atomicExch(err, 1);
-				break;
-			}
-			store(i);
-		}
-		asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
-		return;
-	}
-
-	// consumers (256 threads, named barrier 1)
-	for (int64_t i = 0; i < ntl; i++) {
-		const int b = (int)(i & 1);
-		// all consumers decide together (barrier with an AND), so that none leaves while
-		// the others wait at the named barrier
-		const int ok = mbar_wait(bars + b, (uint32_t)((i >> 1) & 1)) ? 1 : 0;
-		int all_ok;
-		asm volatile("{\n\t.reg .pred p, q;\n\tsetp.ne.s32 p, %1, 0;\n\tbar.red.and.pred q, 1, %2, p;\n\t"
-		             "selp.s32 %0, 1, 0, q;\n\t}"
-		             : "=r"(all_ok) : "r"(ok), "r"(SVD_CONSUMERS) : "memory");
-		if (!all_ok) {
-			if (threadIdx.x == 0) atomicExch(err, 1);
-			return;
-		}
-		V* S = buf(i);
-#pragma unroll 1
-		for (int k = 0; k < ps.K; k++) {
-			const int bi = ps.gi[k], bj = ps.gj[k];
-			const int lo = bi < bj ? bi : bj, hi = bi < bj ? bj : bi;
-			const Gate4<T>& gk = sgate[k];
-			for (int g = threadIdx.x; g < A / 4; g += SVD_CONSUMERS) {
-				int q = g;
-				q = ((q >> lo) << (lo + 1)) | (q & ((1 << lo) - 1));
-				q = ((q >> hi) << (hi + 1)) | (q & ((1 << hi) - 1));
-				const int r0 = q, r1 = q | (1 << bj), r2 = q | (1 << bi), r3 = q | (1 << bi) | (1 << bj);
-				V x[4] = { S[r0], S[r1], S[r2], S[r3] }, y[4];
-				gate_apply(gk, x, y);
-				S[r0] = y[0];
-				S[r1] = y[1];
-				S[r2] = y[2];
-				S[r3] = y[3];
-			}
-			asm volatile("bar.sync 1, %0;" ::"r"(SVD_CONSUMERS) : "memory");
-		}
-		// the stores above (generic proxy) become visible to the producer's bulk copies
-		asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-		__syncwarp();
-		if (lane == 0) mbar_arrive(bars + 2 + b);
 	}
 }
 
@@ -482,30 +345,17 @@ int apply_circuit_fused_t(Runtime& rt, int L, int ngates, const double2* gates, 
 				per_sm = 1;
 			}
 		}
-		const size_t smem2 = 2 * SVT_TILE_BYTES + SVT_MAXRUNS * sizeof(int64_t) + 32 + SV_MAXK * sizeof(Gate4<T>);
-		static bool ready2 = false;
-		if (!ready2) {
-			if ((ret = RQC_CUDA(cudaFuncSetAttribute(k_sv_tile2<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem2))))
-				return ret;
-			ready2 = true;
-		}
 		if ((ret = ensure_device(rt.status, sizeof(int)))) return ret;
 		int* d_err = static_cast<int*>(rt.status.ptr);
 		if ((ret = RQC_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), rt.stream)))) return ret;
 		const cplx<T>* src = d_in;
 		for (int p = 0; p < P; p++) {
 			cplx<T>* dst = ((P - 1 - p) % 2 == 0) ? d_out : tmp;
+			const int grid = (int)std::min<int64_t>(passes[p].ntiles, (int64_t)rt.num_sms * per_sm);
 			cudaEvent_t ev;
 			launch_begin(rt, KC_FUSED, &ev);
-			if (rt.sv_double_buffer) {
-				const int grid = (int)std::min<int64_t>(passes[p].ntiles, (int64_t)rt.num_sms);
-				k_sv_tile2<T><<<grid, SVD_TPB, smem2, rt.stream>>>(src, dst, passes[p],
-				                                                    gates_of(passes[p].first, passes[p].K), d_err);
-			} else {
-				const int grid = (int)std::min<int64_t>(passes[p].ntiles, (int64_t)rt.num_sms * per_sm);
-				k_sv_tile<T><<<grid, SVT_TPB, smem, rt.stream>>>(src, dst, passes[p],
-				                                                 gates_of(passes[p].first, passes[p].K), d_err);
-			}
+			k_sv_tile<T><<<grid, SVT_TPB, smem, rt.stream>>>(src, dst, passes[p], gates_of(passes[p].first, passes[p].K),
+			                                                 d_err);
 			launch_end(rt, KC_FUSED, ev);
 			if ((ret = RQC_CUDA(cudaGetLastError()))) return ret;
 			src = dst;

@@ -121,7 +121,6 @@ _SIGS = {
     "rqcopt_gpu_set_autotune": (I, [I]),
     "rqcopt_gpu_last_config": (I, [VP, VP, VP, VP, VP]),
     "rqcopt_gpu_set_c64_fp32_pipe": (None, [I]),
-    "rqcopt_gpu_set_sv_double_buffer": (None, [I]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
@@ -877,12 +876,6 @@ def last_config():
         raise RqcError("rqcopt_gpu_last_config", tuned)
     return {"gates_per_pass": g.value, "column_chunk": ch.value, "reconstruct": bool(r.value),
             "c64_fp32_pipe": bool(f.value), "ms_per_column": ms.value, "tuned": bool(tuned)}
-
-
-def set_sv_double_buffer(on: bool):
-    """Single-state fused passes: double-buffered producer / consumer tiles (True) or
-    single-buffered tiles, three blocks per SM (False)."""
-    lib().rqcopt_gpu_set_sv_double_buffer(1 if on else 0)
 
 
 def set_c64_fp32_pipe(on: bool):
