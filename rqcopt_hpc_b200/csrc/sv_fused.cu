@@ -183,7 +183,8 @@ __global__ void __launch_bounds__(SVT_TPB, 3) k_sv_tile(const cplx<T>* __restric
 				             ::"r"(smem_u32(S + ((size_t)r << ps.m))), "l"(in + base + roff[r]), "r"(run_bytes),
 				             "r"(smem_u32(bar)) : "memory");
 		}
-		if (!mbar_wait(bar, parity)) {
+		// the block decides together, so that no thread leaves while others wait at a barrier
+		if (!__syncthreads_and(mbar_wait(bar, parity) ? 1 : 0)) {
 			ok = false;
 			if (threadIdx.x == 0) atomicExch(err, 1);
 			break;

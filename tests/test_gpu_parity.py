@@ -254,6 +254,30 @@ def test_complex64_fp32_pipe_matches_tf32_mma(gpu, oracle, L, depth, chunk):
         assert rel_err(g, go) <= 1e-5 and rel_err(h, ho) <= 1e-5 and rel_err(gg, go) <= 1e-5
 
 
+@pytest.mark.parametrize("L", [12, 16, 21])
+def test_single_state_tile_kernels_agree(gpu, oracle, L):
+    """apply_quantum_circuit with several gates per HBM round trip (TMA bulk tiles) and
+    with one kernel per gate give the same state (complex128 1e-13 relative; the oracle
+    at L <= 16), with 2-4 gates per pass and wires on the lowest and highest qubits."""
+    rng = np.random.default_rng(30 + L)
+    G = 23
+    psi = crandn(1 << L, rng)
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    wires[0] = (L - 1, 0)
+    wires[1] = (L - 2, L - 1)
+    try:
+        gpu.set_gates_per_pass(1)
+        ref = gpu.apply_quantum_circuit(gates, wires, psi)
+        for gpp in (2, 3, 4):
+            gpu.set_gates_per_pass(gpp)
+            assert rel_err(gpu.apply_quantum_circuit(gates, wires, psi), ref) <= 1e-13, gpp
+    finally:
+        gpu.set_autotune(True)
+    if L <= 16:
+        assert rel_err(ref, oracle.apply_quantum_circuit(gates, wires, psi)) <= 1e-12
+
+
 def test_forward_adjoint_round_trip(gpu):
     """Forward through 64 random Haar gates on random distinct pairs, then the adjoint
     gates in reverse order, recovers the input state (L = 20, complex128)."""
