@@ -712,9 +712,8 @@ def front_end_path(L=8, depth=5, niter=10, ref_niter=2, seed=50, with_reference=
 def batched_c4(gpu, torch, count=512, niter=30, sample_every=16):
     """C4: 512 independent brickwall instances (even L uniform over 6..12, depth over
     {3,5,7,9}, target depth 3, seeds 30+i / 10000+i), 30 trust-region iterations each.
-    The batched mixed-precision path (complex64 passes with FP64 sums, complex128 f,
-    gradient and refinement; one persistent kernel per round on a device work queue,
-    CUDA-graph rounds) runs all instances.  The plain per-instance complex128 loop
+    The batched complex64 path (complex64 passes with FP64 sums; one persistent kernel
+    per round on a device work queue, CUDA-graph rounds) runs all instances.  The plain per-instance complex128 loop
     (optimize_brickwall_circuit_hvp one instance after another) runs on every
     `sample_every`-th instance, and so does the batched path once more, so the speed-up
     compares the two on identical work; the full loop's time is that sample's time scaled
@@ -727,7 +726,7 @@ def batched_c4(gpu, torch, count=512, niter=30, sample_every=16):
                        f"{niter} RTR iterations each"}
     warm = batch.Batch(16, 2)   # kernel and graph set-up outside the timed runs
     for p in probs[:16]:
-        warm.add(p, 2, gpu.PRECISION_MIXED)
+        warm.add(p, 2, gpu.PRECISION_C64)
     while warm.run(32) > 0:
         pass
     warm.close()
@@ -735,7 +734,7 @@ def batched_c4(gpu, torch, count=512, niter=30, sample_every=16):
     def run_batched(ps):
         b = batch.Batch(len(ps), niter)
         for p in ps:
-            b.add(p, niter, gpu.PRECISION_MIXED)
+            b.add(p, niter, gpu.PRECISION_C64)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         while b.run(32) > 0:
@@ -764,11 +763,11 @@ def batched_c4(gpu, torch, count=512, niter=30, sample_every=16):
     torch.cuda.synchronize()
     tps = time.perf_counter() - t0
     fp = np.array(fp)
-    out["batched_mixed"] = {"instances": count, "seconds": tb, "evaluations": ev, "hvp_evaluations": hv,
+    out["batched_c64"] = {"instances": count, "seconds": tb, "evaluations": ev, "hvp_evaluations": hv,
                             "evals_per_s": ev / tb, "instance_iterations_per_s": count * niter / tb}
-    out["sample"] = {"instances": len(sample), "every": sample_every, "batched_mixed_seconds": tbs,
+    out["sample"] = {"instances": len(sample), "every": sample_every, "batched_c64_seconds": tbs,
                      "per_instance_c128_seconds": tps,
-                     "f_final_max_rel_diff_mixed_vs_c128": float(np.max(np.abs(fbs - fp) / np.abs(fp)))}
+                     "f_final_max_rel_diff_c64_vs_c128": float(np.max(np.abs(fbs - fp) / np.abs(fp)))}
     out["per_instance_c128_full_seconds_scaled"] = tps * count / len(sample)
     out["speedup"] = tps / tbs
     return out
@@ -933,7 +932,7 @@ def summary(line):
                                     for p in ("c128", "c64") for k in (1, 4)}
     bt = line.get("batched")
     if bt:
-        out["c4"] = {"s_batched_512x30": r(g(bt, "batched_mixed", "seconds")), "speedup": r(bt.get("speedup")),
+        out["c4"] = {"s_batched_512x30": r(g(bt, "batched_c64", "seconds")), "speedup": r(bt.get("speedup")),
                      "s_c128_scaled": r(bt.get("per_instance_c128_full_seconds_scaled"))}
     for key, nm in (("serving", "c5"), ("serving_sustainable", "c5_2req_s")):
         sv = line.get(key)
