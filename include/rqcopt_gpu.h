@@ -500,11 +500,6 @@ int rqcopt_gpu_set_autotune(int on);
  * a device */
 int rqcopt_gpu_last_config(int* gates_per_pass, long* column_chunk, int* reconstruct, int* c64_fp32_pipe,
                            double* ms_per_column);
-/* full-Hessian sweep of states of up to 12 qubits (one kernel per brickwall layer): 1
- * (default) runs the contractions with phi and the gates on the FP64 MMA, 0 on DFMAs.
- * Same sums to rounding. */
-void rqcopt_gpu_set_hessian_mma(int on);
-
 /* complex64 fused passes: 1 in FP32 FMAs, four threads per amplitude group and the gate
  * coefficients in registers; 0 (default) on the TF32 tensor-core MMA with the three-term
  * split (FP32 accuracy), which issues about half the instructions and measured faster on

@@ -81,11 +81,6 @@ int rqcopt_gpu_set_column_range(long begin, long end)
 	return 0;
 }
 
-void rqcopt_gpu_set_hessian_mma(int on)
-{
-	if (Runtime* rt = runtime()) rt->hess_mma = on ? 1 : 0;
-}
-
 void rqcopt_gpu_set_c64_fp32_pipe(int on)
 {
 	if (Runtime* rt = runtime()) {

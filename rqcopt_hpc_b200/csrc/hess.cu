@@ -335,191 +335,6 @@ k_hlayer(const double2* __restrict__ psi, int64_t basis_b0, const double2* __res
 	}
 }
 
-// ------------------------------------------------------------------ layer kernel on the FP64 tensor pipe
-
-// The same layer step as k_hlayer with the 4x4 complex products on the FP64 MMA
-// (mma.sync m8n8k4, the pipe that DFMA shares on B200) and the outer sums held as MMA
-// accumulator fragments (two doubles per lane instead of 32 per thread, so nothing
-// spills and three blocks fit per SM).  A warp works on units of eight amplitude groups:
-//   gate       y = G x: rows = the 8 groups, K = 8 reals (member, re/im) in two k-steps,
-//              B = the 8x8 real embedding of G; lane l ends with member l & 3 of group
-//              l >> 2, the member it stores;
-//   outer sum  R += P^T X over 4 groups per MMA (K), rows / columns = (member, re/im) of
-//              phi / x, folded into complex entries by the block reduction:
-//              dG[r][c] = (R[2r][2c] - R[2r+1][2c+1]) + i (R[2r][2c+1] + R[2r+1][2c]).
-__device__ __forceinline__ void hmma(double& d0, double& d1, double a, double b)
-{
-	asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
-	    : "+d"(d0), "+d"(d1)
-	    : "d"(a), "d"(b));
-}
-
-// entry (k, n) of the real 8x8 matrix M with out[n] = sum_k in[k] M[k][n] for y = G x
-// (in / out indices 2 * member + {re, im})
-__device__ __forceinline__ double gate_embed(const double2* g, int k, int n)
-{
-	const int m = k >> 1, a = k & 1, mo = n >> 1, b = n & 1;
-	const double2 v = g[4 * mo + m];
-	return a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
-}
-
-__global__ void __launch_bounds__(HT, 3)
-k_hlayer_mma(const double2* __restrict__ psi, int64_t basis_b0, const double2* __restrict__ phi, double2* __restrict__ tan,
-             Gate4<double> g, LayerGates lgts, int L, int64_t ncols, int64_t sstride, int layer, int last,
-             double* __restrict__ part, int S, double2* __restrict__ fpart)
-{
-	extern __shared__ double2 tile[];
-	__shared__ WirePair sw[HMAXPER];
-	__shared__ double2 sgm[16];
-	__shared__ double rawr[HT / 32][64];
-	if (threadIdx.x < lgts.per) sw[threadIdx.x] = lgts.w[threadIdx.x];
-	if (threadIdx.x < 16) sgm[threadIdx.x] = g.m[threadIdx.x];
-	__syncthreads();
-	const int s = blockIdx.x, bx = blockIdx.y, nbx = gridDim.y;
-	const int t = s - 1;
-	const bool own = s > 0 && (t >> 4) == layer;
-	const int er = (t & 15) >> 2, ec = t & 3;
-	double2* __restrict__ T = s > 0 ? tan + (int64_t)t * sstride : nullptr;
-	const int lg = L - 2;
-	const int64_t gmask = ((int64_t)1 << lg) - 1;
-	const int cb = HTILE >> L;                               // columns per tile
-	const int64_t nblk = (ncols + cb - 1) / cb;
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = HT / 32;
-	// B fragments of the gate embedding (k-steps 0 and 1): lane holds M[4 s + (lane & 3)][lane >> 2]
-	const double bg0 = gate_embed(sgm, lane & 3, lane >> 2), bg1 = gate_embed(sgm, 4 + (lane & 3), lane >> 2);
-	double r0 = 0, r1 = 0;                                   // raw outer sums R[lane >> 2][2 (lane & 3) + {0, 1}]
-	double fx = 0, fy = 0;
-	// lane roles: gate step -> group (lane >> 2) of the unit, input members 2 s + ((lane & 3) >> 1) (part lane & 1),
-	// output member lane & 3; outer step -> group (lane & 3) of a quarter, member lane >> 3, part (lane >> 2) & 1
-	const int ga = lane >> 2, ma0 = (lane & 3) >> 1, pa = lane & 1, mo = lane & 3;
-	const int go = lane & 3, mouter = lane >> 3, pouter = (lane >> 2) & 1;
-	for (int64_t blk = bx; blk < nblk; blk += nbx) {
-		const int64_t col0 = blk * cb;
-		const int cbn = (int)min((int64_t)cb, ncols - col0);
-		const int n = cbn << L;                               // amplitudes of this tile
-		const int64_t gofs = col0 << L;
-		if (s > 0 && !own) {
-			for (int e = threadIdx.x; e < n; e += HT) tile[e] = T[gofs + e];
-			__syncthreads();
-		}
-		const int ngr = n >> 2;
-		for (int k = 0; k < lgts.per; k++) {
-			const int q = lgts.q0 + k;
-			const WirePair w = sw[k];
-			int64_t off[4];
-			group_offsets(w, off);
-			const bool final_gate = last && k == lgts.per - 1;
-			const double2* __restrict__ ph = phi + (int64_t)q * sstride + gofs;
-			const double2* __restrict__ ps = psi + (int64_t)q * sstride + gofs;
-			const bool zero_in = own && k == 0;
-			const bool basis = q == 0 && basis_b0 >= 0;
-			const int64_t offc = ((ec & 2) ? w.si : 0) + ((ec & 1) ? w.sj : 0);
-			// local index (within the tile) of group gi and whether it exists
-			auto li_of = [&](int gi) { return ((int64_t)(gi >> lg) << L) + group_base(gi & gmask, w); };
-			// one real part of member m of group gi of the step's input x
-			auto xin = [&](int gi, int64_t li, int m, int partx) -> double {
-				if (s == 0) {
-					if (basis) {
-						const int cc = gi >> lg;
-						const int64_t loc = group_base(gi & gmask, w);
-						return (partx == 0 && loc + off[m] == basis_b0 + col0 + cc) ? 1.0 : 0.0;
-					}
-					const double2 v = ps[li + off[m]];
-					return partx ? v.y : v.x;
-				}
-				const double2 v = tile[li + off[m]];
-				return partx ? v.y : v.x;
-			};
-			for (int u0 = warp * 8; u0 < ngr; u0 += nwarps * 8) {
-				// outer sums over the unit's groups, four per MMA
-				if (!zero_in) {
-#pragma unroll
-					for (int h = 0; h < 2; h++) {
-						const int gi = u0 + 4 * h + go;
-						double pv = 0, xv = 0;
-						if (gi < ngr) {
-							const int64_t li = li_of(gi);
-							const double2 pp = ph[li + off[mouter]];
-							pv = pouter ? pp.y : pp.x;
-							xv = xin(gi, li, mouter, pouter);
-						}
-						hmma(r0, r1, pv, xv);
-					}
-				}
-				const bool store = s > 0 && !final_gate;
-				const bool fsum = s == 0 && final_gate && fpart;
-				if (!store && !fsum) continue;
-				// y = G x for the unit's groups: lane ends with member mo of group u0 + ga
-				const int gi = u0 + ga;
-				const bool valid = gi < ngr;
-				const int64_t li = valid ? li_of(gi) : 0;
-				double y0 = 0, y1 = 0;
-				if (!zero_in) {
-					const double a0 = valid ? xin(gi, li, ma0, pa) : 0.0;
-					const double a1 = valid ? xin(gi, li, 2 + ma0, pa) : 0.0;
-					hmma(y0, y1, a0, bg0);
-					hmma(y0, y1, a1, bg1);
-				}
-				if (fsum) {
-					if (valid) {
-						const double2 pp = ph[li + off[mo]];
-						fx += pp.x * y0 - pp.y * y1;
-						fy += pp.x * y1 + pp.y * y0;
-					}
-					continue;
-				}
-				if (own && mo == er && valid) {
-					if (basis) {
-						const int cc = gi >> lg;
-						const int64_t loc = group_base(gi & gmask, w);
-						if (loc + offc == basis_b0 + col0 + cc) y0 += 1.0;
-					} else {
-						const double2 v = ps[li + offc];
-						y0 += v.x;
-						y1 += v.y;
-					}
-				}
-				__syncwarp();   // every lane of the warp has read its unit's inputs
-				if (valid) tile[li + off[mo]] = make_double2(y0, y1);
-			}
-			__syncthreads();
-		}
-		if (s > 0 && !last) {
-			for (int e = threadIdx.x; e < n; e += HT) T[gofs + e] = tile[e];
-			__syncthreads();
-		}
-	}
-	// block sum of the raw 8x8 sums, folded into complex dG / Hessian entries
-	rawr[warp][2 * lane] = r0;
-	rawr[warp][2 * lane + 1] = r1;
-	__syncthreads();
-	if (threadIdx.x < 32) {
-		const int c32 = threadIdx.x, e = c32 >> 1, r = e >> 2, c = e & 3, im = c32 & 1;
-		double a = 0, b = 0;
-		for (int w2 = 0; w2 < nwarps; w2++) {
-			a += rawr[w2][(2 * r) * 8 + 2 * c + im];
-			b += rawr[w2][(2 * r + 1) * 8 + 2 * c + 1 - im];
-		}
-		const double v = im ? a + b : a - b;
-		const size_t slot = (size_t)layer * S + s;
-		double* o = part + slot * 32 * nbx + bx + (size_t)c32 * nbx;
-		*o += v;
-	}
-	if (s == 0 && fpart) {
-		__shared__ double fr[2][HT / 32];
-		fx = warp_sum(fx);
-		fy = warp_sum(fy);
-		if (lane == 0) { fr[0][warp] = fx; fr[1][warp] = fy; }
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			double sx = 0, sy = 0;
-			for (int k = 0; k < HT / 32; k++) { sx += fr[0][k]; sy += fr[1][k]; }
-			fpart[bx].x += sx;
-			fpart[bx].y += sy;
-		}
-	}
-}
-
 // ------------------------------------------------------------------ block encoding
 
 // full-register index of half-register basis state b: bit i of b at bit 2 i + 1
@@ -989,9 +804,6 @@ struct Sweep
 			if (int e = RQC_CUDA(cudaFuncSetAttribute(k_hlayer, cudaFuncAttributeMaxDynamicSharedMemorySize,
 			                                          (int)(HTILE * sizeof(double2)))))
 				return e;
-			if (int e = RQC_CUDA(cudaFuncSetAttribute(k_hlayer_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
-			                                          (int)(HTILE * sizeof(double2)))))
-				return e;
 			smem_set = true;
 		}
 		LayerGates lgts;
@@ -1002,14 +814,9 @@ struct Sweep
 		const dim3 grid(psi_only ? 1 : 1 + 16 * (a + 1), nbx);
 		cudaEvent_t ev;
 		launch_begin(rt, KC_HESS, &ev);
-		if (rt.hess_mma)
-			k_hlayer_mma<<<grid, HT, HTILE * sizeof(double2), rt.stream>>>(psi, basis_b0, phi, tan, gg[a], lgts, L, ncols,
-			                                                                 sstride, a, last ? 1 : 0, part, S,
-			                                                                 (with_f && last) ? fpart : nullptr);
-		else
-			k_hlayer<<<grid, HT, HTILE * sizeof(double2), rt.stream>>>(psi, basis_b0, phi, tan, gg[a], lgts, L, ncols, sstride,
-			                                                             a, last ? 1 : 0, part, S,
-			                                                             (with_f && last) ? fpart : nullptr);
+		k_hlayer<<<grid, HT, HTILE * sizeof(double2), rt.stream>>>(psi, basis_b0, phi, tan, gg[a], lgts, L, ncols, sstride, a,
+		                                                             last ? 1 : 0, part, S,
+		                                                             (with_f && last) ? fpart : nullptr);
 		launch_end(rt, KC_HESS, ev);
 		return RQC_CUDA(cudaGetLastError());
 	}

@@ -53,7 +53,6 @@ struct Runtime
 	int real_pairs = 0;          // evaluate(): paired basis columns of a real problem (rqcopt_gpu_set_real_pairs)
 	int gates_per_pass = 4;   // 1: one kernel per gate; 2..4: fused passes
 	int recon_c128 = 1;       // complex128 reverse passes rebuild states with adjoint gates (unitary gates)
-	int hess_mma = 1;         // full-Hessian layer kernel on the FP64 MMA (k_hlayer_mma) or on DFMAs (k_hlayer)
 	int c64_ffma = 0;         // complex64 fused passes on the FP32 pipe (k7) rather than the TF32 MMA (k4 / k5)
 
 	// autotuning of the basis-column engine (autotune.cu): the configuration chosen per

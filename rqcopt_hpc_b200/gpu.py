@@ -121,7 +121,6 @@ _SIGS = {
     "rqcopt_gpu_set_autotune": (I, [I]),
     "rqcopt_gpu_last_config": (I, [VP, VP, VP, VP, VP]),
     "rqcopt_gpu_set_c64_fp32_pipe": (None, [I]),
-    "rqcopt_gpu_set_hessian_mma": (None, [I]),
     "rqcopt_gpu_last_error": (I, []),
     "rqcopt_gpu_optimizer_trace": (I, [VP, VP, VP, VP, I]),
     "rqcopt_gpu_set_gates_per_pass": (I, [I]),
@@ -877,11 +876,6 @@ def last_config():
         raise RqcError("rqcopt_gpu_last_config", tuned)
     return {"gates_per_pass": g.value, "column_chunk": ch.value, "reconstruct": bool(r.value),
             "c64_fp32_pipe": bool(f.value), "ms_per_column": ms.value, "tuned": bool(tuned)}
-
-
-def set_hessian_mma(on: bool):
-    """Full-Hessian layer kernel (L <= 12) on the FP64 MMA (True, default) or on DFMAs (False)."""
-    lib().rqcopt_gpu_set_hessian_mma(1 if on else 0)
 
 
 def set_c64_fp32_pipe(on: bool):

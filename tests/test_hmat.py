@@ -42,40 +42,6 @@ def test_target_hessian_matches_oracle(gpu, oracle):
     assert np.array_equal(H, H.T)
 
 
-@pytest.mark.parametrize("L,depth,chunk", [(6, 3, 0), (8, 5, 24), (10, 4, 0), (12, 3, 0)])
-def test_layer_kernel_on_the_fp64_mma_matches_dfma(gpu, oracle, L, depth, chunk):
-    """The layer kernel of the full-Hessian sweep (L <= 12) on the FP64 MMA and on DFMAs:
-    f, gradient vector and Hessian matrix agree to 1e-12 (and with the oracle at L <= 8),
-    ragged column chunks included; the block-encoding Hessian, which runs the same
-    sweep with a residual seed, too."""
-    vlist, perms, tvlist, tperms = _c1(L=L, depth=depth, seed=20 + L)
-    tg = gpu.Target(brickwall=(tvlist, tperms))
-    gpu.set_column_chunk(chunk)
-    res = {}
-    try:
-        for on in (True, False):
-            gpu.set_hessian_mma(on)
-            res[on] = gpu.brickwall_unitary_target_gradient_vector_hessian_matrix(tg, vlist, perms, L)
-            if (L // 2) % 2 == 0:   # H: a brickwall of depth 2 on the L/2-qubit register
-                hv = tvlist[:2]
-                hp = np.stack([np.arange(L // 2) if l % 2 == 0 else np.roll(np.arange(L // 2), -1) for l in range(2)])
-                res[(on, "benc")] = gpu.brickwall_blockenc_target_gradient_vector_hessian_matrix(
-                    gpu.Target(brickwall=(hv, hp.astype(np.int32))), vlist, perms, L)
-    finally:
-        gpu.set_hessian_mma(True)
-    for key in (None, "benc") if (L // 2) % 2 == 0 else (None,):
-        a = res[True] if key is None else res[(True, key)]
-        b = res[False] if key is None else res[(False, key)]
-        assert abs(a[0] - b[0]) <= 1e-12 * max(abs(b[0]), 1e-300)
-        assert rel_err(a[1], b[1]) <= 1e-12 and rel_err(a[2], b[2]) <= 1e-12
-    if L <= 8:
-        fo, go, Ho = oracle.brickwall_unitary_target_gradient_vector_hessian_matrix(
-            oracle.target("brickwall", (tvlist, tperms)), vlist, perms, L)
-        f, g, H = res[True]
-        assert abs(f - fo) <= 1e-12 * abs(fo)
-        assert rel_err(g, go) <= 1e-12 and rel_err(H, Ho) <= 1e-12
-
-
 def test_target_hessian_matches_compiled_reference(gpu):
     ref_mod = pytest.importorskip("oracle.oracle")
     if not ref_mod.Reference.available():
