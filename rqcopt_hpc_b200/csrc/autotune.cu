@@ -128,7 +128,7 @@ int evaluate_autotuned(Runtime& rt, const CircuitSpec& c, const TargetSpec& t, i
 		// columns per chunk (0: as many as the workspace holds)
 		const Config after_gpp = best;
 		if (!rt.pin_chunk)
-			for (long ch : {0L, 2048L, 512L})
+			for (long ch : {0L, 2048L, 1024L, 512L, 256L, 128L})
 				if (ch != after_gpp.chunk && (ch == 0 || ch < ns))
 					consider({after_gpp.gpp, ch, after_gpp.recon, after_gpp.ffma});
 		// reverse variant (complex128 fused passes of HVP / gradient evaluations)
