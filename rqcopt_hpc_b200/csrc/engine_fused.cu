@@ -556,17 +556,62 @@ __device__ __forceinline__ void apply_unit(const double* in, const double* din, 
 	if (TAN) dout[st] = make_double2(z0, z1);
 }
 
-// apply_unit for two units of a warp at once (u0 and, if has1, u1; has1 is the same for
-// all lanes): both units' operands are loaded before either is stored, so the two
-// independent MMA chains overlap; in place like apply_unit(..., inplace = true).
+// Rows owned by one warp across two gates.  When gates a and b of a pass act on
+// disjoint tile bits, the 2^NB tile rows split into 2^(NB-4) sets of 16 rows that are
+// closed under both gates (the rows that agree outside the four bits), so a warp can
+// apply a then b to its sets with warp-level synchronisation only, and the block
+// barrier between the two gates goes away.
+__device__ __forceinline__ bool gates_disjoint(const PassGeom& pg, int a, int b)
+{
+	return (((1 << pg.gi[a]) | (1 << pg.gj[a])) & ((1 << pg.gi[b]) | (1 << pg.gj[b]))) == 0;
+}
+
+// first row of set s: s with zero bits inserted at the set bits of m (in increasing order)
+__device__ __forceinline__ int set_base(int s, int m)
+{
+#pragma unroll
+	for (int i = 0; i < 4; i++) {
+		const int p = __ffs(m) - 1;
+		s = ((s >> p) << (p + 1)) | (s & ((1 << p) - 1));
+		m &= m - 1;
+	}
+	return s;
+}
+
+// The group bases of the two units a warp works on at once: unit 0 holds the groups at
+// bases b00 and b01, unit 1 those at b10 and b11 (the group base of a unit is selected by
+// lane >> 4, as in apply_unit).
+struct UnitBases
+{
+	int b00, b01, b10, b11;
+};
+
+// units u0 and u1 of a gate's own enumeration (unit u: group bases 2u, 2u+1 with zero
+// bits inserted at the gate's tile bits)
+__device__ __forceinline__ UnitBases unit_pair(int u0, int u1, int lo, int hi)
+{
+	return {insert2(2 * u0, lo, hi), insert2(2 * u0 + 1, lo, hi), insert2(2 * u1, lo, hi),
+	        insert2(2 * u1 + 1, lo, hi)};
+}
+
+// the two units of the row set with first row S for a gate whose partner gate has tile
+// bits (o1, o2): bases S, S|2^o1 and S|2^o2, S|2^o1|2^o2
+__device__ __forceinline__ UnitBases set_units(int S, int o1, int o2)
+{
+	return {S, S | (1 << o1), S | (1 << o2), S | (1 << o1) | (1 << o2)};
+}
+
+// apply_unit for two units of a warp at once; bs0 and bs1 are this lane's group bases of
+// the two units (the second is ignored unless has1, which is the same for all lanes).
+// Both units' operands are loaded before either is stored, so the two independent MMA
+// chains overlap; in place like apply_unit(..., inplace = true).
 template <bool TAN>
-__device__ __forceinline__ void apply_unit2(const double* in, const double* din, double2* out, double2* dout, int u0,
-                                           int u1, bool has1, const StepLane& sl, const double bg[2], const double bz[2],
-                                           bool dzero, int lane)
+__device__ __forceinline__ void apply_bases2(const double* in, const double* din, double2* out, double2* dout,
+                                            int bs0, int bs1, bool has1, const StepLane& sl, const double bg[2],
+                                            const double bz[2], bool dzero, int lane)
 {
 	const int cc = (lane >> 2) & 3;
-	const int bs0 = insert2(2 * u0 + (lane >> 4), sl.lo, sl.hi);
-	const int bs1 = insert2(2 * (has1 ? u1 : u0) + (lane >> 4), sl.lo, sl.hi);
+	if (!has1) bs1 = bs0;
 	const int j00 = sidx(bs0 | sl.m_k0, cc) * 2 + sl.part_out, j01 = sidx(bs0 | sl.m_k1, cc) * 2 + sl.part_out;
 	const int j10 = sidx(bs1 | sl.m_k0, cc) * 2 + sl.part_out, j11 = sidx(bs1 | sl.m_k1, cc) * 2 + sl.part_out;
 	const double a00 = in[j00], a01 = in[j01], a10 = in[j10], a11 = in[j11];
@@ -606,8 +651,37 @@ __device__ __forceinline__ void apply_unit2(const double* in, const double* din,
 	}
 }
 
+// apply_bases2 for units u0 and u1 of a gate (unit u: the group bases 2u, 2u+1 of the
+// gate's own enumeration)
+template <bool TAN>
+__device__ __forceinline__ void apply_unit2(const double* in, const double* din, double2* out, double2* dout, int u0,
+                                           int u1, bool has1, const StepLane& sl, const double bg[2], const double bz[2],
+                                           bool dzero, int lane)
+{
+	const int bs0 = insert2(2 * u0 + (lane >> 4), sl.lo, sl.hi);
+	const int bs1 = insert2(2 * (has1 ? u1 : u0) + (lane >> 4), sl.lo, sl.hi);
+	apply_bases2<TAN>(in, din, out, dout, bs0, bs1, has1, sl, bg, bz, dzero, lane);
+}
+
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only), and its group fences
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+	const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// shared memory of k3_fwd: gates, row offsets and two buffers of (state, tangent) tiles
+inline size_t k3_fwd_smem(int NB)
+{
+	return 32 * MAXK * sizeof(double2) + (1 << MAXNB) * sizeof(int) + 4 * ((size_t)1 << NB) * 4 * sizeof(double2);
+}
+
 // Forward pass (complex128).  Same contract as k2_fwd; OUT 3 writes the pass output
 // and adds f, as the last pass does when the reverse pass rebuilds states from it.
+// Tiles are double-buffered in shared memory: the next tile position's state arrives
+// by cp.async while the gates run on the current one.
 template <bool TAN, int IN, int OUT>
 __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
                                               double2* __restrict__ psi_o, double2* __restrict__ dpsi_o,
@@ -620,61 +694,101 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
 	double2* sg = reinterpret_cast<double2*>(smem_raw);
 	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);
-	double2* S = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));
-	double2* dS = S + A;
+	double2* bufs = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));   // [2][state, tangent][A]
 	gates_to_smem<double>(gates, K, TAN, sg);
 	row_offsets(pg, rowoff);
 	__syncthreads();
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
 	double fx = 0, fy = 0;
 	const int units = R / 8;
-	double2 ra[EPTF], rb[EPTF];
-	auto fetch = [&](int64_t tile) {
+	// the pass input of a tile position into buffer b (IN 0: read from psi, dpsi)
+	auto fetch = [&](int64_t tile, int b) {
+		if (IN != 0 || tile >= pg.ntiles) return;
 		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
 		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW;
-#pragma unroll
-		for (int i = 0; i < EPTF; i++) {
-			const int e = threadIdx.x + i * NTF;
-			if (e >= A || IN != 0 || tile >= pg.ntiles) continue;
-			const int64_t a = (rowbase + rowoff[e >> 2]) * pg.C + colbase + (e & 3);
-			ra[i] = psi[a];
-			if (TAN) rb[i] = dpsi[a];
-		}
-	};
-	fetch(blockIdx.x);
-
-	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
-		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
-		const int64_t rowbase = deposit(rt, pg.rest_mask);
-		const int64_t colbase = cg * CW;
+		double2* dst = bufs + (size_t)b * 2 * A;
 #pragma unroll
 		for (int i = 0; i < EPTF; i++) {
 			const int e = threadIdx.x + i * NTF;
 			if (e >= A) continue;
-			const int r = e >> 2, cc = e & 3;
-			const int pe = sidx(r, cc);
-			if (IN == 0) {
-				S[pe] = ra[i];
-				if (TAN) dS[pe] = rb[i];
-			} else {
+			const int64_t a = (rowbase + rowoff[e >> 2]) * pg.C + colbase + (e & 3);
+			const int pe = sidx(e >> 2, e & 3);
+			cp_async16(dst + pe, psi + a);
+			if (TAN) cp_async16(dst + A + pe, dpsi + a);
+		}
+	};
+	fetch(blockIdx.x, 0);
+	cp_async_commit();
+
+	int buf = 0;
+	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x, buf ^= 1) {
+		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
+		const int64_t rowbase = deposit(rt, pg.rest_mask);
+		const int64_t colbase = cg * CW;
+		double2* S = bufs + (size_t)buf * 2 * A;
+		double2* dS = S + A;
+		if (IN == 0) {
+			cp_async_wait_all();
+		} else {
+#pragma unroll
+			for (int i = 0; i < EPTF; i++) {
+				const int e = threadIdx.x + i * NTF;
+				if (e >= A) continue;
+				const int r = e >> 2, cc = e & 3;
+				const int pe = sidx(r, cc);
 				const int64_t row = rowbase + rowoff[r], col = colbase + cc;
 				S[pe] = make_double2(basis_re(row, pg.b0 + col), basis_im(row, pg.b0 + col));
 				if (TAN) dS[pe] = make_double2(0, 0);
 			}
 		}
+		// every thread's copies (or writes) of this tile have landed, and every thread is
+		// done with the other buffer (its previous tile), which the next fetch overwrites
 		__syncthreads();
-		fetch(tile + gridDim.x);
+		fetch(tile + gridDim.x, buf ^ 1);
+		cp_async_commit();
+		const double* fS = reinterpret_cast<const double*>(S);
+		const double* fdS = reinterpret_cast<const double*>(dS);
+		bool skip = false;   // gate k was applied with gate k-1
 #pragma unroll
 		for (int k = 0; k < MAXK; k++) {
 			if (k >= K) break;
-			const StepLane sl(pg.gi[k], pg.gj[k], lane);
-			double bg[2], bz[2] = {0, 0};
-			bfrag(sg + 32 * k, true, lane, bg);
-			if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
+			if (skip) { skip = false; continue; }
 			const bool dzero = IN == 1 && k == 0;
-			for (int u = warp; u < units; u += 2 * nwarps)
-				apply_unit2<TAN>(reinterpret_cast<const double*>(S), reinterpret_cast<const double*>(dS), S, dS, u,
-				                 u + nwarps, u + nwarps < units, sl, bg, bz, dzero, lane);
+			const int k2 = k + 1 < MAXK ? k + 1 : k;
+			if (k + 1 < K && pg.NB >= 4 && gates_disjoint(pg, k, k2)) {
+				// gates k and k+1 on this warp's row sets, one block barrier for both (each
+				// gate's operands are loaded per set, which keeps registers for one gate)
+				const int m = (1 << pg.gi[k]) | (1 << pg.gj[k]) | (1 << pg.gi[k2]) | (1 << pg.gj[k2]);
+				const int hs = lane >> 4;
+				for (int s = warp; s < (R >> 4); s += nwarps) {
+					const int S0 = set_base(s, m);
+					{
+						const StepLane sl(pg.gi[k], pg.gj[k], lane);
+						double bg[2], bz[2] = {0, 0};
+						bfrag(sg + 32 * k, true, lane, bg);
+						if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
+						const UnitBases ua = set_units(S0, pg.gi[k2], pg.gj[k2]);
+						apply_bases2<TAN>(fS, fdS, S, dS, hs ? ua.b01 : ua.b00, hs ? ua.b11 : ua.b10, true, sl, bg,
+						                  bz, dzero, lane);
+					}
+					__syncwarp();
+					const StepLane sl2(pg.gi[k2], pg.gj[k2], lane);
+					double bg2[2], bz2[2] = {0, 0};
+					bfrag(sg + 32 * k2, true, lane, bg2);
+					if (TAN) bfrag(sg + 32 * k2 + 16, true, lane, bz2);
+					const UnitBases ub = set_units(S0, pg.gi[k], pg.gj[k]);
+					apply_bases2<TAN>(fS, fdS, S, dS, hs ? ub.b01 : ub.b00, hs ? ub.b11 : ub.b10, true, sl2, bg2, bz2,
+					                  false, lane);
+				}
+				skip = true;
+			} else {
+				const StepLane sl(pg.gi[k], pg.gj[k], lane);
+				double bg[2], bz[2] = {0, 0};
+				bfrag(sg + 32 * k, true, lane, bg);
+				if (TAN) bfrag(sg + 32 * k + 16, true, lane, bz);
+				for (int u = warp; u < units; u += 2 * nwarps)
+					apply_unit2<TAN>(fS, fdS, S, dS, u, u + nwarps, u + nwarps < units, sl, bg, bz, dzero, lane);
+			}
 			__syncthreads();
 		}
 		for (int i = 0; i < EPTF; i++) {
@@ -695,8 +809,8 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 				if (TAN) dpsi_o[a] = dS[pe];
 			}
 		}
-		__syncthreads();
 	}
+	cp_async_wait_all();
 	if (OUT == 2 || OUT == 3) {
 		__shared__ double red[2][NTF / 32];
 		fx = warp_sum(fx);
@@ -1076,13 +1190,6 @@ __device__ __forceinline__ void apply_unit4o(const float* in, const float* din, 
 	}
 }
 
-__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
-{
-	const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
-	asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 constexpr int NT4F = 256;   // threads of the complex64 forward kernel (up to three blocks per SM)
 constexpr int NT4R = 256;   // threads of the complex64 reverse kernel
@@ -1682,6 +1789,77 @@ __global__ void __launch_bounds__(NT5, 2) k5_rev(const float2* __restrict__ psi,
 // FP64: gc = conj(G) (as a row-vector operand it applies G^+) and wn = -W, W = G^+ Z G^+.
 struct PassAdj { Gate4<double> gc[MAXK]; Gate4<double> wn[MAXK]; };
 
+// Operands of one gate of the reconstructing reverse pass: B fragments of conj(G) (the
+// adjoint gate as a row-vector operand), -W, G and Z, from the gate block of shared memory
+// ([G, Z, conj(G), -W], 16 complex each).
+template <bool TAN>
+struct RevGate
+{
+	StepLane sl;
+	double bc[2], bw[2] = {0, 0}, bg[2], bz[2] = {0, 0};
+	bool first_gate, last_gate;
+	__device__ __forceinline__ RevGate(const double2* sg, int k, int K, bool first, bool last, const PassGeom& pg,
+	                                   int lane)
+		: sl(pg.gi[k], pg.gj[k], lane), first_gate(first && k == K - 1), last_gate(last && k == 0)
+	{
+		bfrag(sg + 64 * k + 32, false, lane, bc);
+		if (TAN) bfrag(sg + 64 * k + 48, true, lane, bw);
+		bfrag(sg + 64 * k, false, lane, bg);
+		if (TAN) bfrag(sg + 64 * k + 16, false, lane, bz);
+	}
+};
+
+// One gate of the reconstructing reverse pass on two units (the second unless has1 is
+// false): rebuild the state (and tangent) entering the gate, in place; add the outer
+// sums dG += phi (x) psi, HZ += phi (x) dpsi + dphi (x) psi over the units' groups, into
+// fresh partials first (short MMA chains); move phi, dphi through the gate in place.
+template <bool TAN>
+__device__ __forceinline__ void rev_gate6(const RevGate<TAN>& g, const UnitBases& ub, bool has1, double2* Psi,
+                                          double2* dPsi, double2* Phi, double2* dPhi, double& g0, double& g1,
+                                          double& h0, double& h1, int lane)
+{
+	const double* fPsi = reinterpret_cast<const double*>(Psi);
+	const double* fPhi = reinterpret_cast<const double*>(Phi);
+	const double* fdPsi = reinterpret_cast<const double*>(dPsi);
+	const double* fdPhi = reinterpret_cast<const double*>(dPhi);
+	const int hs = lane >> 4;
+	const int bs0 = hs ? ub.b01 : ub.b00, bs1 = hs ? ub.b11 : ub.b10;
+	const StepLane& sl = g.sl;
+	if (TAN && !g.last_gate)
+		apply_bases2<true>(fPsi, fdPsi, Psi, dPsi, bs0, bs1, has1, sl, g.bc, g.bw, false, lane);
+	else
+		apply_bases2<false>(fPsi, nullptr, Psi, nullptr, bs0, bs1, has1, sl, g.bc, g.bw, false, lane);
+	__syncwarp();
+	double tg[2][2] = {{0, 0}, {0, 0}}, th[2][2] = {{0, 0}, {0, 0}};
+#pragma unroll
+	for (int q = 0; q < 2; q++) {
+		if (q == 1 && !has1) break;
+		const int base0 = q ? ub.b10 : ub.b00, base1 = q ? ub.b11 : ub.b01;
+		const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+		const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
+		const double p0 = fPhi[i0], x0 = fPsi[i0], p1 = fPhi[i1], x1 = fPsi[i1];
+		double dx0 = 0, dx1 = 0, dp0 = 0, dp1 = 0;
+		if (TAN && !g.last_gate) { dx0 = fdPsi[i0]; dx1 = fdPsi[i1]; }
+		if (TAN && !g.first_gate) { dp0 = fdPhi[i0]; dp1 = fdPhi[i1]; }
+		dmma(tg[q][0], tg[q][1], p0, x0);
+		if (TAN && !g.last_gate) dmma(th[q][0], th[q][1], p0, dx0);
+		dmma(tg[q][0], tg[q][1], p1, x1);
+		if (TAN && !g.last_gate) dmma(th[q][0], th[q][1], p1, dx1);
+		if (TAN && !g.first_gate) {
+			dmma(th[q][0], th[q][1], dp0, x0);
+			dmma(th[q][0], th[q][1], dp1, x1);
+		}
+	}
+	g0 += tg[0][0] + tg[1][0];
+	g1 += tg[0][1] + tg[1][1];
+	if (TAN) {
+		h0 += th[0][0] + th[1][0];
+		h1 += th[0][1] + th[1][1];
+	}
+	if (g.last_gate) return;
+	apply_bases2<TAN>(fPhi, fdPhi, Phi, dPhi, bs0, bs1, has1, sl, g.bg, g.bz, g.first_gate, lane);
+}
+
 constexpr int NT6 = 256;   // threads of the reconstructing complex128 reverse kernel (two blocks per SM)
 constexpr int EPT6 = (1 << MAXNB) * 4 / NT6;   // tile elements per thread and state
 
@@ -1736,10 +1914,6 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 #pragma unroll
 	for (int k = 0; k < MAXK; k++) { cg0[k] = cg1[k] = ch0[k] = ch1[k] = 0; }
 	const int units = R / 8;
-	double* fPsi = reinterpret_cast<double*>(Psi);
-	double* fPhi = reinterpret_cast<double*>(Phi);
-	double* fdPsi = reinterpret_cast<double*>(dPsi);
-	double* fdPhi = reinterpret_cast<double*>(dPhi);
 
 	for (int64_t tile = blockIdx.x; tile < pg.ntiles; tile += gridDim.x) {
 		const int64_t rt = tile / pg.ncg, cgp = tile - rt * pg.ncg;
@@ -1763,58 +1937,37 @@ __global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi
 		cp_async_commit();
 		cp_async_wait_all();
 		__syncthreads();
+		bool skip = false;   // gate k was done with gate k+1
 #pragma unroll
 		for (int k = MAXK - 1; k >= 0; k--) {
 			if (k >= K) continue;
-			const StepLane sl(pg.gi[k], pg.gj[k], lane);
-			const bool first_gate = FIRST && k == K - 1;
-			const bool last_gate = LAST && k == 0;
-			double bc[2], bw[2] = {0, 0}, bg[2], bz[2] = {0, 0};
-			bfrag(sg + 64 * k + 32, false, lane, bc);             // G^+ (row-vector operand conj(G))
-			if (TAN) bfrag(sg + 64 * k + 48, true, lane, bw);     // -W
-			bfrag(sg + 64 * k, false, lane, bg);                  // G^T (row-vector operand G)
-			if (TAN) bfrag(sg + 64 * k + 16, false, lane, bz);    // Z^T
-			for (int u = warp; u < units; u += 2 * nwarps) {
-				const int u1 = u + nwarps;
-				const bool has1 = u1 < units;   // the same for the whole warp
-				// 1. the state (and tangent) entering gate k, in place, for both units
-				if (TAN && !last_gate)
-					apply_unit2<true>(fPsi, fdPsi, Psi, dPsi, u, u1, has1, sl, bc, bw, false, lane);
-				else
-					apply_unit2<false>(fPsi, nullptr, Psi, nullptr, u, u1, has1, sl, bc, bw, false, lane);
-				__syncwarp();
-				// 2. outer sums over the two sets of four groups of each unit, into fresh
-				//    partial sums per unit (short MMA chains), then added to the gate's sums
-				double tg[2][2] = {{0, 0}, {0, 0}}, th[2][2] = {{0, 0}, {0, 0}};
-#pragma unroll
-				for (int q = 0; q < 2; q++) {
-					if (q == 1 && !has1) break;
-					const int uq = q ? u1 : u;
-					const int base0 = insert2(2 * uq, sl.lo, sl.hi), base1 = insert2(2 * uq + 1, sl.lo, sl.hi);
-					const int i0 = sidx(base0 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
-					const int i1 = sidx(base1 | sl.m_outer, lane & 3) * 2 + sl.part_outer;
-					const double p0 = fPhi[i0], x0 = fPsi[i0], p1 = fPhi[i1], x1 = fPsi[i1];
-					double dx0 = 0, dx1 = 0, dp0 = 0, dp1 = 0;
-					if (TAN && !last_gate) { dx0 = fdPsi[i0]; dx1 = fdPsi[i1]; }
-					if (TAN && !first_gate) { dp0 = fdPhi[i0]; dp1 = fdPhi[i1]; }
-					dmma(tg[q][0], tg[q][1], p0, x0);
-					if (TAN && !last_gate) dmma(th[q][0], th[q][1], p0, dx0);
-					dmma(tg[q][0], tg[q][1], p1, x1);
-					if (TAN && !last_gate) dmma(th[q][0], th[q][1], p1, dx1);
-					if (TAN && !first_gate) {
-						dmma(th[q][0], th[q][1], dp0, x0);
-						dmma(th[q][0], th[q][1], dp1, x1);
+			if (skip) { skip = false; continue; }
+			const int k2 = k >= 1 ? k - 1 : 0;
+			if (k >= 1 && pg.NB >= 4 && gates_disjoint(pg, k, k2)) {
+				// gates k and k-1 on this warp's row sets, one block barrier for both (each
+				// gate's operands are loaded per set, which keeps registers for one gate)
+				const int m = (1 << pg.gi[k]) | (1 << pg.gj[k]) | (1 << pg.gi[k2]) | (1 << pg.gj[k2]);
+				for (int s = warp; s < (R >> 4); s += nwarps) {
+					const int S0 = set_base(s, m);
+					{
+						const RevGate<TAN> ga(sg, k, K, FIRST, LAST, pg, lane);
+						rev_gate6<TAN>(ga, set_units(S0, pg.gi[k2], pg.gj[k2]), true, Psi, dPsi, Phi, dPhi, cg0[k],
+						               cg1[k], ch0[k], ch1[k], lane);
 					}
+					__syncwarp();
+					const RevGate<TAN> gb(sg, k2, K, FIRST, LAST, pg, lane);
+					rev_gate6<TAN>(gb, set_units(S0, pg.gi[k], pg.gj[k]), true, Psi, dPsi, Phi, dPhi, cg0[k2], cg1[k2],
+					               ch0[k2], ch1[k2], lane);
 				}
-				cg0[k] += tg[0][0] + tg[1][0];
-				cg1[k] += tg[0][1] + tg[1][1];
-				if (TAN) {
-					ch0[k] += th[0][0] + th[1][0];
-					ch1[k] += th[0][1] + th[1][1];
+				skip = true;
+			} else {
+				const RevGate<TAN> ga(sg, k, K, FIRST, LAST, pg, lane);
+				for (int u = warp; u < units; u += 2 * nwarps) {
+					const int u1 = u + nwarps;
+					const bool has1 = u1 < units;   // the same for the whole warp
+					rev_gate6<TAN>(ga, unit_pair(u, has1 ? u1 : u, ga.sl.lo, ga.sl.hi), has1, Psi, dPsi, Phi, dPhi,
+					               cg0[k], cg1[k], ch0[k], ch1[k], lane);
 				}
-				if (last_gate) continue;
-				// 3. adjoint outputs: phi' = phi G, dphi' = dphi G + phi Z (in place), both units
-				apply_unit2<TAN>(fPhi, fdPhi, Phi, dPhi, u, u1, has1, sl, bg, bz, first_gate, lane);
 			}
 			__syncthreads();
 		}
@@ -2409,11 +2562,12 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 	static int per_sm = 0;
 	if constexpr (std::is_same<T, double>::value) {
 		if (!per_sm) {
-			int ret = prepare(k3_fwd<TAN, IN, OUT>, fwd_smem<T>(MAXNB), &per_sm, NTF);
+			int ret = prepare(k3_fwd<TAN, IN, OUT>, k3_fwd_smem(MAXNB), &per_sm, NTF);
 			if (ret) return ret;
 		}
 		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
-		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, smem, psi, dpsi, psi_o, dpsi_o, phi, pg, gates, fpart);
+		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, k3_fwd_smem(pg.NB), psi, dpsi, psi_o, dpsi_o, phi,
+		            pg, gates, fpart);
 	} else if (rt.c64_ffma) {
 		static int per_sm7 = 0;
 		if (!per_sm7) {
