@@ -582,8 +582,9 @@ int rqcopt_apply_quantum_circuit_c64(const struct mat4x4 gates[], int ngates, co
  *     with -6 and a message on stderr;
  *   - work is issued on `stream` (a cudaStream_t, NULL for the legacy default
  *     stream) and the call returns after the stream has finished it;
- *   - the first call on a device resolves the scratch address there
- *     (cudaGetSymbolAddress);
+ *   - the first call on a device does the set-up there: it resolves the
+ *     scratch address (cudaGetSymbolAddress) with that device current, so
+ *     make that first call before any stream capture;
  *   - all calls share the scratch: calls whose GPU work overlaps (other
  *     streams, other host threads) race on it.
  * Returns 0, -5 (CUDA error) or -6 (invalid argument).
