@@ -133,3 +133,40 @@ def test_invalid_arguments_refused_before_device_work():
         with pytest.raises(gpu.RqcError) as e:
             call()
         assert e.value.code == -6
+
+
+def test_core_entry_points_refuse_invalid_circuits_before_device_work():
+    """Where the reference asserts (src/quantum_circuit.c:15-16, src/gate.c:12-15),
+    the library refuses with the argument error (-6) before touching the device: an
+    empty circuit, equal or out-of-range wires, statevectors of different sizes (no GPU
+    needed)."""
+    import numpy as np
+    from rqcopt_hpc_b200 import gpu
+    from helpers import haar_unitary
+    rng = np.random.default_rng(5)
+    L = 4
+    gates = np.stack([haar_unitary(rng) for _ in range(3)])
+    psi = np.zeros(1 << L, np.complex128)
+    psi[0] = 1
+    tgt = gpu.Target(fn=lambda x: x)
+    bad = [np.array([[0, 1], [2, 2], [1, 3]], np.int32),     # equal wires
+           np.array([[0, 1], [2, 4], [1, 3]], np.int32),     # wire beyond the register
+           np.array([[0, 1], [-1, 2], [1, 3]], np.int32)]    # negative wire
+    calls = [lambda: gpu.apply_quantum_circuit(gates[:0], np.zeros((0, 2), np.int32), psi)]
+    for w in bad:
+        calls += [lambda w=w: gpu.apply_quantum_circuit(gates, w, psi),
+                  lambda w=w: gpu.circuit_unitary_target_hessian_vector_product(tgt, gates, gates, w, L)]
+    calls.append(lambda: gpu.apply_gate(gates[0], 1, 1, psi))
+    for call in calls:
+        with pytest.raises(gpu.RqcError) as e:
+            call()
+        assert e.value.code == -6
+    # statevectors of different sizes
+    from rqcopt_hpc_b200.abi import Statevector
+    import ctypes
+    out = np.zeros(1 << (L + 1), np.complex128)
+    w = np.array([[0, 1]], np.int32)
+    ret = gpu.lib().apply_quantum_circuit(gates.ctypes.data, 1, w.ctypes.data,
+                                          ctypes.byref(Statevector(psi.ctypes.data, L)),
+                                          ctypes.byref(Statevector(out.ctypes.data, L + 1)))
+    assert ret == -6
