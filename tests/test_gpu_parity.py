@@ -423,3 +423,31 @@ def test_complex64_reverse_paths_match_complex128(gpu, L, depth, per_pass, unita
         assert rel_err(a, b) <= 1e-5
     for a, b in zip(got_g, ref_g):
         assert rel_err(a, b) <= 1e-5
+
+
+@pytest.mark.parametrize("L", [2, 3, 4, 5])
+def test_smallest_registers_match_oracle(gpu, oracle, L):
+    """The smallest registers, on both sides of the engine switch (one kernel per gate
+    below 4 qubits, fused passes from 4): apply_quantum_circuit and the circuit target's
+    f, gradient and HVP against the oracle to 1e-12 (complex128) and 1e-5 (complex64
+    passes), dense target through the host callback."""
+    rng = np.random.default_rng(700 + L)
+    G = 7
+    gates = np.stack([haar_unitary(rng) for _ in range(G)])
+    wires = np.array([rng.choice(L, 2, replace=False) for _ in range(G)], np.int32)
+    dirs = 0.5 * crandn((G, 4, 4), rng)
+    u = crandn((1 << L, 1 << L), rng)
+    psi = crandn(1 << L, rng)
+    psi /= np.linalg.norm(psi)
+    assert np.max(np.abs(gpu.apply_quantum_circuit(gates, wires, psi) -
+                         oracle.apply_quantum_circuit(gates, wires, psi))) <= 1e-12
+    fo = oracle.circuit_unitary_target_hessian_vector_product(oracle.target("dense", u), gates, dirs, wires, L)
+    try:
+        for prec, tol in ((gpu.PRECISION_C128, 1e-12), (gpu.PRECISION_C64, 1e-5)):
+            gpu.set_precision(prec)
+            fg = gpu.circuit_unitary_target_hessian_vector_product(gpu.Target(fn=lambda x: u @ x), gates, dirs, wires, L)
+            assert abs(fg[0] - fo[0]) <= tol * abs(fo[0])
+            assert rel_err(fg[1], fo[1]) <= tol
+            assert rel_err(fg[2], fo[2]) <= tol
+    finally:
+        gpu.set_precision(gpu.PRECISION_C128)
