@@ -1860,7 +1860,7 @@ __device__ __forceinline__ void rev_gate6(const RevGate<TAN>& g, const UnitBases
 	apply_bases2<TAN>(fPhi, fdPhi, Phi, dPhi, bs0, bs1, has1, sl, g.bg, g.bz, g.first_gate, lane);
 }
 
-constexpr int NT6 = 256;   // threads of the reconstructing complex128 reverse kernel (two blocks per SM)
+constexpr int NT6 = 128;   // threads of the reconstructing complex128 reverse kernel (three blocks per SM)
 constexpr int EPT6 = (1 << MAXNB) * 4 / NT6;   // tile elements per thread and state
 
 inline size_t k6_rev_smem(bool tan)
@@ -1882,7 +1882,7 @@ inline size_t k6_rev_smem(bool tan)
 // add the outer sums dG_k += phi (x) psi_k, HZ_k += phi (x) dpsi_k + dphi (x) psi_k; move
 // phi, dphi through gate k.  Partials and contract as in k3_rev.
 template <bool TAN, bool FIRST, bool LAST>
-__global__ void __launch_bounds__(NT6, 2) k6_rev(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+__global__ void __launch_bounds__(NT6, 3) k6_rev(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
                                                  const double2* __restrict__ phi, const double2* __restrict__ dphi,
                                                  double2* __restrict__ phi_o, double2* __restrict__ dphi_o, PassGeom pg,
                                                  PassGates<double> gates, PassAdj adj, double* __restrict__ part, int nblk)
