@@ -1146,9 +1146,9 @@ def main():
                                    "amplitude group: the outer sums dG, HZ and the adjoint updates phi, dphi); states "
                                    "rebuilt inside a pass not counted",
                     "peak_source": "FP64 peak measured in this run (cuBLAS DGEMM 8192^3)",
-                    "traffic": rbytes / max(rev_n, 1) * 0.995,
+                    "traffic": rbytes / max(rev_n, 1) * 0.99,
                     "traffic_source": "ncu capture of one middle k6_rev pass at L=12 (DRAM bytes / algorithmic = "
-                                      "0.995, profiles/k6_rev_c128_L12_d5.md), scaled to the bytes of an average "
+                                      "0.99, profiles/k6_rev_c128_L12_d5.md), scaled to the bytes of an average "
                                       "launch here",
                     "hbm_view": {"achieved_gbs": gbs, "peak_gbs": hbm_peak, "frac": gbs / hbm_peak if gbs else None,
                                  "peak_source": hbm_src},

@@ -486,7 +486,7 @@ __device__ __forceinline__ double embed(const double2* m, int rowk, int coln, bo
 	return a == 0 ? (b == 0 ? v.x : v.y) : (b == 0 ? -v.y : v.x);
 }
 
-constexpr int NTF = 256;   // threads of the complex128 forward kernel
+constexpr int NTF = 128;   // threads of the complex128 forward kernel (three blocks per SM)
 constexpr int NTR = 512;   // threads of the complex128 reverse kernel
 constexpr int NPART3 = 128;   // raw 8x8 sums per gate and block: dG then HZ
 
