@@ -673,9 +673,9 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // shared memory of k3_fwd: gates, row offsets and two buffers of (state, tangent) tiles
-inline size_t k3_fwd_smem(int NB)
+inline size_t k3_fwd_smem(int NB, bool tan)
 {
-	return 32 * MAXK * sizeof(double2) + (1 << MAXNB) * sizeof(int) + 4 * ((size_t)1 << NB) * 4 * sizeof(double2);
+	return 32 * MAXK * sizeof(double2) + (1 << MAXNB) * sizeof(int) + (tan ? 4 : 2) * ((size_t)1 << NB) * 4 * sizeof(double2);
 }
 
 // Forward pass (complex128).  Same contract as k2_fwd; OUT 3 writes the pass output
@@ -683,7 +683,7 @@ inline size_t k3_fwd_smem(int NB)
 // Tiles are double-buffered in shared memory: the next tile position's state arrives
 // by cp.async while the gates run on the current one.
 template <bool TAN, int IN, int OUT>
-__global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
+__global__ void __launch_bounds__(NTF, TAN ? 3 : 6) k3_fwd(const double2* __restrict__ psi, const double2* __restrict__ dpsi,
                                               double2* __restrict__ psi_o, double2* __restrict__ dpsi_o,
                                               const double2* __restrict__ phi, PassGeom pg, PassGates<double> gates,
                                               double2* __restrict__ fpart)
@@ -694,7 +694,7 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 	const int R = 1 << pg.NB, A = R * CW, K = pg.K;
 	double2* sg = reinterpret_cast<double2*>(smem_raw);
 	int* rowoff = reinterpret_cast<int*>(sg + 32 * MAXK);
-	double2* bufs = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));   // [2][state, tangent][A]
+	double2* bufs = reinterpret_cast<double2*>(rowoff + (1 << MAXNB));   // [2][state, tangent][A], or [2][state][A] without tangents
 	gates_to_smem<double>(gates, K, TAN, sg);
 	row_offsets(pg, rowoff);
 	__syncthreads();
@@ -706,7 +706,7 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 		if (IN != 0 || tile >= pg.ntiles) return;
 		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
 		const int64_t rowbase = deposit(rt, pg.rest_mask), colbase = cg * CW;
-		double2* dst = bufs + (size_t)b * 2 * A;
+		double2* dst = bufs + (size_t)b * (TAN ? 2 : 1) * A;
 #pragma unroll
 		for (int i = 0; i < EPTF; i++) {
 			const int e = threadIdx.x + i * NTF;
@@ -725,8 +725,8 @@ __global__ void __launch_bounds__(NTF, 3) k3_fwd(const double2* __restrict__ psi
 		const int64_t rt = tile / pg.ncg, cg = tile - rt * pg.ncg;
 		const int64_t rowbase = deposit(rt, pg.rest_mask);
 		const int64_t colbase = cg * CW;
-		double2* S = bufs + (size_t)buf * 2 * A;
-		double2* dS = S + A;
+		double2* S = bufs + (size_t)buf * (TAN ? 2 : 1) * A;
+		double2* dS = TAN ? S + A : nullptr;
 		if (IN == 0) {
 			cp_async_wait_all();
 		} else {
@@ -2562,11 +2562,11 @@ int launch_fwd(Runtime& rt, const cplx<T>* psi, const cplx<T>* dpsi, cplx<T>* ps
 	static int per_sm = 0;
 	if constexpr (std::is_same<T, double>::value) {
 		if (!per_sm) {
-			int ret = prepare(k3_fwd<TAN, IN, OUT>, k3_fwd_smem(MAXNB), &per_sm, NTF);
+			int ret = prepare(k3_fwd<TAN, IN, OUT>, k3_fwd_smem(MAXNB, TAN), &per_sm, NTF);
 			if (ret) return ret;
 		}
 		const int grid = OUT >= 2 ? fgrid : (int)std::max<int64_t>(1, std::min<int64_t>(pg.ntiles, (int64_t)rt.num_sms * per_sm));
-		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, k3_fwd_smem(pg.NB), psi, dpsi, psi_o, dpsi_o, phi,
+		RQC_LAUNCH3(rt, KC_FUSED, (k3_fwd<TAN, IN, OUT>), grid, NTF, k3_fwd_smem(pg.NB, TAN), psi, dpsi, psi_o, dpsi_o, phi,
 		            pg, gates, fpart);
 	} else if (rt.c64_ffma) {
 		static int per_sm7 = 0;
